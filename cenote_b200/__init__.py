@@ -1,0 +1,475 @@
+"""cenote_b200 — a B200-native wavefront path tracer behind cenote's scene/renderer API.
+
+Python binds the C ABI in ``include/cenote_c.h`` (``libcenote_b200.so``, built
+in-tree by ``cenote_b200.build``) through ctypes. The classes mirror the
+reference crate's types:
+
+    Context          crates/cenote/src/gpu/mod.rs:93          (Context::new)
+    Scene            crates/cenote/src/scene/mod.rs:254       (Scene::new)
+    Renderer         crates/cenote/src/render/mod.rs:151-311  (with_max_bounces, render, accumulate)
+    Film             crates/cenote/src/render/film.rs:102-217 (new, reset, samples, averages)
+
+Errors surface as ``CenoteError`` carrying the library's status code (the
+reference's ``cenote::Error`` variants, crates/cenote/src/error.rs:10-72). There
+is no fallback: without the built library or a capable GPU every entry point
+raises.
+"""
+from __future__ import annotations
+
+import ctypes as C
+from pathlib import Path
+
+import numpy as np
+
+from . import scenes
+from .scenes import SceneSpec
+
+__all__ = ["CenoteError", "Context", "Scene", "Renderer", "Film", "library", "scenes", "LIGHT_SAMPLING_MIS",
+           "LIGHT_SAMPLING_BSDF", "LIGHT_SAMPLING_NEE", "EXPORTED_SYMBOLS"]
+
+LIGHT_SAMPLING_MIS, LIGHT_SAMPLING_BSDF, LIGHT_SAMPLING_NEE = 0, 1, 2
+LIB_PATH = Path(__file__).resolve().parent / "libcenote_b200.so"
+
+STATUS = {
+    0: "ok", -1: "invalid argument", -2: "device error", -3: "no capable GPU", -4: "allocation failed",
+    -5: "scene error", -6: "timeout", -7: "device bound exceeded", -8: "over budget",
+}
+
+
+class CenoteError(RuntimeError):
+    def __init__(self, code: int, message: str):
+        super().__init__(f"{STATUS.get(code, 'error')} ({code}): {message}")
+        self.code = code
+
+
+class Material(C.Structure):
+    _fields_ = [
+        ("base_color", C.c_float * 3), ("base_roughness", C.c_float), ("emission", C.c_float * 3),
+        ("metalness", C.c_float), ("specular_weight", C.c_float), ("specular_roughness", C.c_float),
+        ("specular_ior", C.c_float), ("transmission_weight", C.c_float), ("transmission_color", C.c_float * 3),
+        ("transmission_depth", C.c_float), ("coat_color", C.c_float * 3), ("coat_weight", C.c_float),
+        ("coat_roughness", C.c_float), ("coat_ior", C.c_float), ("coat_darkening", C.c_float),
+        ("fuzz_weight", C.c_float), ("fuzz_color", C.c_float * 3), ("fuzz_roughness", C.c_float),
+        ("opacity", C.c_float), ("thin_walled", C.c_uint32), ("base_color_texture", C.c_uint32),
+        ("specular_roughness_texture", C.c_uint32), ("metalness_texture", C.c_uint32),
+        ("emission_texture", C.c_uint32), ("opacity_texture", C.c_uint32), ("normal_texture", C.c_uint32),
+    ]
+
+
+assert C.sizeof(Material) == 144
+
+
+class Object(C.Structure):
+    _fields_ = [
+        ("positions", C.c_void_p), ("normals", C.c_void_p), ("uvs", C.c_void_p), ("indices", C.c_void_p),
+        ("vertex_count", C.c_uint32), ("triangle_count", C.c_uint32), ("transform", C.c_float * 12),
+        ("material", Material), ("camera_visible", C.c_uint32), ("pad", C.c_uint32),
+    ]
+
+
+class CameraC(C.Structure):
+    _fields_ = [("position", C.c_float * 3), ("look_at", C.c_float * 3), ("up", C.c_float * 3),
+                ("vfov_degrees", C.c_float), ("aperture_radius", C.c_float), ("focus_distance", C.c_float)]
+
+
+class EnvironmentC(C.Structure):
+    _fields_ = [("width", C.c_uint32), ("height", C.c_uint32), ("texels", C.c_void_p)]
+
+
+class DeltaLightC(C.Structure):
+    _fields_ = [("kind", C.c_uint32), ("anchor", C.c_float * 3), ("emission", C.c_float * 3)]
+
+
+class Options(C.Structure):
+    _fields_ = [("device", C.c_int32)]
+
+
+class Stats(C.Structure):
+    _fields_ = [("extension_rays", C.c_uint64), ("shadow_rays", C.c_uint64), ("samples", C.c_uint64),
+                ("node_visits", C.c_uint64), ("triangle_tests", C.c_uint64), ("gpu_ms", C.c_float),
+                ("raygen_ms", C.c_float), ("intersect_ms", C.c_float), ("shade_ms", C.c_float),
+                ("shadow_ms", C.c_float), ("film_ms", C.c_float), ("kernel_launches", C.c_uint32),
+                ("waves", C.c_uint32), ("samples_per_wave", C.c_uint32), ("overflow", C.c_uint32)]
+
+
+PROFILE_TIMING, PROFILE_COUNTS = 1, 2
+
+
+LIGHT_RECORD_DTYPE = np.dtype([
+    ("anchor", "<f4", 3), ("pdf", "<f4"), ("edge1", "<f4", 3), ("alias_threshold", "<f4"), ("edge2", "<f4", 3),
+    ("alias_index", "<u4"), ("emission", "<f4", 3), ("instance", "<u4"), ("kind", "<u4"), ("primitive", "<u4"),
+    ("pad", "<u4", 2),
+])
+assert LIGHT_RECORD_DTYPE.itemsize == 80
+
+# Every entry point include/cenote_c.h declares.
+EXPORTED_SYMBOLS = [
+    "cenote_last_error", "cenote_context_create", "cenote_context_destroy", "cenote_context_stream",
+    "cenote_synchronize", "cenote_scene_create", "cenote_scene_destroy", "cenote_scene_set_camera",
+    "cenote_scene_prep_times", "cenote_scene_device_bytes", "cenote_scene_light_records", "cenote_scene_env_tables",
+    "cenote_renderer_create", "cenote_renderer_destroy", "cenote_renderer_set_samples_per_wave",
+    "cenote_renderer_stats", "cenote_renderer_set_profiling", "cenote_render_once", "cenote_film_create", "cenote_film_destroy", "cenote_film_reset",
+    "cenote_film_samples", "cenote_accumulate", "cenote_accumulate_n", "cenote_film_averages", "cenote_film_sums",
+    "cenote_film_device_sums", "cenote_probe_sampler", "cenote_probe_bsdf", "cenote_probe_bsdf_sample",
+    "cenote_probe_intersect", "cenote_probe_shadow", "cenote_probe_env_sample", "cenote_probe_env_pdf",
+]
+
+_lib = None
+
+
+def library() -> C.CDLL:
+    """Load libcenote_b200.so (raises if it was never built)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not LIB_PATH.exists():
+        raise CenoteError(-3, f"{LIB_PATH.name} is not built; run `python -m cenote_b200.build`")
+    lib = C.CDLL(str(LIB_PATH))
+    P, U32, I32, F = C.c_void_p, C.c_uint32, C.c_int32, C.c_float
+    sig = {
+        "cenote_last_error": (C.c_char_p, []),
+        "cenote_context_create": (I32, [P, P]),
+        "cenote_context_destroy": (None, [P]),
+        "cenote_context_stream": (P, [P]),
+        "cenote_synchronize": (I32, [P]),
+        "cenote_scene_create": (I32, [P, P, U32, P, P, P, U32, P]),
+        "cenote_scene_destroy": (None, [P]),
+        "cenote_scene_set_camera": (I32, [P, P]),
+        "cenote_scene_prep_times": (I32, [P, P]),
+        "cenote_scene_device_bytes": (C.c_uint64, [P]),
+        "cenote_scene_light_records": (I32, [P, P, P]),
+        "cenote_scene_env_tables": (I32, [P, P, P, P, P, P]),
+        "cenote_renderer_create": (I32, [P, U32, U32, U32, P]),
+        "cenote_renderer_destroy": (None, [P]),
+        "cenote_renderer_set_samples_per_wave": (I32, [P, U32]),
+        "cenote_renderer_stats": (I32, [P, P]),
+        "cenote_renderer_set_profiling": (I32, [P, U32]),
+        "cenote_render_once": (I32, [P, P, U32, U32, U32, P]),
+        "cenote_film_create": (I32, [P, U32, U32, P]),
+        "cenote_film_destroy": (None, [P]),
+        "cenote_film_reset": (I32, [P]),
+        "cenote_film_samples": (U32, [P]),
+        "cenote_accumulate": (I32, [P, P, P]),
+        "cenote_accumulate_n": (I32, [P, P, P, U32]),
+        "cenote_film_averages": (I32, [P, P, P, P, P]),
+        "cenote_film_sums": (I32, [P, P]),
+        "cenote_film_device_sums": (P, [P]),
+        "cenote_probe_sampler": (I32, [P, U32, U32, U32, P, P]),
+        "cenote_probe_bsdf": (I32, [P, P, P, P, U32, U32, P, P]),
+        "cenote_probe_bsdf_sample": (I32, [P, P, P, P, U32, U32, P, P, P]),
+        "cenote_probe_intersect": (I32, [P, P, P, U32, P, P]),
+        "cenote_probe_shadow": (I32, [P, P, P, P, P, U32, P]),
+        "cenote_probe_env_sample": (I32, [P, P, U32, P, P, P]),
+        "cenote_probe_env_pdf": (I32, [P, P, U32, P]),
+    }
+    for name, (res, args) in sig.items():
+        fn = getattr(lib, name)
+        fn.restype = res
+        fn.argtypes = args
+    _lib = lib
+    return lib
+
+
+def _check(code: int) -> None:
+    if code != 0:
+        msg = library().cenote_last_error()
+        raise CenoteError(code, msg.decode() if msg else "")
+
+
+def _ptr(a: np.ndarray) -> int:
+    return a.ctypes.data
+
+
+def _c_material(m) -> Material:
+    out = Material()
+    C.memmove(C.addressof(out), np.asarray(m, scenes.MATERIAL_DTYPE).tobytes(), 144)
+    return out
+
+
+def _c_camera(cam: scenes.Camera) -> CameraC:
+    c = CameraC()
+    c.position[:] = [float(v) for v in cam.position]
+    c.look_at[:] = [float(v) for v in cam.look_at]
+    c.up[:] = [float(v) for v in cam.up]
+    c.vfov_degrees = cam.vfov_degrees
+    c.aperture_radius = cam.aperture_radius
+    c.focus_distance = cam.focus_distance
+    return c
+
+
+class Context:
+    """One CUDA device and the stream every handle made from it shares."""
+
+    def __init__(self, device: int = 0):
+        lib = library()
+        h = C.c_void_p()
+        opts = Options(device)
+        _check(lib.cenote_context_create(C.byref(opts), C.byref(h)))
+        self._h = h
+
+    @property
+    def handle(self):
+        return self._h
+
+    @property
+    def stream(self) -> int:
+        return library().cenote_context_stream(self._h) or 0
+
+    def synchronize(self) -> None:
+        _check(library().cenote_synchronize(self._h))
+
+    def close(self) -> None:
+        if self._h:
+            library().cenote_context_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    # ---- probes -------------------------------------------------------------------
+
+    def probe_sampler(self, pixel: int, dimension: int, count: int):
+        pts = np.zeros((count, 2), np.float32)
+        vals = np.zeros(count, np.float32)
+        _check(library().cenote_probe_sampler(self._h, pixel, dimension, count, _ptr(pts), _ptr(vals)))
+        return pts, vals
+
+    def probe_bsdf(self, material, wo: np.ndarray, wi: np.ndarray, exiting: bool = False):
+        wo = np.ascontiguousarray(wo, np.float32)
+        wi = np.ascontiguousarray(wi, np.float32)
+        n = len(wo)
+        f = np.zeros((n, 3), np.float32)
+        pdf = np.zeros(n, np.float32)
+        m = _c_material(material)
+        _check(library().cenote_probe_bsdf(self._h, C.byref(m), _ptr(wo), _ptr(wi), n, int(exiting), _ptr(f), _ptr(pdf)))
+        return f, pdf
+
+    def probe_bsdf_sample(self, material, wo: np.ndarray, u: np.ndarray, exiting: bool = False):
+        wo = np.ascontiguousarray(wo, np.float32)
+        u = np.ascontiguousarray(u, np.float32)
+        n = len(wo)
+        wi = np.zeros((n, 3), np.float32)
+        pdf = np.zeros(n, np.float32)
+        lobe = np.zeros(n, np.uint32)
+        m = _c_material(material)
+        _check(library().cenote_probe_bsdf_sample(self._h, C.byref(m), _ptr(wo), _ptr(u), n, int(exiting), _ptr(wi),
+                                                  _ptr(pdf), _ptr(lobe)))
+        return wi, pdf, lobe
+
+
+class Scene:
+    """Scene::new: meshes, transforms and materials, a camera and an environment."""
+
+    def __init__(self, ctx: Context, spec: SceneSpec):
+        lib = library()
+        self.ctx = ctx
+        self.spec = spec
+        self._keep = []
+        objs = (Object * len(spec.objects))()
+        for i, o in enumerate(spec.objects):
+            m = o.mesh
+            arrays = [np.ascontiguousarray(a) for a in (m.positions, m.normals, m.uvs, m.indices)]
+            self._keep += arrays
+            objs[i].positions, objs[i].normals, objs[i].uvs, objs[i].indices = [_ptr(a) for a in arrays]
+            objs[i].vertex_count = len(m.positions)
+            objs[i].triangle_count = len(m.indices)
+            objs[i].transform[:] = [float(v) for v in np.asarray(o.transform, np.float32)]
+            objs[i].material = _c_material(o.material)
+            objs[i].camera_visible = 1 if o.camera_visible else 0
+        env = spec.environment
+        tex = np.ascontiguousarray(env.texels, np.float32)
+        self._keep.append(tex)
+        envc = EnvironmentC(env.width, env.height, _ptr(tex))
+        deltas = (DeltaLightC * max(1, len(spec.delta_lights)))()
+        for i, d in enumerate(spec.delta_lights):
+            deltas[i].kind = d.kind
+            deltas[i].anchor[:] = list(d.anchor)
+            deltas[i].emission[:] = list(d.emission)
+        cam = _c_camera(spec.camera)
+        h = C.c_void_p()
+        _check(lib.cenote_scene_create(ctx.handle, objs, len(spec.objects), C.byref(cam), C.byref(envc), deltas,
+                                       len(spec.delta_lights), C.byref(h)))
+        self._h = h
+        self._keep = None  # the library copied everything it needs
+
+    @property
+    def handle(self):
+        return self._h
+
+    def set_camera(self, cam: scenes.Camera) -> None:
+        c = _c_camera(cam)
+        _check(library().cenote_scene_set_camera(self._h, C.byref(c)))
+
+    def prep_times_ms(self):
+        out = np.zeros(3, np.float32)
+        _check(library().cenote_scene_prep_times(self._h, _ptr(out)))
+        return out
+
+    def device_bytes(self) -> int:
+        return int(library().cenote_scene_device_bytes(self._h))
+
+    def light_records(self) -> np.ndarray:
+        n = C.c_uint32()
+        _check(library().cenote_scene_light_records(self._h, None, C.byref(n)))
+        out = np.zeros(n.value, LIGHT_RECORD_DTYPE)
+        if n.value:
+            _check(library().cenote_scene_light_records(self._h, _ptr(out), C.byref(n)))
+        return out
+
+    def env_tables(self):
+        env = self.spec.environment
+        w, h = env.width, env.height
+        marginal = np.zeros(h + 1, np.float32)
+        conditional = np.zeros(h * (w + 1), np.float32)
+        pdfs = np.zeros(h * w, np.float32)
+        power = C.c_double()
+        sel = C.c_float()
+        _check(library().cenote_scene_env_tables(self._h, _ptr(marginal), _ptr(conditional), _ptr(pdfs),
+                                                 C.byref(power), C.byref(sel)))
+        return marginal, conditional, pdfs, power.value, sel.value
+
+    def probe_intersect(self, origins: np.ndarray, directions: np.ndarray):
+        o = np.ascontiguousarray(origins, np.float32)
+        d = np.ascontiguousarray(directions, np.float32)
+        n = len(o)
+        hits = np.zeros((n, 4), np.uint32)
+        t = np.zeros(n, np.float32)
+        _check(library().cenote_probe_intersect(self._h, _ptr(o), _ptr(d), n, _ptr(hits), _ptr(t)))
+        return hits, t
+
+    def probe_shadow(self, origins, directions, tmax, targets):
+        o = np.ascontiguousarray(origins, np.float32)
+        d = np.ascontiguousarray(directions, np.float32)
+        tm = np.ascontiguousarray(tmax, np.float32)
+        tg = np.ascontiguousarray(targets, np.uint32)
+        n = len(o)
+        out = np.zeros(n, np.float32)
+        _check(library().cenote_probe_shadow(self._h, _ptr(o), _ptr(d), _ptr(tm), _ptr(tg), n, _ptr(out)))
+        return out
+
+    def probe_env_sample(self, u: np.ndarray):
+        u = np.ascontiguousarray(u, np.float32)
+        n = len(u)
+        d = np.zeros((n, 3), np.float32)
+        pdf = np.zeros(n, np.float32)
+        rc = np.zeros((n, 2), np.uint32)
+        _check(library().cenote_probe_env_sample(self._h, _ptr(u), n, _ptr(d), _ptr(pdf), _ptr(rc)))
+        return d, pdf, rc
+
+    def probe_env_pdf(self, directions: np.ndarray):
+        d = np.ascontiguousarray(directions, np.float32)
+        out = np.zeros(len(d), np.float32)
+        _check(library().cenote_probe_env_pdf(self._h, _ptr(d), len(d), _ptr(out)))
+        return out
+
+    def close(self) -> None:
+        if getattr(self, "_h", None):
+            library().cenote_scene_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class Film:
+    """The progressive film: running sums plus the sample count."""
+
+    def __init__(self, ctx: Context, width: int, height: int):
+        h = C.c_void_p()
+        _check(library().cenote_film_create(ctx.handle, width, height, C.byref(h)))
+        self._h = h
+        self.ctx = ctx
+        self.width, self.height = width, height
+
+    @property
+    def handle(self):
+        return self._h
+
+    @property
+    def samples(self) -> int:
+        return int(library().cenote_film_samples(self._h))
+
+    def reset(self) -> None:
+        _check(library().cenote_film_reset(self._h))
+
+    def averages(self, out: np.ndarray | None = None) -> np.ndarray:
+        if out is None:
+            out = np.zeros((self.height, self.width, 4), np.float32)
+        _check(library().cenote_film_averages(self._h, _ptr(out), None, None, None))
+        return out
+
+    def averages_into(self, ptr: int) -> None:
+        """Resolve into caller memory at `ptr` (pinned host memory for speed)."""
+        _check(library().cenote_film_averages(self._h, ptr, None, None, None))
+
+    def sums(self) -> np.ndarray:
+        out = np.zeros((self.height, self.width, 4), np.float32)
+        _check(library().cenote_film_sums(self._h, _ptr(out)))
+        return out
+
+    def device_sums(self) -> int:
+        return int(library().cenote_film_device_sums(self._h) or 0)
+
+    def close(self) -> None:
+        if getattr(self, "_h", None):
+            library().cenote_film_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class Renderer:
+    """Renderer::with_max_bounces + LightSampling: the wavefront engine."""
+
+    def __init__(self, ctx: Context, max_bounces: int = 8, light_sampling: int = LIGHT_SAMPLING_MIS,
+                 capacity: int = 0, samples_per_wave: int = 0):
+        h = C.c_void_p()
+        _check(library().cenote_renderer_create(ctx.handle, max_bounces, light_sampling, capacity, C.byref(h)))
+        self._h = h
+        self.ctx = ctx
+        if samples_per_wave:
+            self.set_samples_per_wave(samples_per_wave)
+
+    @property
+    def handle(self):
+        return self._h
+
+    def set_samples_per_wave(self, n: int) -> None:
+        _check(library().cenote_renderer_set_samples_per_wave(self._h, n))
+
+    def render(self, scene: Scene, width: int, height: int, sample: int = 0) -> np.ndarray:
+        out = np.zeros((height, width, 4), np.float32)
+        _check(library().cenote_render_once(self._h, scene.handle, width, height, sample, _ptr(out)))
+        return out
+
+    def accumulate(self, scene: Scene, film: Film, count: int = 1) -> None:
+        _check(library().cenote_accumulate_n(self._h, scene.handle, film.handle, count))
+
+    def set_profiling(self, flags: int) -> None:
+        _check(library().cenote_renderer_set_profiling(self._h, flags))
+
+    def stats(self) -> dict:
+        s = Stats()
+        _check(library().cenote_renderer_stats(self._h, C.byref(s)))
+        return {name: getattr(s, name) for name, _ in Stats._fields_}
+
+    def close(self) -> None:
+        if getattr(self, "_h", None):
+            library().cenote_renderer_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

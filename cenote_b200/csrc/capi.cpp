@@ -1,0 +1,1070 @@
+// The C ABI (include/cenote_c.h): context, scene prep, renderer, film and
+// probes. Host arithmetic that feeds bit-exact tables is compiled with
+// -ffp-contract=off so every a·b + c rounds twice, as the reference's Rust does.
+#include <algorithm>
+#include <atomic>
+#include <chrono>
+#include <cmath>
+#include <cstring>
+#include <memory>
+#include <mutex>
+#include <string>
+#include <thread>
+#include <vector>
+
+#include <cuda_runtime.h>
+
+#include "../../include/cenote_c.h"
+#include "bvh_build.h"
+#include "records.h"
+#include "wavefront.h"
+
+namespace cn {
+void launch_env_tables(const float4* texels, const double* sin_theta, const double* solid, uint32_t w, uint32_t h,
+                       double* scratch, float* marginal, float* conditional, float* pdfs, double* totals,
+                       cudaStream_t stream);
+void probe_sampler(uint32_t pixel, uint32_t dim, uint32_t count, float2* points, float* values, cudaStream_t s);
+void probe_bsdf(const float* tables, const Material& m, const float3* wo, const float3* wi, uint32_t n,
+                uint32_t exiting, float3* f, float* pdf, cudaStream_t s);
+void probe_bsdf_sample(const float* tables, const Material& m, const float3* wo, const float3* u, uint32_t n,
+                       uint32_t exiting, float3* wi, float* pdf, uint32_t* lobe, cudaStream_t s);
+void probe_intersect(const DeviceScene& scene, const float3* org, const float3* dir, uint32_t n, uint4* hits, float* t,
+                     uint32_t* flag, cudaStream_t s);
+void probe_shadow(const DeviceScene& scene, const float3* org, const float3* dir, const float* tmax,
+                  const uint2* targets, uint32_t n, float* out, uint32_t* flag, cudaStream_t s);
+void probe_env_sample(const DeviceScene& scene, const float2* u, uint32_t n, float3* dir, float* pdf, uint2* rc,
+                      cudaStream_t s);
+void probe_env_pdf(const DeviceScene& scene, const float3* d, uint32_t n, float* pdf, cudaStream_t s);
+}  // namespace cn
+
+using namespace cn;
+
+namespace {
+
+// The BSDF lookup tables (ggx_energy.bin ++ ltc_sheen.bin, the layout of
+// crates/cenote/src/tables.rs:51-80), embedded at build time.
+const uint32_t kTables[] = {
+#include "tables_blob.inc"
+};
+static_assert(sizeof(kTables) == 16928 * 4, "BSDF tables are 16,928 floats");
+
+thread_local std::string g_error;
+
+int32_t fail(int32_t code, const std::string& msg) {
+    g_error = msg;
+    return code;
+}
+
+#define CN_CUDA(call)                                                                       \
+    do {                                                                                    \
+        cudaError_t e_ = (call);                                                            \
+        if (e_ != cudaSuccess)                                                              \
+            return fail(e_ == cudaErrorMemoryAllocation ? CENOTE_E_ALLOCATION : CENOTE_E_DEVICE, \
+                        std::string(#call ": ") + cudaGetErrorString(e_));                  \
+    } while (0)
+
+#define CN_CHECK(cond, code, msg) \
+    do {                          \
+        if (!(cond)) return fail((code), (msg)); \
+    } while (0)
+
+// Bounded wait: poll an event until it completes or `timeout_ms` passes.
+int32_t wait_stream(cudaStream_t s, cudaEvent_t ev, double timeout_ms) {
+    cudaError_t e = cudaEventRecord(ev, s);
+    if (e != cudaSuccess) return fail(CENOTE_E_DEVICE, std::string("cudaEventRecord: ") + cudaGetErrorString(e));
+    auto t0 = std::chrono::steady_clock::now();
+    for (;;) {
+        e = cudaEventQuery(ev);
+        if (e == cudaSuccess) return CENOTE_OK;
+        if (e != cudaErrorNotReady) return fail(CENOTE_E_DEVICE, std::string("device error: ") + cudaGetErrorString(e));
+        double ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+        if (ms > timeout_ms) return fail(CENOTE_E_TIMEOUT, "device work did not finish within the wait bound");
+        std::this_thread::sleep_for(std::chrono::microseconds(ms < 5.0 ? 20 : 200));
+    }
+}
+
+struct DeviceBuffer {
+    void* ptr = nullptr;
+    size_t bytes = 0;
+    DeviceBuffer() = default;
+    DeviceBuffer(const DeviceBuffer&) = delete;
+    DeviceBuffer& operator=(const DeviceBuffer&) = delete;
+    ~DeviceBuffer() { release(); }
+    void release() {
+        if (ptr) cudaFree(ptr);
+        ptr = nullptr;
+        bytes = 0;
+    }
+    cudaError_t alloc(size_t n) {
+        release();
+        if (n == 0) n = 16;
+        bytes = n;
+        return cudaMalloc(&ptr, n);
+    }
+    template <class T>
+    T* as() const {
+        return static_cast<T*>(ptr);
+    }
+};
+
+struct V3 {
+    float x, y, z;
+};
+V3 v3(const float* f) { return {f[0], f[1], f[2]}; }
+V3 operator-(V3 a, V3 b) { return {a.x - b.x, a.y - b.y, a.z - b.z}; }
+V3 operator*(V3 a, float s) { return {a.x * s, a.y * s, a.z * s}; }
+float dotv(V3 a, V3 b) { return a.x * b.x + a.y * b.y + a.z * b.z; }
+V3 crossv(V3 a, V3 b) { return {a.y * b.z - b.y * a.z, a.z * b.x - b.z * a.x, a.x * b.y - b.x * a.y}; }
+float lengthv(V3 a) { return std::sqrt(dotv(a, a)); }
+
+// color.rs:367-369
+float luminance(V3 c) { return c.x * 0.2722287f + c.y * 0.6740818f + c.z * 0.0536895f; }
+
+// glam's transform_point3 over the top three rows: ((x·p.x + y·p.y) + z·p.z) + w.
+V3 transform_point(const float m[12], V3 p) {
+    return {m[0] * p.x + m[1] * p.y + m[2] * p.z + m[3], m[4] * p.x + m[5] * p.y + m[6] * p.z + m[7],
+            m[8] * p.x + m[9] * p.y + m[10] * p.z + m[11]};
+}
+
+// Inverse of an affine 3×4 (rows), in double, rounded to f32.
+bool invert_affine(const float m[12], float out[3][4]) {
+    double a[3][3], t[3];
+    for (int r = 0; r < 3; ++r) {
+        for (int c = 0; c < 3; ++c) a[r][c] = m[4 * r + c];
+        t[r] = m[4 * r + 3];
+    }
+    double det = a[0][0] * (a[1][1] * a[2][2] - a[1][2] * a[2][1]) - a[0][1] * (a[1][0] * a[2][2] - a[1][2] * a[2][0]) +
+                 a[0][2] * (a[1][0] * a[2][1] - a[1][1] * a[2][0]);
+    if (!(std::fabs(det) > 0.0) || !std::isfinite(det)) return false;
+    double inv[3][3];
+    inv[0][0] = (a[1][1] * a[2][2] - a[1][2] * a[2][1]) / det;
+    inv[0][1] = (a[0][2] * a[2][1] - a[0][1] * a[2][2]) / det;
+    inv[0][2] = (a[0][1] * a[1][2] - a[0][2] * a[1][1]) / det;
+    inv[1][0] = (a[1][2] * a[2][0] - a[1][0] * a[2][2]) / det;
+    inv[1][1] = (a[0][0] * a[2][2] - a[0][2] * a[2][0]) / det;
+    inv[1][2] = (a[0][2] * a[1][0] - a[0][0] * a[1][2]) / det;
+    inv[2][0] = (a[1][0] * a[2][1] - a[1][1] * a[2][0]) / det;
+    inv[2][1] = (a[0][1] * a[2][0] - a[0][0] * a[2][1]) / det;
+    inv[2][2] = (a[0][0] * a[1][1] - a[0][1] * a[1][0]) / det;
+    for (int r = 0; r < 3; ++r) {
+        for (int c = 0; c < 3; ++c) out[r][c] = float(inv[r][c]);
+        out[r][3] = float(-(inv[r][0] * t[0] + inv[r][1] * t[1] + inv[r][2] * t[2]));
+    }
+    return true;
+}
+
+// ---- the light list: crates/cenote/src/lights.rs:123-275 -----------------------
+
+struct TriLight {
+    V3 c[3];
+    V3 emission;
+    uint32_t instance, primitive;
+};
+
+LightRecord make_record(uint32_t kind, V3 anchor, V3 e1, V3 e2, V3 em, uint32_t inst, uint32_t prim) {
+    LightRecord r;
+    std::memset(&r, 0, sizeof r);
+    r.anchor[0] = anchor.x; r.anchor[1] = anchor.y; r.anchor[2] = anchor.z;
+    r.edge1[0] = e1.x; r.edge1[1] = e1.y; r.edge1[2] = e1.z;
+    r.edge2[0] = e2.x; r.edge2[1] = e2.y; r.edge2[2] = e2.z;
+    r.emission[0] = em.x; r.emission[1] = em.y; r.emission[2] = em.z;
+    r.pdf = 0.0f;
+    r.alias_threshold = 1.0f;
+    r.alias_index = 0;
+    r.instance = inst;
+    r.kind = kind;
+    r.primitive = prim;
+    return r;
+}
+
+double record_area(const LightRecord& r) { return double(lengthv(crossv(v3(r.edge1), v3(r.edge2)))) / 2.0; }
+
+double record_power(const LightRecord& r) {
+    double luma = double(luminance(v3(r.emission)));
+    if (r.kind == KIND_TRIANGLE) return 3.141592653589793 * luma * record_area(r);
+    if (r.kind == KIND_DISTANT) return luma;
+    return 4.0 * 3.141592653589793 * luma;
+}
+
+// Walker/Vose over f64 shares: stable small/large partition, both popped
+// from the back, leftovers keep threshold 1.
+std::vector<LightRecord> build_lights(const std::vector<TriLight>& tris, const cenote_delta_light* deltas,
+                                      uint32_t n_deltas, double* total_out) {
+    std::vector<LightRecord> recs;
+    recs.reserve(tris.size() + n_deltas);
+    for (const TriLight& t : tris)
+        recs.push_back(make_record(KIND_TRIANGLE, t.c[0], t.c[1] - t.c[0], t.c[2] - t.c[0], t.emission, t.instance,
+                                   t.primitive));
+    for (uint32_t i = 0; i < n_deltas; ++i)
+        recs.push_back(make_record(deltas[i].kind, v3(deltas[i].anchor), {0, 0, 0}, {0, 0, 0}, v3(deltas[i].emission),
+                                   LIGHT_NONE, 0));
+    std::vector<double> power(recs.size());
+    double total = 0.0;
+    for (size_t i = 0; i < recs.size(); ++i) {
+        power[i] = record_power(recs[i]);
+        total += power[i];
+    }
+    *total_out = total;
+    if (total <= 0.0) return recs;
+    for (size_t i = 0; i < recs.size(); ++i) {
+        double sel = power[i] / total;
+        if (recs[i].kind == KIND_TRIANGLE) {
+            double area = record_area(recs[i]);
+            recs[i].pdf = area > 0.0 ? float(sel / area) : 0.0f;
+        } else {
+            recs[i].pdf = float(sel);
+        }
+    }
+    const double n = double(recs.size());
+    std::vector<double> share(recs.size());
+    std::vector<uint32_t> small, large;
+    for (size_t i = 0; i < recs.size(); ++i) {
+        share[i] = power[i] * n / total;
+        (share[i] < 1.0 ? small : large).push_back(uint32_t(i));
+    }
+    while (!small.empty() && !large.empty()) {
+        uint32_t poor = small.back(), rich = large.back();
+        small.pop_back();
+        large.pop_back();
+        recs[poor].alias_threshold = float(share[poor]);
+        recs[poor].alias_index = rich;
+        share[rich] -= 1.0 - share[poor];
+        (share[rich] < 1.0 ? small : large).push_back(rich);
+    }
+    return recs;
+}
+
+// scene/mod.rs:665-671
+float select_probability(double env_power, double light_power) {
+    if (light_power == 0.0) return env_power > 0.0 ? 1.0f : 0.0f;
+    return float(env_power / (env_power + light_power));
+}
+
+// Camera::basis (scene/mod.rs:448-460), scaled to the focal plane when the
+// lens is open (wavefront.rs:633-650).
+void camera_basis(const cenote_camera& cam, float aspect, WaveParams& wp) {
+    V3 pos = v3(cam.position), look = v3(cam.look_at), up = v3(cam.up);
+    V3 d = look - pos;
+    V3 f = d * (1.0f / lengthv(d));
+    V3 c = crossv(f, up);
+    V3 r = c * (1.0f / lengthv(c));
+    V3 u = crossv(r, f);
+    float half_h = std::tan(cam.vfov_degrees * (3.14159265358979323846f / 180.0f) / 2.0f);
+    V3 right = r * half_h * aspect, upv = u * half_h, fwd = f;
+    if (cam.aperture_radius > 0.0f) {
+        right = right * cam.focus_distance;
+        upv = upv * cam.focus_distance;
+        fwd = fwd * cam.focus_distance;
+    }
+    wp.cam_pos = make_float3(pos.x, pos.y, pos.z);
+    wp.cam_right = make_float3(right.x, right.y, right.z);
+    wp.cam_up = make_float3(upv.x, upv.y, upv.z);
+    wp.cam_fwd = make_float3(fwd.x, fwd.y, fwd.z);
+    wp.aperture = cam.aperture_radius;
+}
+
+bool camera_valid(const cenote_camera& cam) {
+    V3 pos = v3(cam.position), look = v3(cam.look_at), up = v3(cam.up);
+    V3 d = look - pos;
+    float l = lengthv(d);
+    if (!(l > 0.0f) || !std::isfinite(l)) return false;
+    V3 c = crossv(d * (1.0f / l), up);
+    float cl = lengthv(c);
+    return cl > 0.0f && std::isfinite(cl) && cam.vfov_degrees > 0.0f && cam.vfov_degrees < 180.0f &&
+           !(cam.aperture_radius > 0.0f && !(cam.focus_distance > 0.0f));
+}
+
+}  // namespace
+
+struct cenote_context {
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    cudaEvent_t sync_ev = nullptr;
+    cudaEvent_t t0 = nullptr, t1 = nullptr;
+    LaunchShape shape{};
+    DeviceBuffer tables;
+    std::mutex mu;
+};
+
+struct cenote_scene {
+    cenote_context* ctx = nullptr;
+    DeviceScene ds{};
+    std::vector<std::unique_ptr<DeviceBuffer>> buffers;
+    cudaArray_t env_array = nullptr;
+    cudaTextureObject_t env_tex = 0;
+    cenote_camera camera{};
+    std::vector<LightRecord> lights;
+    uint32_t env_w = 1, env_h = 1;
+    double env_power = 0.0;
+    float select_prob = 0.0f;
+    float prep_ms[3] = {0, 0, 0};
+    uint64_t device_bytes = 0;
+    DeviceBuffer* env_marginal = nullptr;
+    DeviceBuffer* env_conditional = nullptr;
+    DeviceBuffer* env_pdfs = nullptr;
+
+    DeviceBuffer* add(size_t bytes, cudaError_t* err) {
+        buffers.push_back(std::make_unique<DeviceBuffer>());
+        *err = buffers.back()->alloc(bytes);
+        device_bytes += bytes;
+        return buffers.back().get();
+    }
+    ~cenote_scene() {
+        if (env_tex) cudaDestroyTextureObject(env_tex);
+        if (env_array) cudaFreeArray(env_array);
+    }
+};
+
+struct cenote_renderer {
+    cenote_context* ctx = nullptr;
+    uint32_t max_bounces = 8;
+    uint32_t light_sampling = 0;
+    uint32_t capacity_req = 0;
+    uint32_t samples_per_wave = 0;
+    uint32_t profiling = 0;
+    std::vector<cudaEvent_t> events;
+    PathPool pool{};
+    DeviceBuffer org, dir, thr, hit, ps, state, rad, q0, q1, shadows, counters, tally, scratch;
+    size_t pool_cap = 0;
+    cenote_stats stats{};
+    unsigned long long tally_prev[5] = {0, 0, 0, 0, 0};
+
+    ~cenote_renderer() {
+        for (cudaEvent_t e : events) cudaEventDestroy(e);
+    }
+    cudaEvent_t event(size_t i) {
+        while (events.size() <= i) {
+            cudaEvent_t e;
+            if (cudaEventCreate(&e) != cudaSuccess) return nullptr;
+            events.push_back(e);
+        }
+        return events[i];
+    }
+
+    cudaError_t ensure(size_t cap) {
+        if (cap <= pool_cap) return cudaSuccess;
+        cudaError_t e;
+        if ((e = org.alloc(cap * 16)) || (e = dir.alloc(cap * 16)) || (e = thr.alloc(cap * 16)) ||
+            (e = hit.alloc(cap * 16)) || (e = ps.alloc(cap * 8)) || (e = state.alloc(cap * 4)) ||
+            (e = rad.alloc(cap * 16)) || (e = q0.alloc(cap * 4)) || (e = q1.alloc(cap * 4)) ||
+            (e = shadows.alloc(cap * sizeof(ShadowRay))))
+            return e;
+        pool.org = org.as<float4>();
+        pool.dir = dir.as<float4>();
+        pool.thr = thr.as<float4>();
+        pool.hit = hit.as<uint4>();
+        pool.ps = ps.as<uint2>();
+        pool.state = state.as<uint32_t>();
+        pool.rad = rad.as<float4>();
+        pool.queue[0] = q0.as<uint32_t>();
+        pool.queue[1] = q1.as<uint32_t>();
+        pool.shadows = shadows.as<ShadowRay>();
+        pool.capacity = uint32_t(cap);
+        pool_cap = cap;
+        return cudaSuccess;
+    }
+};
+
+struct cenote_film {
+    cenote_context* ctx = nullptr;
+    uint32_t width = 0, height = 0;
+    uint32_t samples = 0;
+    DeviceBuffer sum, avg;
+};
+
+extern "C" {
+
+const char* cenote_last_error(void) { return g_error.c_str(); }
+
+int32_t cenote_context_create(const cenote_options* options, cenote_context** out) {
+    CN_CHECK(out, CENOTE_E_INVALID_ARGUMENT, "null output handle");
+    *out = nullptr;
+    int count = 0;
+    cudaError_t e = cudaGetDeviceCount(&count);
+    if (e != cudaSuccess || count == 0) return fail(CENOTE_E_NO_CAPABLE_GPU, "no CUDA device is visible");
+    int dev = options ? options->device : 0;
+    CN_CHECK(dev >= 0 && dev < count, CENOTE_E_INVALID_ARGUMENT, "device ordinal out of range");
+    cudaDeviceProp prop;
+    CN_CUDA(cudaGetDeviceProperties(&prop, dev));
+    if (prop.major < 10) return fail(CENOTE_E_NO_CAPABLE_GPU, "the kernels are built for sm_100a (B200)");
+    CN_CUDA(cudaSetDevice(dev));
+    auto ctx = std::make_unique<cenote_context>();
+    ctx->device = dev;
+    CN_CUDA(cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking));
+    CN_CUDA(cudaEventCreateWithFlags(&ctx->sync_ev, cudaEventDisableTiming));
+    CN_CUDA(cudaEventCreate(&ctx->t0));
+    CN_CUDA(cudaEventCreate(&ctx->t1));
+    ctx->shape = launch_shape(dev);
+    CN_CUDA(ctx->tables.alloc(sizeof(kTables)));
+    CN_CUDA(cudaMemcpy(ctx->tables.ptr, kTables, sizeof(kTables), cudaMemcpyHostToDevice));
+    *out = ctx.release();
+    return CENOTE_OK;
+}
+
+void cenote_context_destroy(cenote_context* ctx) {
+    if (!ctx) return;
+    cudaSetDevice(ctx->device);
+    if (ctx->stream) cudaStreamSynchronize(ctx->stream);
+    ctx->tables.release();
+    if (ctx->sync_ev) cudaEventDestroy(ctx->sync_ev);
+    if (ctx->t0) cudaEventDestroy(ctx->t0);
+    if (ctx->t1) cudaEventDestroy(ctx->t1);
+    if (ctx->stream) cudaStreamDestroy(ctx->stream);
+    delete ctx;
+}
+
+void* cenote_context_stream(cenote_context* ctx) { return ctx ? static_cast<void*>(ctx->stream) : nullptr; }
+
+int32_t cenote_synchronize(cenote_context* ctx) {
+    CN_CHECK(ctx, CENOTE_E_INVALID_ARGUMENT, "null context");
+    return wait_stream(ctx->stream, ctx->sync_ev, 600000.0);
+}
+
+// ---- scene -------------------------------------------------------------------------
+
+int32_t cenote_scene_create(cenote_context* ctx, const cenote_object* objects, uint32_t object_count,
+                            const cenote_camera* camera, const cenote_environment* env,
+                            const cenote_delta_light* deltas, uint32_t delta_count, cenote_scene** out) {
+    CN_CHECK(ctx && out, CENOTE_E_INVALID_ARGUMENT, "null context or output handle");
+    *out = nullptr;
+    CN_CHECK(objects && object_count > 0, CENOTE_E_INVALID_ARGUMENT, "a scene needs at least one object");
+    CN_CHECK(object_count < 0xffffffu, CENOTE_E_INVALID_ARGUMENT, "instance index exceeds 24 bits");
+    CN_CHECK(camera && camera_valid(*camera), CENOTE_E_INVALID_ARGUMENT, "degenerate camera");
+    CN_CHECK(env && env->width > 0 && env->height > 0 && env->texels, CENOTE_E_INVALID_ARGUMENT,
+             "environment needs width, height and texels");
+    CN_CHECK(delta_count == 0 || deltas, CENOTE_E_INVALID_ARGUMENT, "null delta-light array");
+    for (uint32_t i = 0; i < delta_count; ++i)
+        CN_CHECK(deltas[i].kind == KIND_DISTANT || deltas[i].kind == KIND_POINT, CENOTE_E_INVALID_ARGUMENT,
+                 "unknown delta-light kind");
+    std::lock_guard<std::mutex> lock(ctx->mu);
+    CN_CUDA(cudaSetDevice(ctx->device));
+    auto t_start = std::chrono::steady_clock::now();
+    auto sc = std::make_unique<cenote_scene>();
+    sc->ctx = ctx;
+    sc->camera = *camera;
+    cudaError_t err = cudaSuccess;
+
+    std::vector<GeomRecord> geoms(object_count);
+    std::vector<Material> mats(object_count);
+    std::vector<BuildTri> tris;
+    std::vector<TriLight> tri_lights;
+    size_t total_tris = 0;
+    for (uint32_t i = 0; i < object_count; ++i) total_tris += objects[i].triangle_count;
+    tris.reserve(total_tris);
+    bool nonopaque = false;
+    for (uint32_t i = 0; i < object_count; ++i) {
+        const cenote_object& o = objects[i];
+        CN_CHECK(o.positions && o.normals && o.uvs && o.indices && o.vertex_count > 0, CENOTE_E_INVALID_ARGUMENT,
+                 "object " + std::to_string(i) + " lacks attributes");
+        for (uint64_t k = 0; k < uint64_t(o.triangle_count) * 3; ++k)
+            CN_CHECK(o.indices[k] < o.vertex_count, CENOTE_E_SCENE,
+                     "object " + std::to_string(i) + " indexes past its vertices");
+        GeomRecord& g = geoms[i];
+        std::memset(&g, 0, sizeof g);
+        std::memcpy(g.o2w, o.transform, sizeof g.o2w);
+        CN_CHECK(invert_affine(o.transform, g.w2o), CENOTE_E_INVALID_ARGUMENT,
+                 "object " + std::to_string(i) + " transform is not invertible");
+        g.light = LIGHT_NONE;
+        DeviceBuffer* bp = sc->add(size_t(o.vertex_count) * 12, &err);
+        CN_CUDA(err);
+        DeviceBuffer* bn = sc->add(size_t(o.vertex_count) * 12, &err);
+        CN_CUDA(err);
+        DeviceBuffer* bu = sc->add(size_t(o.vertex_count) * 8, &err);
+        CN_CUDA(err);
+        DeviceBuffer* bi = sc->add(size_t(o.triangle_count) * 12, &err);
+        CN_CUDA(err);
+        CN_CUDA(cudaMemcpyAsync(bp->ptr, o.positions, size_t(o.vertex_count) * 12, cudaMemcpyHostToDevice, ctx->stream));
+        CN_CUDA(cudaMemcpyAsync(bn->ptr, o.normals, size_t(o.vertex_count) * 12, cudaMemcpyHostToDevice, ctx->stream));
+        CN_CUDA(cudaMemcpyAsync(bu->ptr, o.uvs, size_t(o.vertex_count) * 8, cudaMemcpyHostToDevice, ctx->stream));
+        if (o.triangle_count)
+            CN_CUDA(cudaMemcpyAsync(bi->ptr, o.indices, size_t(o.triangle_count) * 12, cudaMemcpyHostToDevice,
+                                    ctx->stream));
+        g.positions = bp->as<float>();
+        g.normals = bn->as<float>();
+        g.uvs = bu->as<float>();
+        g.indices = bi->as<uint32_t>();
+        mats[i] = o.material;
+        V3 em = v3(o.material.emission);
+        bool emissive = em.x != 0.0f || em.y != 0.0f || em.z != 0.0f;
+        bool opaque = o.material.opacity >= 1.0f && o.material.opacity_texture == TEXTURE_NONE;
+        nonopaque = nonopaque || !opaque;
+        uint32_t flags = (o.camera_visible ? RAY_MASK_ALL : (RAY_MASK_ALL & ~RAY_MASK_CAMERA)) | (opaque ? TRI_OPAQUE : 0u);
+        for (uint32_t t = 0; t < o.triangle_count; ++t) {
+            BuildTri bt;
+            V3 c[3];
+            for (int k = 0; k < 3; ++k) {
+                uint32_t vi = o.indices[3 * t + k];
+                c[k] = transform_point(o.transform, v3(o.positions + 3 * size_t(vi)));
+                bt.v[k][0] = c[k].x;
+                bt.v[k][1] = c[k].y;
+                bt.v[k][2] = c[k].z;
+            }
+            bt.instance = i;
+            bt.primitive = t;
+            bt.flags = flags;
+            tris.push_back(bt);
+            if (emissive) {
+                if (g.light == LIGHT_NONE) g.light = uint32_t(tri_lights.size());
+                tri_lights.push_back({{c[0], c[1], c[2]}, em, i, t});
+            }
+        }
+    }
+    double light_power = 0.0;
+    sc->lights = build_lights(tri_lights, deltas, delta_count, &light_power);
+
+    auto t_bvh = std::chrono::steady_clock::now();
+    WideBvh bvh = build_wide_bvh(tris, std::max(1u, std::thread::hardware_concurrency()));
+    sc->prep_ms[0] = float(std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t_bvh).count());
+    DeviceBuffer* bnodes = sc->add(bvh.nodes.size() * sizeof(WideNode), &err);
+    CN_CUDA(err);
+    DeviceBuffer* btris = sc->add(bvh.tris.size() * 4, &err);
+    CN_CUDA(err);
+    if (!bvh.nodes.empty()) {
+        CN_CUDA(cudaMemcpyAsync(bnodes->ptr, bvh.nodes.data(), bvh.nodes.size() * sizeof(WideNode),
+                                cudaMemcpyHostToDevice, ctx->stream));
+        CN_CUDA(cudaMemcpyAsync(btris->ptr, bvh.tris.data(), bvh.tris.size() * 4, cudaMemcpyHostToDevice, ctx->stream));
+    }
+    DeviceBuffer* bgeo = sc->add(geoms.size() * sizeof(GeomRecord), &err);
+    CN_CUDA(err);
+    CN_CUDA(cudaMemcpyAsync(bgeo->ptr, geoms.data(), geoms.size() * sizeof(GeomRecord), cudaMemcpyHostToDevice,
+                            ctx->stream));
+    DeviceBuffer* bmat = sc->add(mats.size() * sizeof(Material), &err);
+    CN_CUDA(err);
+    CN_CUDA(cudaMemcpyAsync(bmat->ptr, mats.data(), mats.size() * sizeof(Material), cudaMemcpyHostToDevice, ctx->stream));
+    DeviceBuffer* blights = sc->add(std::max<size_t>(1, sc->lights.size()) * sizeof(LightRecord), &err);
+    CN_CUDA(err);
+    if (!sc->lights.empty())
+        CN_CUDA(cudaMemcpyAsync(blights->ptr, sc->lights.data(), sc->lights.size() * sizeof(LightRecord),
+                                cudaMemcpyHostToDevice, ctx->stream));
+
+    // Environment: texels → device, FP64 tables on the device, texture object.
+    auto t_env = std::chrono::steady_clock::now();
+    const uint32_t ew = env->width, eh = env->height;
+    const size_t en = size_t(ew) * eh;
+    sc->env_w = ew;
+    sc->env_h = eh;
+    DeviceBuffer* btex = sc->add(en * 16, &err);
+    CN_CUDA(err);
+    CN_CUDA(cudaMemcpyAsync(btex->ptr, env->texels, en * 16, cudaMemcpyHostToDevice, ctx->stream));
+    std::vector<double> rowc(2 * size_t(eh));
+    const double PI = 3.141592653589793;
+    for (uint32_t r = 0; r < eh; ++r) {
+        rowc[r] = std::sin((double(r) + 0.5) / double(eh) * PI);
+        double th0 = double(r) / double(eh) * PI, th1 = double(r + 1) / double(eh) * PI;
+        rowc[eh + r] = 2.0 * PI / double(ew) * (std::cos(th0) - std::cos(th1));
+    }
+    DeviceBuffer* brow = sc->add(rowc.size() * 8, &err);
+    CN_CUDA(err);
+    CN_CUDA(cudaMemcpyAsync(brow->ptr, rowc.data(), rowc.size() * 8, cudaMemcpyHostToDevice, ctx->stream));
+    DeviceBuffer scratch;
+    CN_CUDA(scratch.alloc((2 * en + 2 * size_t(eh) + 4) * 8));
+    sc->env_marginal = sc->add((eh + 1) * 4, &err);
+    CN_CUDA(err);
+    sc->env_conditional = sc->add(size_t(eh) * (ew + 1) * 4, &err);
+    CN_CUDA(err);
+    sc->env_pdfs = sc->add(en * 4, &err);
+    CN_CUDA(err);
+    double* totals = scratch.as<double>() + 2 * en + 2 * size_t(eh);
+    launch_env_tables(btex->as<float4>(), brow->as<double>(), brow->as<double>() + eh, ew, eh, scratch.as<double>(),
+                      sc->env_marginal->as<float>(), sc->env_conditional->as<float>(), sc->env_pdfs->as<float>(), totals,
+                      ctx->stream);
+    CN_CUDA(cudaGetLastError());
+    double host_totals[2] = {0, 0};
+    CN_CUDA(cudaMemcpyAsync(host_totals, totals, 16, cudaMemcpyDeviceToHost, ctx->stream));
+    cudaChannelFormatDesc fmt = cudaCreateChannelDesc<float4>();
+    CN_CUDA(cudaMallocArray(&sc->env_array, &fmt, ew, eh));
+    sc->device_bytes += en * 16;
+    CN_CUDA(cudaMemcpy2DToArrayAsync(sc->env_array, 0, 0, env->texels, size_t(ew) * 16, size_t(ew) * 16, eh,
+                                     cudaMemcpyHostToDevice, ctx->stream));
+    int32_t rc = wait_stream(ctx->stream, ctx->sync_ev, 600000.0);
+    if (rc != CENOTE_OK) return rc;
+    sc->prep_ms[1] = float(std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t_env).count());
+    sc->env_power = host_totals[1];
+    sc->select_prob = select_probability(sc->env_power, light_power);
+    cudaResourceDesc res;
+    std::memset(&res, 0, sizeof res);
+    res.resType = cudaResourceTypeArray;
+    res.res.array.array = sc->env_array;
+    cudaTextureDesc td;
+    std::memset(&td, 0, sizeof td);
+    td.addressMode[0] = cudaAddressModeWrap;   // u wraps in azimuth
+    td.addressMode[1] = cudaAddressModeClamp;  // v clamps at the poles
+    td.filterMode = cudaFilterModeLinear;
+    td.readMode = cudaReadModeElementType;
+    td.normalizedCoords = 1;
+    CN_CUDA(cudaCreateTextureObject(&sc->env_tex, &res, &td, nullptr));
+
+    DeviceScene& ds = sc->ds;
+    ds.nodes = bnodes->as<WideNode>();
+    ds.tris = btris->as<float4>();
+    ds.geometry = bgeo->as<GeomRecord>();
+    ds.materials = bmat->as<Material>();
+    ds.lights = blights->as<LightRecord>();
+    ds.bsdf_tables = ctx->tables.as<float>();
+    ds.env_marginal = sc->env_marginal->as<float>();
+    ds.env_conditional = sc->env_conditional->as<float>();
+    ds.env_pdfs = sc->env_pdfs->as<float>();
+    ds.env_tex = sc->env_tex;
+    ds.env_w = ew;
+    ds.env_h = eh;
+    ds.select_prob = sc->select_prob;
+    ds.light_count = uint32_t(sc->lights.size());
+    ds.node_count = uint32_t(bvh.nodes.size());
+    ds.tri_count = uint32_t(bvh.tris.size() / 12);
+    ds.has_nonopaque = nonopaque ? 1u : 0u;
+    sc->prep_ms[2] = float(std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t_start).count());
+    *out = sc.release();
+    return CENOTE_OK;
+}
+
+void cenote_scene_destroy(cenote_scene* scene) {
+    if (!scene) return;
+    cudaSetDevice(scene->ctx->device);
+    cudaStreamSynchronize(scene->ctx->stream);
+    delete scene;
+}
+
+int32_t cenote_scene_set_camera(cenote_scene* scene, const cenote_camera* camera) {
+    CN_CHECK(scene && camera && camera_valid(*camera), CENOTE_E_INVALID_ARGUMENT, "degenerate camera");
+    scene->camera = *camera;
+    return CENOTE_OK;
+}
+
+int32_t cenote_scene_prep_times(cenote_scene* scene, float* ms3) {
+    CN_CHECK(scene && ms3, CENOTE_E_INVALID_ARGUMENT, "null argument");
+    std::memcpy(ms3, scene->prep_ms, sizeof scene->prep_ms);
+    return CENOTE_OK;
+}
+
+uint64_t cenote_scene_device_bytes(cenote_scene* scene) { return scene ? scene->device_bytes : 0; }
+
+int32_t cenote_scene_light_records(cenote_scene* scene, void* out_records, uint32_t* out_count) {
+    CN_CHECK(scene && out_count, CENOTE_E_INVALID_ARGUMENT, "null argument");
+    *out_count = uint32_t(scene->lights.size());
+    if (out_records && !scene->lights.empty()) {
+        CN_CUDA(cudaSetDevice(scene->ctx->device));
+        CN_CUDA(cudaMemcpy(out_records, scene->ds.lights, scene->lights.size() * sizeof(LightRecord),
+                           cudaMemcpyDeviceToHost));
+    }
+    return CENOTE_OK;
+}
+
+int32_t cenote_scene_env_tables(cenote_scene* scene, float* marginal, float* conditional, float* pdfs, double* power,
+                                float* select_prob) {
+    CN_CHECK(scene, CENOTE_E_INVALID_ARGUMENT, "null scene");
+    CN_CUDA(cudaSetDevice(scene->ctx->device));
+    if (marginal)
+        CN_CUDA(cudaMemcpy(marginal, scene->env_marginal->ptr, (scene->env_h + 1) * 4, cudaMemcpyDeviceToHost));
+    if (conditional)
+        CN_CUDA(cudaMemcpy(conditional, scene->env_conditional->ptr, size_t(scene->env_h) * (scene->env_w + 1) * 4,
+                           cudaMemcpyDeviceToHost));
+    if (pdfs)
+        CN_CUDA(cudaMemcpy(pdfs, scene->env_pdfs->ptr, size_t(scene->env_h) * scene->env_w * 4, cudaMemcpyDeviceToHost));
+    if (power) *power = scene->env_power;
+    if (select_prob) *select_prob = scene->select_prob;
+    return CENOTE_OK;
+}
+
+// ---- renderer and film -------------------------------------------------------------------
+
+int32_t cenote_renderer_create(cenote_context* ctx, uint32_t max_bounces, uint32_t light_sampling, uint32_t capacity,
+                               cenote_renderer** out) {
+    CN_CHECK(ctx && out, CENOTE_E_INVALID_ARGUMENT, "null context or output handle");
+    *out = nullptr;
+    CN_CHECK(max_bounces >= 1 && max_bounces <= MAX_BOUNCES, CENOTE_E_INVALID_ARGUMENT,
+             "bounce cap outside 1..=255");
+    CN_CHECK(light_sampling <= CENOTE_LIGHT_SAMPLING_NEE, CENOTE_E_INVALID_ARGUMENT, "unknown light-sampling mode");
+    CN_CUDA(cudaSetDevice(ctx->device));
+    auto r = std::make_unique<cenote_renderer>();
+    r->ctx = ctx;
+    r->max_bounces = max_bounces;
+    r->light_sampling = light_sampling;
+    r->capacity_req = capacity;
+    CN_CUDA(r->counters.alloc(CTR_COUNT * 4));
+    CN_CUDA(r->tally.alloc(8 * 8));
+    CN_CUDA(cudaMemset(r->tally.ptr, 0, 64));
+    r->pool.counters = r->counters.as<uint32_t>();
+    *out = r.release();
+    return CENOTE_OK;
+}
+
+void cenote_renderer_destroy(cenote_renderer* r) {
+    if (!r) return;
+    cudaSetDevice(r->ctx->device);
+    cudaStreamSynchronize(r->ctx->stream);
+    delete r;
+}
+
+int32_t cenote_renderer_set_samples_per_wave(cenote_renderer* r, uint32_t spw) {
+    CN_CHECK(r, CENOTE_E_INVALID_ARGUMENT, "null renderer");
+    r->samples_per_wave = spw;
+    return CENOTE_OK;
+}
+
+int32_t cenote_renderer_set_profiling(cenote_renderer* r, uint32_t flags) {
+    CN_CHECK(r, CENOTE_E_INVALID_ARGUMENT, "null renderer");
+    CN_CHECK((flags & ~3u) == 0, CENOTE_E_INVALID_ARGUMENT, "unknown profiling flag");
+    r->profiling = flags;
+    return CENOTE_OK;
+}
+
+int32_t cenote_renderer_stats(cenote_renderer* r, cenote_stats* out) {
+    CN_CHECK(r && out, CENOTE_E_INVALID_ARGUMENT, "null argument");
+    *out = r->stats;
+    return CENOTE_OK;
+}
+
+int32_t cenote_film_create(cenote_context* ctx, uint32_t width, uint32_t height, cenote_film** out) {
+    CN_CHECK(ctx && out, CENOTE_E_INVALID_ARGUMENT, "null context or output handle");
+    *out = nullptr;
+    CN_CHECK(width > 0 && height > 0, CENOTE_E_INVALID_ARGUMENT, "zero-sized film");
+    CN_CHECK(uint64_t(width) * height < (1ull << 31), CENOTE_E_INVALID_ARGUMENT, "film too large");
+    CN_CUDA(cudaSetDevice(ctx->device));
+    auto f = std::make_unique<cenote_film>();
+    f->ctx = ctx;
+    f->width = width;
+    f->height = height;
+    size_t px = size_t(width) * height;
+    CN_CUDA(f->sum.alloc(px * 16));
+    CN_CUDA(f->avg.alloc(px * 16));
+    CN_CUDA(cudaMemsetAsync(f->sum.ptr, 0, px * 16, ctx->stream));
+    *out = f.release();
+    return CENOTE_OK;
+}
+
+void cenote_film_destroy(cenote_film* film) {
+    if (!film) return;
+    cudaSetDevice(film->ctx->device);
+    cudaStreamSynchronize(film->ctx->stream);
+    delete film;
+}
+
+int32_t cenote_film_reset(cenote_film* film) {
+    CN_CHECK(film, CENOTE_E_INVALID_ARGUMENT, "null film");
+    CN_CUDA(cudaSetDevice(film->ctx->device));
+    CN_CUDA(cudaMemsetAsync(film->sum.ptr, 0, size_t(film->width) * film->height * 16, film->ctx->stream));
+    film->samples = 0;
+    return CENOTE_OK;
+}
+
+uint32_t cenote_film_samples(cenote_film* film) { return film ? film->samples : 0; }
+
+void* cenote_film_device_sums(cenote_film* film) { return film ? film->sum.ptr : nullptr; }
+
+namespace {
+
+// Trace `count` samples starting at `sample0` for every pixel; each wave's
+// samples go either into the film (ascending order) or, for a one-shot
+// render, into `oneshot` as raw RGBA.
+int32_t run_waves(cenote_renderer* r, cenote_scene* sc, uint32_t width, uint32_t height, uint32_t sample0,
+                  uint32_t count, cenote_film* film, float4* oneshot) {
+    cenote_context* ctx = r->ctx;
+    const uint64_t pixels = uint64_t(width) * height;
+    uint32_t range = uint32_t(pixels);
+    uint32_t spw;
+    if (r->capacity_req && r->capacity_req < pixels) {
+        range = r->capacity_req;
+        spw = 1;
+    } else if (r->samples_per_wave) {
+        spw = r->samples_per_wave;
+    } else {
+        // Enough paths per wave to keep 148 SMs busy through the tail bounces.
+        uint64_t want = (uint64_t(1) << 22) / pixels;
+        spw = uint32_t(std::max<uint64_t>(1, std::min<uint64_t>(want, 64)));
+    }
+    if (oneshot) spw = 1;
+    spw = std::min(spw, count);
+    uint64_t need = uint64_t(range) * spw;
+    if (r->capacity_req) need = std::max<uint64_t>(need, std::min<uint64_t>(r->capacity_req, need));
+    CN_CHECK(need < (1ull << 31), CENOTE_E_INVALID_ARGUMENT, "wave too large");
+    CN_CUDA(r->ensure(need));
+
+    WaveParams wp{};
+    wp.width = width;
+    wp.height = height;
+    wp.max_bounces = r->max_bounces;
+    wp.light_sampling = r->light_sampling;
+    camera_basis(sc->camera, float(width) / float(height), wp);
+
+    const bool timing = (r->profiling & CENOTE_PROFILE_TIMING) != 0;
+    const bool counting = (r->profiling & CENOTE_PROFILE_COUNTS) != 0;
+    // Stage event layout per wave: [begin, after raygen, (after isect, shade, shadow) × bounces, after film].
+    const size_t per_wave = 3 + 3 * size_t(r->max_bounces);
+    size_t ev = 0;
+    uint32_t launches = 0, waves = 0;
+    auto mark = [&]() {
+        if (timing) cudaEventRecord(r->event(ev++), ctx->stream);
+    };
+    CN_CUDA(cudaEventRecord(ctx->t0, ctx->stream));
+    for (uint32_t done = 0; done < count;) {
+        uint32_t s = std::min(spw, count - done);
+        for (uint64_t base = 0; base < pixels; base += range) {
+            wp.pixel_base = uint32_t(base);
+            wp.pixel_count = uint32_t(std::min<uint64_t>(range, pixels - base));
+            wp.samples = s;
+            wp.sample_base = sample0 + done;
+            const uint32_t n0 = wp.pixel_count * s;
+            mark();
+            launch_wave_begin(r->pool, wp, ctx->shape, ctx->stream);
+            mark();
+            for (uint32_t b = 0; b < r->max_bounces; ++b) {
+                launch_intersect(sc->ds, r->pool, b, n0, ctx->shape, counting, ctx->stream);
+                mark();
+                launch_shade(sc->ds, r->pool, b, wp, n0, ctx->shape, ctx->stream);
+                mark();
+                launch_shadow(sc->ds, r->pool, b, ctx->shape, counting, ctx->stream);
+                mark();
+            }
+            launch_tally(r->pool, r->tally.as<unsigned long long>(), n0, r->max_bounces, ctx->stream);
+            if (film)
+                launch_accumulate(r->pool, film->sum.as<float4>(), wp.pixel_base, wp.pixel_count, s, false, ctx->stream);
+            else
+                launch_copy_rad(r->pool, oneshot, wp.pixel_base, wp.pixel_count, ctx->stream);
+            mark();
+            launches += 3 + 3 * r->max_bounces;
+            waves++;
+        }
+        done += s;
+    }
+    CN_CUDA(cudaEventRecord(ctx->t1, ctx->stream));
+    CN_CUDA(cudaGetLastError());
+    int32_t rc = wait_stream(ctx->stream, ctx->sync_ev, 600000.0);
+    if (rc != CENOTE_OK) return rc;
+    unsigned long long t[5];
+    CN_CUDA(cudaMemcpy(t, r->tally.ptr, sizeof t, cudaMemcpyDeviceToHost));
+    float ms = 0.0f;
+    cudaEventElapsedTime(&ms, ctx->t0, ctx->t1);
+    cenote_stats st{};
+    st.extension_rays = t[0] - r->tally_prev[0];
+    st.shadow_rays = t[1] - r->tally_prev[1];
+    st.overflow = uint32_t(t[2]);
+    st.node_visits = t[3] - r->tally_prev[3];
+    st.triangle_tests = t[4] - r->tally_prev[4];
+    st.samples = pixels * count;
+    st.gpu_ms = ms;
+    st.kernel_launches = launches;
+    st.waves = waves;
+    st.samples_per_wave = spw;
+    if (timing) {
+        for (size_t w = 0; w + per_wave <= ev; w += per_wave) {
+            auto el = [&](size_t a) {
+                float x = 0.0f;
+                cudaEventElapsedTime(&x, r->events[w + a], r->events[w + a + 1]);
+                return x;
+            };
+            st.raygen_ms += el(0);
+            for (uint32_t b = 0; b < r->max_bounces; ++b) {
+                st.intersect_ms += el(1 + 3 * b);
+                st.shade_ms += el(2 + 3 * b);
+                st.shadow_ms += el(3 + 3 * b);
+            }
+            st.film_ms += el(1 + 3 * r->max_bounces);
+        }
+    }
+    r->stats = st;
+    for (int k = 0; k < 5; ++k) r->tally_prev[k] = t[k];
+    if (t[2]) return fail(CENOTE_E_OVERFLOW, "a traversal stack or queue bound was exceeded");
+    return CENOTE_OK;
+}
+
+}  // namespace
+
+int32_t cenote_accumulate_n(cenote_renderer* r, cenote_scene* scene, cenote_film* film, uint32_t count) {
+    CN_CHECK(r && scene && film, CENOTE_E_INVALID_ARGUMENT, "null argument");
+    CN_CHECK(r->ctx == scene->ctx && r->ctx == film->ctx, CENOTE_E_INVALID_ARGUMENT, "handles from different contexts");
+    if (count == 0) return CENOTE_OK;
+    std::lock_guard<std::mutex> lock(r->ctx->mu);
+    CN_CUDA(cudaSetDevice(r->ctx->device));
+    int32_t rc = run_waves(r, scene, film->width, film->height, film->samples, count, film, nullptr);
+    if (rc == CENOTE_OK) film->samples += count;
+    return rc;
+}
+
+int32_t cenote_accumulate(cenote_renderer* r, cenote_scene* scene, cenote_film* film) {
+    return cenote_accumulate_n(r, scene, film, 1);
+}
+
+int32_t cenote_render_once(cenote_renderer* r, cenote_scene* scene, uint32_t width, uint32_t height, uint32_t sample,
+                           float* rgba_out) {
+    CN_CHECK(r && scene && rgba_out, CENOTE_E_INVALID_ARGUMENT, "null argument");
+    CN_CHECK(width > 0 && height > 0, CENOTE_E_INVALID_ARGUMENT, "zero-sized trace target");
+    CN_CHECK(uint64_t(width) * height < (1ull << 31), CENOTE_E_INVALID_ARGUMENT, "target too large");
+    std::lock_guard<std::mutex> lock(r->ctx->mu);
+    CN_CUDA(cudaSetDevice(r->ctx->device));
+    DeviceBuffer out;
+    size_t bytes = size_t(width) * height * 16;
+    CN_CUDA(out.alloc(bytes));
+    int32_t rc = run_waves(r, scene, width, height, sample, 1, nullptr, out.as<float4>());
+    if (rc != CENOTE_OK) return rc;
+    CN_CUDA(cudaMemcpy(rgba_out, out.ptr, bytes, cudaMemcpyDeviceToHost));
+    return CENOTE_OK;
+}
+
+int32_t cenote_film_averages(cenote_film* film, float* beauty, float* albedo, float* normal, float* depth) {
+    CN_CHECK(film, CENOTE_E_INVALID_ARGUMENT, "null film");
+    std::lock_guard<std::mutex> lock(film->ctx->mu);
+    CN_CUDA(cudaSetDevice(film->ctx->device));
+    size_t px = size_t(film->width) * film->height;
+    if (beauty) {
+        launch_resolve(film->sum.as<float4>(), film->avg.as<float4>(), uint32_t(px), float(std::max(1u, film->samples)),
+                       film->ctx->stream);
+        CN_CUDA(cudaGetLastError());
+        CN_CUDA(cudaMemcpyAsync(beauty, film->avg.ptr, px * 16, cudaMemcpyDeviceToHost, film->ctx->stream));
+    }
+    // The guide AOVs are not traced by this build: report zeros, depth +inf.
+    if (albedo) std::memset(albedo, 0, px * 16);
+    if (normal) std::memset(normal, 0, px * 16);
+    if (depth) std::fill(depth, depth + px, std::numeric_limits<float>::infinity());
+    return wait_stream(film->ctx->stream, film->ctx->sync_ev, 600000.0);
+}
+
+int32_t cenote_film_sums(cenote_film* film, float* beauty_sum) {
+    CN_CHECK(film && beauty_sum, CENOTE_E_INVALID_ARGUMENT, "null argument");
+    std::lock_guard<std::mutex> lock(film->ctx->mu);
+    CN_CUDA(cudaSetDevice(film->ctx->device));
+    CN_CUDA(cudaMemcpyAsync(beauty_sum, film->sum.ptr, size_t(film->width) * film->height * 16, cudaMemcpyDeviceToHost,
+                            film->ctx->stream));
+    return wait_stream(film->ctx->stream, film->ctx->sync_ev, 600000.0);
+}
+
+// ---- probes ------------------------------------------------------------------------------
+
+}  // extern "C"
+
+namespace {
+template <class F>
+int32_t with_device_io(cenote_context* ctx, std::vector<std::pair<const void*, size_t>> in,
+                       std::vector<std::pair<void*, size_t>> out, F&& launch) {
+    std::vector<std::unique_ptr<DeviceBuffer>> din, dout;
+    std::vector<void*> pin, pout;
+    for (auto& b : in) {
+        din.push_back(std::make_unique<DeviceBuffer>());
+        CN_CUDA(din.back()->alloc(b.second));
+        CN_CUDA(cudaMemcpyAsync(din.back()->ptr, b.first, b.second, cudaMemcpyHostToDevice, ctx->stream));
+        pin.push_back(din.back()->ptr);
+    }
+    for (auto& b : out) {
+        dout.push_back(std::make_unique<DeviceBuffer>());
+        CN_CUDA(dout.back()->alloc(b.second));
+        CN_CUDA(cudaMemsetAsync(dout.back()->ptr, 0, b.second, ctx->stream));
+        pout.push_back(dout.back()->ptr);
+    }
+    launch(pin, pout);
+    CN_CUDA(cudaGetLastError());
+    for (size_t i = 0; i < out.size(); ++i)
+        CN_CUDA(cudaMemcpyAsync(out[i].first, pout[i], out[i].second, cudaMemcpyDeviceToHost, ctx->stream));
+    return wait_stream(ctx->stream, ctx->sync_ev, 600000.0);
+}
+}  // namespace
+
+extern "C" {
+
+int32_t cenote_probe_sampler(cenote_context* ctx, uint32_t pixel, uint32_t dimension, uint32_t count, float* points,
+                             float* values) {
+    CN_CHECK(ctx && points && values, CENOTE_E_INVALID_ARGUMENT, "null argument");
+    if (count == 0) return CENOTE_OK;
+    std::lock_guard<std::mutex> lock(ctx->mu);
+    CN_CUDA(cudaSetDevice(ctx->device));
+    return with_device_io(ctx, {}, {{points, size_t(count) * 8}, {values, size_t(count) * 4}},
+                          [&](std::vector<void*>&, std::vector<void*>& o) {
+                              probe_sampler(pixel, dimension, count, static_cast<float2*>(o[0]), static_cast<float*>(o[1]),
+                                            ctx->stream);
+                          });
+}
+
+int32_t cenote_probe_bsdf(cenote_context* ctx, const cenote_material* m, const float* wo, const float* wi, uint32_t n,
+                          uint32_t exiting, float* f, float* pdf) {
+    CN_CHECK(ctx && m && wo && wi && f && pdf, CENOTE_E_INVALID_ARGUMENT, "null argument");
+    if (n == 0) return CENOTE_OK;
+    std::lock_guard<std::mutex> lock(ctx->mu);
+    CN_CUDA(cudaSetDevice(ctx->device));
+    return with_device_io(ctx, {{wo, size_t(n) * 12}, {wi, size_t(n) * 12}}, {{f, size_t(n) * 12}, {pdf, size_t(n) * 4}},
+                          [&](std::vector<void*>& i, std::vector<void*>& o) {
+                              probe_bsdf(ctx->tables.as<float>(), *m, static_cast<float3*>(i[0]),
+                                         static_cast<float3*>(i[1]), n, exiting, static_cast<float3*>(o[0]),
+                                         static_cast<float*>(o[1]), ctx->stream);
+                          });
+}
+
+int32_t cenote_probe_bsdf_sample(cenote_context* ctx, const cenote_material* m, const float* wo, const float* u,
+                                 uint32_t n, uint32_t exiting, float* wi, float* pdf, uint32_t* lobe) {
+    CN_CHECK(ctx && m && wo && u && wi && pdf && lobe, CENOTE_E_INVALID_ARGUMENT, "null argument");
+    if (n == 0) return CENOTE_OK;
+    std::lock_guard<std::mutex> lock(ctx->mu);
+    CN_CUDA(cudaSetDevice(ctx->device));
+    return with_device_io(ctx, {{wo, size_t(n) * 12}, {u, size_t(n) * 12}},
+                          {{wi, size_t(n) * 12}, {pdf, size_t(n) * 4}, {lobe, size_t(n) * 4}},
+                          [&](std::vector<void*>& i, std::vector<void*>& o) {
+                              probe_bsdf_sample(ctx->tables.as<float>(), *m, static_cast<float3*>(i[0]),
+                                                static_cast<float3*>(i[1]), n, exiting, static_cast<float3*>(o[0]),
+                                                static_cast<float*>(o[1]), static_cast<uint32_t*>(o[2]), ctx->stream);
+                          });
+}
+
+int32_t cenote_probe_intersect(cenote_scene* sc, const float* origins, const float* directions, uint32_t n,
+                               uint32_t* hits, float* t) {
+    CN_CHECK(sc && origins && directions && hits && t, CENOTE_E_INVALID_ARGUMENT, "null argument");
+    if (n == 0) return CENOTE_OK;
+    cenote_context* ctx = sc->ctx;
+    std::lock_guard<std::mutex> lock(ctx->mu);
+    CN_CUDA(cudaSetDevice(ctx->device));
+    uint32_t flag = 0;
+    int32_t rc = with_device_io(ctx, {{origins, size_t(n) * 12}, {directions, size_t(n) * 12}},
+                                {{hits, size_t(n) * 16}, {t, size_t(n) * 4}, {&flag, 4}},
+                                [&](std::vector<void*>& i, std::vector<void*>& o) {
+                                    probe_intersect(sc->ds, static_cast<float3*>(i[0]), static_cast<float3*>(i[1]), n,
+                                                    static_cast<uint4*>(o[0]), static_cast<float*>(o[1]),
+                                                    static_cast<uint32_t*>(o[2]), ctx->stream);
+                                });
+    if (rc == CENOTE_OK && flag) return fail(CENOTE_E_OVERFLOW, "traversal bound exceeded");
+    return rc;
+}
+
+int32_t cenote_probe_shadow(cenote_scene* sc, const float* origins, const float* directions, const float* tmax,
+                            const uint32_t* targets, uint32_t n, float* out) {
+    CN_CHECK(sc && origins && directions && tmax && targets && out, CENOTE_E_INVALID_ARGUMENT, "null argument");
+    if (n == 0) return CENOTE_OK;
+    cenote_context* ctx = sc->ctx;
+    std::lock_guard<std::mutex> lock(ctx->mu);
+    CN_CUDA(cudaSetDevice(ctx->device));
+    uint32_t flag = 0;
+    int32_t rc = with_device_io(
+        ctx, {{origins, size_t(n) * 12}, {directions, size_t(n) * 12}, {tmax, size_t(n) * 4}, {targets, size_t(n) * 8}},
+        {{out, size_t(n) * 4}, {&flag, 4}}, [&](std::vector<void*>& i, std::vector<void*>& o) {
+            probe_shadow(sc->ds, static_cast<float3*>(i[0]), static_cast<float3*>(i[1]), static_cast<float*>(i[2]),
+                         static_cast<uint2*>(i[3]), n, static_cast<float*>(o[0]), static_cast<uint32_t*>(o[1]),
+                         ctx->stream);
+        });
+    if (rc == CENOTE_OK && flag) return fail(CENOTE_E_OVERFLOW, "traversal bound exceeded");
+    return rc;
+}
+
+int32_t cenote_probe_env_sample(cenote_scene* sc, const float* u, uint32_t n, float* directions, float* pdf,
+                                uint32_t* row_col) {
+    CN_CHECK(sc && u && directions && pdf && row_col, CENOTE_E_INVALID_ARGUMENT, "null argument");
+    if (n == 0) return CENOTE_OK;
+    cenote_context* ctx = sc->ctx;
+    std::lock_guard<std::mutex> lock(ctx->mu);
+    CN_CUDA(cudaSetDevice(ctx->device));
+    return with_device_io(ctx, {{u, size_t(n) * 8}},
+                          {{directions, size_t(n) * 12}, {pdf, size_t(n) * 4}, {row_col, size_t(n) * 8}},
+                          [&](std::vector<void*>& i, std::vector<void*>& o) {
+                              probe_env_sample(sc->ds, static_cast<float2*>(i[0]), n, static_cast<float3*>(o[0]),
+                                               static_cast<float*>(o[1]), static_cast<uint2*>(o[2]), ctx->stream);
+                          });
+}
+
+int32_t cenote_probe_env_pdf(cenote_scene* sc, const float* directions, uint32_t n, float* pdf) {
+    CN_CHECK(sc && directions && pdf, CENOTE_E_INVALID_ARGUMENT, "null argument");
+    if (n == 0) return CENOTE_OK;
+    cenote_context* ctx = sc->ctx;
+    std::lock_guard<std::mutex> lock(ctx->mu);
+    CN_CUDA(cudaSetDevice(ctx->device));
+    return with_device_io(ctx, {{directions, size_t(n) * 12}}, {{pdf, size_t(n) * 4}},
+                          [&](std::vector<void*>& i, std::vector<void*>& o) {
+                              probe_env_pdf(sc->ds, static_cast<float3*>(i[0]), n, static_cast<float*>(o[0]),
+                                            ctx->stream);
+                          });
+}
+
+}  // extern "C"

@@ -1,0 +1,125 @@
+// The environment's importance-sampling tables, built on the device in FP64.
+//
+// Same tables and the same arithmetic as the host build of
+// crates/cenote/src/environment.rs:130-218: f32 luminance, 3×3-max dilation
+// (wrap in u, clamp in v) times the row's sin θ, f64 marginal and conditional
+// CDFs cast to f32, the separate f32 pdf table and the f64 power integral.
+// Every sum runs in the reference's sequential order — one thread per row for
+// the row sums, one thread for the flat total — because a tree-ordered f64
+// sum rounds differently and the CDF indices must match bit for bit. The
+// per-row sin θ and solid angles are evaluated on the host with the same libm
+// call the reference makes, so they are bit-identical inputs here.
+#include <cuda_runtime.h>
+#include <cstdint>
+
+namespace cn {
+namespace {
+
+__device__ __forceinline__ float luminance_rn(float r, float g, float b) {
+    return __fadd_rn(__fadd_rn(__fmul_rn(r, 0.2722287f), __fmul_rn(g, 0.6740818f)), __fmul_rn(b, 0.0536895f));
+}
+
+__global__ void k_env_lum(const float4* __restrict__ tex, double* __restrict__ lum, uint32_t n) {
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        float4 t = tex[i];
+        lum[i] = double(luminance_rn(t.x, t.y, t.z));
+    }
+}
+
+__global__ void k_env_weight(const double* __restrict__ lum, const double* __restrict__ sin_theta,
+                             double* __restrict__ weight, uint32_t w, uint32_t h) {
+    uint32_t n = w * h;
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        uint32_t row = i / w, col = i - row * w;
+        double peak = 0.0;
+        for (int dr = -1; dr <= 1; ++dr) {
+            int rr = int(row) + dr;
+            uint32_t r = rr < 0 ? 0u : min(uint32_t(rr), h - 1);
+            for (int dc = -1; dc <= 1; ++dc) {
+                int cc = int(col) + dc;
+                uint32_t c = cc < 0 ? uint32_t(cc + int(w)) : (uint32_t(cc) >= w ? uint32_t(cc) - w : uint32_t(cc));
+                peak = fmax(peak, lum[size_t(r) * w + c]);
+            }
+        }
+        weight[i] = __dmul_rn(peak, sin_theta[row]);
+    }
+}
+
+// One thread per row: the row sum, the row's conditional CDF and the
+// undilated luminance sum for the power integral, all sequential in f64.
+__global__ void k_env_rows(const double* __restrict__ weight, const double* __restrict__ lum,
+                           double* __restrict__ row_sum, double* __restrict__ lum_sum, float* __restrict__ conditional,
+                           uint32_t w, uint32_t h) {
+    uint32_t row = blockIdx.x * blockDim.x + threadIdx.x;
+    if (row >= h) return;
+    const double* wr = weight + size_t(row) * w;
+    double rs = 0.0;
+    for (uint32_t c = 0; c < w; ++c) rs = __dadd_rn(rs, wr[c]);
+    row_sum[row] = rs;
+    float* cdf = conditional + size_t(row) * (w + 1);
+    cdf[0] = 0.0f;
+    double run = 0.0;
+    for (uint32_t c = 0; c < w; ++c) {
+        run = __dadd_rn(run, wr[c]);
+        cdf[c + 1] = rs > 0.0 ? __double2float_rn(__ddiv_rn(run, rs)) : 0.0f;
+    }
+    cdf[w] = 1.0f;
+    const double* lr = lum + size_t(row) * w;
+    double ls = 0.0;
+    for (uint32_t c = 0; c < w; ++c) ls = __dadd_rn(ls, lr[c]);
+    lum_sum[row] = ls;
+}
+
+// The flat total over every weight in row-major order, the marginal CDF and
+// the power integral: sequential by definition, one thread.
+__global__ void k_env_marginal(const double* __restrict__ weight, const double* __restrict__ row_sum,
+                               const double* __restrict__ lum_sum, const double* __restrict__ solid,
+                               float* __restrict__ marginal, double* __restrict__ out, uint32_t w, uint32_t h) {
+    if (blockIdx.x != 0 || threadIdx.x != 0) return;
+    const size_t n = size_t(w) * h;
+    double total = 0.0;
+    for (size_t i = 0; i < n; ++i) total = __dadd_rn(total, weight[i]);
+    marginal[0] = 0.0f;
+    double run = 0.0;
+    for (uint32_t r = 0; r < h; ++r) {
+        run = __dadd_rn(run, row_sum[r]);
+        marginal[r + 1] = total > 0.0 ? __double2float_rn(__ddiv_rn(run, total)) : 0.0f;
+    }
+    marginal[h] = 1.0f;
+    double power = 0.0;
+    for (uint32_t r = 0; r < h; ++r) power = __dadd_rn(power, __dmul_rn(solid[r], lum_sum[r]));
+    out[0] = total;
+    out[1] = power;
+}
+
+__global__ void k_env_pdfs(const double* __restrict__ weight, const double* __restrict__ totals, float* __restrict__ pdfs,
+                           uint32_t w, uint32_t h) {
+    const double total = totals[0];
+    const double scale = total > 0.0 ? __ddiv_rn(double(size_t(w) * h), total) : 0.0;
+    size_t n = size_t(w) * h;
+    for (size_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += size_t(gridDim.x) * blockDim.x)
+        pdfs[i] = __double2float_rn(__dmul_rn(weight[i], scale));
+}
+
+}  // namespace
+
+// scratch: 3·w·h + 3·h doubles + 2 doubles; results into marginal (h+1),
+// conditional (h·(w+1)), pdfs (w·h) and totals (total, power).
+void launch_env_tables(const float4* texels, const double* sin_theta, const double* solid, uint32_t w, uint32_t h,
+                       double* scratch, float* marginal, float* conditional, float* pdfs, double* totals,
+                       cudaStream_t stream) {
+    const size_t n = size_t(w) * h;
+    double* lum = scratch;
+    double* weight = lum + n;
+    double* row_sum = weight + n;
+    double* lum_sum = row_sum + h;
+    int grid = int((n + 255) / 256);
+    if (grid > 148 * 32) grid = 148 * 32;
+    k_env_lum<<<grid, 256, 0, stream>>>(texels, lum, uint32_t(n));
+    k_env_weight<<<grid, 256, 0, stream>>>(lum, sin_theta, weight, w, h);
+    k_env_rows<<<(h + 63) / 64, 64, 0, stream>>>(weight, lum, row_sum, lum_sum, conditional, w, h);
+    k_env_marginal<<<1, 1, 0, stream>>>(weight, row_sum, lum_sum, solid, marginal, totals, w, h);
+    k_env_pdfs<<<grid, 256, 0, stream>>>(weight, totals, pdfs, w, h);
+}
+
+}  // namespace cn

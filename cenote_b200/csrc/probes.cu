@@ -1,0 +1,152 @@
+// Probe kernels: the test entry points that expose one device function at a
+// time for parity checks — the sampler dump of crates/cenote/shaders/rng_test.slang,
+// closure eval/pdf/sample, closest-hit and shadow queries, and environment
+// sampling. They run the same device code the wavefront kernels inline.
+#include <cuda_runtime.h>
+
+#include "lights_env.cuh"
+#include "openpbr.cuh"
+#include "sampler.cuh"
+#include "traverse.cuh"
+
+namespace cn {
+namespace {
+
+__global__ void k_probe_sampler(uint32_t pixel, uint32_t dim, uint32_t count, float2* points, float* values) {
+    uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= count) return;
+    points[i] = sample_2d(pixel, i, dim);
+    values[i] = sample_1d(pixel, i, dim);
+}
+
+__global__ void k_probe_bsdf(const float* tables, Material m, const float3* wo, const float3* wi, uint32_t n,
+                             uint32_t exiting, float3* f, float* pdf) {
+    uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    Closure c = resolve_closure(tables, m, wo[i], exiting != 0);
+    f[i] = eval_bsdf(c, wi[i], wo[i]);
+    pdf[i] = bsdf_pdf(c, wi[i], wo[i]);
+}
+
+__global__ void k_probe_bsdf_sample(const float* tables, Material m, const float3* wo, const float3* u, uint32_t n,
+                                    uint32_t exiting, float3* wi, float* pdf, uint32_t* lobe) {
+    uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    Closure c = resolve_closure(tables, m, wo[i], exiting != 0);
+    BsdfSample s = sample_bsdf(c, wo[i], u[i].x, u[i].y, u[i].z);
+    wi[i] = s.wi;
+    pdf[i] = s.pdf;
+    lobe[i] = s.lobe;
+}
+
+__global__ void k_probe_intersect(DeviceScene scene, const float3* org, const float3* dir, uint32_t n, uint4* hits,
+                                  float* tout, uint32_t* flag) {
+    uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    Ray ray = make_ray(org[i], dir[i]);
+    float tmax = 1e30f;
+    uint32_t bi = LIGHT_NONE, bp = 0;
+    float b1s = 0.0f, b2s = 0.0f;
+    bool ok = traverse(scene, ray, tmax, [&](uint32_t, float4 a, float4 b, float4 c, float& tm) {
+        float t, b1, b2;
+        if (!tri_hit(ray, a, b, c, tm, t, b1, b2)) return false;
+        uint32_t inst = __float_as_uint(a.w), prim = __float_as_uint(b.w);
+        if (!(t < tm || (t == tm && (inst < bi || (inst == bi && prim < bp))))) return false;
+        tm = t;
+        bi = inst;
+        bp = prim;
+        b1s = b1;
+        b2s = b2;
+        return false;
+    });
+    if (!ok) atomicOr(flag, 1u);
+    hits[i] = make_uint4(bi, bp, __float_as_uint(b1s), __float_as_uint(b2s));
+    tout[i] = bi == LIGHT_NONE ? -1.0f : tmax;
+}
+
+__global__ void k_probe_shadow(DeviceScene scene, const float3* org, const float3* dir, const float* tmaxs,
+                               const uint2* targets, uint32_t n, float* out, uint32_t* flag) {
+    uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    Ray ray = make_ray(org[i], dir[i]);
+    float tmax = tmaxs[i];
+    uint32_t light = targets[i].x, lprim = targets[i].y;
+    float atten = 1.0f;
+    bool occluded = false;
+    uint32_t bi = LIGHT_NONE, bp = 0;
+    bool ok = traverse(scene, ray, tmax, [&](uint32_t, float4 a, float4 b, float4 c, float& tm) {
+        float t, b1, b2;
+        if (!tri_hit(ray, a, b, c, tm, t, b1, b2)) return false;
+        uint32_t inst = __float_as_uint(a.w), prim = __float_as_uint(b.w);
+        if (!(t < tm || (t == tm && (inst < bi || (inst == bi && prim < bp))))) return false;
+        bool target = inst == light && prim == lprim;
+        if (!(__float_as_uint(c.w) & TRI_OPAQUE) && !target) {
+            atten *= 1.0f - __ldg(&scene.materials[inst].opacity);
+            if (atten < 1e-4f) {
+                occluded = true;
+                return true;
+            }
+            return false;
+        }
+        if (light == LIGHT_NONE) {
+            occluded = true;
+            return true;
+        }
+        tm = t;
+        bi = inst;
+        bp = prim;
+        return false;
+    });
+    if (!ok) atomicOr(flag, 1u);
+    bool vis = !occluded && (bi == LIGHT_NONE || (bi == light && bp == lprim));
+    out[i] = vis ? atten : -1.0f;
+}
+
+__global__ void k_probe_env_sample(DeviceScene scene, const float2* u, uint32_t n, float3* dir, float* pdf,
+                                   uint2* rc) {
+    uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    EnvSample s = env_sample(scene, u[i]);
+    dir[i] = s.direction;
+    pdf[i] = s.pdf;
+    rc[i] = make_uint2(s.row, s.col);
+}
+
+__global__ void k_probe_env_pdf(DeviceScene scene, const float3* d, uint32_t n, float* pdf) {
+    uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    pdf[i] = env_pdf(scene, d[i]);
+}
+
+inline int blocks(uint32_t n) { return int((n + 127) / 128); }
+
+}  // namespace
+
+void probe_sampler(uint32_t pixel, uint32_t dim, uint32_t count, float2* points, float* values, cudaStream_t s) {
+    k_probe_sampler<<<blocks(count), 128, 0, s>>>(pixel, dim, count, points, values);
+}
+void probe_bsdf(const float* tables, const Material& m, const float3* wo, const float3* wi, uint32_t n,
+                uint32_t exiting, float3* f, float* pdf, cudaStream_t s) {
+    k_probe_bsdf<<<blocks(n), 128, 0, s>>>(tables, m, wo, wi, n, exiting, f, pdf);
+}
+void probe_bsdf_sample(const float* tables, const Material& m, const float3* wo, const float3* u, uint32_t n,
+                       uint32_t exiting, float3* wi, float* pdf, uint32_t* lobe, cudaStream_t s) {
+    k_probe_bsdf_sample<<<blocks(n), 128, 0, s>>>(tables, m, wo, u, n, exiting, wi, pdf, lobe);
+}
+void probe_intersect(const DeviceScene& scene, const float3* org, const float3* dir, uint32_t n, uint4* hits, float* t,
+                     uint32_t* flag, cudaStream_t s) {
+    k_probe_intersect<<<blocks(n), 128, 0, s>>>(scene, org, dir, n, hits, t, flag);
+}
+void probe_shadow(const DeviceScene& scene, const float3* org, const float3* dir, const float* tmax,
+                  const uint2* targets, uint32_t n, float* out, uint32_t* flag, cudaStream_t s) {
+    k_probe_shadow<<<blocks(n), 128, 0, s>>>(scene, org, dir, tmax, targets, n, out, flag);
+}
+void probe_env_sample(const DeviceScene& scene, const float2* u, uint32_t n, float3* dir, float* pdf, uint2* rc,
+                      cudaStream_t s) {
+    k_probe_env_sample<<<blocks(n), 128, 0, s>>>(scene, u, n, dir, pdf, rc);
+}
+void probe_env_pdf(const DeviceScene& scene, const float3* d, uint32_t n, float* pdf, cudaStream_t s) {
+    k_probe_env_pdf<<<blocks(n), 128, 0, s>>>(scene, d, n, pdf);
+}
+
+}  // namespace cn

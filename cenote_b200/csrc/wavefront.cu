@@ -1,0 +1,596 @@
+// The wavefront engine's kernels for sm_100a.
+//
+// Stage order per wave follows crates/cenote/src/wavefront.rs:727-828 —
+// raygen, then per bounce intersect → shade (miss | surface) → shadow — and
+// each stage's arithmetic follows its Slang kernel (raygen.slang,
+// intersect.slang, shade_miss.slang, shade_surface.slang, trace_shadow.slang).
+// The B200 shape differs from the reference's:
+//  * a wave may carry several samples of every pixel (path = s·count + pixel),
+//    so one launch fills all 148 SMs even at small resolutions; radiance is
+//    path-owned and the film adds samples in ascending order, which keeps the
+//    result bitwise identical to one-sample waves;
+//  * there is no indirect dispatch: the traversal and shading kernels are
+//    persistent grids (a multiple of the SM count) whose warps pull 32 work
+//    items at a time from a per-stage counter, so a stage costs one launch
+//    whatever its queue length and load-balances divergent rays;
+//  * queue pushes are warp-aggregated (one atomic per warp, ballot + popc);
+//  * miss and surface shading share one kernel — a path is in exactly one of
+//    the two, so the per-path write stays single and ordered.
+#include "wavefront.h"
+
+#include "lights_env.cuh"
+#include "openpbr.cuh"
+#include "sampler.cuh"
+#include "traverse.cuh"
+
+namespace cn {
+
+namespace {
+
+constexpr int BLOCK = 128;
+
+__device__ __forceinline__ uint32_t lane_id() { return threadIdx.x & 31u; }
+
+// Fetch the next 32 work items for this warp; every lane gets the same base.
+__device__ __forceinline__ uint32_t warp_fetch(uint32_t* counter) {
+    uint32_t base = 0;
+    if (lane_id() == 0) base = atomicAdd(counter, 32u);
+    return __shfl_sync(0xffffffffu, base, 0);
+}
+
+// Warp-aggregated append: returns this lane's slot, or ~0u if !pred. Must be
+// called by all 32 lanes together.
+__device__ __forceinline__ uint32_t warp_push(uint32_t* counter, bool pred) {
+    uint32_t mask = __ballot_sync(0xffffffffu, pred);
+    if (mask == 0) return ~0u;
+    uint32_t leader = __ffs(mask) - 1u;
+    uint32_t base = 0;
+    if (lane_id() == leader) base = atomicAdd(counter, uint32_t(__popc(mask)));
+    base = __shfl_sync(0xffffffffu, base, leader);
+    return pred ? base + __popc(mask & ((1u << lane_id()) - 1u)) : ~0u;
+}
+
+__device__ __forceinline__ void flag_overflow(uint32_t* counters) { atomicOr(counters + CTR_OVERFLOW, 1u); }
+
+// Instrumented launches: one 64-bit add per warp for the traversal tallies.
+__device__ __forceinline__ void flush_counts(uint32_t* counters, uint32_t visits, uint32_t tests) {
+    for (int o = 16; o > 0; o >>= 1) {
+        visits += __shfl_xor_sync(0xffffffffu, visits, o);
+        tests += __shfl_xor_sync(0xffffffffu, tests, o);
+    }
+    if (lane_id() == 0) {
+        atomicAdd(reinterpret_cast<unsigned long long*>(counters + CTR_VISITS), (unsigned long long)visits);
+        atomicAdd(reinterpret_cast<unsigned long long*>(counters + CTR_TESTS), (unsigned long long)tests);
+    }
+}
+
+// ---- raygen (raygen.slang:47-112) ----------------------------------------------
+
+__device__ __forceinline__ float2 concentric_disk(float2 u) {
+    float ox = 2.0f * u.x - 1.0f, oy = 2.0f * u.y - 1.0f;
+    if (ox == 0.0f && oy == 0.0f) return make_float2(0.0f, 0.0f);
+    float r, th;
+    if (fabsf(ox) > fabsf(oy)) {
+        r = ox;
+        th = (ENV_PI / 4.0f) * (oy / ox);
+    } else {
+        r = oy;
+        th = (ENV_PI / 2.0f) - (ENV_PI / 4.0f) * (ox / oy);
+    }
+    float s, c;
+    sincosf(th, &s, &c);
+    return make_float2(r * c, r * s);
+}
+
+__global__ void __launch_bounds__(BLOCK) k_raygen(PathPool pool, WaveParams wp) {
+    uint32_t n = wp.pixel_count * wp.samples;
+    for (uint32_t p = blockIdx.x * blockDim.x + threadIdx.x; p < n; p += gridDim.x * blockDim.x) {
+        uint32_t s = p / wp.pixel_count;
+        uint32_t pixel = wp.pixel_base + (p - s * wp.pixel_count);
+        uint32_t sample = wp.sample_base + s;
+        float2 j = sample_2d(pixel, sample, CAMERA_JITTER);
+        float xx = float(pixel % wp.width) + j.x, yy = float(pixel / wp.width) + j.y;
+        float ux = xx / float(wp.width), uy = yy / float(wp.height);
+        float nx = 2.0f * ux - 1.0f, ny = 1.0f - 2.0f * uy;
+        float3 target = wp.cam_fwd + nx * wp.cam_right + ny * wp.cam_up;
+        float3 org = wp.cam_pos;
+        float3 dir = normalize(target);
+        if (wp.aperture > 0.0f) {
+            float2 d = concentric_disk(sample_2d(pixel, sample, CAMERA_LENS));
+            d.x *= wp.aperture;
+            d.y *= wp.aperture;
+            float3 off = d.x * normalize(wp.cam_right) + d.y * normalize(wp.cam_up);
+            org = org + off;
+            dir = normalize(target - off);
+        }
+        pool.org[p] = f4(org, 0.0f);
+        pool.dir[p] = f4(dir, dot(dir, normalize(wp.cam_fwd)));
+        pool.thr[p] = make_float4(1.0f, 1.0f, 1.0f, 0.0f);
+        pool.ps[p] = make_uint2(pixel, sample);
+        pool.state[p] = MEDIUM_NONE;
+        pool.rad[p] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+    }
+}
+
+// ---- intersect (intersect.slang:47-88) -------------------------------------------
+
+template <bool COUNT>
+__global__ void __launch_bounds__(BLOCK) k_intersect(DeviceScene scene, PathPool pool, uint32_t bounce, uint32_t n0) {
+    uint32_t visits = 0, tests = 0;
+    const uint32_t count = bounce == 0 ? n0 : pool.counters[CTR_RAYS + bounce];
+    const uint32_t* queue = pool.queue[bounce & 1u];
+    const uint32_t mask = bounce == 0 ? RAY_MASK_CAMERA : RAY_MASK_ALL;
+    for (;;) {
+        uint32_t base = warp_fetch(pool.counters + CTR_FETCH_ISECT + bounce);
+        if (base >= count) break;
+        uint32_t i = base + lane_id();
+        if (i >= count) continue;
+        uint32_t path = bounce == 0 ? i : queue[i];
+        float4 o = pool.org[path], d = pool.dir[path];
+        Ray ray = make_ray(xyz(o), xyz(d));
+        float tmax = 1e30f;
+        uint32_t best_inst = LIGHT_NONE, best_prim = 0;
+        float best_b1 = 0.0f, best_b2 = 0.0f;
+        uint32_t crossings = 0;
+        uint32_t pixel = 0, sample = 0;
+        if (scene.has_nonopaque) {
+            uint2 ps = pool.ps[path];
+            pixel = ps.x;
+            sample = ps.y;
+        }
+        bool ok = traverse<COUNT>(scene, ray, tmax, [&](uint32_t, float4 a, float4 b, float4 c, float& tm) {
+            uint32_t flags = __float_as_uint(c.w);
+            if (!(flags & mask)) return false;
+            float t, b1, b2;
+            if (!tri_hit(ray, a, b, c, tm, t, b1, b2)) return false;
+            uint32_t inst = __float_as_uint(a.w), prim = __float_as_uint(b.w);
+            if (!(t < tm || (t == tm && (inst < best_inst || (inst == best_inst && prim < best_prim))))) return false;
+            if (!(flags & TRI_OPAQUE)) {
+                float opacity = __ldg(&scene.materials[inst].opacity);
+                bool commit = crossings >= TRANSPARENT_CAP || hash_uniform(pixel, sample, bounce, crossings) < opacity;
+                crossings++;
+                if (!commit) return false;
+            }
+            tm = t;
+            best_inst = inst;
+            best_prim = prim;
+            best_b1 = b1;
+            best_b2 = b2;
+            return false;
+        }, &visits, &tests);
+        if (!ok) flag_overflow(pool.counters);
+        pool.hit[path] = make_uint4(best_inst, best_prim, __float_as_uint(best_b1), __float_as_uint(best_b2));
+    }
+    if (COUNT) flush_counts(pool.counters, visits, tests);
+}
+
+// ---- shade: shade_miss.slang:29-75 and shade_surface.slang:235-521 -----------------
+
+struct Spawn {
+    float3 position, below, normal, shading;
+    bool front;
+};
+
+__device__ __forceinline__ float3 fetch3(const float* a, uint32_t v) {
+    return f3(__ldg(a + 3 * v), __ldg(a + 3 * v + 1), __ldg(a + 3 * v + 2));
+}
+
+// shade_surface.slang:96-181 (van Antwerpen's rigorous spawn offsets).
+__device__ __forceinline__ Spawn spawn_point(const GeomRecord& g, uint32_t prim, float b1, float b2, float3 rd) {
+    uint32_t i0 = __ldg(g.indices + 3 * prim), i1 = __ldg(g.indices + 3 * prim + 1), i2 = __ldg(g.indices + 3 * prim + 2);
+    float3 v0 = fetch3(g.positions, i0), v1 = fetch3(g.positions, i1), v2 = fetch3(g.positions, i2);
+    float3 e1 = v1 - v0, e2 = v2 - v0;
+    float3 op = v0 + fma3(f3(b1), e1, b2 * e2);
+    float3 on = cross(e1, e2);
+    float3 r0 = f3(g.o2w[0][0], g.o2w[0][1], g.o2w[0][2]), r1 = f3(g.o2w[1][0], g.o2w[1][1], g.o2w[1][2]),
+           r2 = f3(g.o2w[2][0], g.o2w[2][1], g.o2w[2][2]);
+    float3 tw = f3(g.o2w[0][3], g.o2w[1][3], g.o2w[2][3]);
+    float3 wp = f3(tw.x + fmaf(r0.x, op.x, fmaf(r0.y, op.y, r0.z * op.z)),
+                   tw.y + fmaf(r1.x, op.x, fmaf(r1.y, op.y, r1.z * op.z)),
+                   tw.z + fmaf(r2.x, op.x, fmaf(r2.y, op.y, r2.z * op.z)));
+    float3 w0 = f3(g.w2o[0][0], g.w2o[0][1], g.w2o[0][2]), w1 = f3(g.w2o[1][0], g.w2o[1][1], g.w2o[1][2]),
+           w2 = f3(g.w2o[2][0], g.w2o[2][1], g.w2o[2][2]);
+    float3 wn = w0 * on.x + w1 * on.y + w2 * on.z;
+    float wscale = rsqrtf(dot(wn, wn));
+    wn = wn * wscale;
+    const float c0 = 5.9604644775390625e-8f;
+    const float c1 = 1.788139769587360206060111522674560546875e-7f;
+    const float c2 = 1.19209317972490680404007434844970703125e-7f;
+    float3 ext3 = fabs3(e1) + fabs3(e2) + fabs3(e1 - e2);
+    float extent = fmaxf(fmaxf(ext3.x, ext3.y), ext3.z);
+    float3 oerr = fma3(f3(c0), fabs3(v0), f3(c1 * extent));
+    float3 aop = fabs3(op);
+    float3 werr = fma3(f3(c1), f3(dot(fabs3(r0), aop), dot(fabs3(r1), aop), dot(fabs3(r2), aop)), c2 * fabs3(tw));
+    float3 awp = fabs3(wp);
+    oerr = fma3(f3(c2),
+                f3(dot(fabs3(w0), awp) + fabsf(g.w2o[0][3]), dot(fabs3(w1), awp) + fabsf(g.w2o[1][3]),
+                   dot(fabs3(w2), awp) + fabsf(g.w2o[2][3])),
+                oerr);
+    float woff = dot(werr, fabs3(wn));
+    float ooff = dot(oerr, fabs3(on));
+    woff = fmaf(wscale, ooff, woff);
+    Spawn sp;
+    sp.front = dot(wn, rd) < 0.0f;
+    if (dot(wn, rd) > 0.0f) wn = -wn;
+    float3 n0 = fetch3(g.normals, i0), n1 = fetch3(g.normals, i1), n2 = fetch3(g.normals, i2);
+    float3 os = n0 + b1 * (n1 - n0) + b2 * (n2 - n0);
+    float3 sh = normalize(w0 * os.x + w1 * os.y + w2 * os.z);
+    if (dot(sh, wn) < 0.0f) sh = -sh;
+    sp.position = fma3(f3(woff), wn, wp);
+    sp.below = fma3(f3(-woff), wn, wp);
+    sp.normal = wn;
+    sp.shading = sh;
+    return sp;
+}
+
+__device__ __forceinline__ void load_geom(const GeomRecord* rec, GeomRecord& g) {
+    const uint4* src = reinterpret_cast<const uint4*>(rec);
+    uint4* dst = reinterpret_cast<uint4*>(&g);
+#pragma unroll
+    for (int k = 0; k < int(sizeof(GeomRecord) / 16); ++k) dst[k] = __ldg(src + k);
+}
+
+__device__ __forceinline__ void load_material(const Material* rec, Material& m) {
+    const uint4* src = reinterpret_cast<const uint4*>(rec);
+    uint4* dst = reinterpret_cast<uint4*>(&m);
+#pragma unroll
+    for (int k = 0; k < int(sizeof(Material) / 16); ++k) dst[k] = __ldg(src + k);
+}
+
+__global__ void __launch_bounds__(BLOCK) k_shade(DeviceScene scene, PathPool pool, uint32_t bounce,
+                                                 uint32_t max_bounces, uint32_t light_sampling, uint32_t n0) {
+    const uint32_t count = bounce == 0 ? n0 : pool.counters[CTR_RAYS + bounce];
+    const uint32_t* queue = pool.queue[bounce & 1u];
+    uint32_t* next_queue = pool.queue[(bounce + 1u) & 1u];
+    for (;;) {
+        uint32_t base = warp_fetch(pool.counters + CTR_FETCH_SHADE + bounce);
+        if (base >= count) break;
+        uint32_t i = base + lane_id();
+        bool push_ray = false, push_shadow = false;
+        uint32_t path = 0;
+        ShadowRay sr;
+        if (i < count) {
+            path = bounce == 0 ? i : queue[i];
+            uint4 h = pool.hit[path];
+            float4 d4 = pool.dir[path];
+            float3 dir = xyz(d4);
+            float4 t4 = pool.thr[path];
+            float3 thr = xyz(t4);
+            float4 rad = pool.rad[path];
+            if (h.x == LIGHT_NONE) {
+                // shade_miss.slang:29-75
+                float weight = 1.0f;
+                if (t4.w > 0.0f) {
+                    if (light_sampling == CENOTE_LIGHT_SAMPLING_NEE) weight = 0.0f;
+                    else if (light_sampling == CENOTE_LIGHT_SAMPLING_MIS)
+                        weight = power_heuristic(t4.w, scene.select_prob * env_pdf(scene, dir));
+                }
+                float3 c = thr * env_radiance(scene, dir) * weight;
+                pool.rad[path] = make_float4(rad.x + c.x, rad.y + c.y, rad.z + c.z, rad.w + 1.0f);
+            } else {
+                const uint32_t inst = h.x, prim = h.y;
+                const float b1 = __uint_as_float(h.z), b2 = __uint_as_float(h.w);
+                uint2 ps = pool.ps[path];
+                const uint32_t pixel = ps.x, sample = ps.y;
+                float3 origin = xyz(pool.org[path]);
+                GeomRecord g;
+                load_geom(scene.geometry + inst, g);
+                Material mat;
+                load_material(scene.materials + inst, mat);
+                Spawn sp = spawn_point(g, prim, b1, b2, dir);
+                uint32_t medium = bounce == 0 ? MEDIUM_NONE : (pool.state[path] & 0xffffffu);
+                if (medium != MEDIUM_NONE) {
+                    const Material& in = scene.materials[medium];
+                    float depth = __ldg(&in.transmission_depth);
+                    if (depth > 0.0f) {
+                        float3 tc = f3(__ldg(&in.transmission_color[0]), __ldg(&in.transmission_color[1]),
+                                       __ldg(&in.transmission_color[2]));
+                        float3 sigma = -log3(clamp3(tc, 1e-4f, 1.0f)) / depth;
+                        thr = thr * exp3(-sigma * length(origin - sp.position));
+                    }
+                }
+                float3 contribution = f3(0.0f);
+                if (g.light != LIGHT_NONE && sp.front) {
+                    float weight = 1.0f;
+                    if (t4.w > 0.0f) {
+                        if (light_sampling == CENOTE_LIGHT_SAMPLING_NEE) weight = 0.0f;
+                        else if (light_sampling == CENOTE_LIGHT_SAMPLING_MIS) {
+                            float3 delta = sp.position - origin;
+                            float cl = fabsf(dot(sp.normal, dir));
+                            float lp = __ldg(&scene.lights[g.light + prim].pdf);
+                            float nee = (1.0f - scene.select_prob) * lp * dot(delta, delta) / cl;
+                            weight = power_heuristic(t4.w, nee);
+                        }
+                    }
+                    contribution = thr * ld3(mat.emission) * weight;
+                }
+                Frame frame(sp.shading);
+                float3 wo = frame.to_local(-dir);
+                Closure cl = resolve_closure(scene.bsdf_tables, mat, wo, medium == inst);
+                if (bounce + 1 >= max_bounces) {
+                    pool.rad[path] = make_float4(rad.x + contribution.x, rad.y + contribution.y, rad.z + contribution.z,
+                                                 rad.w + 1.0f);
+                } else {
+                    const float env_prob = scene.select_prob;
+                    if (light_sampling != CENOTE_LIGHT_SAMPLING_BSDF && (scene.light_count > 0 || env_prob > 0.0f)) {
+                        float u_light = sample_1d(pixel, sample, bounce_dim(bounce, NEE_LIGHT));
+                        float2 u_point = sample_2d(pixel, sample, bounce_dim(bounce, NEE_POINT));
+                        float3 unshadowed = f3(0.0f);
+                        float3 sdir = f3(0.0f), sorg = f3(0.0f);
+                        float stmax = 1e30f;
+                        uint32_t slight = LIGHT_NONE, sprim = 0;
+                        if (u_light < env_prob) {
+                            EnvSample cand = env_sample(scene, u_point);
+                            float3 wl = frame.to_local(cand.direction);
+                            bool through = dot(cand.direction, sp.normal) < 0.0f;
+                            if (cand.pdf > 0.0f && wl.z != 0.0f && (wl.z < 0.0f) == through) {
+                                float nee = env_prob * cand.pdf;
+                                float spdf = bsdf_pdf(cl, wl, wo);
+                                float w = light_sampling == CENOTE_LIGHT_SAMPLING_MIS ? power_heuristic(nee, spdf) : 1.0f;
+                                unshadowed = thr * cand.radiance * eval_bsdf(cl, wl, wo) * fabsf(wl.z) * (w / nee);
+                                sorg = through ? sp.below : sp.position;
+                                sdir = cand.direction;
+                            }
+                        } else {
+                            float u_list = (u_light - env_prob) / (1.0f - env_prob);
+                            LightConn cand = sample_lights(scene.lights, scene.light_count, u_list, u_point, sp.position);
+                            float3 wl = frame.to_local(cand.direction);
+                            bool through = dot(cand.direction, sp.normal) < 0.0f;
+                            if (cand.pdf > 0.0f && wl.z != 0.0f && (wl.z < 0.0f) == through) {
+                                float nee = (1.0f - env_prob) * cand.pdf;
+                                float w = !cand.delta && light_sampling == CENOTE_LIGHT_SAMPLING_MIS
+                                              ? power_heuristic(nee, bsdf_pdf(cl, wl, wo))
+                                              : 1.0f;
+                                unshadowed = thr * cand.radiance * eval_bsdf(cl, wl, wo) * fabsf(wl.z) * (w / nee);
+                                sorg = through ? sp.below : sp.position;
+                                slight = cand.instance;
+                                sprim = cand.primitive;
+                                sdir = cand.direction;
+                                stmax = cand.tmax;
+                            }
+                        }
+                        if (any_pos(unshadowed)) {
+                            push_shadow = true;
+                            sr.org[0] = sorg.x; sr.org[1] = sorg.y; sr.org[2] = sorg.z;
+                            sr.tmax = stmax;
+                            sr.dir[0] = sdir.x; sr.dir[1] = sdir.y; sr.dir[2] = sdir.z;
+                            sr.path = path;
+                            sr.contrib[0] = unshadowed.x; sr.contrib[1] = unshadowed.y; sr.contrib[2] = unshadowed.z;
+                            sr.light = slight;
+                            sr.primitive = sprim;
+                        }
+                    }
+                    float u_lobe = sample_1d(pixel, sample, bounce_dim(bounce, BSDF_LOBE));
+                    float2 u = sample_2d(pixel, sample, bounce_dim(bounce, BSDF_DIR));
+                    BsdfSample sc = sample_bsdf(cl, wo, u_lobe, u.x, u.y);
+                    float3 wiw = frame.to_world(sc.wi);
+                    float3 scattered = f3(0.0f);
+                    if (sc.pdf > 0.0f && sc.wi.z != 0.0f && (sc.wi.z > 0.0f) == (dot(wiw, sp.normal) > 0.0f))
+                        scattered = thr * eval_bsdf(cl, sc.wi, wo) * (fabsf(sc.wi.z) / sc.pdf);
+                    float survival = max3(scattered);
+                    bool terminal = false;
+                    if (survival <= 0.0f) {
+                        terminal = true;
+                    } else if (bounce >= ROULETTE_START) {
+                        survival = fminf(1.0f, survival);
+                        if (sample_1d(pixel, sample, bounce_dim(bounce, RR)) >= survival) terminal = true;
+                        else scattered = scattered / survival;
+                    }
+                    if (terminal) {
+                        pool.rad[path] = make_float4(rad.x + contribution.x, rad.y + contribution.y,
+                                                     rad.z + contribution.z, rad.w + 1.0f);
+                    } else {
+                        if (sc.lobe == LOBE_TRANSMISSION && mat.thin_walled == 0)
+                            medium = medium == inst ? MEDIUM_NONE : inst;
+                        pool.org[path] = f4(sc.wi.z < 0.0f ? sp.below : sp.position, 0.0f);
+                        pool.dir[path] = f4(wiw, 0.0f);
+                        pool.thr[path] = f4(scattered, sc.pdf);
+                        pool.state[path] = (sc.lobe << 24) | (medium & 0xffffffu);
+                        push_ray = true;
+                        if (any_pos(contribution))
+                            pool.rad[path] =
+                                make_float4(rad.x + contribution.x, rad.y + contribution.y, rad.z + contribution.z, rad.w);
+                    }
+                }
+            }
+        }
+        uint32_t slot = warp_push(pool.counters + CTR_RAYS + bounce + 1, push_ray);
+        if (push_ray) {
+            if (slot < pool.capacity) next_queue[slot] = path;
+            else flag_overflow(pool.counters);
+        }
+        uint32_t sslot = warp_push(pool.counters + CTR_SHADOWS + bounce, push_shadow);
+        if (push_shadow) {
+            if (sslot < pool.capacity) {
+                float4* dst = reinterpret_cast<float4*>(pool.shadows + sslot);
+                const float4* src = reinterpret_cast<const float4*>(&sr);
+                dst[0] = src[0];
+                dst[1] = src[1];
+                dst[2] = src[2];
+                dst[3] = src[3];
+            } else {
+                flag_overflow(pool.counters);
+            }
+        }
+    }
+}
+
+// ---- trace_shadow (trace_shadow.slang:29-72) ----------------------------------------
+
+template <bool COUNT>
+__global__ void __launch_bounds__(BLOCK) k_shadow(DeviceScene scene, PathPool pool, uint32_t bounce) {
+    const uint32_t count = min(pool.counters[CTR_SHADOWS + bounce], pool.capacity);
+    uint32_t visits = 0, tests = 0;
+    for (;;) {
+        uint32_t base = warp_fetch(pool.counters + CTR_FETCH_SHADOW + bounce);
+        if (base >= count) break;
+        uint32_t i = base + lane_id();
+        if (i >= count) continue;
+        const float4* rec = reinterpret_cast<const float4*>(pool.shadows + i);
+        float4 q0 = rec[0], q1 = rec[1], q2 = rec[2], q3 = rec[3];
+        uint32_t path = __float_as_uint(q1.w);
+        uint32_t light = __float_as_uint(q2.w), lprim = __float_as_uint(q3.x);
+        Ray ray = make_ray(xyz(q0), xyz(q1));
+        float tmax = q0.w;
+        float atten = 1.0f;
+        bool occluded = false;
+        uint32_t best_inst = LIGHT_NONE, best_prim = 0;
+        bool ok = traverse<COUNT>(scene, ray, tmax, [&](uint32_t, float4 a, float4 b, float4 c, float& tm) {
+            float t, b1, b2;
+            if (!tri_hit(ray, a, b, c, tm, t, b1, b2)) return false;
+            uint32_t inst = __float_as_uint(a.w), prim = __float_as_uint(b.w);
+            if (!(t < tm || (t == tm && (inst < best_inst || (inst == best_inst && prim < best_prim))))) return false;
+            uint32_t flags = __float_as_uint(c.w);
+            bool target = inst == light && prim == lprim;
+            if (!(flags & TRI_OPAQUE) && !target) {
+                atten *= 1.0f - __ldg(&scene.materials[inst].opacity);
+                if (atten < 1e-4f) {
+                    occluded = true;
+                    return true;
+                }
+                return false;
+            }
+            if (light == LIGHT_NONE) {  // nothing may commit: the first opaque hit decides
+                occluded = true;
+                return true;
+            }
+            tm = t;
+            best_inst = inst;
+            best_prim = prim;
+            return false;
+        }, &visits, &tests);
+        if (!ok) {
+            flag_overflow(pool.counters);
+            continue;
+        }
+        if (occluded) continue;
+        if (best_inst == LIGHT_NONE || (best_inst == light && best_prim == lprim)) {
+            float4 r = pool.rad[path];
+            pool.rad[path] = make_float4(r.x + q2.x * atten, r.y + q2.y * atten, r.z + q2.z * atten, r.w);
+        }
+    }
+    if (COUNT) flush_counts(pool.counters, visits, tests);
+}
+
+// ---- film --------------------------------------------------------------------------
+
+__device__ __forceinline__ bool finite4(float4 v) {
+    return isfinite(v.x) && isfinite(v.y) && isfinite(v.z) && isfinite(v.w);
+}
+
+__global__ void k_accumulate(const float4* __restrict__ rad, float4* __restrict__ sum, uint32_t pixel_base,
+                             uint32_t count, uint32_t samples, uint32_t reset) {
+    for (uint32_t p = blockIdx.x * blockDim.x + threadIdx.x; p < count; p += gridDim.x * blockDim.x) {
+        float4 acc = reset ? make_float4(0.0f, 0.0f, 0.0f, 0.0f) : sum[pixel_base + p];
+        for (uint32_t s = 0; s < samples; ++s) {
+            float4 v = rad[size_t(s) * count + p];
+            if (!finite4(v)) v = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+            if (reset && s == 0) acc = v;
+            else acc = make_float4(acc.x + v.x, acc.y + v.y, acc.z + v.z, acc.w + v.w);
+        }
+        sum[pixel_base + p] = acc;
+    }
+}
+
+__global__ void k_resolve(const float4* __restrict__ sum, float4* __restrict__ avg, uint32_t n, float samples) {
+    for (uint32_t p = blockIdx.x * blockDim.x + threadIdx.x; p < n; p += gridDim.x * blockDim.x) {
+        float4 v = sum[p];
+        avg[p] = make_float4(v.x / samples, v.y / samples, v.z / samples, v.w / samples);
+    }
+}
+
+__global__ void k_copy_rad(const float4* __restrict__ rad, float4* __restrict__ out, uint32_t base, uint32_t count) {
+    for (uint32_t p = blockIdx.x * blockDim.x + threadIdx.x; p < count; p += gridDim.x * blockDim.x)
+        out[base + p] = rad[p];
+}
+
+// Fold one wave's queue counters into the renderer's running totals:
+// tally[0] += extension rays, tally[1] += shadow rays, tally[2] |= overflow.
+__global__ void k_tally(const uint32_t* counters, unsigned long long* tally, uint32_t n0, uint32_t max_bounces) {
+    if (threadIdx.x != 0 || blockIdx.x != 0) return;
+    unsigned long long rays = n0, shadows = 0;
+    for (uint32_t b = 1; b < max_bounces; ++b) rays += counters[CTR_RAYS + b];
+    for (uint32_t b = 0; b < max_bounces; ++b) shadows += counters[CTR_SHADOWS + b];
+    tally[0] += rays;
+    tally[1] += shadows;
+    tally[2] |= counters[CTR_OVERFLOW];
+    tally[3] += *reinterpret_cast<const unsigned long long*>(counters + CTR_VISITS);
+    tally[4] += *reinterpret_cast<const unsigned long long*>(counters + CTR_TESTS);
+}
+
+}  // namespace
+
+void launch_tally(const PathPool& pool, unsigned long long* tally, uint32_t n0, uint32_t max_bounces,
+                  cudaStream_t stream) {
+    k_tally<<<1, 32, 0, stream>>>(pool.counters, tally, n0, max_bounces);
+}
+
+LaunchShape launch_shape(int device) {
+    int sms = 148;
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
+    LaunchShape ls;
+    ls.block = BLOCK;
+    int occ = 0;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_intersect<false>, BLOCK, 0);
+    ls.grid_isect = sms * (occ > 0 ? occ : 4);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_shade, BLOCK, 0);
+    ls.grid_shade = sms * (occ > 0 ? occ : 4);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_shadow<false>, BLOCK, 0);
+    ls.grid_shadow = sms * (occ > 0 ? occ : 4);
+    ls.grid_stream = sms * 8;
+    return ls;
+}
+
+void launch_wave_begin(const PathPool& pool, const WaveParams& wp, const LaunchShape& ls, cudaStream_t stream) {
+    cudaMemsetAsync(pool.counters, 0, CTR_COUNT * sizeof(uint32_t), stream);
+    k_raygen<<<ls.grid_stream, BLOCK, 0, stream>>>(pool, wp);
+}
+
+void launch_intersect(const DeviceScene& scene, const PathPool& pool, uint32_t bounce, uint32_t n0,
+                      const LaunchShape& ls, bool count_visits, cudaStream_t stream) {
+    if (count_visits) k_intersect<true><<<ls.grid_isect, BLOCK, 0, stream>>>(scene, pool, bounce, n0);
+    else k_intersect<false><<<ls.grid_isect, BLOCK, 0, stream>>>(scene, pool, bounce, n0);
+}
+
+void launch_shade(const DeviceScene& scene, const PathPool& pool, uint32_t bounce, const WaveParams& wp, uint32_t n0,
+                  const LaunchShape& ls, cudaStream_t stream) {
+    k_shade<<<ls.grid_shade, BLOCK, 0, stream>>>(scene, pool, bounce, wp.max_bounces, wp.light_sampling, n0);
+}
+
+void launch_shadow(const DeviceScene& scene, const PathPool& pool, uint32_t bounce, const LaunchShape& ls,
+                   bool count_visits, cudaStream_t stream) {
+    if (count_visits) k_shadow<true><<<ls.grid_shadow, BLOCK, 0, stream>>>(scene, pool, bounce);
+    else k_shadow<false><<<ls.grid_shadow, BLOCK, 0, stream>>>(scene, pool, bounce);
+}
+
+void launch_wave(const DeviceScene& scene, const PathPool& pool, const WaveParams& wp, const LaunchShape& ls,
+                 cudaStream_t stream) {
+    const uint32_t n0 = wp.pixel_count * wp.samples;
+    launch_wave_begin(pool, wp, ls, stream);
+    for (uint32_t b = 0; b < wp.max_bounces; ++b) {
+        launch_intersect(scene, pool, b, n0, ls, false, stream);
+        launch_shade(scene, pool, b, wp, n0, ls, stream);
+        launch_shadow(scene, pool, b, ls, false, stream);
+    }
+}
+
+void launch_accumulate(const PathPool& pool, float4* sum, uint32_t pixel_base, uint32_t pixel_count, uint32_t samples,
+                       bool reset, cudaStream_t stream) {
+    int grid = int((pixel_count + 255) / 256);
+    if (grid > 148 * 16) grid = 148 * 16;
+    k_accumulate<<<grid, 256, 0, stream>>>(pool.rad, sum, pixel_base, pixel_count, samples, reset ? 1u : 0u);
+}
+
+void launch_resolve(const float4* sum, float4* avg, uint32_t pixels, float samples, cudaStream_t stream) {
+    int grid = int((pixels + 255) / 256);
+    if (grid > 148 * 16) grid = 148 * 16;
+    k_resolve<<<grid, 256, 0, stream>>>(sum, avg, pixels, samples);
+}
+
+void launch_copy_rad(const PathPool& pool, float4* out, uint32_t pixel_base, uint32_t pixel_count, cudaStream_t stream) {
+    int grid = int((pixel_count + 255) / 256);
+    if (grid > 148 * 16) grid = 148 * 16;
+    k_copy_rad<<<grid, 256, 0, stream>>>(pool.rad, out, pixel_base, pixel_count);
+}
+
+}  // namespace cn

@@ -1,0 +1,83 @@
+// Host-side view of the wavefront engine: path pool layout and the launch
+// entry points of wavefront.cu.
+#pragma once
+#include <cstdint>
+#include <cuda_runtime.h>
+#include "records.h"
+
+namespace cn {
+
+// Per-wave device counters, one uint32 each, zeroed at wave start.
+constexpr uint32_t MAX_BOUNCES = 255;
+constexpr uint32_t CTR_RAYS = 0;        // [b]: paths entering bounce b (b = 0 is the camera wave)
+constexpr uint32_t CTR_SHADOWS = 256;   // [b]: shadow rays pushed at bounce b
+constexpr uint32_t CTR_FETCH_ISECT = 512;
+constexpr uint32_t CTR_FETCH_SHADE = 768;
+constexpr uint32_t CTR_FETCH_SHADOW = 1024;
+constexpr uint32_t CTR_OVERFLOW = 1280;
+constexpr uint32_t CTR_VISITS = 1284;   // 64-bit: wide nodes visited (instrumented launches only)
+constexpr uint32_t CTR_TESTS = 1286;    // 64-bit: triangles tested (instrumented launches only)
+constexpr uint32_t CTR_COUNT = 1296;
+
+// Structure-of-arrays path state: one 16-byte lane per logical field, so
+// every stage reads and writes with coalesced 128-bit accesses.
+struct PathPool {
+    float4* org;       // xyz origin
+    float4* dir;       // xyz direction, w = cosine to the camera's forward axis
+    float4* thr;       // xyz throughput, w = pdf of the scatter that made the ray (0: camera ray)
+    uint4* hit;        // (instance | 0xffffffff on a miss, primitive, b1 bits, b2 bits)
+    uint2* ps;         // (pixel, sample index)
+    uint32_t* state;   // lobe << 24 | medium
+    float4* rad;       // the path's radiance, alpha = finished
+    uint32_t* queue[2];   // ray queues, ping-pong by bounce parity
+    ShadowRay* shadows;
+    uint32_t* counters;
+    uint32_t capacity;
+};
+
+struct WaveParams {
+    uint32_t width, height;
+    uint32_t pixel_base, pixel_count;  // the pixel range of this wave
+    uint32_t samples;                  // samples of each pixel traced in this wave
+    uint32_t sample_base;              // sample index of the first
+    uint32_t max_bounces;
+    uint32_t light_sampling;
+    float3 cam_pos, cam_right, cam_up, cam_fwd;  // basis pre-scaled to the focal plane when the lens is open
+    float aperture;
+};
+
+struct LaunchShape {
+    int grid_isect, grid_shade, grid_shadow, grid_stream;
+    int block;
+};
+
+LaunchShape launch_shape(int device);
+
+// One wave: raygen, then max_bounces × (intersect, shade, shadow). Path
+// radiance lands in pool.rad[path] with path = s · pixel_count + local pixel.
+// The stages are also exposed one by one so a caller can time them.
+void launch_wave(const DeviceScene& scene, const PathPool& pool, const WaveParams& wp, const LaunchShape& ls,
+                 cudaStream_t stream);
+void launch_wave_begin(const PathPool& pool, const WaveParams& wp, const LaunchShape& ls, cudaStream_t stream);
+// `count_visits` selects the instrumented traversal that tallies wide-node
+// visits and triangle tests into the counters (for the roofline's traffic).
+void launch_intersect(const DeviceScene& scene, const PathPool& pool, uint32_t bounce, uint32_t n0,
+                      const LaunchShape& ls, bool count_visits, cudaStream_t stream);
+void launch_shade(const DeviceScene& scene, const PathPool& pool, uint32_t bounce, const WaveParams& wp, uint32_t n0,
+                  const LaunchShape& ls, cudaStream_t stream);
+void launch_shadow(const DeviceScene& scene, const PathPool& pool, uint32_t bounce, const LaunchShape& ls,
+                   bool count_visits, cudaStream_t stream);
+
+// Film: sum[pixel] += guarded rad[s · count + local], s ascending (the
+// film's guard, crates/cenote/shaders/accumulate.slang:38-44); reset
+// overwrites with the first sample instead.
+void launch_accumulate(const PathPool& pool, float4* sum, uint32_t pixel_base, uint32_t pixel_count, uint32_t samples,
+                       bool reset, cudaStream_t stream);
+void launch_resolve(const float4* sum, float4* avg, uint32_t pixels, float samples, cudaStream_t stream);
+// tally[0] += extension rays, [1] += shadow rays, [2] |= overflow,
+// [3] += node visits, [4] += triangle tests.
+void launch_tally(const PathPool& pool, unsigned long long* tally, uint32_t n0, uint32_t max_bounces,
+                  cudaStream_t stream);
+void launch_copy_rad(const PathPool& pool, float4* out, uint32_t pixel_base, uint32_t pixel_count, cudaStream_t stream);
+
+}  // namespace cn

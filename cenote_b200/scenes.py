@@ -1,0 +1,400 @@
+"""Procedural scene inputs: meshes, materials, cameras and environments.
+
+Everything here is plain data (numpy float32/uint32 arrays and the 144-byte
+material record), the same arrays whether they go to the CUDA library or to a
+CPU check. The material constructors follow crates/cenote/src/material.rs:118-248,
+the solids crates/cenote/src/scene/shapes.rs:21-117, and authored colours enter
+through the Rec.709 -> ACEScg matrix of crates/cenote/src/color.rs:351-361.
+
+The named workloads:
+
+* ``cornell``   -- a closed box of five 2x2 quads, two white boxes and a 0.5x0.5
+  ceiling emitter (36 triangles), pinhole 40 deg, 256x256, 16 spp, 8 bounces.
+* ``chart``     -- a 5x5 grid of radius-0.4 icospheres (subdivision 3) sweeping
+  roughness along x and metalness along z on a 20x20 glossy ground, a 1x1
+  warm quad light and a procedural 2048x1024 HDRI sky with a 0.5 deg sun;
+  1280x720, 64 spp, 12 bounces.
+* ``terrain``   -- a 1024^2 fBm heightfield with 500 instanced glass, coated and
+  fuzz meshes and 4096 lognormal-power emissive triangles; 1920x1080, 64 spp,
+  16 bounces.
+"""
+from __future__ import annotations
+
+import math
+from dataclasses import dataclass, field
+
+import numpy as np
+
+TEXTURE_NONE = 0xFFFFFFFF
+
+MATERIAL_DTYPE = np.dtype(
+    [
+        ("base_color", "<f4", 3),
+        ("base_roughness", "<f4"),
+        ("emission", "<f4", 3),
+        ("metalness", "<f4"),
+        ("specular_weight", "<f4"),
+        ("specular_roughness", "<f4"),
+        ("specular_ior", "<f4"),
+        ("transmission_weight", "<f4"),
+        ("transmission_color", "<f4", 3),
+        ("transmission_depth", "<f4"),
+        ("coat_color", "<f4", 3),
+        ("coat_weight", "<f4"),
+        ("coat_roughness", "<f4"),
+        ("coat_ior", "<f4"),
+        ("coat_darkening", "<f4"),
+        ("fuzz_weight", "<f4"),
+        ("fuzz_color", "<f4", 3),
+        ("fuzz_roughness", "<f4"),
+        ("opacity", "<f4"),
+        ("thin_walled", "<u4"),
+        ("base_color_texture", "<u4"),
+        ("specular_roughness_texture", "<u4"),
+        ("metalness_texture", "<u4"),
+        ("emission_texture", "<u4"),
+        ("opacity_texture", "<u4"),
+        ("normal_texture", "<u4"),
+    ]
+)
+assert MATERIAL_DTYPE.itemsize == 144
+
+# color.rs:351-355, applied as a column-major Mat3 in f32.
+_ACESCG_FROM_REC709 = np.array(
+    [
+        [0.6130974, 0.33952314, 0.04737945],
+        [0.07019373, 0.9163539, 0.013452399],
+        [0.020615594, 0.10956978, 0.86981466],
+    ],
+    dtype=np.float32,
+)
+
+
+def acescg(rec709) -> np.ndarray:
+    """Linear Rec.709 -> ACEScg, summed left to right in f32 like glam."""
+    c = np.asarray(rec709, dtype=np.float32)
+    m = _ACESCG_FROM_REC709
+    out = np.empty(3, dtype=np.float32)
+    for r in range(3):
+        out[r] = (m[r, 0] * c[0] + m[r, 1] * c[1]) + m[r, 2] * c[2]
+    return out
+
+
+def material(**overrides) -> np.ndarray:
+    """Material::matte(white, 0) with fields overridden (material.rs:122-151)."""
+    m = np.zeros((), dtype=MATERIAL_DTYPE)
+    m["base_color"] = (1.0, 1.0, 1.0)
+    m["base_roughness"] = 0.0
+    m["emission"] = (0.0, 0.0, 0.0)
+    m["metalness"] = 0.0
+    m["specular_weight"] = 0.0
+    m["specular_roughness"] = 0.0
+    m["specular_ior"] = 1.5
+    m["transmission_weight"] = 0.0
+    m["transmission_color"] = (1.0, 1.0, 1.0)
+    m["transmission_depth"] = 0.0
+    m["coat_color"] = (1.0, 1.0, 1.0)
+    m["coat_weight"] = 0.0
+    m["coat_roughness"] = 0.0
+    m["coat_ior"] = 1.6
+    m["coat_darkening"] = 1.0
+    m["fuzz_weight"] = 0.0
+    m["fuzz_color"] = (1.0, 1.0, 1.0)
+    m["fuzz_roughness"] = 0.5
+    m["opacity"] = 1.0
+    m["thin_walled"] = 0
+    for k in (
+        "base_color_texture",
+        "specular_roughness_texture",
+        "metalness_texture",
+        "emission_texture",
+        "opacity_texture",
+        "normal_texture",
+    ):
+        m[k] = TEXTURE_NONE
+    for k, v in overrides.items():
+        m[k] = v
+    return m
+
+
+def matte(base_color, base_roughness=0.0):
+    return material(base_color=base_color, base_roughness=base_roughness)
+
+
+def glossy(base_color, base_roughness, specular_roughness):
+    return material(base_color=base_color, base_roughness=base_roughness, specular_weight=1.0,
+                    specular_roughness=specular_roughness)
+
+
+def metal(base_color, specular_roughness):
+    return material(base_color=base_color, metalness=1.0, specular_weight=1.0,
+                    specular_roughness=specular_roughness)
+
+
+def glass(specular_roughness, specular_ior):
+    return material(transmission_weight=1.0, specular_weight=1.0, specular_roughness=specular_roughness,
+                    specular_ior=specular_ior)
+
+
+def emitter(emission):
+    return material(base_color=(0.0, 0.0, 0.0), emission=emission)
+
+
+# ---- meshes -----------------------------------------------------------------
+
+
+@dataclass
+class Mesh:
+    positions: np.ndarray  # (V, 3) f32
+    normals: np.ndarray    # (V, 3) f32
+    uvs: np.ndarray        # (V, 2) f32
+    indices: np.ndarray    # (T, 3) u32, counter-clockwise outward
+
+    @property
+    def triangle_count(self) -> int:
+        return int(self.indices.shape[0])
+
+
+def _mesh(p, n, uv, idx) -> Mesh:
+    return Mesh(np.ascontiguousarray(p, np.float32), np.ascontiguousarray(n, np.float32),
+                np.ascontiguousarray(uv, np.float32), np.ascontiguousarray(idx, np.uint32))
+
+
+def icosphere(subdivisions: int) -> Mesh:
+    """Unit icosphere by 4-way splits with a shared midpoint cache (shapes.rs:21-57)."""
+    phi = np.float32((1.0 + math.sqrt(5.0)) / 2.0)
+    base = [[-1, phi, 0], [1, phi, 0], [-1, -phi, 0], [1, -phi, 0], [0, -1, phi], [0, 1, phi],
+            [0, -1, -phi], [0, 1, -phi], [phi, 0, -1], [phi, 0, 1], [-phi, 0, -1], [-phi, 0, 1]]
+    pos = [np.asarray(p, np.float32) / np.float32(np.sqrt(np.float32(np.dot(np.asarray(p, np.float32),
+                                                                              np.asarray(p, np.float32)))))
+           for p in base]
+    tris = [[0, 11, 5], [0, 5, 1], [0, 1, 7], [0, 7, 10], [0, 10, 11], [1, 5, 9], [5, 11, 4], [11, 10, 2],
+            [10, 7, 6], [7, 1, 8], [3, 9, 4], [3, 4, 2], [3, 2, 6], [3, 6, 8], [3, 8, 9], [4, 9, 5], [2, 4, 11],
+            [6, 2, 10], [8, 6, 7], [9, 8, 1]]
+    for _ in range(subdivisions):
+        cache: dict = {}
+
+        def mid(a, b):
+            key = (min(a, b), max(a, b))
+            if key not in cache:
+                m = (pos[a] + pos[b]) * np.float32(0.5)
+                m = m / np.float32(np.sqrt(np.float32(np.dot(m, m))))
+                cache[key] = len(pos)
+                pos.append(m.astype(np.float32))
+            return cache[key]
+
+        faces = []
+        for a, b, c in tris:
+            ab, bc, ca = mid(a, b), mid(b, c), mid(c, a)
+            faces += [[a, ab, ca], [ab, b, bc], [ca, bc, c], [ab, bc, ca]]
+        tris = faces
+    p = np.stack(pos).astype(np.float32)
+    return _mesh(p, p.copy(), np.zeros((len(p), 2), np.float32), np.asarray(tris, np.uint32))
+
+
+def quad(corners, normal=None, uvs=None) -> Mesh:
+    """Two triangles over four corners given counter-clockwise seen from the front."""
+    c = np.asarray(corners, np.float32)
+    n = np.cross(c[1] - c[0], c[2] - c[0]) if normal is None else np.asarray(normal, np.float32)
+    n = (n / np.linalg.norm(n)).astype(np.float32)
+    uv = np.array([[0, 0], [0, 1], [1, 1], [1, 0]], np.float32) if uvs is None else uvs
+    return _mesh(c, np.tile(n, (4, 1)), uv, [[0, 1, 2], [0, 2, 3]])
+
+
+def ground_plane(half_extent: float) -> Mesh:
+    """The XZ plane at y = 0, normal +Y (shapes.rs:117-139)."""
+    e = half_extent
+    return _mesh([[-e, 0, -e], [-e, 0, e], [e, 0, e], [e, 0, -e]], [[0, 1, 0]] * 4,
+                 [[0, 0], [0, 1], [1, 1], [1, 0]], [[0, 1, 2], [0, 2, 3]])
+
+
+def box(sx: float, sy: float, sz: float) -> Mesh:
+    """An axis-aligned box centred at the origin, flat-shaded, 12 outward triangles."""
+    hx, hy, hz = sx / 2, sy / 2, sz / 2
+    faces = [  # (normal, 4 corners counter-clockwise from outside)
+        ((1, 0, 0), [(hx, -hy, hz), (hx, -hy, -hz), (hx, hy, -hz), (hx, hy, hz)]),
+        ((-1, 0, 0), [(-hx, -hy, -hz), (-hx, -hy, hz), (-hx, hy, hz), (-hx, hy, -hz)]),
+        ((0, 1, 0), [(-hx, hy, hz), (hx, hy, hz), (hx, hy, -hz), (-hx, hy, -hz)]),
+        ((0, -1, 0), [(-hx, -hy, -hz), (hx, -hy, -hz), (hx, -hy, hz), (-hx, -hy, hz)]),
+        ((0, 0, 1), [(-hx, -hy, hz), (hx, -hy, hz), (hx, hy, hz), (-hx, hy, hz)]),
+        ((0, 0, -1), [(hx, -hy, -hz), (-hx, -hy, -hz), (-hx, hy, -hz), (hx, hy, -hz)]),
+    ]
+    p, n, uv, idx = [], [], [], []
+    for normal, corners in faces:
+        b = len(p)
+        p += corners
+        n += [normal] * 4
+        uv += [(0, 0), (1, 0), (1, 1), (0, 1)]
+        idx += [[b, b + 1, b + 2], [b, b + 2, b + 3]]
+    return _mesh(p, n, uv, idx)
+
+
+# ---- transforms -----------------------------------------------------------------
+
+
+def translate(x, y, z) -> np.ndarray:
+    m = np.eye(4)
+    m[:3, 3] = (x, y, z)
+    return m
+
+
+def rotate_y(deg) -> np.ndarray:
+    a = math.radians(deg)
+    m = np.eye(4)
+    m[0, 0], m[0, 2], m[2, 0], m[2, 2] = math.cos(a), math.sin(a), -math.sin(a), math.cos(a)
+    return m
+
+
+def rotate_x(deg) -> np.ndarray:
+    a = math.radians(deg)
+    m = np.eye(4)
+    m[1, 1], m[1, 2], m[2, 1], m[2, 2] = math.cos(a), -math.sin(a), math.sin(a), math.cos(a)
+    return m
+
+
+def scale(s) -> np.ndarray:
+    m = np.eye(4)
+    m[0, 0] = m[1, 1] = m[2, 2] = s
+    return m
+
+
+def rows(m4: np.ndarray) -> np.ndarray:
+    """The top three rows of a 4x4 as the 12 f32 values a record carries."""
+    return np.ascontiguousarray(np.asarray(m4, np.float64)[:3, :4], np.float32).reshape(12)
+
+
+# ---- scenes ---------------------------------------------------------------------
+
+
+@dataclass
+class Object:
+    mesh: Mesh
+    transform: np.ndarray  # 12 f32, rows of a 3x4
+    material: np.ndarray   # MATERIAL_DTYPE scalar
+    camera_visible: bool = True
+
+
+@dataclass
+class Camera:
+    position: tuple
+    look_at: tuple
+    up: tuple = (0.0, 1.0, 0.0)
+    vfov_degrees: float = 40.0
+    aperture_radius: float = 0.0
+    focus_distance: float = 1.0
+
+
+@dataclass
+class Environment:
+    width: int
+    height: int
+    texels: np.ndarray  # (H, W, 4) f32, ACEScg, row 0 = +Y
+
+    @staticmethod
+    def constant(rgb) -> "Environment":
+        t = np.array([[[rgb[0], rgb[1], rgb[2], 1.0]]], np.float32)
+        return Environment(1, 1, t)
+
+
+@dataclass
+class DeltaLight:
+    kind: int  # 1 distant (anchor = unit travel direction), 2 point (anchor = position)
+    anchor: tuple
+    emission: tuple
+
+
+@dataclass
+class SceneSpec:
+    name: str
+    objects: list
+    camera: Camera
+    environment: Environment
+    width: int
+    height: int
+    spp: int
+    max_bounces: int
+    delta_lights: list = field(default_factory=list)
+
+    @property
+    def triangle_count(self) -> int:
+        return sum(o.mesh.triangle_count for o in self.objects)
+
+
+def cornell(width=256, height=256, spp=16, max_bounces=8) -> SceneSpec:
+    white = matte(acescg((0.73, 0.73, 0.73)))
+    red = matte(acescg((0.63, 0.065, 0.05)))
+    green = matte(acescg((0.14, 0.45, 0.09)))
+    ident = rows(np.eye(4))
+    objs = [
+        Object(quad([(-1, 0, -1), (-1, 0, 1), (1, 0, 1), (1, 0, -1)]), ident, white),     # floor, +y
+        Object(quad([(-1, 2, -1), (1, 2, -1), (1, 2, 1), (-1, 2, 1)]), ident, white),     # ceiling, -y
+        Object(quad([(-1, 0, -1), (1, 0, -1), (1, 2, -1), (-1, 2, -1)]), ident, white),   # back, +z
+        Object(quad([(-1, 0, -1), (-1, 2, -1), (-1, 2, 1), (-1, 0, 1)]), ident, red),     # left, +x
+        Object(quad([(1, 0, -1), (1, 0, 1), (1, 2, 1), (1, 2, -1)]), ident, green),       # right, -x
+        Object(box(0.6, 0.6, 0.6), rows(translate(0.33, 0.3, 0.3) @ rotate_y(17.0)), white),
+        Object(box(0.6, 1.2, 0.6), rows(translate(-0.33, 0.6, -0.3) @ rotate_y(-18.0)), white),
+        Object(quad([(-0.25, 1.999, -0.25), (0.25, 1.999, -0.25), (0.25, 1.999, 0.25), (-0.25, 1.999, 0.25)]),
+               ident, emitter(acescg((17.0, 12.0, 4.0)))),
+    ]
+    cam = Camera((0.0, 1.0, 3.8), (0.0, 1.0, 0.0), vfov_degrees=40.0)
+    return SceneSpec("cornell", objs, cam, Environment.constant((0.0, 0.0, 0.0)), width, height, spp, max_bounces)
+
+
+def sky_hdri(width=2048, height=1024, sun_elevation_deg=35.0, sun_azimuth_deg=30.0, sun_sigma_deg=0.5,
+             sun_peak=5.0e4) -> Environment:
+    """Gradient sky (0.3, 0.5, 1.0) at the zenith to white at the horizon, a dim
+    ground below it, plus a Gaussian sun lobe; texel centres follow the
+    equirect mapping of crates/cenote/shaders/environment.slang:74-85."""
+    u = (np.arange(width, dtype=np.float64) + 0.5) / width
+    v = (np.arange(height, dtype=np.float64) + 0.5) / height
+    phi = 2.0 * np.pi * (u - 0.5)
+    theta = np.pi * v
+    st, ct = np.sin(theta)[:, None], np.cos(theta)[:, None]
+    d = np.stack([st * np.sin(phi)[None, :], np.broadcast_to(ct, (height, width)), -st * np.cos(phi)[None, :]], -1)
+    y = d[..., 1]
+    t = np.sqrt(np.clip(y, 0.0, 1.0))[..., None]
+    sky = (1.0 - t) * np.array([1.0, 1.0, 1.0]) + t * np.array([0.3, 0.5, 1.0])
+    ground = np.array([0.25, 0.22, 0.2]) * np.clip(1.0 + y, 0.2, 1.0)[..., None]
+    rgb = np.where((y >= 0.0)[..., None], sky, ground)
+    el, az = math.radians(sun_elevation_deg), math.radians(sun_azimuth_deg)
+    sun = np.array([math.cos(el) * math.sin(az), math.sin(el), -math.cos(el) * math.cos(az)])
+    ang = np.arccos(np.clip(d @ sun, -1.0, 1.0))
+    sig = math.radians(sun_sigma_deg)
+    lobe = sun_peak * np.exp(-0.5 * (ang / sig) ** 2)
+    rgb = rgb + lobe[..., None] * np.array([1.0, 0.95, 0.85])
+    tex = np.empty((height, width, 4), np.float32)
+    tex[..., :3] = rgb
+    tex[..., 3] = 1.0
+    return Environment(width, height, tex)
+
+
+def chart(width=1280, height=720, spp=64, max_bounces=12, env_size=(2048, 1024)) -> SceneSpec:
+    sphere = icosphere(3)
+    base = acescg((0.8, 0.35, 0.2))
+    objs = []
+    for iz in range(5):
+        for ix in range(5):
+            rough = ix / 4.0
+            metalness = iz / 4.0
+            m = glossy(base, 0.0, rough)
+            m["metalness"] = metalness
+            xf = translate((ix - 2) * 1.0, 0.4, (iz - 2) * 1.0) @ scale(0.4)
+            objs.append(Object(sphere, rows(xf), m))
+    objs.append(Object(ground_plane(10.0), rows(np.eye(4)), glossy(acescg((0.5, 0.5, 0.5)), 0.0, 0.3)))
+    light = quad([(-0.5, 0, -0.5), (0.5, 0, -0.5), (0.5, 0, 0.5), (-0.5, 0, 0.5)])  # faces -y
+    objs.append(Object(light, rows(translate(1.5, 3.0, 1.5) @ rotate_x(-20.0)), emitter(acescg((8.0, 6.0, 4.0)))))
+    cam = Camera((0.0, 2.6, 5.8), (0.0, 0.35, 0.0), vfov_degrees=40.0)
+    return SceneSpec("chart", objs, cam, sky_hdri(*env_size), width, height, spp, max_bounces)
+
+
+def furnace(mat, size=32, sky=0.5, center=(0.0, 0.0, 0.0), scl=1.0, aperture=0.0, focus=1.0) -> SceneSpec:
+    """One large plane under a uniform grey sky, camera just above it looking
+    obliquely down (render/tests.rs:51-84)."""
+    c = np.asarray(center, np.float64)
+    obj = Object(ground_plane(5.0), rows(translate(*c) @ scale(scl)), mat)
+    cam = Camera(tuple(c + (0.0, scl, 0.0)), tuple(c + (0.0, 0.0, -scl)), vfov_degrees=40.0,
+                 aperture_radius=aperture, focus_distance=focus)
+    return SceneSpec("furnace", [obj], cam, Environment.constant((sky, sky, sky)), size, size, 16, 8)
+
+
+SCENES = {"cornell": cornell, "chart": chart}

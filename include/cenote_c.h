@@ -1,0 +1,265 @@
+/*
+ * cenote_c.h — the C ABI of the B200 wavefront path tracer.
+ *
+ * This is the boundary a host (the reference's Rust crate through a bindgen'd
+ * `cenote-sys`, the C++ CLI, or Python through ctypes) binds. It replaces the
+ * `cenote` crate's scene/renderer API:
+ *
+ *   Scene::new(&Context, &[Object], Camera, &Environment)   crates/cenote/src/scene/mod.rs:254
+ *   Renderer::with_max_bounces(&Context, u32)               crates/cenote/src/render/mod.rs:151
+ *   Renderer::render(&self, &Context, &Scene, w, h)         crates/cenote/src/render/mod.rs:209
+ *   Renderer::accumulate(&self, &Context, &Scene, &mut Film) crates/cenote/src/render/mod.rs:245
+ *   Film::{new, reset, samples, averages}                   crates/cenote/src/render/film.rs:102-217
+ *   Wavefront::trace(&Context, &Scene, &Buffer, w, h, sample) crates/cenote/src/wavefront.rs:568
+ *   LightSampling {Mis, BsdfOnly, NeeOnly}                  crates/cenote/src/wavefront.rs (LIGHT_SAMPLING_* in shaders/lights.slang:32-34)
+ *
+ * Conventions (bindgen-friendly): opaque handles, POD structs, every call
+ * returns an int32_t status (0 ok, negative = cenote error). A caller bug that
+ * the reference catches with `assert!` (zero-sized target, bounce cap outside
+ * 1..=255, empty scene, non-invertible transform) returns
+ * CENOTE_E_INVALID_ARGUMENT instead of aborting. cenote_last_error() returns
+ * the calling thread's last message. Output buffers are caller-owned host
+ * memory unless a name says "device". A handle is not thread-safe by itself;
+ * every handle created from one context shares that context's CUDA stream.
+ */
+#ifndef CENOTE_C_H
+#define CENOTE_C_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* Status codes, mirroring cenote::Error (crates/cenote/src/error.rs:10-72). */
+#define CENOTE_OK 0
+#define CENOTE_E_INVALID_ARGUMENT (-1)
+#define CENOTE_E_DEVICE (-2)        /* CUDA runtime error (the reference's Error::Vulkan) */
+#define CENOTE_E_NO_CAPABLE_GPU (-3) /* Error::NoCapableGpu */
+#define CENOTE_E_ALLOCATION (-4)    /* Error::Allocation */
+#define CENOTE_E_SCENE (-5)         /* Error::Scene */
+#define CENOTE_E_TIMEOUT (-6)       /* a bounded device wait gave up */
+#define CENOTE_E_OVERFLOW (-7)      /* a device-side bound (stack, queue) was exceeded */
+#define CENOTE_E_BUDGET (-8)        /* a job does not fit the server's HBM budget */
+
+/* LightSampling (wavefront.rs; LIGHT_SAMPLING_* in shaders/lights.slang:32-34). */
+#define CENOTE_LIGHT_SAMPLING_MIS 0u
+#define CENOTE_LIGHT_SAMPLING_BSDF 1u
+#define CENOTE_LIGHT_SAMPLING_NEE 2u
+
+/* "No texture" in a material's texture slots (material.rs TEXTURE_NONE). */
+#define CENOTE_TEXTURE_NONE 0xffffffffu
+
+/* Delta-light kinds (lights.rs KIND_*). */
+#define CENOTE_LIGHT_DISTANT 1u
+#define CENOTE_LIGHT_POINT 2u
+
+typedef struct cenote_context cenote_context;
+typedef struct cenote_scene cenote_scene;
+typedef struct cenote_renderer cenote_renderer;
+typedef struct cenote_film cenote_film;
+
+/* The 144-byte OpenPBR record, field for field crates/cenote/src/material.rs:28-109. */
+typedef struct cenote_material {
+    float base_color[3];
+    float base_roughness;
+    float emission[3];
+    float metalness;
+    float specular_weight;
+    float specular_roughness;
+    float specular_ior;
+    float transmission_weight;
+    float transmission_color[3];
+    float transmission_depth;
+    float coat_color[3];
+    float coat_weight;
+    float coat_roughness;
+    float coat_ior;
+    float coat_darkening;
+    float fuzz_weight;
+    float fuzz_color[3];
+    float fuzz_roughness;
+    float opacity;
+    uint32_t thin_walled;
+    uint32_t base_color_texture;
+    uint32_t specular_roughness_texture;
+    uint32_t metalness_texture;
+    uint32_t emission_texture;
+    uint32_t opacity_texture;
+    uint32_t normal_texture;
+} cenote_material;
+
+/* One scene object: mesh + placement + surface (scene/mod.rs:61-86).
+ * positions/normals are 3 floats per vertex, uvs 2 floats, indices 3 per
+ * triangle (counter-clockwise outward); transform = rows of the 3×4
+ * object-to-world matrix. The library copies everything it needs. */
+typedef struct cenote_object {
+    const float* positions;
+    const float* normals;
+    const float* uvs;
+    const uint32_t* indices;
+    uint32_t vertex_count;
+    uint32_t triangle_count;
+    float transform[12];
+    cenote_material material;
+    uint32_t camera_visible; /* 0: camera rays pass it (ray_mask::CAMERA) */
+    uint32_t pad;
+} cenote_object;
+
+/* Camera (scene/mod.rs:392-422); aperture_radius 0 is a pinhole. */
+typedef struct cenote_camera {
+    float position[3];
+    float look_at[3];
+    float up[3];
+    float vfov_degrees;
+    float aperture_radius;
+    float focus_distance;
+} cenote_camera;
+
+/* Equirect environment, RGBA f32 ACEScg, row 0 = +Y (environment.rs:33-79). */
+typedef struct cenote_environment {
+    uint32_t width;
+    uint32_t height;
+    const float* texels;
+} cenote_environment;
+
+/* A delta light (lights.rs:57-73): kind CENOTE_LIGHT_DISTANT with anchor =
+ * unit travel direction and emission = irradiance, or CENOTE_LIGHT_POINT with
+ * anchor = position and emission = intensity. ACEScg. */
+typedef struct cenote_delta_light {
+    uint32_t kind;
+    float anchor[3];
+    float emission[3];
+} cenote_delta_light;
+
+typedef struct cenote_options {
+    int32_t device; /* CUDA ordinal */
+} cenote_options;
+
+/* Per-renderer counters of the last accumulate/render call. */
+typedef struct cenote_stats {
+    uint64_t extension_rays;  /* camera + scattered rays traced */
+    uint64_t shadow_rays;
+    uint64_t samples;         /* pixel samples completed */
+    uint64_t node_visits;     /* wide BVH nodes visited (CENOTE_PROFILE_COUNTS only) */
+    uint64_t triangle_tests;  /* ray-triangle tests (CENOTE_PROFILE_COUNTS only) */
+    float gpu_ms;             /* device time of the call's waves */
+    float raygen_ms;          /* per-stage device time (CENOTE_PROFILE_TIMING only) */
+    float intersect_ms;
+    float shade_ms;
+    float shadow_ms;
+    float film_ms;
+    uint32_t kernel_launches; /* kernels this library launched in the call */
+    uint32_t waves;
+    uint32_t samples_per_wave;
+    uint32_t overflow;        /* nonzero: a device-side bound was hit */
+} cenote_stats;
+
+/* Profiling switches for subsequent calls (bit flags). TIMING records CUDA
+ * events around every stage launch; COUNTS runs the instrumented traversal
+ * that tallies node visits and triangle tests (slower: keep it out of timed
+ * runs). */
+#define CENOTE_PROFILE_TIMING 1u
+#define CENOTE_PROFILE_COUNTS 2u
+
+/* ---- context -------------------------------------------------------------- */
+
+const char* cenote_last_error(void);
+int32_t cenote_context_create(const cenote_options* options, cenote_context** out);
+void cenote_context_destroy(cenote_context* ctx);
+/* The context's cudaStream_t, for callers that time or order work on it. */
+void* cenote_context_stream(cenote_context* ctx);
+int32_t cenote_synchronize(cenote_context* ctx);
+
+/* ---- scene (Scene::new, scene/mod.rs:254) ------------------------------------ */
+
+int32_t cenote_scene_create(cenote_context* ctx, const cenote_object* objects, uint32_t object_count,
+                            const cenote_camera* camera, const cenote_environment* environment,
+                            const cenote_delta_light* deltas, uint32_t delta_count, cenote_scene** out);
+void cenote_scene_destroy(cenote_scene* scene);
+/* Replace the camera (the viewer's orbit control writes Scene::camera_mut). */
+int32_t cenote_scene_set_camera(cenote_scene* scene, const cenote_camera* camera);
+/* Scene-prep timings (ms): [0] BVH build, [1] env tables on the GPU, [2] total. */
+int32_t cenote_scene_prep_times(cenote_scene* scene, float* ms3);
+/* Device bytes the scene holds (BVH + triangles + records + textures + env). */
+uint64_t cenote_scene_device_bytes(cenote_scene* scene);
+/* The light list as built (80-byte records of lights.rs:79-109), and its length. */
+int32_t cenote_scene_light_records(cenote_scene* scene, void* out_records, uint32_t* out_count);
+/* The environment tables built on the device (environment.rs:221-233 layout),
+ * the emitted power and the environment selection probability. Any output may
+ * be NULL. */
+int32_t cenote_scene_env_tables(cenote_scene* scene, float* marginal, float* conditional, float* pdfs,
+                                double* power, float* select_prob);
+
+/* ---- renderer (Renderer::with_max_bounces, render/mod.rs:151) ----------------- */
+
+/* capacity = paths in flight per wave (0 = one full sample of the largest
+ * target seen, grown on demand). */
+int32_t cenote_renderer_create(cenote_context* ctx, uint32_t max_bounces, uint32_t light_sampling,
+                               uint32_t capacity, cenote_renderer** out);
+void cenote_renderer_destroy(cenote_renderer* r);
+/* Samples traced per wave: 0 picks automatically; 1 is the reference's
+ * one-sample waves. Results are bitwise identical for every setting. */
+int32_t cenote_renderer_set_samples_per_wave(cenote_renderer* r, uint32_t samples_per_wave);
+int32_t cenote_renderer_stats(cenote_renderer* r, cenote_stats* out);
+int32_t cenote_renderer_set_profiling(cenote_renderer* r, uint32_t flags);
+
+/* Renderer::render: one wave at sample index `sample`, RGBA f32 row-major,
+ * pixel (0,0) top-left, into caller-owned host memory (w·h·4 floats). */
+int32_t cenote_render_once(cenote_renderer* r, cenote_scene* scene, uint32_t width, uint32_t height,
+                           uint32_t sample, float* rgba_out);
+
+/* ---- film (render/film.rs) -------------------------------------------------------- */
+
+int32_t cenote_film_create(cenote_context* ctx, uint32_t width, uint32_t height, cenote_film** out);
+void cenote_film_destroy(cenote_film* film);
+int32_t cenote_film_reset(cenote_film* film);
+uint32_t cenote_film_samples(cenote_film* film);
+/* Renderer::accumulate: trace the film's next sample and add it (non-finite guarded). */
+int32_t cenote_accumulate(cenote_renderer* r, cenote_scene* scene, cenote_film* film);
+/* `count` consecutive accumulate calls in one submission (bitwise identical). */
+int32_t cenote_accumulate_n(cenote_renderer* r, cenote_scene* scene, cenote_film* film, uint32_t count);
+/* Film::averages: sums / samples into host memory; any pointer may be NULL.
+ * beauty/albedo/normal are w·h·4 floats, depth w·h floats. */
+int32_t cenote_film_averages(cenote_film* film, float* beauty, float* albedo, float* normal, float* depth);
+/* The raw running beauty sums (w·h·4 floats). */
+int32_t cenote_film_sums(cenote_film* film, float* beauty_sum);
+/* Device pointer to the beauty sums (float4 per pixel). */
+void* cenote_film_device_sums(cenote_film* film);
+
+/* ---- probes (test entry points; rng_test.slang and friends) ------------------------- */
+
+/* Sampler dump (shaders/rng_test.slang:23): sample_2d and sample_1d for sample
+ * indices 0..count-1 of one (pixel, dimension). points: 2·count floats. */
+int32_t cenote_probe_sampler(cenote_context* ctx, uint32_t pixel, uint32_t dimension, uint32_t count,
+                             float* points, float* values);
+/* Closure eval + pdf for n (wo, wi) pairs in the shading frame, FP32 on the
+ * device: f = 3 floats per pair, pdf = 1. */
+int32_t cenote_probe_bsdf(cenote_context* ctx, const cenote_material* material, const float* wo,
+                          const float* wi, uint32_t n, uint32_t exiting, float* f, float* pdf);
+/* Closure sampling: u = (u_lobe, u.x, u.y) per entry; wi = 3 floats, pdf, lobe. */
+int32_t cenote_probe_bsdf_sample(cenote_context* ctx, const cenote_material* material, const float* wo,
+                                 const float* u, uint32_t n, uint32_t exiting, float* wi, float* pdf,
+                                 uint32_t* lobe);
+/* Closest hit for n rays (all instances visible): hits = (instance, primitive,
+ * b1 bits, b2 bits) per ray, instance 0xffffffff on a miss; t = hit distance. */
+int32_t cenote_probe_intersect(cenote_scene* scene, const float* origins, const float* directions, uint32_t n,
+                               uint32_t* hits, float* t);
+/* Shadow query: attenuation ≥ 0 when the (instance, primitive) target — or
+ * nothing, for target instance 0xffffffff — is the closest hit within tmax;
+ * -1 when occluded. */
+int32_t cenote_probe_shadow(cenote_scene* scene, const float* origins, const float* directions,
+                            const float* tmax, const uint32_t* targets, uint32_t n, float* out);
+/* Environment importance sampling (environment.slang:94-107) for n uniform
+ * pairs: direction (3 floats), pdf, and the sampled (row, column). */
+int32_t cenote_probe_env_sample(cenote_scene* scene, const float* u, uint32_t n, float* directions,
+                                float* pdf, uint32_t* row_col);
+/* Environment pdf for n directions (environment.slang:111-120). */
+int32_t cenote_probe_env_pdf(cenote_scene* scene, const float* directions, uint32_t n, float* pdf);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* CENOTE_C_H */

@@ -1,0 +1,26 @@
+// Host definitions of the handful of CUDA device intrinsics the traversal
+// header uses, so tests can compile cenote_b200/csrc/traverse.cuh with g++
+// and run the exact kernel traversal code on the CPU. Compiled with
+// -ffp-contract=off, the *_rn helpers round exactly like the device ones.
+#pragma once
+#include <cstdint>
+#include <cstring>
+#include <cmath>
+#include <cuda_runtime.h>
+
+inline float __fadd_rn(float a, float b) { return a + b; }
+inline float __fsub_rn(float a, float b) { return a - b; }
+inline float __fmul_rn(float a, float b) { return a * b; }
+inline float __fdiv_rn(float a, float b) { return a / b; }
+inline double __dadd_rn(double a, double b) { return a + b; }
+inline double __dsub_rn(double a, double b) { return a - b; }
+inline double __dmul_rn(double a, double b) { return a * b; }
+inline double __ddiv_rn(double a, double b) { return a / b; }
+inline float __double2float_rn(double d) { return float(d); }
+inline float __uint_as_float(uint32_t u) { float f; std::memcpy(&f, &u, 4); return f; }
+inline uint32_t __float_as_uint(float f) { uint32_t u; std::memcpy(&u, &f, 4); return u; }
+inline int __clz(uint32_t x) { return x ? __builtin_clz(x) : 32; }
+inline int __popc(uint32_t x) { return __builtin_popcount(x); }
+inline int __ffs(uint32_t x) { return __builtin_ffs(int(x)); }
+inline uint32_t min(uint32_t a, uint32_t b) { return a < b ? a : b; }
+template <class T> inline T __ldg(const T* p) { return *p; }

@@ -1,0 +1,137 @@
+"""The kernels' BVH on the CPU: the library's wide-BVH builder and the device
+traversal header (cenote_b200/csrc/traverse.cuh), compiled for the host
+through tests/host/cuda_host_shim.h, must produce a well-formed tree (every
+index in range, every triangle in exactly one leaf) and commit bit-identical
+closest hits to the oracle's independent binary BVH on the same rays.
+
+This validates traversal logic and memory safety before any GPU runs it; the
+GPU tests repeat the comparison on the device."""
+import pathlib
+import subprocess
+
+import numpy as np
+import pytest
+
+import oracle
+from cenote_b200 import scenes
+
+ROOT = pathlib.Path(__file__).resolve().parents[1]
+CSRC = ROOT / "cenote_b200" / "csrc"
+HOST = ROOT / "tests" / "host"
+
+
+def cuda_include():
+    import shutil
+    nvcc = shutil.which("nvcc") or "/usr/local/cuda/bin/nvcc"
+    return pathlib.Path(nvcc).resolve().parent.parent / "include"
+
+
+@pytest.fixture(scope="module")
+def harness(tmp_path_factory):
+    out = tmp_path_factory.mktemp("host") / "traverse_host"
+    cmd = ["g++", "-O2", "-std=c++17", "-ffp-contract=off", f"-I{HOST}", f"-I{CSRC}", f"-I{cuda_include()}",
+           "-include", str(HOST / "cuda_host_shim.h"), str(HOST / "traverse_host.cpp"), str(CSRC / "bvh_build.cpp"),
+           "-o", str(out), "-lpthread"]
+    subprocess.run(cmd, check=True)
+    return out
+
+
+def world_triangles(spec):
+    """World-space corners in the library's f32 operation order (glam's
+    transform_point3: ((x·p.x + y·p.y) + z·p.z) + w)."""
+    out = []
+    for inst, o in enumerate(spec.objects):
+        m = np.asarray(o.transform, np.float32).reshape(3, 4)
+        p = o.mesh.positions.astype(np.float32)
+        w = np.empty_like(p)
+        for r in range(3):
+            w[:, r] = ((m[r, 0] * p[:, 0] + m[r, 1] * p[:, 1]) + m[r, 2] * p[:, 2]) + m[r, 3]
+        c = w[o.mesh.indices]  # (T, 3, 3)
+        ids = np.zeros((len(c), 3), np.uint32)
+        ids[:, 0] = inst
+        ids[:, 1] = np.arange(len(c))
+        ids[:, 2] = 0xFF | 0x100
+        out.append((c.reshape(-1, 9), ids))
+    return np.concatenate([c for c, _ in out]), np.concatenate([i for _, i in out])
+
+
+def random_rays(spec, n, seed):
+    rng = np.random.default_rng(seed)
+    tris, _ = world_triangles(spec)
+    pts = tris.reshape(-1, 3)
+    lo, hi = pts.min(0), pts.max(0)
+    org = (lo + (hi - lo) * rng.random((n, 3))).astype(np.float32)
+    d = rng.normal(size=(n, 3))
+    # A few axis-aligned and exactly-zero components to exercise the slab edge cases.
+    d[: n // 16, 1] = 0.0
+    d[n // 16: n // 8, :2] = 0.0
+    d = (d / np.linalg.norm(d, axis=1, keepdims=True)).astype(np.float32)
+    return org, d
+
+
+def run_harness(harness, tmp_path, tris, ids, org, d):
+    tb = tmp_path / "tris.bin"
+    with open(tb, "wb") as f:
+        f.write(np.uint32(len(tris)).tobytes())
+        rec = np.concatenate([tris.view(np.uint32), ids], axis=1).astype(np.uint32)
+        f.write(rec.tobytes())
+    rb = tmp_path / "rays.bin"
+    with open(rb, "wb") as f:
+        f.write(np.uint32(len(org)).tobytes())
+        f.write(np.concatenate([org, d], axis=1).astype(np.float32).tobytes())
+    hb = tmp_path / "hits.bin"
+    r = subprocess.run([str(harness), str(tb), str(rb), str(hb)], capture_output=True, text=True)
+    assert r.returncode == 0, r.stdout + r.stderr
+    h = np.fromfile(hb, np.uint32).reshape(-1, 5)
+    return h[:, :4], h[:, 4].view(np.float32), r.stdout
+
+
+@pytest.mark.parametrize("name", ["cornell", "chart"])
+def test_wide_bvh_matches_oracle_hits(harness, tmp_path, name):
+    spec = scenes.cornell() if name == "cornell" else scenes.chart(env_size=(8, 4))
+    tris, ids = world_triangles(spec)
+    org, d = random_rays(spec, 20000, seed=1)
+    hits, t, log = run_harness(harness, tmp_path, tris, ids, org, d)
+    ref_hits, ref_t = oracle.OracleScene(spec).intersect(org, d)
+    assert np.array_equal(hits, ref_hits), log
+    assert np.array_equal(t.view(np.uint32), ref_t.view(np.uint32))
+    assert (hits[:, 0] != 0xFFFFFFFF).mean() > 0.3
+
+
+def test_wide_bvh_random_soup(harness, tmp_path):
+    """A dense random triangle soup: many overlapping boxes, deep trees."""
+    rng = np.random.default_rng(7)
+    n = 30000
+    c = rng.random((n, 1, 3)) * 10.0 + rng.normal(scale=0.05, size=(n, 3, 3))
+    tris = c.astype(np.float32).reshape(n, 9)
+    ids = np.zeros((n, 3), np.uint32)
+    ids[:, 1] = np.arange(n)
+    ids[:, 2] = 0x1FF
+    org = (rng.random((5000, 3)) * 10.0).astype(np.float32)
+    d = rng.normal(size=(5000, 3))
+    d = (d / np.linalg.norm(d, axis=1, keepdims=True)).astype(np.float32)
+    hits, t, _ = run_harness(harness, tmp_path, tris, ids, org, d)
+    # Brute force on the CPU with the oracle's watertight test, via a one-object scene.
+    mesh = scenes.Mesh(tris.reshape(-1, 3), np.tile([0, 1, 0], (3 * n, 1)).astype(np.float32),
+                       np.zeros((3 * n, 2), np.float32), np.arange(3 * n, dtype=np.uint32).reshape(n, 3))
+    spec = scenes.SceneSpec("soup", [scenes.Object(mesh, scenes.rows(np.eye(4)), scenes.matte((0.5, 0.5, 0.5)))],
+                            scenes.Camera((0, 0, 20), (5, 5, 5)), scenes.Environment.constant((0, 0, 0)), 8, 8, 1, 1)
+    ref_hits, ref_t = oracle.OracleScene(spec).intersect(org, d)
+    assert np.array_equal(hits, ref_hits)
+    assert np.array_equal(t.view(np.uint32), ref_t.view(np.uint32))
+
+
+def test_degenerate_inputs(harness, tmp_path):
+    """One triangle; coincident centroids; a flat (zero-extent) axis."""
+    one = np.array([[0, 0, 0, 1, 0, 0, 0, 1, 0]], np.float32)
+    same = np.tile(one, (40, 1))
+    flat = np.random.default_rng(3).random((500, 9)).astype(np.float32)
+    flat[:, 2::3] = 0.25
+    for tris in (one, same, flat):
+        ids = np.zeros((len(tris), 3), np.uint32)
+        ids[:, 1] = np.arange(len(tris))
+        ids[:, 2] = 0x1FF
+        org = np.array([[0.2, 0.2, 1.0], [0.2, 0.2, -1.0], [5, 5, 5]], np.float32)
+        d = np.array([[0, 0, -1], [0, 0, 1], [0, 0, 1]], np.float32)
+        hits, t, _ = run_harness(harness, tmp_path, tris, ids, org, d)
+        assert hits[2, 0] == 0xFFFFFFFF
