@@ -277,6 +277,10 @@ bool camera_valid(const cenote_camera& cam) {
 }  // namespace
 
 struct cenote_context {
+    // Handles made from this context hold a reference; the context is freed
+    // when cenote_context_destroy has been called and the last one is gone,
+    // so destroy order never leaves a dangling pointer.
+    std::atomic<int> refs{1};
     int device = 0;
     cudaStream_t stream = nullptr;
     cudaEvent_t sync_ev = nullptr;
@@ -372,6 +376,23 @@ struct cenote_film {
     DeviceBuffer sum, avg;
 };
 
+namespace {
+void free_context(cenote_context* ctx) {
+    cudaSetDevice(ctx->device);
+    if (ctx->stream) cudaStreamSynchronize(ctx->stream);
+    ctx->tables.release();
+    if (ctx->sync_ev) cudaEventDestroy(ctx->sync_ev);
+    if (ctx->t0) cudaEventDestroy(ctx->t0);
+    if (ctx->t1) cudaEventDestroy(ctx->t1);
+    if (ctx->stream) cudaStreamDestroy(ctx->stream);
+    delete ctx;
+}
+void retain(cenote_context* ctx) { ctx->refs.fetch_add(1); }
+void release(cenote_context* ctx) {
+    if (ctx->refs.fetch_sub(1) == 1) free_context(ctx);
+}
+}  // namespace
+
 extern "C" {
 
 const char* cenote_last_error(void) { return g_error.c_str(); }
@@ -402,15 +423,7 @@ int32_t cenote_context_create(const cenote_options* options, cenote_context** ou
 }
 
 void cenote_context_destroy(cenote_context* ctx) {
-    if (!ctx) return;
-    cudaSetDevice(ctx->device);
-    if (ctx->stream) cudaStreamSynchronize(ctx->stream);
-    ctx->tables.release();
-    if (ctx->sync_ev) cudaEventDestroy(ctx->sync_ev);
-    if (ctx->t0) cudaEventDestroy(ctx->t0);
-    if (ctx->t1) cudaEventDestroy(ctx->t1);
-    if (ctx->stream) cudaStreamDestroy(ctx->stream);
-    delete ctx;
+    if (ctx) release(ctx);
 }
 
 void* cenote_context_stream(cenote_context* ctx) { return ctx ? static_cast<void*>(ctx->stream) : nullptr; }
@@ -613,15 +626,18 @@ int32_t cenote_scene_create(cenote_context* ctx, const cenote_object* objects, u
     ds.tri_count = uint32_t(bvh.tris.size() / 12);
     ds.has_nonopaque = nonopaque ? 1u : 0u;
     sc->prep_ms[2] = float(std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t_start).count());
+    retain(ctx);
     *out = sc.release();
     return CENOTE_OK;
 }
 
 void cenote_scene_destroy(cenote_scene* scene) {
     if (!scene) return;
-    cudaSetDevice(scene->ctx->device);
-    cudaStreamSynchronize(scene->ctx->stream);
+    cenote_context* ctx = scene->ctx;
+    cudaSetDevice(ctx->device);
+    cudaStreamSynchronize(ctx->stream);
     delete scene;
+    release(ctx);
 }
 
 int32_t cenote_scene_set_camera(cenote_scene* scene, const cenote_camera* camera) {
@@ -684,15 +700,18 @@ int32_t cenote_renderer_create(cenote_context* ctx, uint32_t max_bounces, uint32
     CN_CUDA(r->tally.alloc(8 * 8));
     CN_CUDA(cudaMemset(r->tally.ptr, 0, 64));
     r->pool.counters = r->counters.as<uint32_t>();
+    retain(ctx);
     *out = r.release();
     return CENOTE_OK;
 }
 
 void cenote_renderer_destroy(cenote_renderer* r) {
     if (!r) return;
-    cudaSetDevice(r->ctx->device);
-    cudaStreamSynchronize(r->ctx->stream);
+    cenote_context* ctx = r->ctx;
+    cudaSetDevice(ctx->device);
+    cudaStreamSynchronize(ctx->stream);
     delete r;
+    release(ctx);
 }
 
 int32_t cenote_renderer_set_samples_per_wave(cenote_renderer* r, uint32_t spw) {
@@ -728,15 +747,18 @@ int32_t cenote_film_create(cenote_context* ctx, uint32_t width, uint32_t height,
     CN_CUDA(f->sum.alloc(px * 16));
     CN_CUDA(f->avg.alloc(px * 16));
     CN_CUDA(cudaMemsetAsync(f->sum.ptr, 0, px * 16, ctx->stream));
+    retain(ctx);
     *out = f.release();
     return CENOTE_OK;
 }
 
 void cenote_film_destroy(cenote_film* film) {
     if (!film) return;
-    cudaSetDevice(film->ctx->device);
-    cudaStreamSynchronize(film->ctx->stream);
+    cenote_context* ctx = film->ctx;
+    cudaSetDevice(ctx->device);
+    cudaStreamSynchronize(ctx->stream);
     delete film;
+    release(ctx);
 }
 
 int32_t cenote_film_reset(cenote_film* film) {

@@ -117,7 +117,7 @@ __global__ void __launch_bounds__(BLOCK) k_raygen(PathPool pool, WaveParams wp) 
 template <bool COUNT>
 __global__ void __launch_bounds__(BLOCK) k_intersect(DeviceScene scene, PathPool pool, uint32_t bounce, uint32_t n0) {
     uint32_t visits = 0, tests = 0;
-    const uint32_t count = bounce == 0 ? n0 : pool.counters[CTR_RAYS + bounce];
+    const uint32_t count = min(bounce == 0 ? n0 : pool.counters[CTR_RAYS + bounce], pool.capacity);
     const uint32_t* queue = pool.queue[bounce & 1u];
     const uint32_t mask = bounce == 0 ? RAY_MASK_CAMERA : RAY_MASK_ALL;
     for (;;) {
@@ -239,7 +239,7 @@ __device__ __forceinline__ void load_material(const Material* rec, Material& m) 
 
 __global__ void __launch_bounds__(BLOCK) k_shade(DeviceScene scene, PathPool pool, uint32_t bounce,
                                                  uint32_t max_bounces, uint32_t light_sampling, uint32_t n0) {
-    const uint32_t count = bounce == 0 ? n0 : pool.counters[CTR_RAYS + bounce];
+    const uint32_t count = min(bounce == 0 ? n0 : pool.counters[CTR_RAYS + bounce], pool.capacity);
     const uint32_t* queue = pool.queue[bounce & 1u];
     uint32_t* next_queue = pool.queue[(bounce + 1u) & 1u];
     for (;;) {

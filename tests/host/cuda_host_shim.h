@@ -24,3 +24,6 @@ inline int __popc(uint32_t x) { return __builtin_popcount(x); }
 inline int __ffs(uint32_t x) { return __builtin_ffs(int(x)); }
 inline uint32_t min(uint32_t a, uint32_t b) { return a < b ? a : b; }
 template <class T> inline T __ldg(const T* p) { return *p; }
+inline void sincosf(float x, float* s, float* c) { *s = std::sin(x); *c = std::cos(x); }
+inline float rsqrtf(float x) { return 1.0f / std::sqrt(x); }
+inline float saturate_host(float x) { return x < 0 ? 0 : (x > 1 ? 1 : x); }
