@@ -17,6 +17,7 @@ raises.
 from __future__ import annotations
 
 import ctypes as C
+import os
 from pathlib import Path
 
 import numpy as np
@@ -28,7 +29,8 @@ __all__ = ["CenoteError", "Context", "Scene", "Renderer", "Film", "library", "sc
            "LIGHT_SAMPLING_BSDF", "LIGHT_SAMPLING_NEE", "EXPORTED_SYMBOLS"]
 
 LIGHT_SAMPLING_MIS, LIGHT_SAMPLING_BSDF, LIGHT_SAMPLING_NEE = 0, 1, 2
-LIB_PATH = Path(__file__).resolve().parent / "libcenote_b200.so"
+# CENOTE_B200_LIB selects another build of the same library (tuning variants).
+LIB_PATH = Path(os.environ.get("CENOTE_B200_LIB", Path(__file__).resolve().parent / "libcenote_b200.so"))
 
 STATUS = {
     0: "ok", -1: "invalid argument", -2: "device error", -3: "no capable GPU", -4: "allocation failed",

@@ -58,21 +58,27 @@ def _run(cmd):
     return r
 
 
-def build(verbose: bool = False, ptxas_info: bool = False) -> Path:
-    OUT.mkdir(exist_ok=True)
+def build(verbose: bool = False, ptxas_info: bool = False, defines=(), out_dir: Path | None = None,
+          lib: Path | None = None) -> Path:
+    """Compile and link. `defines`, `out_dir` and `lib` build tuning variants
+    of the library side by side (objects and .so elsewhere than the default)."""
+    out = Path(out_dir) if out_dir else OUT
+    lib = Path(lib) if lib else LIB
+    out.mkdir(parents=True, exist_ok=True)
     nvcc = _nvcc()
     inc = _tables_blob().parent
+    dflags = [f"-D{d}" for d in defines]
     headers = list(CSRC.glob("*.h")) + list(CSRC.glob("*.cuh")) + [PKG.parent / "include" / "cenote_c.h"]
     newest_header = max(p.stat().st_mtime for p in headers)
     objs = []
     for src in CU_SOURCES:
         s = CSRC / src
-        o = OUT / (src + ".o")
+        o = out / (src + ".o")
         objs.append(o)
         if o.exists() and o.stat().st_mtime > max(s.stat().st_mtime, newest_header) and not ptxas_info:
             continue
         cmd = [nvcc, *ARCH, "-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "--expt-relaxed-constexpr",
-               "-c", str(s), "-o", str(o)]
+               *dflags, "-c", str(s), "-o", str(o)]
         if ptxas_info:
             cmd.insert(1, "-Xptxas=-v")
         r = _run(cmd)
@@ -80,16 +86,16 @@ def build(verbose: bool = False, ptxas_info: bool = False) -> Path:
             sys.stderr.write(r.stderr)
     for src in CPP_SOURCES:
         s = CSRC / src
-        o = OUT / (src + ".o")
+        o = out / (src + ".o")
         objs.append(o)
         if o.exists() and o.stat().st_mtime > max(s.stat().st_mtime, newest_header,
                                                   (inc / "tables_blob.inc").stat().st_mtime):
             continue
         _run(["g++", "-O2", "-std=c++17", "-fPIC", "-ffp-contract=off", "-Wall", "-Wextra", "-Wno-unused-parameter",
               f"-I{_cuda_include(nvcc)}", f"-I{inc}", "-c", str(s), "-o", str(o)])
-    if not LIB.exists() or LIB.stat().st_mtime < max(o.stat().st_mtime for o in objs):
-        _run([nvcc, *ARCH, "-shared", "-o", str(LIB), *map(str, objs), "-lpthread"])
-    return LIB
+    if not lib.exists() or lib.stat().st_mtime < max(o.stat().st_mtime for o in objs):
+        _run([nvcc, *ARCH, "-shared", "-o", str(lib), *map(str, objs), "-lpthread"])
+    return lib
 
 
 if __name__ == "__main__":

@@ -537,6 +537,17 @@ int32_t cenote_scene_create(cenote_context* ctx, const cenote_object* objects, u
                                 cudaMemcpyHostToDevice, ctx->stream));
         CN_CUDA(cudaMemcpyAsync(btris->ptr, bvh.tris.data(), bvh.tris.size() * 4, cudaMemcpyHostToDevice, ctx->stream));
     }
+    // Each emissive triangle's leaf index, for the shadow query's target test.
+    std::vector<uint32_t> light_leaf(std::max<size_t>(1, sc->lights.size()), 0xffffffffu);
+    for (size_t leaf = 0; leaf < bvh.tris.size() / 12; ++leaf) {
+        uint32_t inst, prim;
+        std::memcpy(&inst, &bvh.tris[12 * leaf + 3], 4);
+        std::memcpy(&prim, &bvh.tris[12 * leaf + 7], 4);
+        if (geoms[inst].light != LIGHT_NONE) light_leaf[geoms[inst].light + prim] = uint32_t(leaf);
+    }
+    DeviceBuffer* bleaf = sc->add(light_leaf.size() * 4, &err);
+    CN_CUDA(err);
+    CN_CUDA(cudaMemcpyAsync(bleaf->ptr, light_leaf.data(), light_leaf.size() * 4, cudaMemcpyHostToDevice, ctx->stream));
     DeviceBuffer* bgeo = sc->add(geoms.size() * sizeof(GeomRecord), &err);
     CN_CUDA(err);
     CN_CUDA(cudaMemcpyAsync(bgeo->ptr, geoms.data(), geoms.size() * sizeof(GeomRecord), cudaMemcpyHostToDevice,
@@ -625,6 +636,7 @@ int32_t cenote_scene_create(cenote_context* ctx, const cenote_object* objects, u
     ds.node_count = uint32_t(bvh.nodes.size());
     ds.tri_count = uint32_t(bvh.tris.size() / 12);
     ds.has_nonopaque = nonopaque ? 1u : 0u;
+    ds.light_leaf = bleaf->as<uint32_t>();
     sc->prep_ms[2] = float(std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t_start).count());
     retain(ctx);
     *out = sc.release();

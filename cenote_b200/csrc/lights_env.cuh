@@ -19,14 +19,16 @@ struct LightConn {
     float pdf;
     bool delta;
     uint32_t instance, primitive;
+    uint32_t record;  // the light record drawn (slot or its alias)
 };
 
 __device__ __forceinline__ LightConn sample_lights(const LightRecord* lights, uint32_t count, float u, float2 up,
                                                    float3 from) {
     float scaled = u * float(count);
     uint32_t slot = min(uint32_t(scaled), count - 1);
-    const LightRecord* L = lights + slot;
-    if (scaled - float(slot) >= __ldg(&L->alias_threshold)) L = lights + __ldg(&L->alias_index);
+    uint32_t rec = slot;
+    if (scaled - float(slot) >= __ldg(&lights[slot].alias_threshold)) rec = __ldg(&lights[slot].alias_index);
+    const LightRecord* L = lights + rec;
     // The record in five 16-byte loads.
     const float4* q = reinterpret_cast<const float4*>(L);
     float4 a = __ldg(q), b = __ldg(q + 1), c = __ldg(q + 2), d = __ldg(q + 3), e = __ldg(q + 4);
@@ -41,6 +43,7 @@ __device__ __forceinline__ LightConn sample_lights(const LightRecord* lights, ui
     r.delta = kind != KIND_TRIANGLE;
     r.instance = __float_as_uint(d.w);
     r.primitive = __float_as_uint(e.y);
+    r.record = rec;
     if (kind == KIND_TRIANGLE) {
         float su = sqrtf(up.x);
         float b1 = 1.0f - su, b2 = up.y * su;

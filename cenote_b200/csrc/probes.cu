@@ -7,6 +7,7 @@
 #include "lights_env.cuh"
 #include "openpbr.cuh"
 #include "sampler.cuh"
+#include "shadow.cuh"
 #include "traverse.cuh"
 
 namespace cn {
@@ -69,37 +70,17 @@ __global__ void k_probe_shadow(DeviceScene scene, const float3* org, const float
     uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
     Ray ray = make_ray(org[i], dir[i]);
-    float tmax = tmaxs[i];
     uint32_t light = targets[i].x, lprim = targets[i].y;
-    float atten = 1.0f;
-    bool occluded = false;
-    uint32_t bi = LIGHT_NONE, bp = 0;
-    bool ok = traverse(scene, ray, tmax, [&](uint32_t, float4 a, float4 b, float4 c, float& tm) {
-        float t, b1, b2;
-        if (!tri_hit(ray, a, b, c, tm, t, b1, b2)) return false;
-        uint32_t inst = __float_as_uint(a.w), prim = __float_as_uint(b.w);
-        if (!(t < tm || (t == tm && (inst < bi || (inst == bi && prim < bp))))) return false;
-        bool target = inst == light && prim == lprim;
-        if (!(__float_as_uint(c.w) & TRI_OPAQUE) && !target) {
-            atten *= 1.0f - __ldg(&scene.materials[inst].opacity);
-            if (atten < 1e-4f) {
-                occluded = true;
-                return true;
-            }
-            return false;
-        }
-        if (light == LIGHT_NONE) {
-            occluded = true;
-            return true;
-        }
-        tm = t;
-        bi = inst;
-        bp = prim;
-        return false;
-    });
-    if (!ok) atomicOr(flag, 1u);
-    bool vis = !occluded && (bi == LIGHT_NONE || (bi == light && bp == lprim));
-    out[i] = vis ? atten : -1.0f;
+    // The leaf of an emissive target comes from its light record, as in the
+    // wavefront (GeometryRecord.light + primitive).
+    uint32_t leaf = 0xffffffffu;
+    if (light != LIGHT_NONE) {
+        uint32_t first = scene.geometry[light].light;
+        if (first != LIGHT_NONE) leaf = scene.light_leaf[first + lprim];
+    }
+    float a = shadow_query(scene, ray, tmaxs[i], light, lprim, leaf);
+    if (a == -2.0f) atomicOr(flag, 1u);
+    out[i] = a < 0.0f ? -1.0f : a;
 }
 
 __global__ void k_probe_env_sample(DeviceScene scene, const float2* u, uint32_t n, float3* dir, float* pdf,

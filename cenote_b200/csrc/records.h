@@ -96,6 +96,7 @@ struct DeviceScene {
     uint32_t node_count, tri_count;
     uint32_t has_nonopaque;
     uint32_t pad;
+    const uint32_t* light_leaf;  // per light record: its triangle's leaf index, ~0 for delta lights
 };
 
 // One queued shadow ray: 64 bytes, four 16-byte lanes.
@@ -107,7 +108,8 @@ struct alignas(16) ShadowRay {
     float contrib[3];
     uint32_t light;
     uint32_t primitive;
-    uint32_t pad[3];
+    uint32_t leaf;     // the target triangle's leaf index, ~0 when unknown or none
+    uint32_t pad[2];
 };
 
 }  // namespace cn

@@ -142,46 +142,63 @@ __device__ __forceinline__ uint32_t intersect_node(const WideNode* nodes, uint32
 // Walk the BVH, handing each candidate triangle to `visit(tri_index, v0, v1,
 // v2, tmax&)`, which may shrink tmax and returns true to stop the walk.
 // Returns false if a bound was exceeded (the caller flags an overflow).
-// With COUNT, node visits and triangle tests are tallied into *visits/*tests.
+//
+// Node groups and triangle groups share the stack (a group with bits 24-31
+// set is a node group; otherwise its low 24 bits are pending triangles).
+// When fewer than POSTPONE lanes of the warp have triangles to test, the
+// triangle group is pushed and the lane keeps walking nodes, so warps test
+// triangles together instead of idling through each other's leaves
+// (Ylitie et al. 2017, postponement).
+constexpr uint32_t POSTPONE = 6;
+
 template <bool COUNT = false, class Visit>
 __device__ __forceinline__ bool traverse(const DeviceScene& s, const Ray& r, float& tmax, Visit&& visit,
                                          uint32_t* visits = nullptr, uint32_t* tests = nullptr) {
     if (s.node_count == 0) return true;
     uint2 stack[TRAVERSAL_STACK];
     int sp = 0;
-    uint32_t g_base = 0;
-    uint32_t g_bits = (1u << (24u + r.oct_inv)) | 1u;  // the root: inner slot 0 of a virtual parent
-    const uint32_t max_iter = 2u * s.node_count + 64u;
+    uint2 g = make_uint2(0u, (1u << (24u + r.oct_inv)) | 1u);  // the root: inner slot 0 of a virtual parent
+    uint2 t = make_uint2(0u, 0u);
+    bool resumed;  // the triangle group came off the stack: never postpone it twice
+    const uint32_t max_iter = 4u * (s.node_count + s.tri_count) + 64u;
     for (uint32_t iter = 0; iter < max_iter; ++iter) {
-        if (g_bits & 0xff000000u) {
-            uint32_t pos = 31u - __clz(g_bits & 0xff000000u);
-            g_bits &= ~(1u << pos);
+        if (g.y & 0xff000000u) {
+            uint32_t pos = 31u - __clz(g.y & 0xff000000u);
+            g.y &= ~(1u << pos);
             uint32_t slot = (pos - 24u) ^ r.oct_inv;
-            uint32_t ni = g_base + __popc(g_bits & 0xffu & ((1u << slot) - 1u));
-            if (g_bits & 0xff000000u) {
+            uint32_t ni = g.x + __popc(g.y & 0xffu & ((1u << slot) - 1u));
+            if (g.y & 0xff000000u) {
                 if (sp >= TRAVERSAL_STACK) return false;
-                stack[sp++] = make_uint2(g_base, g_bits);
+                stack[sp++] = g;
             }
             uint32_t bc, bt, im;
             uint32_t hits = intersect_node(s.nodes, ni, r, tmax, bc, bt, im);
             if (COUNT) ++*visits;
-            g_base = bc;
-            g_bits = (hits & 0xff000000u) | im;
-            uint32_t tbits = hits & 0x00ffffffu;
-            while (tbits) {
-                uint32_t k = __ffs(tbits) - 1u;
-                tbits &= tbits - 1u;
-                uint32_t ti = bt + k;
-                const float4* tp = s.tris + 3u * ti;
-                float4 a = __ldg(tp), b = __ldg(tp + 1), c = __ldg(tp + 2);
-                if (COUNT) ++*tests;
-                if (visit(ti, a, b, c, tmax)) return true;
-            }
+            g = make_uint2(bc, (hits & 0xff000000u) | im);
+            t = make_uint2(bt, hits & 0x00ffffffu);
+            resumed = false;
         } else {
+            t = g;  // a postponed triangle group came off the stack
+            g = make_uint2(0u, 0u);
+            resumed = true;
+        }
+        while (t.y & 0x00ffffffu) {
+            if (!resumed && uint32_t(__popc(__activemask())) < POSTPONE) {
+                if (sp >= TRAVERSAL_STACK) return false;
+                stack[sp++] = t;
+                break;
+            }
+            uint32_t k = __ffs(t.y) - 1u;
+            t.y &= t.y - 1u;
+            uint32_t ti = t.x + k;
+            const float4* tp = s.tris + 3u * ti;
+            float4 a = __ldg(tp), b = __ldg(tp + 1), c = __ldg(tp + 2);
+            if (COUNT) ++*tests;
+            if (visit(ti, a, b, c, tmax)) return true;
+        }
+        if (!(g.y & 0xff000000u)) {
             if (sp == 0) return true;
-            --sp;
-            g_base = stack[sp].x;
-            g_bits = stack[sp].y;
+            g = stack[--sp];
         }
     }
     return false;

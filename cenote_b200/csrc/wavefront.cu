@@ -21,6 +21,7 @@
 #include "lights_env.cuh"
 #include "openpbr.cuh"
 #include "sampler.cuh"
+#include "shadow.cuh"
 #include "traverse.cuh"
 
 namespace cn {
@@ -28,6 +29,13 @@ namespace cn {
 namespace {
 
 constexpr int BLOCK = 128;
+
+// Minimum resident 128-thread blocks per SM for the shading kernel: the
+// register cap that trades spills against occupancy (5 → 96 registers,
+// measured fastest on the 1280x720 chart: 421 vs 414 at 4 and 391 uncapped).
+#ifndef CN_SHADE_MIN_BLOCKS
+#define CN_SHADE_MIN_BLOCKS 5
+#endif
 
 __device__ __forceinline__ uint32_t lane_id() { return threadIdx.x & 31u; }
 
@@ -237,7 +245,7 @@ __device__ __forceinline__ void load_material(const Material* rec, Material& m) 
     for (int k = 0; k < int(sizeof(Material) / 16); ++k) dst[k] = __ldg(src + k);
 }
 
-__global__ void __launch_bounds__(BLOCK) k_shade(DeviceScene scene, PathPool pool, uint32_t bounce,
+__global__ void __launch_bounds__(BLOCK, CN_SHADE_MIN_BLOCKS) k_shade(DeviceScene scene, PathPool pool, uint32_t bounce,
                                                  uint32_t max_bounces, uint32_t light_sampling, uint32_t n0) {
     const uint32_t count = min(bounce == 0 ? n0 : pool.counters[CTR_RAYS + bounce], pool.capacity);
     const uint32_t* queue = pool.queue[bounce & 1u];
@@ -311,53 +319,55 @@ __global__ void __launch_bounds__(BLOCK) k_shade(DeviceScene scene, PathPool poo
                     pool.rad[path] = make_float4(rad.x + contribution.x, rad.y + contribution.y, rad.z + contribution.z,
                                                  rad.w + 1.0f);
                 } else {
+                    // Next-event estimation (shade_surface.slang:363-446): one candidate,
+                    // the environment or a light from the list, then one shared
+                    // eval/pdf of the closure for it.
                     const float env_prob = scene.select_prob;
                     if (light_sampling != CENOTE_LIGHT_SAMPLING_BSDF && (scene.light_count > 0 || env_prob > 0.0f)) {
                         float u_light = sample_1d(pixel, sample, bounce_dim(bounce, NEE_LIGHT));
                         float2 u_point = sample_2d(pixel, sample, bounce_dim(bounce, NEE_POINT));
-                        float3 unshadowed = f3(0.0f);
-                        float3 sdir = f3(0.0f), sorg = f3(0.0f);
-                        float stmax = 1e30f;
-                        uint32_t slight = LIGHT_NONE, sprim = 0;
+                        float3 cdir, crad;
+                        float cpdf, nee, ctmax = 1e30f;
+                        bool cdelta = false;
+                        uint32_t clight = LIGHT_NONE, cprim = 0, cleaf = 0xffffffffu;
                         if (u_light < env_prob) {
                             EnvSample cand = env_sample(scene, u_point);
-                            float3 wl = frame.to_local(cand.direction);
-                            bool through = dot(cand.direction, sp.normal) < 0.0f;
-                            if (cand.pdf > 0.0f && wl.z != 0.0f && (wl.z < 0.0f) == through) {
-                                float nee = env_prob * cand.pdf;
-                                float spdf = bsdf_pdf(cl, wl, wo);
-                                float w = light_sampling == CENOTE_LIGHT_SAMPLING_MIS ? power_heuristic(nee, spdf) : 1.0f;
-                                unshadowed = thr * cand.radiance * eval_bsdf(cl, wl, wo) * fabsf(wl.z) * (w / nee);
-                                sorg = through ? sp.below : sp.position;
-                                sdir = cand.direction;
-                            }
+                            cdir = cand.direction;
+                            crad = cand.radiance;
+                            cpdf = cand.pdf;
+                            nee = env_prob * cand.pdf;
                         } else {
                             float u_list = (u_light - env_prob) / (1.0f - env_prob);
                             LightConn cand = sample_lights(scene.lights, scene.light_count, u_list, u_point, sp.position);
-                            float3 wl = frame.to_local(cand.direction);
-                            bool through = dot(cand.direction, sp.normal) < 0.0f;
-                            if (cand.pdf > 0.0f && wl.z != 0.0f && (wl.z < 0.0f) == through) {
-                                float nee = (1.0f - env_prob) * cand.pdf;
-                                float w = !cand.delta && light_sampling == CENOTE_LIGHT_SAMPLING_MIS
-                                              ? power_heuristic(nee, bsdf_pdf(cl, wl, wo))
-                                              : 1.0f;
-                                unshadowed = thr * cand.radiance * eval_bsdf(cl, wl, wo) * fabsf(wl.z) * (w / nee);
-                                sorg = through ? sp.below : sp.position;
-                                slight = cand.instance;
-                                sprim = cand.primitive;
-                                sdir = cand.direction;
-                                stmax = cand.tmax;
-                            }
+                            cdir = cand.direction;
+                            crad = cand.radiance;
+                            cpdf = cand.pdf;
+                            nee = (1.0f - env_prob) * cand.pdf;
+                            cdelta = cand.delta;
+                            clight = cand.instance;
+                            cprim = cand.primitive;
+                            ctmax = cand.tmax;
+                            if (!cand.delta) cleaf = __ldg(scene.light_leaf + cand.record);
                         }
-                        if (any_pos(unshadowed)) {
-                            push_shadow = true;
-                            sr.org[0] = sorg.x; sr.org[1] = sorg.y; sr.org[2] = sorg.z;
-                            sr.tmax = stmax;
-                            sr.dir[0] = sdir.x; sr.dir[1] = sdir.y; sr.dir[2] = sdir.z;
-                            sr.path = path;
-                            sr.contrib[0] = unshadowed.x; sr.contrib[1] = unshadowed.y; sr.contrib[2] = unshadowed.z;
-                            sr.light = slight;
-                            sr.primitive = sprim;
+                        float3 wl = frame.to_local(cdir);
+                        bool through = dot(cdir, sp.normal) < 0.0f;
+                        if (cpdf > 0.0f && wl.z != 0.0f && (wl.z < 0.0f) == through) {
+                            // A delta light has no competing BSDF strategy: weight 1.
+                            bool mis = !cdelta && light_sampling == CENOTE_LIGHT_SAMPLING_MIS;
+                            float w = mis ? power_heuristic(nee, bsdf_pdf(cl, wl, wo)) : 1.0f;
+                            float3 unshadowed = thr * crad * eval_bsdf(cl, wl, wo) * fabsf(wl.z) * (w / nee);
+                            if (any_pos(unshadowed)) {
+                                float3 sorg = through ? sp.below : sp.position;
+                                push_shadow = true;
+                                sr.org[0] = sorg.x; sr.org[1] = sorg.y; sr.org[2] = sorg.z;
+                                sr.tmax = ctmax;
+                                sr.dir[0] = cdir.x; sr.dir[1] = cdir.y; sr.dir[2] = cdir.z;
+                                sr.path = path;
+                                sr.contrib[0] = unshadowed.x; sr.contrib[1] = unshadowed.y; sr.contrib[2] = unshadowed.z;
+                                sr.light = clight;
+                                sr.primitive = cprim;
+                                sr.leaf = cleaf;
+                            }
                         }
                     }
                     float u_lobe = sample_1d(pixel, sample, bounce_dim(bounce, BSDF_LOBE));
@@ -431,40 +441,12 @@ __global__ void __launch_bounds__(BLOCK) k_shadow(DeviceScene scene, PathPool po
         uint32_t path = __float_as_uint(q1.w);
         uint32_t light = __float_as_uint(q2.w), lprim = __float_as_uint(q3.x);
         Ray ray = make_ray(xyz(q0), xyz(q1));
-        float tmax = q0.w;
-        float atten = 1.0f;
-        bool occluded = false;
-        uint32_t best_inst = LIGHT_NONE, best_prim = 0;
-        bool ok = traverse<COUNT>(scene, ray, tmax, [&](uint32_t, float4 a, float4 b, float4 c, float& tm) {
-            float t, b1, b2;
-            if (!tri_hit(ray, a, b, c, tm, t, b1, b2)) return false;
-            uint32_t inst = __float_as_uint(a.w), prim = __float_as_uint(b.w);
-            if (!(t < tm || (t == tm && (inst < best_inst || (inst == best_inst && prim < best_prim))))) return false;
-            uint32_t flags = __float_as_uint(c.w);
-            bool target = inst == light && prim == lprim;
-            if (!(flags & TRI_OPAQUE) && !target) {
-                atten *= 1.0f - __ldg(&scene.materials[inst].opacity);
-                if (atten < 1e-4f) {
-                    occluded = true;
-                    return true;
-                }
-                return false;
-            }
-            if (light == LIGHT_NONE) {  // nothing may commit: the first opaque hit decides
-                occluded = true;
-                return true;
-            }
-            tm = t;
-            best_inst = inst;
-            best_prim = prim;
-            return false;
-        }, &visits, &tests);
-        if (!ok) {
+        float atten = shadow_query<COUNT>(scene, ray, q0.w, light, lprim, __float_as_uint(q3.y), &visits, &tests);
+        if (atten == -2.0f) {
             flag_overflow(pool.counters);
             continue;
         }
-        if (occluded) continue;
-        if (best_inst == LIGHT_NONE || (best_inst == light && best_prim == lprim)) {
+        if (atten >= 0.0f) {
             float4 r = pool.rad[path];
             pool.rad[path] = make_float4(r.x + q2.x * atten, r.y + q2.y * atten, r.z + q2.z * atten, r.w);
         }

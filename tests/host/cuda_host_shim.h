@@ -27,3 +27,16 @@ template <class T> inline T __ldg(const T* p) { return *p; }
 inline void sincosf(float x, float* s, float* c) { *s = std::sin(x); *c = std::cos(x); }
 inline float rsqrtf(float x) { return 1.0f / std::sqrt(x); }
 inline float saturate_host(float x) { return x < 0 ? 0 : (x > 1 ? 1 : x); }
+// A pseudo-random lane count, so host runs exercise the traversal's
+// postponement path (its result must not depend on those decisions).
+// CN_HOST_LANES=1 reports a lone lane every time (the worst case for
+// postponement, which must still terminate).
+#include <cstdlib>
+inline unsigned __activemask() {
+    static const bool lone = std::getenv("CN_HOST_LANES") && std::atoi(std::getenv("CN_HOST_LANES")) == 1;
+    if (lone) return 1u;
+    static thread_local uint32_t x = 0x9e3779b9u;
+    x ^= x << 13; x ^= x >> 17; x ^= x << 5;
+    uint32_t lanes = x % 33u;
+    return lanes == 32u ? 0xffffffffu : ((1u << lanes) - 1u);
+}

@@ -69,7 +69,7 @@ def random_rays(spec, n, seed):
     return org, d
 
 
-def run_harness(harness, tmp_path, tris, ids, org, d):
+def run_harness(harness, tmp_path, tris, ids, org, d, lanes=None):
     tb = tmp_path / "tris.bin"
     with open(tb, "wb") as f:
         f.write(np.uint32(len(tris)).tobytes())
@@ -80,18 +80,23 @@ def run_harness(harness, tmp_path, tris, ids, org, d):
         f.write(np.uint32(len(org)).tobytes())
         f.write(np.concatenate([org, d], axis=1).astype(np.float32).tobytes())
     hb = tmp_path / "hits.bin"
-    r = subprocess.run([str(harness), str(tb), str(rb), str(hb)], capture_output=True, text=True)
+    import os
+    env = dict(os.environ)
+    if lanes is not None:
+        env["CN_HOST_LANES"] = str(lanes)
+    r = subprocess.run([str(harness), str(tb), str(rb), str(hb)], capture_output=True, text=True, env=env)
     assert r.returncode == 0, r.stdout + r.stderr
     h = np.fromfile(hb, np.uint32).reshape(-1, 5)
     return h[:, :4], h[:, 4].view(np.float32), r.stdout
 
 
+@pytest.mark.parametrize("lanes", [None, 1], ids=["random-lanes", "lone-lane"])
 @pytest.mark.parametrize("name", ["cornell", "chart"])
-def test_wide_bvh_matches_oracle_hits(harness, tmp_path, name):
+def test_wide_bvh_matches_oracle_hits(harness, tmp_path, name, lanes):
     spec = scenes.cornell() if name == "cornell" else scenes.chart(env_size=(8, 4))
     tris, ids = world_triangles(spec)
     org, d = random_rays(spec, 20000, seed=1)
-    hits, t, log = run_harness(harness, tmp_path, tris, ids, org, d)
+    hits, t, log = run_harness(harness, tmp_path, tris, ids, org, d, lanes)
     ref_hits, ref_t = oracle.OracleScene(spec).intersect(org, d)
     assert np.array_equal(hits, ref_hits), log
     assert np.array_equal(t.view(np.uint32), ref_t.view(np.uint32))
