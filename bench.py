@@ -282,7 +282,7 @@ def main():
         e2e_step = float(t.item())
     e2e_value = W * H * spp * world / (e2e_step / 1e3) / 1e6
 
-    # Roofline of the traversal kernels (intersect + shadow): SURVEY's
+    # Roofline of the traversal kernels (intersect + shadow): the
     # algorithmic bytes per ray = 32 (origin, direction) + 4 (queue slot) +
     # 16 (hit record) for extension rays or 64 (shadow record) for shadow
     # rays, plus 80 B per wide node visited and 36 B per triangle tested.
