@@ -114,6 +114,7 @@ EXPORTED_SYMBOLS = [
     "cenote_film_samples", "cenote_accumulate", "cenote_accumulate_n", "cenote_film_averages", "cenote_film_sums",
     "cenote_film_device_sums", "cenote_probe_sampler", "cenote_probe_bsdf", "cenote_probe_bsdf_sample",
     "cenote_probe_intersect", "cenote_probe_shadow", "cenote_probe_env_sample", "cenote_probe_env_pdf",
+    "cenote_env_tables_static",
 ]
 
 _lib = None
@@ -163,6 +164,7 @@ def library() -> C.CDLL:
         "cenote_probe_shadow": (I32, [P, P, P, P, P, U32, P]),
         "cenote_probe_env_sample": (I32, [P, P, U32, P, P, P]),
         "cenote_probe_env_pdf": (I32, [P, P, U32, P]),
+        "cenote_env_tables_static": (I32, [P, P, U32, U32, P, P, P, P]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(lib, name)
@@ -260,6 +262,18 @@ class Context:
         _check(library().cenote_probe_bsdf_sample(self._h, C.byref(m), _ptr(wo), _ptr(u), n, int(exiting), _ptr(wi),
                                                   _ptr(pdf), _ptr(lobe)))
         return wi, pdf, lobe
+
+
+def env_tables_static(ctx: "Context", texels_ptr: int, width: int, height: int, marginal_ptr: int,
+                      conditional_ptr: int, pdfs_ptr: int) -> float:
+    """The environment tables into caller-owned device memory, with no device
+    allocation inside the library (see cenote_env_tables_static in
+    include/cenote_c.h for who needs that and its size limit). Returns the
+    emitted power."""
+    power = C.c_double()
+    _check(library().cenote_env_tables_static(ctx.handle, texels_ptr, width, height, marginal_ptr, conditional_ptr,
+                                              pdfs_ptr, C.byref(power)))
+    return power.value
 
 
 class Scene:

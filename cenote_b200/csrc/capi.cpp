@@ -35,6 +35,7 @@ void probe_shadow(const DeviceScene& scene, const float3* org, const float3* dir
 void probe_env_sample(const DeviceScene& scene, const float2* u, uint32_t n, float3* dir, float* pdf, uint2* rc,
                       cudaStream_t s);
 void probe_env_pdf(const DeviceScene& scene, const float3* d, uint32_t n, float* pdf, cudaStream_t s);
+cudaError_t static_env_scratch(int device, double** out, size_t* max_texels, uint32_t* max_rows);
 }  // namespace cn
 
 using namespace cn;
@@ -1099,6 +1100,45 @@ int32_t cenote_probe_env_pdf(cenote_scene* sc, const float* directions, uint32_t
                               probe_env_pdf(sc->ds, static_cast<float3*>(i[0]), n, static_cast<float*>(o[0]),
                                             ctx->stream);
                           });
+}
+
+// ---- environment tables without device allocation ------------------------------------
+
+int32_t cenote_env_tables_static(cenote_context* ctx, const float* texels, uint32_t width, uint32_t height,
+                                 float* marginal, float* conditional, float* pdfs, double* power) {
+    CN_CHECK(ctx && texels && marginal && conditional && pdfs, CENOTE_E_INVALID_ARGUMENT, "null argument");
+    CN_CHECK(width > 0 && height > 0, CENOTE_E_INVALID_ARGUMENT, "zero-sized environment");
+    std::lock_guard<std::mutex> lock(ctx->mu);
+    CN_CUDA(cudaSetDevice(ctx->device));
+    double* scratch = nullptr;
+    size_t max_texels = 0;
+    uint32_t max_rows = 0;
+    CN_CUDA(static_env_scratch(ctx->device, &scratch, &max_texels, &max_rows));
+    const size_t n = size_t(width) * height;
+    CN_CHECK(n <= max_texels && height <= max_rows, CENOTE_E_INVALID_ARGUMENT,
+             "environment " + std::to_string(width) + "x" + std::to_string(height) +
+                 " exceeds the allocation-free build's limit of " + std::to_string(max_texels) + " texels and " +
+                 std::to_string(max_rows) + " rows");
+    // Row constants from the host's libm, as the allocating build computes them.
+    std::vector<double> rows(2 * size_t(height));
+    const double PI = 3.141592653589793;
+    for (uint32_t r = 0; r < height; ++r) {
+        rows[r] = std::sin((double(r) + 0.5) / double(height) * PI);
+        double th0 = double(r) / double(height) * PI, th1 = double(r + 1) / double(height) * PI;
+        rows[height + r] = 2.0 * PI / double(width) * (std::cos(th0) - std::cos(th1));
+    }
+    double* totals = scratch + 2 * n + 2 * size_t(height);
+    double* row_consts = totals + 2;
+    CN_CUDA(cudaMemcpyAsync(row_consts, rows.data(), rows.size() * 8, cudaMemcpyHostToDevice, ctx->stream));
+    launch_env_tables(reinterpret_cast<const float4*>(texels), row_consts, row_consts + height, width, height, scratch,
+                      marginal, conditional, pdfs, totals, ctx->stream);
+    CN_CUDA(cudaGetLastError());
+    double host_totals[2] = {0.0, 0.0};
+    CN_CUDA(cudaMemcpyAsync(host_totals, totals, sizeof host_totals, cudaMemcpyDeviceToHost, ctx->stream));
+    int32_t rc = wait_stream(ctx->stream, ctx->sync_ev, 600000.0);
+    if (rc != CENOTE_OK) return rc;
+    if (power) *power = host_totals[1];
+    return CENOTE_OK;
 }
 
 }  // extern "C"

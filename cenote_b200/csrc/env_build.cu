@@ -11,6 +11,7 @@
 // call the reference makes, so they are bit-identical inputs here.
 #include <cuda_runtime.h>
 #include <cstdint>
+#include <mutex>
 
 namespace cn {
 namespace {
@@ -136,6 +137,50 @@ void launch_env_tables(const float4* texels, const double* sin_theta, const doub
     k_env_rows<<<(h + 63) / 64, 64, 0, stream>>>(weight, lum, row_sum, lum_sum, conditional, w, h);
     k_env_marginal<<<1, 32, 0, stream>>>(weight, row_sum, lum_sum, solid, marginal, totals, w, h);
     k_env_pdfs<<<grid, 256, 0, stream>>>(weight, totals, pdfs, w, h);
+}
+
+// ---- scratch for the allocation-free entry point --------------------------------
+//
+// cenote_env_tables_static builds the same tables with its FP64 scratch in
+// this file-scope device array instead of cudaMalloc'd memory. Every device
+// that loads the library holds it until the process exits; every call on a
+// device shares it, so calls whose work overlaps on the GPU race (the
+// context's lock serialises calls made through one context). Layout, in
+// doubles: luminance (n) | weights (n) | row sums (h) | luminance row sums (h)
+// | total and power (2) | sin θ per row (h) | solid angle per row (h). Every
+// element a call reads was written earlier in the same call, so nothing needs
+// clearing between calls.
+constexpr size_t STATIC_ENV_MAX_TEXELS = size_t(1) << 18;  // 262,144 texels: 512x512, 1024x256, ...
+constexpr uint32_t STATIC_ENV_MAX_ROWS = 1024;
+constexpr size_t STATIC_ENV_SCRATCH_DOUBLES = 2 * STATIC_ENV_MAX_TEXELS + 4 * size_t(STATIC_ENV_MAX_ROWS) + 2;
+
+static __device__ __align__(256) double g_env_scratch[STATIC_ENV_SCRATCH_DOUBLES];
+
+namespace {
+constexpr int kMaxDevices = 64;
+std::mutex g_env_scratch_mu;
+double* g_env_scratch_ptr[kMaxDevices] = {};
+}  // namespace
+
+// The device address of g_env_scratch on the current device. The host-side
+// name is a stand-in, not a device address; the real one comes from
+// cudaGetSymbolAddress, looked up once per device (with that device current)
+// and cached. The first lookup may load this library's kernels onto the
+// device, which is why a caller's first call should come before any stream
+// capture.
+cudaError_t static_env_scratch(int device, double** out, size_t* max_texels, uint32_t* max_rows) {
+    *max_texels = STATIC_ENV_MAX_TEXELS;
+    *max_rows = STATIC_ENV_MAX_ROWS;
+    if (device < 0 || device >= kMaxDevices) return cudaErrorInvalidDevice;
+    std::lock_guard<std::mutex> lock(g_env_scratch_mu);
+    if (!g_env_scratch_ptr[device]) {
+        void* ptr = nullptr;
+        cudaError_t e = cudaGetSymbolAddress(&ptr, g_env_scratch);
+        if (e != cudaSuccess) return e;
+        g_env_scratch_ptr[device] = static_cast<double*>(ptr);
+    }
+    *out = g_env_scratch_ptr[device];
+    return cudaSuccess;
 }
 
 }  // namespace cn

@@ -258,6 +258,28 @@ int32_t cenote_probe_env_sample(cenote_scene* scene, const float* u, uint32_t n,
 /* Environment pdf for n directions (environment.slang:111-120). */
 int32_t cenote_probe_env_pdf(cenote_scene* scene, const float* directions, uint32_t n, float* pdf);
 
+/* ---- environment tables without device allocation --------------------------------- */
+
+/* The environment's sampling tables (the same bits cenote_scene_create
+ * builds: marginal h+1, conditional h·(w+1) and pdf w·h floats, plus the
+ * emitted power) for callers that cannot allocate device memory: a host that
+ * hands the library a fixed arena and accounts for every byte of HBM, code
+ * that must not stall the device on cudaMalloc/cudaFree (a per-frame
+ * environment edit in an interactive loop), or a binding that only holds
+ * memory another runtime owns. This entry point has no counterpart in the
+ * reference, which builds these tables on the host. `texels` (RGBA f32, w·h)
+ * and the three outputs are device pointers the caller owns; `power` is host
+ * memory (may be NULL). The FP64 scratch lives in one static device array per
+ * device, sized for at most 262,144 texels and 1,024 rows; larger inputs are
+ * rejected with CENOTE_E_INVALID_ARGUMENT. The call allocates nothing on the
+ * device and returns when the tables are written. Every call on a device
+ * shares that scratch, so calls whose GPU work overlaps (from different
+ * contexts, or threads bypassing one context) race. The first call on a
+ * device looks up the scratch's device address and may load the kernels, so
+ * make it before any stream capture. */
+int32_t cenote_env_tables_static(cenote_context* ctx, const float* texels, uint32_t width, uint32_t height,
+                                 float* marginal, float* conditional, float* pdfs, double* power);
+
 #ifdef __cplusplus
 }
 #endif
