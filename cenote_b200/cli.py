@@ -1,0 +1,86 @@
+"""Headless command line, the `cenote-cli render` contract
+(crates/cenote-cli/src/main.rs:30-65, 96-244):
+
+    python -m cenote_b200.cli render [SCENE] [--spp N] [--width W] [--height H]
+                                     [--depth D] [--out render.exr] [--frames K]
+
+SCENE is a built-in workload (cornell, chart) or a pbrt-v4 file (.pbrt, the
+subset cenote_b200.pbrt imports). Unset flags take the scene's own settings.
+Accumulates SPP samples and writes the linear averages as an EXR (R, G, B, A).
+--frames repeats the render (profiling); --stats prints the renderer's counters.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import sys
+import time
+
+import numpy as np
+
+from . import Context, Film, Renderer, Scene, scenes
+from .exr import write_exr
+
+
+def load_scene(name: str):
+    if name.endswith(".pbrt"):
+        from .pbrt import import_pbrt
+        return import_pbrt(name)
+    if name in scenes.SCENES:
+        return scenes.SCENES[name]()
+    raise SystemExit(f"unknown scene {name!r}: use one of {sorted(scenes.SCENES)} or a .pbrt file")
+
+
+def render(args) -> int:
+    spec = load_scene(args.scene)
+    width = args.width or spec.width
+    height = args.height or spec.height
+    spp = args.spp or spec.spp
+    depth = args.depth or spec.max_bounces
+    ctx = Context(args.device)
+    t0 = time.perf_counter()
+    scene = Scene(ctx, spec)
+    prep = time.perf_counter() - t0
+    renderer = Renderer(ctx, depth)
+    film = Film(ctx, width, height)
+    t0 = time.perf_counter()
+    for _ in range(max(1, args.frames)):
+        film.reset()
+        renderer.accumulate(scene, film, spp)
+    dt = (time.perf_counter() - t0) / max(1, args.frames)
+    img = film.averages()
+    if args.out:
+        write_exr(args.out, {"R": img[..., 0], "G": img[..., 1], "B": img[..., 2], "A": img[..., 3]})
+    st = renderer.stats()
+    msg = (f"wrote {args.out} ({width}x{height}, {spp} spp, depth {depth}) in {dt * 1e3:.1f} ms/frame, "
+           f"{width * height * spp / dt / 1e6:.1f} Msamples/s, prep {prep * 1e3:.1f} ms")
+    print(msg, file=sys.stderr)
+    if args.stats:
+        print(json.dumps(st))
+    return 0
+
+
+def main(argv=None) -> int:
+    ap = argparse.ArgumentParser(prog="cenote-cli", description="cenote-b200: a B200 path tracer")
+    sub = ap.add_subparsers(dest="command", required=True)
+    r = sub.add_parser("render", help="render a scene to an EXR")
+    r.add_argument("scene", nargs="?", default="chart")
+    r.add_argument("--spp", type=int, default=0)
+    r.add_argument("--width", type=int, default=0)
+    r.add_argument("--height", type=int, default=0)
+    r.add_argument("--depth", type=int, default=0)
+    r.add_argument("--out", default="render.exr")
+    r.add_argument("--frames", type=int, default=1)
+    r.add_argument("--device", type=int, default=0)
+    r.add_argument("--stats", action="store_true")
+    args = ap.parse_args(argv)
+    for v in (args.spp, args.width, args.height):
+        if v < 0:
+            ap.error("sizes must be positive")
+    if args.depth and not 1 <= args.depth <= 255:
+        ap.error("--depth must be in 1..=255")
+    return render(args)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -36,6 +36,10 @@ constexpr int BLOCK = 128;
 #ifndef CN_SHADE_MIN_BLOCKS
 #define CN_SHADE_MIN_BLOCKS 5
 #endif
+// The same for the traversal kernels (8 → 64 registers).
+#ifndef CN_TRAV_MIN_BLOCKS
+#define CN_TRAV_MIN_BLOCKS 8
+#endif
 
 __device__ __forceinline__ uint32_t lane_id() { return threadIdx.x & 31u; }
 
@@ -123,7 +127,7 @@ __global__ void __launch_bounds__(BLOCK) k_raygen(PathPool pool, WaveParams wp) 
 // ---- intersect (intersect.slang:47-88) -------------------------------------------
 
 template <bool COUNT>
-__global__ void __launch_bounds__(BLOCK) k_intersect(DeviceScene scene, PathPool pool, uint32_t bounce, uint32_t n0) {
+__global__ void __launch_bounds__(BLOCK, CN_TRAV_MIN_BLOCKS) k_intersect(DeviceScene scene, PathPool pool, uint32_t bounce, uint32_t n0) {
     uint32_t visits = 0, tests = 0;
     const uint32_t count = min(bounce == 0 ? n0 : pool.counters[CTR_RAYS + bounce], pool.capacity);
     const uint32_t* queue = pool.queue[bounce & 1u];
@@ -428,7 +432,7 @@ __global__ void __launch_bounds__(BLOCK, CN_SHADE_MIN_BLOCKS) k_shade(DeviceScen
 // ---- trace_shadow (trace_shadow.slang:29-72) ----------------------------------------
 
 template <bool COUNT>
-__global__ void __launch_bounds__(BLOCK) k_shadow(DeviceScene scene, PathPool pool, uint32_t bounce) {
+__global__ void __launch_bounds__(BLOCK, CN_TRAV_MIN_BLOCKS) k_shadow(DeviceScene scene, PathPool pool, uint32_t bounce) {
     const uint32_t count = min(pool.counters[CTR_SHADOWS + bounce], pool.capacity);
     uint32_t visits = 0, tests = 0;
     for (;;) {

@@ -1,0 +1,140 @@
+"""Minimal OpenEXR scanline writer/reader: FLOAT channels, no compression or
+RLE (compression 0/1), one scanline per block — enough for the renderer's
+linear output (crates/cenote/src/output.rs writes the same channel set:
+R, G, B, A, albedo.*, normal.*, Z) and for reading the reference's RLE
+goldens. Written from the OpenEXR file-layout document.
+"""
+from __future__ import annotations
+
+import struct
+
+import numpy as np
+
+MAGIC = 20000630
+FLOAT = 2
+
+
+def _attr(name: str, typ: str, data: bytes) -> bytes:
+    return name.encode() + b"\0" + typ.encode() + b"\0" + struct.pack("<i", len(data)) + data
+
+
+def write_exr(path, layers: dict[str, np.ndarray], compression: int = 0) -> None:
+    """layers: channel name -> (H, W) float32 array. Channels are stored in
+    sorted-name order, as the format requires. compression 0 = none."""
+    names = sorted(layers)
+    h, w = next(iter(layers.values())).shape
+    chlist = b"".join(n.encode() + b"\0" + struct.pack("<iB3xii", FLOAT, 0, 1, 1) for n in names) + b"\0"
+    header = struct.pack("<ii", MAGIC, 2)
+    header += _attr("channels", "chlist", chlist)
+    header += _attr("compression", "compression", bytes([compression]))
+    header += _attr("dataWindow", "box2i", struct.pack("<iiii", 0, 0, w - 1, h - 1))
+    header += _attr("displayWindow", "box2i", struct.pack("<iiii", 0, 0, w - 1, h - 1))
+    header += _attr("lineOrder", "lineOrder", bytes([0]))
+    header += _attr("pixelAspectRatio", "float", struct.pack("<f", 1.0))
+    header += _attr("screenWindowCenter", "v2f", struct.pack("<ff", 0.0, 0.0))
+    header += _attr("screenWindowWidth", "float", struct.pack("<f", 1.0))
+    # ACEScg (AP1) chromaticities: red, green, blue, white (D60).
+    header += _attr("chromaticities", "chromaticities",
+                    struct.pack("<8f", 0.713, 0.293, 0.165, 0.830, 0.128, 0.044, 0.32168, 0.33767))
+    header += b"\0"
+    data = [np.ascontiguousarray(layers[n], np.float32) for n in names]
+    offsets_pos = len(header)
+    first = offsets_pos + 8 * h
+    blocks, offsets = [], []
+    pos = first
+    for y in range(h):
+        payload = b"".join(d[y].tobytes() for d in data)
+        block = struct.pack("<ii", y, len(payload)) + payload
+        offsets.append(pos)
+        blocks.append(block)
+        pos += len(block)
+    with open(path, "wb") as f:
+        f.write(header)
+        f.write(struct.pack(f"<{h}Q", *offsets))
+        for b in blocks:
+            f.write(b)
+
+
+def _rle_decode(src: bytes, n: int) -> bytes:
+    out = bytearray()
+    i = 0
+    while i < len(src) and len(out) < n:
+        c = struct.unpack("<b", src[i:i + 1])[0]
+        i += 1
+        if c < 0:
+            out += src[i:i - c]
+            i += -c
+        else:
+            out += src[i:i + 1] * (c + 1)
+            i += 1
+    # predictor + interleave reversal (OpenEXR RLE/ZIP pre-processing)
+    buf = bytearray(out)
+    for k in range(1, len(buf)):
+        buf[k] = (buf[k - 1] + buf[k] - 128) & 0xFF
+    half = (len(buf) + 1) // 2
+    res = bytearray(len(buf))
+    res[0::2] = buf[:half]
+    res[1::2] = buf[half:]
+    return bytes(res)
+
+
+def read_exr(path) -> dict[str, np.ndarray]:
+    """FLOAT scanline images, compression none or RLE."""
+    raw = open(path, "rb").read()
+    assert struct.unpack("<i", raw[:4])[0] == MAGIC
+    pos = 8
+    attrs = {}
+    while raw[pos] != 0:
+        e = raw.index(b"\0", pos)
+        name = raw[pos:e].decode()
+        e2 = raw.index(b"\0", e + 1)
+        typ = raw[e + 1:e2].decode()
+        size = struct.unpack("<i", raw[e2 + 1:e2 + 5])[0]
+        attrs[name] = (typ, raw[e2 + 5:e2 + 5 + size])
+        pos = e2 + 5 + size
+    pos += 1
+    chans = []
+    cl = attrs["channels"][1]
+    i = 0
+    while cl[i] != 0:
+        e = cl.index(b"\0", i)
+        name = cl[i:e].decode()
+        ptype = struct.unpack("<i", cl[e + 1:e + 5])[0]
+        chans.append((name, ptype))
+        i = e + 17
+    x0, y0, x1, y1 = struct.unpack("<iiii", attrs["dataWindow"][1])
+    w, h = x1 - x0 + 1, y1 - y0 + 1
+    comp = attrs["compression"][1][0]
+    sizes = {2: 4, 1: 2, 0: 4}
+    out = {n: np.zeros((h, w), np.float32) for n, _ in chans}
+
+    def unpack(payload, n, rows, cols, y_at, x_at):
+        expect = sum(sizes[t] for _, t in chans) * rows * cols
+        if comp == 1 and n < expect:
+            payload = _rle_decode(payload, expect)
+        p = 0
+        for r in range(rows):
+            for name, t in chans:
+                if t == 2:
+                    v = np.frombuffer(payload[p:p + 4 * cols], "<f4")
+                elif t == 1:
+                    v = np.frombuffer(payload[p:p + 2 * cols], "<f2").astype(np.float32)
+                else:
+                    v = np.frombuffer(payload[p:p + 4 * cols], "<u4").astype(np.float32)
+                out[name][y_at + r, x_at:x_at + cols] = v
+                p += sizes[t] * cols
+
+    if "tiles" in attrs:  # single-level tiled image
+        tx, ty = struct.unpack("<II", attrs["tiles"][1][:8])
+        ntx, nty = (w + tx - 1) // tx, (h + ty - 1) // ty
+        offsets = struct.unpack(f"<{ntx * nty}Q", raw[pos:pos + 8 * ntx * nty])
+        for off in offsets:
+            cx, cy, _, _, n = struct.unpack("<iiiii", raw[off:off + 20])
+            cols, rows = min(tx, w - cx * tx), min(ty, h - cy * ty)
+            unpack(raw[off + 20:off + 20 + n], n, rows, cols, cy * ty, cx * tx)
+        return out
+    offsets = struct.unpack(f"<{h}Q", raw[pos:pos + 8 * h])
+    for off in offsets:
+        y, n = struct.unpack("<ii", raw[off:off + 8])
+        unpack(raw[off + 8:off + 8 + n], n, 1, w, y - y0, 0)
+    return out

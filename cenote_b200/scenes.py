@@ -398,3 +398,44 @@ def furnace(mat, size=32, sky=0.5, center=(0.0, 0.0, 0.0), scl=1.0, aperture=0.0
 
 
 SCENES = {"cornell": cornell, "chart": chart}
+
+
+# ---- flat archive -----------------------------------------------------------------
+
+
+def save_spec(path, spec: SceneSpec, **extra) -> None:
+    """Store a scene description as one .npz: meshes, transforms, materials,
+    camera, environment, delta lights and settings. `extra` arrays ride along."""
+    arrs = {}
+    for i, o in enumerate(spec.objects):
+        m = o.mesh
+        arrs.update({f"o{i}_positions": m.positions, f"o{i}_normals": m.normals, f"o{i}_uvs": m.uvs,
+                     f"o{i}_indices": m.indices, f"o{i}_transform": np.asarray(o.transform, np.float32),
+                     f"o{i}_material": np.frombuffer(np.asarray(o.material, MATERIAL_DTYPE).tobytes(), np.uint8),
+                     f"o{i}_visible": np.array(o.camera_visible)})
+    c = spec.camera
+    arrs["camera"] = np.array([*c.position, *c.look_at, *c.up, c.vfov_degrees, c.aperture_radius,
+                               c.focus_distance], np.float64)
+    arrs["env"] = np.asarray(spec.environment.texels, np.float32)
+    arrs["delta"] = np.array([[d.kind, *d.anchor, *d.emission] for d in spec.delta_lights], np.float64).reshape(-1, 7)
+    arrs["settings"] = np.array([spec.width, spec.height, spec.spp, spec.max_bounces, len(spec.objects)], np.int64)
+    arrs["name"] = np.array(spec.name)
+    arrs.update({f"x_{k}": np.asarray(v) for k, v in extra.items()})
+    np.savez_compressed(path, **arrs)
+
+
+def load_spec(path) -> tuple[SceneSpec, dict]:
+    """Inverse of save_spec: the scene and the extra arrays stored with it."""
+    z = np.load(path)
+    w, h, spp, mb, n = (int(v) for v in z["settings"])
+    objs = []
+    for i in range(n):
+        mesh = Mesh(z[f"o{i}_positions"], z[f"o{i}_normals"], z[f"o{i}_uvs"], z[f"o{i}_indices"])
+        mat = np.frombuffer(z[f"o{i}_material"].tobytes(), MATERIAL_DTYPE)[0]
+        objs.append(Object(mesh, z[f"o{i}_transform"], mat, bool(z[f"o{i}_visible"])))
+    c = z["camera"]
+    cam = Camera(tuple(c[0:3]), tuple(c[3:6]), tuple(c[6:9]), float(c[9]), float(c[10]), float(c[11]))
+    env = z["env"]
+    deltas = [DeltaLight(int(d[0]), tuple(d[1:4]), tuple(d[4:7])) for d in z["delta"]]
+    spec = SceneSpec(str(z["name"]), objs, cam, Environment(env.shape[1], env.shape[0], env), w, h, spp, mb, deltas)
+    return spec, {k[2:]: z[k] for k in z.files if k.startswith("x_")}
