@@ -302,7 +302,8 @@ def main():
                    "parallelism": f"sample-interleaved x{world}" if world > 1 else "1 GPU",
                    "l2": "256 MB buffer written between timed steps (L2 flush); the path pool per wave also "
                          "exceeds L2",
-                   "samples_per_wave": counts["samples_per_wave"], "waves_per_step": counts["waves"]},
+                   "samples_per_wave": counts["samples_per_wave"], "waves_per_step": counts["waves"],
+                   "guides": "albedo, normal and depth traced and accumulated every sample, as Renderer::accumulate does"},
         "e2e": {"value": e2e_value, "unit": "Msamples/s", "ms_per_step": e2e_step,
                 "h2d_bytes_per_step": 48, "d2h_bytes_per_step": W * H * 16},
         "gpu_launches": launches,

@@ -420,6 +420,14 @@ class Film:
         _check(library().cenote_film_averages(self._h, _ptr(out), None, None, None))
         return out
 
+    def all_averages(self) -> dict:
+        """Film::averages (film.rs:183-191): beauty, albedo, normal (H, W, 4) and depth (H, W)."""
+        out = {k: np.zeros((self.height, self.width, 4), np.float32) for k in ("beauty", "albedo", "normal")}
+        out["depth"] = np.zeros((self.height, self.width), np.float32)
+        _check(library().cenote_film_averages(self._h, _ptr(out["beauty"]), _ptr(out["albedo"]), _ptr(out["normal"]),
+                                              _ptr(out["depth"])))
+        return out
+
     def averages_into(self, ptr: int) -> None:
         """Resolve into caller memory at `ptr` (pinned host memory for speed)."""
         _check(library().cenote_film_averages(self._h, ptr, None, None, None))

@@ -6,8 +6,11 @@
 
 SCENE is a built-in workload (cornell, chart) or a pbrt-v4 file (.pbrt, the
 subset cenote_b200.pbrt imports). Unset flags take the scene's own settings.
-Accumulates SPP samples and writes the linear averages as an EXR (R, G, B, A).
---frames repeats the render (profiling); --stats prints the renderer's counters.
+Accumulates SPP samples and writes the linear averages as one multi-layer
+EXR: beauty R/G/B/A, the denoiser guides albedo.R/G/B and normal.X/Y/Z, depth Z
+(crates/cenote-cli/src/main.rs:196-216).
+--frames repeats the render (profiling); --samples-per-wave fixes how many
+samples of every pixel one wave carries; --stats prints the renderer's counters.
 """
 from __future__ import annotations
 
@@ -19,7 +22,7 @@ import time
 import numpy as np
 
 from . import Context, Film, Renderer, Scene, scenes
-from .exr import write_exr
+from .exr import write_aov_exr
 
 
 def load_scene(name: str):
@@ -41,18 +44,19 @@ def render(args) -> int:
     t0 = time.perf_counter()
     scene = Scene(ctx, spec)
     prep = time.perf_counter() - t0
-    renderer = Renderer(ctx, depth)
+    renderer = Renderer(ctx, depth, samples_per_wave=args.samples_per_wave)
     film = Film(ctx, width, height)
     t0 = time.perf_counter()
     for _ in range(max(1, args.frames)):
         film.reset()
         renderer.accumulate(scene, film, spp)
     dt = (time.perf_counter() - t0) / max(1, args.frames)
-    img = film.averages()
     if args.out:
-        write_exr(args.out, {"R": img[..., 0], "G": img[..., 1], "B": img[..., 2], "A": img[..., 3]})
+        av = film.all_averages()
+        write_aov_exr(args.out, av["beauty"], av["albedo"], av["normal"], av["depth"])
     st = renderer.stats()
-    msg = (f"wrote {args.out} ({width}x{height}, {spp} spp, depth {depth}) in {dt * 1e3:.1f} ms/frame, "
+    msg = (f"wrote {args.out} ({width}x{height}, {spp} spp, depth {depth}; layers: beauty, albedo, normal, Z) "
+           f"in {dt * 1e3:.1f} ms/frame, "
            f"{width * height * spp / dt / 1e6:.1f} Msamples/s, prep {prep * 1e3:.1f} ms")
     print(msg, file=sys.stderr)
     if args.stats:
@@ -72,9 +76,10 @@ def main(argv=None) -> int:
     r.add_argument("--out", default="render.exr")
     r.add_argument("--frames", type=int, default=1)
     r.add_argument("--device", type=int, default=0)
+    r.add_argument("--samples-per-wave", type=int, default=0, help="0 = automatic")
     r.add_argument("--stats", action="store_true")
     args = ap.parse_args(argv)
-    for v in (args.spp, args.width, args.height):
+    for v in (args.spp, args.width, args.height, args.samples_per_wave):
         if v < 0:
             ap.error("sizes must be positive")
     if args.depth and not 1 <= args.depth <= 255:

@@ -2,6 +2,7 @@
 // probes. Host arithmetic that feeds bit-exact tables is compiled with
 // -ffp-contract=off so every a·b + c rounds twice, as the reference's Rust does.
 #include <algorithm>
+#include <utility>
 #include <atomic>
 #include <chrono>
 #include <cmath>
@@ -330,7 +331,8 @@ struct cenote_renderer {
     std::vector<cudaEvent_t> events;
     PathPool pool{};
     DeviceBuffer org, dir, thr, hit, ps, state, rad, q0, q1, shadows, counters, tally, scratch;
-    size_t pool_cap = 0;
+    DeviceBuffer aov_albedo, aov_normal, aov_depth, aov_guide;
+    size_t pool_cap = 0, aov_cap = 0;
     cenote_stats stats{};
     unsigned long long tally_prev[5] = {0, 0, 0, 0, 0};
 
@@ -368,6 +370,23 @@ struct cenote_renderer {
         pool_cap = cap;
         return cudaSuccess;
     }
+
+    // The guide lanes: allocated on the first wave that traces guides,
+    // detached (null) for waves that do not.
+    cudaError_t set_guides(bool on) {
+        if (on && aov_cap < pool_cap) {
+            cudaError_t e;
+            if ((e = aov_albedo.alloc(pool_cap * 16)) || (e = aov_normal.alloc(pool_cap * 16)) ||
+                (e = aov_depth.alloc(pool_cap * 4)) || (e = aov_guide.alloc(pool_cap * 16)))
+                return e;
+            aov_cap = pool_cap;
+        }
+        pool.aov_albedo = on ? aov_albedo.as<float4>() : nullptr;
+        pool.aov_normal = on ? aov_normal.as<float4>() : nullptr;
+        pool.aov_depth = on ? aov_depth.as<float>() : nullptr;
+        pool.aov_guide = on ? aov_guide.as<float4>() : nullptr;
+        return cudaSuccess;
+    }
 };
 
 struct cenote_film {
@@ -375,6 +394,10 @@ struct cenote_film {
     uint32_t width = 0, height = 0;
     uint32_t samples = 0;
     DeviceBuffer sum, avg;
+    DeviceBuffer albedo, normal, depth;  // guide sums (film.rs:95-112)
+    FilmTargets targets() {
+        return {sum.as<float4>(), albedo.as<float4>(), normal.as<float4>(), depth.as<float>()};
+    }
 };
 
 namespace {
@@ -759,7 +782,13 @@ int32_t cenote_film_create(cenote_context* ctx, uint32_t width, uint32_t height,
     size_t px = size_t(width) * height;
     CN_CUDA(f->sum.alloc(px * 16));
     CN_CUDA(f->avg.alloc(px * 16));
+    CN_CUDA(f->albedo.alloc(px * 16));
+    CN_CUDA(f->normal.alloc(px * 16));
+    CN_CUDA(f->depth.alloc(px * 4));
     CN_CUDA(cudaMemsetAsync(f->sum.ptr, 0, px * 16, ctx->stream));
+    CN_CUDA(cudaMemsetAsync(f->albedo.ptr, 0, px * 16, ctx->stream));
+    CN_CUDA(cudaMemsetAsync(f->normal.ptr, 0, px * 16, ctx->stream));
+    CN_CUDA(cudaMemsetAsync(f->depth.ptr, 0, px * 4, ctx->stream));
     retain(ctx);
     *out = f.release();
     return CENOTE_OK;
@@ -777,7 +806,13 @@ void cenote_film_destroy(cenote_film* film) {
 int32_t cenote_film_reset(cenote_film* film) {
     CN_CHECK(film, CENOTE_E_INVALID_ARGUMENT, "null film");
     CN_CUDA(cudaSetDevice(film->ctx->device));
-    CN_CUDA(cudaMemsetAsync(film->sum.ptr, 0, size_t(film->width) * film->height * 16, film->ctx->stream));
+    // The next sample overwrites the sums (film.rs:140-145); clearing them
+    // too keeps a read of an empty film's sums at zero.
+    const size_t px = size_t(film->width) * film->height;
+    CN_CUDA(cudaMemsetAsync(film->sum.ptr, 0, px * 16, film->ctx->stream));
+    CN_CUDA(cudaMemsetAsync(film->albedo.ptr, 0, px * 16, film->ctx->stream));
+    CN_CUDA(cudaMemsetAsync(film->normal.ptr, 0, px * 16, film->ctx->stream));
+    CN_CUDA(cudaMemsetAsync(film->depth.ptr, 0, px * 4, film->ctx->stream));
     film->samples = 0;
     return CENOTE_OK;
 }
@@ -813,6 +848,8 @@ int32_t run_waves(cenote_renderer* r, cenote_scene* sc, uint32_t width, uint32_t
     if (r->capacity_req) need = std::max<uint64_t>(need, std::min<uint64_t>(r->capacity_req, need));
     CN_CHECK(need < (1ull << 31), CENOTE_E_INVALID_ARGUMENT, "wave too large");
     CN_CUDA(r->ensure(need));
+    // Films trace the guides (Renderer::accumulate); one-shot renders do not.
+    CN_CUDA(r->set_guides(film != nullptr));
 
     WaveParams wp{};
     wp.width = width;
@@ -852,7 +889,8 @@ int32_t run_waves(cenote_renderer* r, cenote_scene* sc, uint32_t width, uint32_t
             }
             launch_tally(r->pool, r->tally.as<unsigned long long>(), n0, r->max_bounces, ctx->stream);
             if (film)
-                launch_accumulate(r->pool, film->sum.as<float4>(), wp.pixel_base, wp.pixel_count, s, false, ctx->stream);
+                launch_accumulate(r->pool, film->targets(), wp.pixel_base, wp.pixel_count, s,
+                                  film->samples == 0 && done == 0, ctx->stream);
             else
                 launch_copy_rad(r->pool, oneshot, wp.pixel_base, wp.pixel_count, ctx->stream);
             mark();
@@ -946,10 +984,20 @@ int32_t cenote_film_averages(cenote_film* film, float* beauty, float* albedo, fl
         CN_CUDA(cudaGetLastError());
         CN_CUDA(cudaMemcpyAsync(beauty, film->avg.ptr, px * 16, cudaMemcpyDeviceToHost, film->ctx->stream));
     }
-    // The guide AOVs are not traced by this build: report zeros, depth +inf.
-    if (albedo) std::memset(albedo, 0, px * 16);
-    if (normal) std::memset(normal, 0, px * 16);
-    if (depth) std::fill(depth, depth + px, std::numeric_limits<float>::infinity());
+    const float n = float(std::max(1u, film->samples));
+    float4* avg = film->avg.as<float4>();
+    for (auto [src, dst] : {std::pair<float4*, float*>{film->albedo.as<float4>(), albedo},
+                            std::pair<float4*, float*>{film->normal.as<float4>(), normal}}) {
+        if (!dst) continue;
+        launch_resolve(src, avg, uint32_t(px), n, film->ctx->stream);
+        CN_CUDA(cudaGetLastError());
+        CN_CUDA(cudaMemcpyAsync(dst, avg, px * 16, cudaMemcpyDeviceToHost, film->ctx->stream));
+    }
+    if (depth) {
+        launch_resolve1(film->depth.as<float>(), film->avg.as<float>(), uint32_t(px), n, film->ctx->stream);
+        CN_CUDA(cudaGetLastError());
+        CN_CUDA(cudaMemcpyAsync(depth, film->avg.ptr, px * 4, cudaMemcpyDeviceToHost, film->ctx->stream));
+    }
     return wait_stream(film->ctx->stream, film->ctx->sync_ev, 600000.0);
 }
 

@@ -121,6 +121,11 @@ __global__ void __launch_bounds__(BLOCK) k_raygen(PathPool pool, WaveParams wp) 
         pool.ps[p] = make_uint2(pixel, sample);
         pool.state[p] = MEDIUM_NONE;
         pool.rad[p] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+        if (pool.aov_albedo) {
+            pool.aov_albedo[p] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+            pool.aov_normal[p] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+            pool.aov_depth[p] = 0.0f;
+        }
     }
 }
 
@@ -249,6 +254,14 @@ __device__ __forceinline__ void load_material(const Material* rec, Material& m) 
     for (int k = 0; k < int(sizeof(Material) / 16); ++k) dst[k] = __ldg(src + k);
 }
 
+// shade_surface.slang:59-63: the open guides record this surface.
+__device__ __forceinline__ void record_guides(const PathPool& pool, uint32_t path, float3 w, float3 albedo, float3 n) {
+    float4 a = pool.aov_albedo[path], b = pool.aov_normal[path];
+    pool.aov_albedo[path] = make_float4(a.x + w.x * albedo.x, a.y + w.y * albedo.y, a.z + w.z * albedo.z, a.w);
+    pool.aov_normal[path] = make_float4(b.x + w.x * n.x, b.y + w.y * n.y, b.z + w.z * n.z, b.w);
+}
+
+template <bool AOV>
 __global__ void __launch_bounds__(BLOCK, CN_SHADE_MIN_BLOCKS) k_shade(DeviceScene scene, PathPool pool, uint32_t bounce,
                                                  uint32_t max_bounces, uint32_t light_sampling, uint32_t n0) {
     const uint32_t count = min(bounce == 0 ? n0 : pool.counters[CTR_RAYS + bounce], pool.capacity);
@@ -276,6 +289,15 @@ __global__ void __launch_bounds__(BLOCK, CN_SHADE_MIN_BLOCKS) k_shade(DeviceScen
                     if (light_sampling == CENOTE_LIGHT_SAMPLING_NEE) weight = 0.0f;
                     else if (light_sampling == CENOTE_LIGHT_SAMPLING_MIS)
                         weight = power_heuristic(t4.w, scene.select_prob * env_pdf(scene, dir));
+                }
+                if (AOV) {
+                    // shade_miss.slang:52-66: depth +inf on a camera ray; the
+                    // open guides record the environment as white albedo.
+                    const bool camera_ray = t4.w == 0.0f;
+                    if (camera_ray) pool.aov_depth[path] += __int_as_float(0x7f800000);
+                    float3 guide = camera_ray ? f3(1.0f) : xyz(pool.aov_guide[path]);
+                    float4 a = pool.aov_albedo[path];
+                    pool.aov_albedo[path] = make_float4(a.x + guide.x, a.y + guide.y, a.z + guide.z, a.w);
                 }
                 float3 c = thr * env_radiance(scene, dir) * weight;
                 pool.rad[path] = make_float4(rad.x + c.x, rad.y + c.y, rad.z + c.z, rad.w + 1.0f);
@@ -319,7 +341,16 @@ __global__ void __launch_bounds__(BLOCK, CN_SHADE_MIN_BLOCKS) k_shade(DeviceScen
                 Frame frame(sp.shading);
                 float3 wo = frame.to_local(-dir);
                 Closure cl = resolve_closure(scene.bsdf_tables, mat, wo, medium == inst);
+                // Guides (shade_surface.slang:322-340): camera rays are fully
+                // open; the first hit records camera-plane depth.
+                float3 guide = f3(0.0f), aov_alb = f3(0.0f);
+                if (AOV) {
+                    guide = bounce == 0 ? f3(1.0f) : xyz(pool.aov_guide[path]);
+                    if (bounce == 0) pool.aov_depth[path] += length(origin - sp.position) * d4.w;
+                    aov_alb = saturate3(cl.aov_albedo);
+                }
                 if (bounce + 1 >= max_bounces) {
+                    if (AOV && any_pos(guide)) record_guides(pool, path, guide, aov_alb, sp.shading);
                     pool.rad[path] = make_float4(rad.x + contribution.x, rad.y + contribution.y, rad.z + contribution.z,
                                                  rad.w + 1.0f);
                 } else {
@@ -391,9 +422,17 @@ __global__ void __launch_bounds__(BLOCK, CN_SHADE_MIN_BLOCKS) k_shade(DeviceScen
                         else scattered = scattered / survival;
                     }
                     if (terminal) {
+                        if (AOV && any_pos(guide)) record_guides(pool, path, guide, aov_alb, sp.shading);
                         pool.rad[path] = make_float4(rad.x + contribution.x, rad.y + contribution.y,
                                                      rad.z + contribution.z, rad.w + 1.0f);
                     } else {
+                        if (AOV) {
+                            // shade_surface.slang:488-503: the sampled lobe splits the
+                            // open guides between this surface and the scattered ray.
+                            float rec = aov_record_fraction(cl, sc.lobe);
+                            if (rec > 0.0f && any_pos(guide)) record_guides(pool, path, guide * rec, aov_alb, sp.shading);
+                            pool.aov_guide[path] = f4(guide * (1.0f - rec) * aov_pass_tint(cl, sc.lobe), 0.0f);
+                        }
                         if (sc.lobe == LOBE_TRANSMISSION && mat.thin_walled == 0)
                             medium = medium == inst ? MEDIUM_NONE : inst;
                         pool.org[path] = f4(sc.wi.z < 0.0f ? sp.below : sp.position, 0.0f);
@@ -464,17 +503,47 @@ __device__ __forceinline__ bool finite4(float4 v) {
     return isfinite(v.x) && isfinite(v.y) && isfinite(v.z) && isfinite(v.w);
 }
 
-__global__ void k_accumulate(const float4* __restrict__ rad, float4* __restrict__ sum, uint32_t pixel_base,
-                             uint32_t count, uint32_t samples, uint32_t reset) {
+__device__ __forceinline__ float4 add4(float4 a, float4 b) {
+    return make_float4(a.x + b.x, a.y + b.y, a.z + b.z, a.w + b.w);
+}
+
+// accumulate.slang:38-67, all samples of a wave in ascending order.
+template <bool AOV>
+__global__ void k_accumulate(PathPool pool, FilmTargets film, uint32_t pixel_base, uint32_t count, uint32_t samples,
+                             uint32_t reset) {
+    const float4 zero = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
     for (uint32_t p = blockIdx.x * blockDim.x + threadIdx.x; p < count; p += gridDim.x * blockDim.x) {
-        float4 acc = reset ? make_float4(0.0f, 0.0f, 0.0f, 0.0f) : sum[pixel_base + p];
-        for (uint32_t s = 0; s < samples; ++s) {
-            float4 v = rad[size_t(s) * count + p];
-            if (!finite4(v)) v = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
-            if (reset && s == 0) acc = v;
-            else acc = make_float4(acc.x + v.x, acc.y + v.y, acc.z + v.z, acc.w + v.w);
+        const uint32_t px = pixel_base + p;
+        float4 acc = reset ? zero : film.sum[px];
+        float4 alb = zero, nrm = zero;
+        float dep = 0.0f;
+        if (AOV && !reset) {
+            alb = film.albedo[px];
+            nrm = film.normal[px];
+            dep = film.depth[px];
         }
-        sum[pixel_base + p] = acc;
+        for (uint32_t s = 0; s < samples; ++s) {
+            const size_t q = size_t(s) * count + p;
+            float4 v = pool.rad[q];
+            if (!finite4(v)) v = zero;
+            acc = (reset && s == 0) ? v : add4(acc, v);
+            if (AOV) {
+                float4 a = pool.aov_albedo[q], n = pool.aov_normal[q];
+                float d = pool.aov_depth[q];
+                if (!finite4(a)) a = zero;
+                if (!finite4(n)) n = zero;
+                if (isnan(d)) d = 0.0f;
+                alb = (reset && s == 0) ? a : add4(alb, a);
+                nrm = (reset && s == 0) ? n : add4(nrm, n);
+                dep = (reset && s == 0) ? d : dep + d;
+            }
+        }
+        film.sum[px] = acc;
+        if (AOV) {
+            film.albedo[px] = alb;
+            film.normal[px] = nrm;
+            film.depth[px] = dep;
+        }
     }
 }
 
@@ -483,6 +552,10 @@ __global__ void k_resolve(const float4* __restrict__ sum, float4* __restrict__ a
         float4 v = sum[p];
         avg[p] = make_float4(v.x / samples, v.y / samples, v.z / samples, v.w / samples);
     }
+}
+
+__global__ void k_resolve1(const float* __restrict__ sum, float* __restrict__ avg, uint32_t n, float samples) {
+    for (uint32_t p = blockIdx.x * blockDim.x + threadIdx.x; p < n; p += gridDim.x * blockDim.x) avg[p] = sum[p] / samples;
 }
 
 __global__ void k_copy_rad(const float4* __restrict__ rad, float4* __restrict__ out, uint32_t base, uint32_t count) {
@@ -519,7 +592,7 @@ LaunchShape launch_shape(int device) {
     int occ = 0;
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_intersect<false>, BLOCK, 0);
     ls.grid_isect = sms * (occ > 0 ? occ : 4);
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_shade, BLOCK, 0);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_shade<true>, BLOCK, 0);
     ls.grid_shade = sms * (occ > 0 ? occ : 4);
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_shadow<false>, BLOCK, 0);
     ls.grid_shadow = sms * (occ > 0 ? occ : 4);
@@ -540,7 +613,10 @@ void launch_intersect(const DeviceScene& scene, const PathPool& pool, uint32_t b
 
 void launch_shade(const DeviceScene& scene, const PathPool& pool, uint32_t bounce, const WaveParams& wp, uint32_t n0,
                   const LaunchShape& ls, cudaStream_t stream) {
-    k_shade<<<ls.grid_shade, BLOCK, 0, stream>>>(scene, pool, bounce, wp.max_bounces, wp.light_sampling, n0);
+    if (pool.aov_albedo)
+        k_shade<true><<<ls.grid_shade, BLOCK, 0, stream>>>(scene, pool, bounce, wp.max_bounces, wp.light_sampling, n0);
+    else
+        k_shade<false><<<ls.grid_shade, BLOCK, 0, stream>>>(scene, pool, bounce, wp.max_bounces, wp.light_sampling, n0);
 }
 
 void launch_shadow(const DeviceScene& scene, const PathPool& pool, uint32_t bounce, const LaunchShape& ls,
@@ -560,11 +636,20 @@ void launch_wave(const DeviceScene& scene, const PathPool& pool, const WaveParam
     }
 }
 
-void launch_accumulate(const PathPool& pool, float4* sum, uint32_t pixel_base, uint32_t pixel_count, uint32_t samples,
-                       bool reset, cudaStream_t stream) {
+void launch_accumulate(const PathPool& pool, const FilmTargets& film, uint32_t pixel_base, uint32_t pixel_count,
+                       uint32_t samples, bool reset, cudaStream_t stream) {
     int grid = int((pixel_count + 255) / 256);
     if (grid > 148 * 16) grid = 148 * 16;
-    k_accumulate<<<grid, 256, 0, stream>>>(pool.rad, sum, pixel_base, pixel_count, samples, reset ? 1u : 0u);
+    if (pool.aov_albedo && film.albedo)
+        k_accumulate<true><<<grid, 256, 0, stream>>>(pool, film, pixel_base, pixel_count, samples, reset ? 1u : 0u);
+    else
+        k_accumulate<false><<<grid, 256, 0, stream>>>(pool, film, pixel_base, pixel_count, samples, reset ? 1u : 0u);
+}
+
+void launch_resolve1(const float* sum, float* avg, uint32_t pixels, float samples, cudaStream_t stream) {
+    int grid = int((pixels + 255) / 256);
+    if (grid > 148 * 16) grid = 148 * 16;
+    k_resolve1<<<grid, 256, 0, stream>>>(sum, avg, pixels, samples);
 }
 
 void launch_resolve(const float4* sum, float4* avg, uint32_t pixels, float samples, cudaStream_t stream) {

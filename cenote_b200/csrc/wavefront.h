@@ -29,6 +29,15 @@ struct PathPool {
     uint2* ps;         // (pixel, sample index)
     uint32_t* state;   // lobe << 24 | medium
     float4* rad;       // the path's radiance, alpha = finished
+    // Denoiser guides (pathstate.slang:82-106), all null on a wave that
+    // traces none. Path-owned accumulators zeroed by raygen: albedo and
+    // normal (xyz, w = 0) and camera-plane depth of the first hit (+inf on
+    // a miss); `aov_guide` is the feature throughput still open, written by
+    // scatters and read from bounce 1 on (a camera ray's is 1).
+    float4* aov_albedo;
+    float4* aov_normal;
+    float* aov_depth;
+    float4* aov_guide;
     uint32_t* queue[2];   // ray queues, ping-pong by bounce parity
     ShadowRay* shadows;
     uint32_t* counters;
@@ -68,12 +77,23 @@ void launch_shade(const DeviceScene& scene, const PathPool& pool, uint32_t bounc
 void launch_shadow(const DeviceScene& scene, const PathPool& pool, uint32_t bounce, const LaunchShape& ls,
                    bool count_visits, cudaStream_t stream);
 
+// The film's running sums. The guide sums may be null (no guides traced).
+struct FilmTargets {
+    float4* sum;
+    float4* albedo;
+    float4* normal;
+    float* depth;
+};
+
 // Film: sum[pixel] += guarded rad[s · count + local], s ascending (the
-// film's guard, crates/cenote/shaders/accumulate.slang:38-44); reset
-// overwrites with the first sample instead.
-void launch_accumulate(const PathPool& pool, float4* sum, uint32_t pixel_base, uint32_t pixel_count, uint32_t samples,
-                       bool reset, cudaStream_t stream);
+// film's guard, crates/cenote/shaders/accumulate.slang:38-67: a non-finite
+// channel drops that buffer's sample, depth drops only NaN); reset
+// overwrites with the first sample instead. The guides accumulate when both
+// the pool and the film carry them.
+void launch_accumulate(const PathPool& pool, const FilmTargets& film, uint32_t pixel_base, uint32_t pixel_count,
+                       uint32_t samples, bool reset, cudaStream_t stream);
 void launch_resolve(const float4* sum, float4* avg, uint32_t pixels, float samples, cudaStream_t stream);
+void launch_resolve1(const float* sum, float* avg, uint32_t pixels, float samples, cudaStream_t stream);
 // tally[0] += extension rays, [1] += shadow rays, [2] |= overflow,
 // [3] += node visits, [4] += triangle tests.
 void launch_tally(const PathPool& pool, unsigned long long* tally, uint32_t n0, uint32_t max_bounces,

@@ -11,6 +11,7 @@ import struct
 import numpy as np
 
 MAGIC = 20000630
+HALF = 1
 FLOAT = 2
 
 
@@ -19,11 +20,13 @@ def _attr(name: str, typ: str, data: bytes) -> bytes:
 
 
 def write_exr(path, layers: dict[str, np.ndarray], compression: int = 0) -> None:
-    """layers: channel name -> (H, W) float32 array. Channels are stored in
-    sorted-name order, as the format requires. compression 0 = none."""
+    """layers: channel name -> (H, W) array, float16 (stored HALF) or
+    anything else (stored FLOAT). Channels are stored in sorted-name order,
+    as the format requires. compression 0 = none."""
     names = sorted(layers)
     h, w = next(iter(layers.values())).shape
-    chlist = b"".join(n.encode() + b"\0" + struct.pack("<iB3xii", FLOAT, 0, 1, 1) for n in names) + b"\0"
+    kinds = {n: HALF if np.asarray(layers[n]).dtype == np.float16 else FLOAT for n in names}
+    chlist = b"".join(n.encode() + b"\0" + struct.pack("<iB3xii", kinds[n], 0, 1, 1) for n in names) + b"\0"
     header = struct.pack("<ii", MAGIC, 2)
     header += _attr("channels", "chlist", chlist)
     header += _attr("compression", "compression", bytes([compression]))
@@ -37,7 +40,7 @@ def write_exr(path, layers: dict[str, np.ndarray], compression: int = 0) -> None
     header += _attr("chromaticities", "chromaticities",
                     struct.pack("<8f", 0.713, 0.293, 0.165, 0.830, 0.128, 0.044, 0.32168, 0.33767))
     header += b"\0"
-    data = [np.ascontiguousarray(layers[n], np.float32) for n in names]
+    data = [np.ascontiguousarray(layers[n], np.float16 if kinds[n] == HALF else np.float32) for n in names]
     offsets_pos = len(header)
     first = offsets_pos + 8 * h
     blocks, offsets = [], []
@@ -53,6 +56,17 @@ def write_exr(path, layers: dict[str, np.ndarray], compression: int = 0) -> None
         f.write(struct.pack(f"<{h}Q", *offsets))
         for b in blocks:
             f.write(b)
+
+
+def write_aov_exr(path, beauty, albedo, normal, depth) -> None:
+    """The CLI's multi-layer output (crates/cenote/src/output.rs:61-135):
+    beauty as bare R/G/B/A, the guides as albedo.R/G/B and normal.X/Y/Z, all
+    in f16, and depth as the bare f32 Z (+inf marks the sky)."""
+    layers = {c: beauty[..., k].astype(np.float16) for k, c in enumerate("RGBA")}
+    layers.update({f"albedo.{c}": albedo[..., k].astype(np.float16) for k, c in enumerate("RGB")})
+    layers.update({f"normal.{c}": normal[..., k].astype(np.float16) for k, c in enumerate("XYZ")})
+    layers["Z"] = np.asarray(depth, np.float32)
+    write_exr(path, layers)
 
 
 def _rle_decode(src: bytes, n: int) -> bytes:

@@ -49,7 +49,7 @@ def library() -> C.CDLL:
         "oracle_scene_select_prob": (F, [P]),
         "oracle_scene_env_power": (D, [P]),
         "oracle_scene_env_tables": (None, [P, P, P, P]),
-        "oracle_render": (None, [P, U32, U32, U32, U32, U32, U32, U32, P, P]),
+        "oracle_render": (None, [P, U32, U32, U32, U32, U32, U32, U32, P, P, P, P, P]),
         "oracle_camera_basis": (None, [P, F, P, P, P]),
         "oracle_sampler": (None, [U32, U32, U32, P, P]),
         "oracle_hash_uniform": (F, [U32, U32, U32, U32]),
@@ -153,7 +153,20 @@ class OracleScene:
         counts = np.zeros(2, np.uint64)
         threads = threads or os.cpu_count() or 1
         library().oracle_render(self._h, width, height, sample_begin, sample_count, max_bounces, light_sampling,
-                                threads, _p(out), _p(counts))
+                                threads, _p(out), _p(counts), None, None, None)
+        self.last_ray_counts = counts
+        return out
+
+    def render_guides(self, width, height, sample_begin, sample_count, max_bounces, light_sampling=0, threads=0):
+        """Beauty and guide sums: dict of beauty/albedo/normal (H, W, 4) and depth (H, W)."""
+        import os
+        out = {k: np.zeros((height, width, 4), np.float32) for k in ("beauty", "albedo", "normal")}
+        out["depth"] = np.zeros((height, width), np.float32)
+        counts = np.zeros(2, np.uint64)
+        threads = threads or os.cpu_count() or 1
+        library().oracle_render(self._h, width, height, sample_begin, sample_count, max_bounces, light_sampling,
+                                threads, _p(out["beauty"]), _p(counts), _p(out["albedo"]), _p(out["normal"]),
+                                _p(out["depth"]))
         self.last_ray_counts = counts
         return out
 

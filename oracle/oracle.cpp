@@ -247,9 +247,22 @@ struct RayCounts {
     uint64_t extension = 0, shadow = 0;
 };
 
+// One sample's denoiser guides (pathstate.slang:82-106): albedo and normal
+// (xyz), camera-plane depth of the first hit (+inf on a miss).
+struct Guides {
+    float albedo[4] = {0, 0, 0, 0};
+    float normal[4] = {0, 0, 0, 0};
+    float depth = 0.0f;
+    void record(V3f w, V3f a, V3f n) {  // shade_surface.slang:59-63
+        albedo[0] += w.x * a.x; albedo[1] += w.y * a.y; albedo[2] += w.z * a.z;
+        normal[0] += w.x * n.x; normal[1] += w.y * n.y; normal[2] += w.z * n.z;
+    }
+};
+
 // One sample of one pixel: raygen, then the bounce loop. Returns RGBA.
 void trace_path(const Scene& s, uint32_t width, uint32_t height, uint32_t pixel, uint32_t sample,
-                uint32_t max_bounces, uint32_t light_sampling, float out[4], RayCounts& counts) {
+                uint32_t max_bounces, uint32_t light_sampling, float out[4], RayCounts& counts,
+                Guides* aov = nullptr) {
     float rad[4] = {0, 0, 0, 0};
     // raygen.slang:66-112 with the basis of wavefront.rs:633-675
     V3f right = s.cam_right, up = s.cam_up, fwd = s.cam_fwd;
@@ -276,7 +289,7 @@ void trace_path(const Scene& s, uint32_t width, uint32_t height, uint32_t pixel,
         dir = normalize(target - off);
     }
     float dir_w = dot(dir, normalize(fwd));
-    (void)dir_w;
+    V3f guide(1.0f);  // the open feature throughput; a camera ray's is 1
     V3f thr(1.0f);
     float thr_w = 0.0f;
     uint32_t medium = MEDIUM_NONE;
@@ -293,6 +306,10 @@ void trace_path(const Scene& s, uint32_t width, uint32_t height, uint32_t pixel,
                 if (light_sampling == LIGHT_SAMPLING_NEE) weight = 0.0f;
                 else if (light_sampling == LIGHT_SAMPLING_MIS)
                     weight = power_heuristic(thr_w, s.select_prob * env_pdf(s.env, dir));
+            }
+            if (aov) {  // shade_miss.slang:52-66
+                if (thr_w == 0.0f) aov->depth += INFINITY;
+                aov->albedo[0] += guide.x; aov->albedo[1] += guide.y; aov->albedo[2] += guide.z;
             }
             V3f c = thr * env_radiance(s.env, dir) * weight;
             rad[0] += c.x; rad[1] += c.y; rad[2] += c.z; rad[3] += 1.0f;
@@ -330,6 +347,14 @@ void trace_path(const Scene& s, uint32_t width, uint32_t height, uint32_t pixel,
         V3f wo = frame.to_local(-dir);
         MaterialT<float> mt = to_t<float>(mat);
         BF::Closure closure = BF::resolve(tables, mt, wo, medium == hit.instance);
+        V3f aov_alb(0.0f);
+        if (aov) {  // shade_surface.slang:322-340
+            if (bounce == 0) aov->depth += length(origin - spawn.position) * dir_w;
+            aov_alb = vclamp(closure.aov_albedo, 0.0f, 1.0f);
+        }
+        auto record_open = [&](V3f w) {
+            if (aov && any_gt0(w)) aov->record(w, aov_alb, shading);
+        };
 
         bool shadow_live = false;
         V3f sh_org, sh_dir, sh_contrib;
@@ -338,6 +363,7 @@ void trace_path(const Scene& s, uint32_t width, uint32_t height, uint32_t pixel,
         bool terminal = false, cont = false;
 
         if (bounce + 1 >= max_bounces) {
+            record_open(guide);
             rad[0] += contribution.x; rad[1] += contribution.y; rad[2] += contribution.z; rad[3] += 1.0f;
             break;
         }
@@ -401,8 +427,14 @@ void trace_path(const Scene& s, uint32_t width, uint32_t height, uint32_t pixel,
             else scattered = scattered / survival;
         }
         if (terminal) {
+            record_open(guide);
             rad[0] += contribution.x; rad[1] += contribution.y; rad[2] += contribution.z; rad[3] += 1.0f;
         } else {
+            if (aov) {  // shade_surface.slang:488-503
+                float rec = BF::aov_record_fraction(closure, sc.lobe);
+                if (rec > 0.0f) record_open(guide * rec);
+                guide = guide * (1.0f - rec) * BF::aov_pass_tint(closure, sc.lobe);
+            }
             if (sc.lobe == LOBE_TRANSMISSION && mat.thin_walled == 0)
                 medium = medium == hit.instance ? MEDIUM_NONE : hit.instance;
             bool transmitted = sc.wi.z < 0.0f;
@@ -555,9 +587,11 @@ void oracle_scene_env_tables(void* p, float* marginal, float* conditional, float
 // Accumulate samples [sample_begin, sample_begin + sample_count) into
 // sum_rgba (w·h·4 floats, added to what is there) with the film's
 // non-finite guard (accumulate.slang:38-44), over `threads` host threads.
+// The guide sums (albedo/normal w·h·4, depth w·h) are accumulated alongside
+// when the pointers are non-null, each with its own guard (accumulate.slang:49-67).
 void oracle_render(void* p, uint32_t width, uint32_t height, uint32_t sample_begin, uint32_t sample_count,
                    uint32_t max_bounces, uint32_t light_sampling, uint32_t threads, float* sum_rgba,
-                   uint64_t* ray_counts) {
+                   uint64_t* ray_counts, float* albedo_sum, float* normal_sum, float* depth_sum) {
     Scene* s = static_cast<Scene*>(p);
     oracle_camera cam;
     wr3(cam.position, s->cam_pos);
@@ -581,9 +615,18 @@ void oracle_render(void* p, uint32_t width, uint32_t height, uint32_t sample_beg
                 float* dst = sum_rgba + size_t(4) * pixel;
                 for (uint32_t k = 0; k < sample_count; ++k) {
                     float v[4];
-                    trace_path(*s, width, height, pixel, sample_begin + k, max_bounces, light_sampling, v, rc);
+                    Guides g;
+                    trace_path(*s, width, height, pixel, sample_begin + k, max_bounces, light_sampling, v, rc,
+                               albedo_sum ? &g : nullptr);
                     if (finite4(v))
                         for (int c = 0; c < 4; ++c) dst[c] += v[c];
+                    if (albedo_sum) {
+                        if (finite4(g.albedo))
+                            for (int c = 0; c < 4; ++c) albedo_sum[size_t(4) * pixel + c] += g.albedo[c];
+                        if (finite4(g.normal))
+                            for (int c = 0; c < 4; ++c) normal_sum[size_t(4) * pixel + c] += g.normal[c];
+                        depth_sum[pixel] += std::isnan(g.depth) ? 0.0f : g.depth;
+                    }
                 }
             }
         }
