@@ -114,7 +114,8 @@ EXPORTED_SYMBOLS = [
     "cenote_film_samples", "cenote_accumulate", "cenote_accumulate_n", "cenote_film_averages", "cenote_film_sums",
     "cenote_film_device_sums", "cenote_probe_sampler", "cenote_probe_bsdf", "cenote_probe_bsdf_sample",
     "cenote_probe_intersect", "cenote_probe_shadow", "cenote_probe_env_sample", "cenote_probe_env_pdf",
-    "cenote_env_tables_static",
+    "cenote_env_tables_static", "cenote_scene_create_textured", "cenote_texture_bytes", "cenote_texture_encode",
+    "cenote_probe_texture",
 ]
 
 _lib = None
@@ -136,6 +137,10 @@ def library() -> C.CDLL:
         "cenote_context_stream": (P, [P]),
         "cenote_synchronize": (I32, [P]),
         "cenote_scene_create": (I32, [P, P, U32, P, P, P, U32, P]),
+        "cenote_scene_create_textured": (I32, [P, P, U32, P, P, P, U32, P, U32, P]),
+        "cenote_texture_bytes": (C.c_uint64, [U32, U32, U32]),
+        "cenote_texture_encode": (I32, [U32, P, U32, U32, P]),
+        "cenote_probe_texture": (I32, [P, U32, U32, P, U32, P]),
         "cenote_scene_destroy": (None, [P]),
         "cenote_scene_set_camera": (I32, [P, P]),
         "cenote_scene_prep_times": (I32, [P, P]),
@@ -276,6 +281,26 @@ def env_tables_static(ctx: "Context", texels_ptr: int, width: int, height: int, 
     return power.value
 
 
+class TextureC(C.Structure):
+    _fields_ = [("format", C.c_uint32), ("width", C.c_uint32), ("height", C.c_uint32), ("pad", C.c_uint32),
+                ("data", C.c_void_p)]
+
+
+def texture_bytes(fmt: int, width: int, height: int) -> int:
+    return int(library().cenote_texture_bytes(fmt, width, height))
+
+
+def encode_texture(fmt: int, tex: scenes.Texture) -> scenes.Texture:
+    """BC-encode an RGBA8 texture (the host prep step; no device needed)."""
+    src = np.ascontiguousarray(tex.data, np.uint8)
+    n = texture_bytes(fmt, tex.width, tex.height)
+    if n == 0:
+        raise CenoteError(-1, f"format {fmt} cannot hold a {tex.width}x{tex.height} texture")
+    out = np.zeros(n, np.uint8)
+    _check(library().cenote_texture_encode(fmt, _ptr(src), tex.width, tex.height, _ptr(out)))
+    return scenes.Texture(fmt, tex.width, tex.height, out)
+
+
 class Scene:
     """Scene::new: meshes, transforms and materials, a camera and an environment."""
 
@@ -305,9 +330,16 @@ class Scene:
             deltas[i].anchor[:] = list(d.anchor)
             deltas[i].emission[:] = list(d.emission)
         cam = _c_camera(spec.camera)
+        texs = (TextureC * max(1, len(spec.textures)))()
+        for k, t in enumerate(spec.textures):
+            data = np.ascontiguousarray(t.data)
+            self._keep.append(data)
+            texs[k].format, texs[k].width, texs[k].height = t.format, t.width, t.height
+            texs[k].data = _ptr(data)
         h = C.c_void_p()
-        _check(lib.cenote_scene_create(ctx.handle, objs, len(spec.objects), C.byref(cam), C.byref(envc), deltas,
-                                       len(spec.delta_lights), C.byref(h)))
+        _check(lib.cenote_scene_create_textured(ctx.handle, objs, len(spec.objects), C.byref(cam), C.byref(envc),
+                                                deltas, len(spec.delta_lights), texs, len(spec.textures),
+                                                C.byref(h)))
         self._h = h
         self._keep = None  # the library copied everything it needs
 
@@ -374,6 +406,13 @@ class Scene:
         rc = np.zeros((n, 2), np.uint32)
         _check(library().cenote_probe_env_sample(self._h, _ptr(u), n, _ptr(d), _ptr(pdf), _ptr(rc)))
         return d, pdf, rc
+
+    def probe_texture(self, index: int, uv: np.ndarray, mode: int = 0) -> np.ndarray:
+        """n taps of bindless slot `index`: 0 filtered texel, 1 sampleColor, 2 sampleScalar, 3 sampleNormal."""
+        u = np.ascontiguousarray(uv, np.float32).reshape(-1, 2)
+        out = np.zeros((len(u), 4), np.float32)
+        _check(library().cenote_probe_texture(self._h, index, mode, _ptr(u), len(u), _ptr(out)))
+        return out
 
     def probe_env_pdf(self, directions: np.ndarray):
         d = np.ascontiguousarray(directions, np.float32)

@@ -18,6 +18,7 @@
 #include "../../include/cenote_c.h"
 #include "bvh_build.h"
 #include "records.h"
+#include "texture_prep.h"
 #include "wavefront.h"
 
 namespace cn {
@@ -36,6 +37,8 @@ void probe_shadow(const DeviceScene& scene, const float3* org, const float3* dir
 void probe_env_sample(const DeviceScene& scene, const float2* u, uint32_t n, float3* dir, float* pdf, uint2* rc,
                       cudaStream_t s);
 void probe_env_pdf(const DeviceScene& scene, const float3* d, uint32_t n, float* pdf, cudaStream_t s);
+void probe_texture(const DeviceScene& scene, uint32_t index, uint32_t mode, const float2* uv, uint32_t n, float4* out,
+                   cudaStream_t s);
 cudaError_t static_env_scratch(int device, double** out, size_t* max_texels, uint32_t* max_rows);
 }  // namespace cn
 
@@ -308,6 +311,8 @@ struct cenote_scene {
     DeviceBuffer* env_marginal = nullptr;
     DeviceBuffer* env_conditional = nullptr;
     DeviceBuffer* env_pdfs = nullptr;
+    std::vector<cudaArray_t> tex_arrays;            // the bindless table's storage
+    std::vector<cudaTextureObject_t> tex_objects;
 
     DeviceBuffer* add(size_t bytes, cudaError_t* err) {
         buffers.push_back(std::make_unique<DeviceBuffer>());
@@ -316,6 +321,8 @@ struct cenote_scene {
         return buffers.back().get();
     }
     ~cenote_scene() {
+        for (cudaTextureObject_t t : tex_objects) cudaDestroyTextureObject(t);
+        for (cudaArray_t a : tex_arrays) cudaFreeArray(a);
         if (env_tex) cudaDestroyTextureObject(env_tex);
         if (env_array) cudaFreeArray(env_array);
     }
@@ -459,9 +466,93 @@ int32_t cenote_synchronize(cenote_context* ctx) {
 
 // ---- scene -------------------------------------------------------------------------
 
+}  // extern "C"
+
+namespace {
+
+// One bindless slot: a CUDA array holding the texels (BC formats: an array
+// of the block-compressed channel kind, texel extents, filled one block row
+// at a time) and a bilinear, repeat-addressed texture object over normalised
+// coordinates.
+cudaError_t upload_texture(const cenote_texture& t, cudaStream_t stream, cudaArray_t* arr, cudaTextureObject_t* obj,
+                           uint64_t* bytes) {
+    const uint32_t w = t.width, h = t.height;
+    cudaChannelFormatDesc fmt{};
+    size_t row = 0, rows = h;
+    bool block = false;
+    switch (t.format) {
+    case CENOTE_TEXTURE_RGBA8_SRGB:
+    case CENOTE_TEXTURE_RGBA8_UNORM:
+        fmt = cudaCreateChannelDesc<uchar4>();
+        row = size_t(w) * 4;
+        break;
+    case CENOTE_TEXTURE_RGBA32F:
+        fmt = cudaCreateChannelDesc<float4>();
+        row = size_t(w) * 16;
+        break;
+    case CENOTE_TEXTURE_BC1_SRGB:
+        fmt = cudaCreateChannelDesc<cudaChannelFormatKindUnsignedBlockCompressed1SRGB>();
+        block = true;
+        break;
+    case CENOTE_TEXTURE_BC1_UNORM:
+        fmt = cudaCreateChannelDesc<cudaChannelFormatKindUnsignedBlockCompressed1>();
+        block = true;
+        break;
+    case CENOTE_TEXTURE_BC4_UNORM:
+        fmt = cudaCreateChannelDesc<cudaChannelFormatKindUnsignedBlockCompressed4>();
+        block = true;
+        break;
+    case CENOTE_TEXTURE_BC5_UNORM:
+        fmt = cudaCreateChannelDesc<cudaChannelFormatKindUnsignedBlockCompressed5>();
+        block = true;
+        break;
+    default:
+        return cudaErrorInvalidValue;
+    }
+    if (block) {
+        row = size_t(w / 4) * (t.format == CENOTE_TEXTURE_BC5_UNORM ? 16 : 8);
+        rows = h / 4;
+    }
+    cudaError_t e = cudaMallocArray(arr, &fmt, w, h);
+    if (e != cudaSuccess) return e;
+    *bytes += row * rows;
+    e = cudaMemcpy2DToArrayAsync(*arr, 0, 0, t.data, row, row, rows, cudaMemcpyHostToDevice, stream);
+    if (e != cudaSuccess) return e;
+    cudaResourceDesc res{};
+    res.resType = cudaResourceTypeArray;
+    res.res.array.array = *arr;
+    cudaTextureDesc td{};
+    td.addressMode[0] = cudaAddressModeWrap;
+    td.addressMode[1] = cudaAddressModeWrap;
+    td.filterMode = cudaFilterModeLinear;
+    td.normalizedCoords = 1;
+    td.sRGB = (t.format == CENOTE_TEXTURE_RGBA8_SRGB || t.format == CENOTE_TEXTURE_BC1_SRGB) ? 1 : 0;
+    td.readMode = t.format == CENOTE_TEXTURE_RGBA32F ? cudaReadModeElementType : cudaReadModeNormalizedFloat;
+    e = cudaCreateTextureObject(obj, &res, &td, nullptr);
+    if (e != cudaSuccess && block) {
+        // Block formats decode to unorm floats by themselves; accept the
+        // element-type read mode where the runtime asks for it.
+        cudaGetLastError();
+        td.readMode = cudaReadModeElementType;
+        e = cudaCreateTextureObject(obj, &res, &td, nullptr);
+    }
+    return e;
+}
+
+}  // namespace
+
+extern "C" {
+
 int32_t cenote_scene_create(cenote_context* ctx, const cenote_object* objects, uint32_t object_count,
                             const cenote_camera* camera, const cenote_environment* env,
                             const cenote_delta_light* deltas, uint32_t delta_count, cenote_scene** out) {
+    return cenote_scene_create_textured(ctx, objects, object_count, camera, env, deltas, delta_count, nullptr, 0, out);
+}
+
+int32_t cenote_scene_create_textured(cenote_context* ctx, const cenote_object* objects, uint32_t object_count,
+                                     const cenote_camera* camera, const cenote_environment* env,
+                                     const cenote_delta_light* deltas, uint32_t delta_count,
+                                     const cenote_texture* textures, uint32_t texture_count, cenote_scene** out) {
     CN_CHECK(ctx && out, CENOTE_E_INVALID_ARGUMENT, "null context or output handle");
     *out = nullptr;
     CN_CHECK(objects && object_count > 0, CENOTE_E_INVALID_ARGUMENT, "a scene needs at least one object");
@@ -473,6 +564,19 @@ int32_t cenote_scene_create(cenote_context* ctx, const cenote_object* objects, u
     for (uint32_t i = 0; i < delta_count; ++i)
         CN_CHECK(deltas[i].kind == KIND_DISTANT || deltas[i].kind == KIND_POINT, CENOTE_E_INVALID_ARGUMENT,
                  "unknown delta-light kind");
+    CN_CHECK(texture_count == 0 || textures, CENOTE_E_INVALID_ARGUMENT, "null texture array");
+    for (uint32_t k = 0; k < texture_count; ++k)
+        CN_CHECK(textures[k].data && texture_bytes(textures[k].format, textures[k].width, textures[k].height) > 0,
+                 CENOTE_E_INVALID_ARGUMENT, "texture " + std::to_string(k) + " has an unknown format, no data, or a "
+                 "size its format cannot take");
+    for (uint32_t i = 0; i < object_count; ++i) {
+        const cenote_material& m = objects[i].material;
+        for (uint32_t slot : {m.base_color_texture, m.specular_roughness_texture, m.metalness_texture,
+                              m.emission_texture, m.opacity_texture, m.normal_texture})
+            CN_CHECK(slot == TEXTURE_NONE || slot < texture_count, CENOTE_E_SCENE,
+                     "object " + std::to_string(i) + " names texture slot " + std::to_string(slot) + " of " +
+                         std::to_string(texture_count));
+    }
     std::lock_guard<std::mutex> lock(ctx->mu);
     CN_CUDA(cudaSetDevice(ctx->device));
     auto t_start = std::chrono::steady_clock::now();
@@ -642,7 +746,27 @@ int32_t cenote_scene_create(cenote_context* ctx, const cenote_object* objects, u
     td.normalizedCoords = 1;
     CN_CUDA(cudaCreateTextureObject(&sc->env_tex, &res, &td, nullptr));
 
+    // The bindless table.
+    sc->tex_arrays.assign(texture_count, nullptr);
+    sc->tex_objects.assign(texture_count, 0);
+    for (uint32_t k = 0; k < texture_count; ++k) {
+        cudaError_t te = upload_texture(textures[k], ctx->stream, &sc->tex_arrays[k], &sc->tex_objects[k],
+                                        &sc->device_bytes);
+        if (te != cudaSuccess) {
+            cudaGetLastError();
+            return fail(CENOTE_E_DEVICE, "texture " + std::to_string(k) + ": " + cudaGetErrorString(te));
+        }
+    }
+    DeviceBuffer* btexs = sc->add(std::max<size_t>(1, texture_count) * 8, &err);
+    CN_CUDA(err);
+    if (texture_count)
+        CN_CUDA(cudaMemcpyAsync(btexs->ptr, sc->tex_objects.data(), size_t(texture_count) * 8, cudaMemcpyHostToDevice,
+                                ctx->stream));
+    CN_CUDA(cudaStreamSynchronize(ctx->stream));
+
     DeviceScene& ds = sc->ds;
+    ds.textures = btexs->as<unsigned long long>();
+    ds.texture_count = texture_count;
     ds.nodes = bnodes->as<WideNode>();
     ds.tris = btris->as<float4>();
     ds.geometry = bgeo->as<GeomRecord>();
@@ -1148,6 +1272,34 @@ int32_t cenote_probe_env_pdf(cenote_scene* sc, const float* directions, uint32_t
                               probe_env_pdf(sc->ds, static_cast<float3*>(i[0]), n, static_cast<float*>(o[0]),
                                             ctx->stream);
                           });
+}
+
+int32_t cenote_probe_texture(cenote_scene* sc, uint32_t index, uint32_t mode, const float* uv, uint32_t n, float* rgba) {
+    CN_CHECK(sc && uv && rgba, CENOTE_E_INVALID_ARGUMENT, "null argument");
+    CN_CHECK(index < sc->ds.texture_count, CENOTE_E_INVALID_ARGUMENT, "texture index out of range");
+    CN_CHECK(mode <= 3, CENOTE_E_INVALID_ARGUMENT, "unknown probe mode");
+    if (n == 0) return CENOTE_OK;
+    cenote_context* ctx = sc->ctx;
+    std::lock_guard<std::mutex> lock(ctx->mu);
+    CN_CUDA(cudaSetDevice(ctx->device));
+    return with_device_io(ctx, {{uv, size_t(n) * 8}}, {{rgba, size_t(n) * 16}},
+                          [&](std::vector<void*>& i, std::vector<void*>& o) {
+                              probe_texture(sc->ds, index, mode, static_cast<float2*>(i[0]), n,
+                                            static_cast<float4*>(o[0]), ctx->stream);
+                          });
+}
+
+// ---- texture prep ----------------------------------------------------------------------
+
+uint64_t cenote_texture_bytes(uint32_t format, uint32_t width, uint32_t height) {
+    return texture_bytes(format, width, height);
+}
+
+int32_t cenote_texture_encode(uint32_t format, const uint8_t* rgba8, uint32_t width, uint32_t height, void* out) {
+    CN_CHECK(rgba8 && out, CENOTE_E_INVALID_ARGUMENT, "null argument");
+    CN_CHECK(texture_encode(format, rgba8, width, height, static_cast<uint8_t*>(out)), CENOTE_E_INVALID_ARGUMENT,
+             "not a BC format, or a size it cannot take (BC extents are multiples of 4)");
+    return CENOTE_OK;
 }
 
 // ---- environment tables without device allocation ------------------------------------

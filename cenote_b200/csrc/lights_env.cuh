@@ -20,6 +20,7 @@ struct LightConn {
     bool delta;
     uint32_t instance, primitive;
     uint32_t record;  // the light record drawn (slot or its alias)
+    float b1, b2;     // triangle lights: the sampled point's barycentrics (lights.slang:76-87)
 };
 
 __device__ __forceinline__ LightConn sample_lights(const LightRecord* lights, uint32_t count, float u, float2 up,
@@ -44,9 +45,12 @@ __device__ __forceinline__ LightConn sample_lights(const LightRecord* lights, ui
     r.instance = __float_as_uint(d.w);
     r.primitive = __float_as_uint(e.y);
     r.record = rec;
+    r.b1 = r.b2 = 0.0f;
     if (kind == KIND_TRIANGLE) {
         float su = sqrtf(up.x);
         float b1 = 1.0f - su, b2 = up.y * su;
+        r.b1 = b1;
+        r.b2 = b2;
         float3 pos = anchor + b1 * edge1 + b2 * edge2;
         float3 delta = pos - from;
         float r2 = dot(delta, delta);

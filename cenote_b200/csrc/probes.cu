@@ -8,6 +8,7 @@
 #include "openpbr.cuh"
 #include "sampler.cuh"
 #include "shadow.cuh"
+#include "textures.cuh"
 #include "traverse.cuh"
 
 namespace cn {
@@ -99,6 +100,27 @@ __global__ void k_probe_env_pdf(DeviceScene scene, const float3* d, uint32_t n, 
     pdf[i] = env_pdf(scene, d[i]);
 }
 
+// One raw tap per UV of a bindless slot (mode 0: the texel as filtered;
+// 1: sampleColor; 2: sampleScalar in x; 3: sampleNormal).
+__global__ void k_probe_texture(DeviceScene scene, uint32_t index, uint32_t mode, const float2* uv, uint32_t n,
+                                float4* out) {
+    uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    float4 r;
+    if (mode == 1) {
+        float3 c = sample_color(scene, index, uv[i]);
+        r = make_float4(c.x, c.y, c.z, 0.0f);
+    } else if (mode == 2) {
+        r = make_float4(sample_scalar(scene, index, uv[i]), 0.0f, 0.0f, 0.0f);
+    } else if (mode == 3) {
+        float3 c = sample_normal(scene, index, uv[i]);
+        r = make_float4(c.x, c.y, c.z, 0.0f);
+    } else {
+        r = sample_texture(scene, index, uv[i]);
+    }
+    out[i] = r;
+}
+
 inline int blocks(uint32_t n) { return int((n + 127) / 128); }
 
 }  // namespace
@@ -128,6 +150,10 @@ void probe_env_sample(const DeviceScene& scene, const float2* u, uint32_t n, flo
 }
 void probe_env_pdf(const DeviceScene& scene, const float3* d, uint32_t n, float* pdf, cudaStream_t s) {
     k_probe_env_pdf<<<blocks(n), 128, 0, s>>>(scene, d, n, pdf);
+}
+void probe_texture(const DeviceScene& scene, uint32_t index, uint32_t mode, const float2* uv, uint32_t n, float4* out,
+                   cudaStream_t s) {
+    k_probe_texture<<<blocks(n), 128, 0, s>>>(scene, index, mode, uv, n, out);
 }
 
 }  // namespace cn

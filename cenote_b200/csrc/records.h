@@ -97,6 +97,9 @@ struct DeviceScene {
     uint32_t has_nonopaque;
     uint32_t pad;
     const uint32_t* light_leaf;  // per light record: its triangle's leaf index, ~0 for delta lights
+    const unsigned long long* textures;  // cudaTextureObject_t per bindless slot
+    uint32_t texture_count;
+    uint32_t pad2;
 };
 
 // One queued shadow ray: 64 bytes, four 16-byte lanes.

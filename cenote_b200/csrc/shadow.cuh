@@ -10,6 +10,7 @@
 // transparency in, as the reference's candidate loop does.
 #pragma once
 #include "records.h"
+#include "textures.cuh"
 #include "traverse.cuh"
 
 namespace cn {
@@ -49,7 +50,7 @@ __device__ __forceinline__ float shadow_query(const DeviceScene& scene, const Ra
             return false;  // the target wins the tie
         }
         if (!(__float_as_uint(c.w) & TRI_OPAQUE) && !target) {
-            atten *= 1.0f - __ldg(&scene.materials[inst].opacity);
+            atten *= 1.0f - opacity_at(scene, inst, prim, b1, b2);
             if (atten < 1e-4f) {
                 occluded = true;
                 return true;

@@ -1,0 +1,14 @@
+// Host texture prep (texture_prep.cpp): data sizes and the BC block encoder.
+#pragma once
+#include <cstdint>
+
+namespace cn {
+
+// Bytes of a texture's data for its format and size; 0 when invalid (unknown
+// format, zero or oversize extent, BC extents not multiples of 4).
+uint64_t texture_bytes(uint32_t format, uint32_t width, uint32_t height);
+// RGBA8 texels -> BC1 (RGB), BC4 (R) or BC5 (R, G) blocks; false if the
+// format is not a BC format or the size is invalid.
+bool texture_encode(uint32_t format, const uint8_t* rgba, uint32_t width, uint32_t height, uint8_t* out);
+
+}  // namespace cn

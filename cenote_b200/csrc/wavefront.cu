@@ -22,6 +22,7 @@
 #include "openpbr.cuh"
 #include "sampler.cuh"
 #include "shadow.cuh"
+#include "textures.cuh"
 #include "traverse.cuh"
 
 namespace cn {
@@ -163,7 +164,7 @@ __global__ void __launch_bounds__(BLOCK, CN_TRAV_MIN_BLOCKS) k_intersect(DeviceS
             uint32_t inst = __float_as_uint(a.w), prim = __float_as_uint(b.w);
             if (!(t < tm || (t == tm && (inst < best_inst || (inst == best_inst && prim < best_prim))))) return false;
             if (!(flags & TRI_OPAQUE)) {
-                float opacity = __ldg(&scene.materials[inst].opacity);
+                float opacity = opacity_at(scene, inst, prim, b1, b2);
                 bool commit = crossings >= TRANSPARENT_CAP || hash_uniform(pixel, sample, bounce, crossings) < opacity;
                 crossings++;
                 if (!commit) return false;
@@ -311,7 +312,17 @@ __global__ void __launch_bounds__(BLOCK, CN_SHADE_MIN_BLOCKS) k_shade(DeviceScen
                 load_geom(scene.geometry + inst, g);
                 Material mat;
                 load_material(scene.materials + inst, mat);
+                // Textured parameters resolve once at the hit's UV
+                // (shade_surface.slang:249-252).
+                const bool normal_map = mat.normal_texture != TEXTURE_NONE;
+                float2 uv = make_float2(0.0f, 0.0f);
+                if (has_parameter_maps(mat) || normal_map) {
+                    uv = interpolate_uv(g.uvs, g.indices, prim, b1, b2);
+                    resolve_material(scene, mat, uv);
+                }
                 Spawn sp = spawn_point(g, prim, b1, b2, dir);
+                if (normal_map)
+                    sp.shading = mapped_shading_normal(scene, inst, prim, uv, mat.normal_texture, sp.shading, sp.normal);
                 uint32_t medium = bounce == 0 ? MEDIUM_NONE : (pool.state[path] & 0xffffffu);
                 if (medium != MEDIUM_NONE) {
                     const Material& in = scene.materials[medium];
@@ -374,6 +385,14 @@ __global__ void __launch_bounds__(BLOCK, CN_SHADE_MIN_BLOCKS) k_shade(DeviceScen
                         } else {
                             float u_list = (u_light - env_prob) / (1.0f - env_prob);
                             LightConn cand = sample_lights(scene.lights, scene.light_count, u_list, u_point, sp.position);
+                            if (!cand.delta) {
+                                // A textured emitter evaluates its map at the sampled point
+                                // (shade_surface.slang:405-418).
+                                uint32_t em = __ldg(&scene.materials[cand.instance].emission_texture);
+                                if (em != TEXTURE_NONE)
+                                    cand.radiance = cand.radiance * emission_map(scene, em, cand.instance,
+                                                                                 cand.primitive, cand.b1, cand.b2);
+                            }
                             cdir = cand.direction;
                             crad = cand.radiance;
                             cpdf = cand.pdf;

@@ -303,6 +303,64 @@ class DeltaLight:
     emission: tuple
 
 
+# Texture formats of the bindless table (include/cenote_c.h CENOTE_TEXTURE_*).
+TEX_RGBA8_SRGB, TEX_RGBA8_UNORM, TEX_RGBA32F = 1, 2, 3
+TEX_BC1_SRGB, TEX_BC1_UNORM, TEX_BC4_UNORM, TEX_BC5_UNORM = 4, 5, 6, 7
+
+
+@dataclass
+class Texture:
+    """One slot of the bindless table: `data` is the texels (RGBA8 as uint8
+    (H, W, 4), RGBA32F as float32 (H, W, 4)) or the BC blocks as uint8."""
+    format: int
+    width: int
+    height: int
+    data: np.ndarray
+
+
+def rgba8_texture(rgb, srgb: bool = True, alpha=None) -> Texture:
+    """An RGBA8 texture from float RGB in [0, 1] (H, W, 3), stored sRGB-encoded
+    (colour) or linear (scalars, normal maps)."""
+    rgb = np.clip(np.asarray(rgb, np.float64), 0.0, 1.0)
+    if srgb:
+        rgb = np.where(rgb <= 0.0031308, rgb * 12.92, 1.055 * rgb ** (1 / 2.4) - 0.055)
+    h, w = rgb.shape[:2]
+    a = np.ones((h, w)) if alpha is None else np.clip(alpha, 0, 1)
+    px = np.round(np.concatenate([rgb, a[..., None]], -1) * 255.0).astype(np.uint8)
+    return Texture(TEX_RGBA8_SRGB if srgb else TEX_RGBA8_UNORM, w, h, np.ascontiguousarray(px))
+
+
+def value_noise(size: int, seed: int, octaves: int = 4, base: int = 8) -> np.ndarray:
+    """Seeded tileable value noise in [0, 1], (size, size): smoothstep-
+    interpolated lattice values, octaves summed with halving amplitude."""
+    rng = np.random.default_rng(seed)
+    out = np.zeros((size, size))
+    amp, total = 1.0, 0.0
+    for o in range(octaves):
+        cells = base << o
+        lattice = rng.random((cells, cells))
+        x = np.arange(size) * cells / size
+        i0 = np.floor(x).astype(int) % cells
+        i1 = (i0 + 1) % cells
+        f = x - np.floor(x)
+        f = f * f * (3 - 2 * f)
+        rows = lattice[i0][:, i0] * (1 - f)[None, :] + lattice[i0][:, i1] * f[None, :]
+        rows1 = lattice[i1][:, i0] * (1 - f)[None, :] + lattice[i1][:, i1] * f[None, :]
+        out += amp * (rows * (1 - f)[:, None] + rows1 * f[:, None])
+        total += amp
+        amp *= 0.5
+    return out / total
+
+
+def normal_map_from_height(height: np.ndarray, strength: float = 4.0) -> np.ndarray:
+    """Tangent-space normals (x, y in [0, 1] encoding) of a tileable height field."""
+    gx = (np.roll(height, -1, 1) - np.roll(height, 1, 1)) * 0.5 * strength
+    gy = (np.roll(height, -1, 0) - np.roll(height, 1, 0)) * 0.5 * strength
+    n = np.stack([-gx, -gy, np.ones_like(height)], -1)
+    n /= np.linalg.norm(n, axis=-1, keepdims=True)
+    return n * 0.5 + 0.5
+
+
 @dataclass
 class SceneSpec:
     name: str
@@ -314,6 +372,7 @@ class SceneSpec:
     spp: int
     max_bounces: int
     delta_lights: list = field(default_factory=list)
+    textures: list = field(default_factory=list)
 
     @property
     def triangle_count(self) -> int:
@@ -420,6 +479,9 @@ def save_spec(path, spec: SceneSpec, **extra) -> None:
     arrs["delta"] = np.array([[d.kind, *d.anchor, *d.emission] for d in spec.delta_lights], np.float64).reshape(-1, 7)
     arrs["settings"] = np.array([spec.width, spec.height, spec.spp, spec.max_bounces, len(spec.objects)], np.int64)
     arrs["name"] = np.array(spec.name)
+    for k, t in enumerate(spec.textures):
+        arrs[f"t{k}_shape"] = np.array([t.format, t.width, t.height], np.int64)
+        arrs[f"t{k}_data"] = np.asarray(t.data)
     arrs.update({f"x_{k}": np.asarray(v) for k, v in extra.items()})
     np.savez_compressed(path, **arrs)
 
@@ -437,5 +499,56 @@ def load_spec(path) -> tuple[SceneSpec, dict]:
     cam = Camera(tuple(c[0:3]), tuple(c[3:6]), tuple(c[6:9]), float(c[9]), float(c[10]), float(c[11]))
     env = z["env"]
     deltas = [DeltaLight(int(d[0]), tuple(d[1:4]), tuple(d[4:7])) for d in z["delta"]]
-    spec = SceneSpec(str(z["name"]), objs, cam, Environment(env.shape[1], env.shape[0], env), w, h, spp, mb, deltas)
+    textures = []
+    while f"t{len(textures)}_shape" in z.files:
+        k = len(textures)
+        fmt, tw, th = (int(v) for v in z[f"t{k}_shape"])
+        textures.append(Texture(fmt, tw, th, z[f"t{k}_data"]))
+    spec = SceneSpec(str(z["name"]), objs, cam, Environment(env.shape[1], env.shape[0], env), w, h, spp, mb, deltas,
+                     textures)
     return spec, {k[2:]: z[k] for k in z.files if k.startswith("x_")}
+
+
+def textured(width=160, height=90, spp=8, max_bounces=6, size=64, seed=7) -> SceneSpec:
+    """Every texture slot and format on one small set: a ground tiled 4x with a
+    BC1 sRGB base colour, a BC5 normal map and a BC4 roughness map; a metal
+    panel with an RGBA8 metalness map; a leaf quad cut out by a BC4 opacity
+    map; a ceiling emitter whose emission an RGBA8 sRGB map modulates; an
+    RGBA32F base colour on a back wall. Textures are seeded value noise."""
+    from . import encode_texture  # host BC encoder of the library
+
+    noise = [value_noise(size, seed + k) for k in range(6)]
+    col = np.stack([0.2 + 0.7 * noise[0], 0.2 + 0.6 * noise[1], 0.1 + 0.5 * noise[0] * noise[2]], -1)
+    textures = [
+        encode_texture(TEX_BC1_SRGB, rgba8_texture(col, srgb=True)),                                 # 0 base colour
+        encode_texture(TEX_BC5_UNORM, rgba8_texture(normal_map_from_height(noise[3], 6.0), False)),  # 1 normal
+        encode_texture(TEX_BC4_UNORM, rgba8_texture(np.repeat(0.15 + 0.8 * noise[4][..., None], 3, -1), False)),
+        rgba8_texture(np.repeat((noise[5] > 0.5)[..., None].astype(float), 3, -1), srgb=False),       # 3 metalness
+        encode_texture(TEX_BC4_UNORM, rgba8_texture(np.repeat((noise[2] > 0.45)[..., None].astype(float), 3, -1),
+                                                    False)),                                          # 4 opacity
+        rgba8_texture(np.stack([np.linspace(0.2, 1, size)[None, :].repeat(size, 0)] * 3, -1), srgb=True),  # 5 emission
+        Texture(TEX_RGBA32F, 8, 8, np.ascontiguousarray(
+            np.concatenate([np.random.default_rng(seed).random((8, 8, 3)), np.ones((8, 8, 1))], -1), np.float32)),
+    ]
+    ident = rows(np.eye(4))
+    tiled = np.array([[0, 0], [0, 4], [4, 4], [4, 0]], np.float32)
+    ground = material(base_color=(0.8, 0.8, 0.8), specular_weight=1.0, specular_roughness=0.5)
+    ground["base_color_texture"], ground["normal_texture"], ground["specular_roughness_texture"] = 0, 1, 2
+    panel = metal(acescg((0.9, 0.7, 0.5)), 0.25)
+    panel["metalness_texture"] = 3
+    leaf = matte(acescg((0.3, 0.6, 0.2)))
+    leaf["opacity_texture"] = 4
+    lamp = emitter(acescg((6.0, 5.0, 4.0)))
+    lamp["emission_texture"] = 5
+    wall = matte(acescg((1.0, 1.0, 1.0)))
+    wall["base_color_texture"] = 6
+    objs = [
+        Object(quad([(-3, 0, -3), (-3, 0, 3), (3, 0, 3), (3, 0, -3)], uvs=tiled), ident, ground),
+        Object(quad([(-1.6, 0, -1.0), (-0.4, 0, -1.4), (-0.4, 1.2, -1.4), (-1.6, 1.2, -1.0)]), ident, panel),
+        Object(quad([(0.2, 0.1, 0.2), (1.4, 0.1, 0.2), (1.4, 1.3, -0.2), (0.2, 1.3, -0.2)]), ident, leaf),
+        Object(quad([(-0.8, 2.5, -0.8), (0.8, 2.5, -0.8), (0.8, 2.5, 0.8), (-0.8, 2.5, 0.8)]), ident, lamp),
+        Object(quad([(-3, 0, -2.5), (3, 0, -2.5), (3, 3, -2.5), (-3, 3, -2.5)]), ident, wall),
+    ]
+    cam = Camera((0.0, 1.4, 4.0), (0.0, 0.6, 0.0), vfov_degrees=45.0)
+    return SceneSpec("textured", objs, cam, Environment.constant((0.15, 0.18, 0.25)), width, height, spp,
+                     max_bounces, textures=textures)

@@ -117,6 +117,36 @@ typedef struct cenote_camera {
     float focus_distance;
 } cenote_camera;
 
+/* A material texture of the bindless table (crates/cenote/src/texture.rs,
+ * shaders/textures.slang): one level, bilinear, repeat addressing. Materials
+ * name it by its index in the array given to cenote_scene_create_textured.
+ * Usages: colour slots read RGB (sRGB storage decoded per texel, then
+ * Rec.709 -> ACEScg), scalar slots read R, normal maps read R/G as x/y. */
+#define CENOTE_TEXTURE_RGBA8_SRGB 1u  /* 8-bit RGBA, colour in sRGB transfer */
+#define CENOTE_TEXTURE_RGBA8_UNORM 2u /* 8-bit RGBA, linear */
+#define CENOTE_TEXTURE_RGBA32F 3u     /* float RGBA, linear (HDR colour) */
+#define CENOTE_TEXTURE_BC1_SRGB 4u    /* BC1 blocks, colour in sRGB transfer */
+#define CENOTE_TEXTURE_BC1_UNORM 5u   /* BC1 blocks, linear */
+#define CENOTE_TEXTURE_BC4_UNORM 6u   /* BC4 blocks: one channel (scalar masks) */
+#define CENOTE_TEXTURE_BC5_UNORM 7u   /* BC5 blocks: two channels (tangent-space normals) */
+
+typedef struct cenote_texture {
+    uint32_t format; /* CENOTE_TEXTURE_* */
+    uint32_t width;  /* texels; a multiple of 4 for the BC formats */
+    uint32_t height;
+    uint32_t pad;
+    /* Row 0 first: w·h texels, or the 4x4 blocks row-major over w/4 x h/4
+     * (8 bytes per BC1/BC4 block, 16 per BC5 block). */
+    const void* data;
+} cenote_texture;
+
+/* Bytes of `data` for a texture of this format and size; 0 if invalid. */
+uint64_t cenote_texture_bytes(uint32_t format, uint32_t width, uint32_t height);
+/* Encode RGBA8 texels (w·h·4 bytes, row 0 first) into BC1 (RGB), BC4 (R) or
+ * BC5 (R, G) blocks: `out` holds cenote_texture_bytes(format, w, h) bytes.
+ * Host work, no device needed (the prep step of texture.rs:221-405). */
+int32_t cenote_texture_encode(uint32_t format, const uint8_t* rgba8, uint32_t width, uint32_t height, void* out);
+
 /* Equirect environment, RGBA f32 ACEScg, row 0 = +Y (environment.rs:33-79). */
 typedef struct cenote_environment {
     uint32_t width;
@@ -177,6 +207,12 @@ int32_t cenote_synchronize(cenote_context* ctx);
 int32_t cenote_scene_create(cenote_context* ctx, const cenote_object* objects, uint32_t object_count,
                             const cenote_camera* camera, const cenote_environment* environment,
                             const cenote_delta_light* deltas, uint32_t delta_count, cenote_scene** out);
+/* Scene::prep with material textures (scene/prep.rs, lower.rs:92-206): every
+ * texture slot a material names must index `textures`. */
+int32_t cenote_scene_create_textured(cenote_context* ctx, const cenote_object* objects, uint32_t object_count,
+                                     const cenote_camera* camera, const cenote_environment* environment,
+                                     const cenote_delta_light* deltas, uint32_t delta_count,
+                                     const cenote_texture* textures, uint32_t texture_count, cenote_scene** out);
 void cenote_scene_destroy(cenote_scene* scene);
 /* Replace the camera (the viewer's orbit control writes Scene::camera_mut). */
 int32_t cenote_scene_set_camera(cenote_scene* scene, const cenote_camera* camera);
@@ -257,6 +293,11 @@ int32_t cenote_probe_env_sample(cenote_scene* scene, const float* u, uint32_t n,
                                 float* pdf, uint32_t* row_col);
 /* Environment pdf for n directions (environment.slang:111-120). */
 int32_t cenote_probe_env_pdf(cenote_scene* scene, const float* directions, uint32_t n, float* pdf);
+/* n taps of bindless slot `index` at uv (n·2 floats) into rgba (n·4 floats):
+ * mode 0 the filtered texel, 1 sampleColor, 2 sampleScalar, 3 sampleNormal
+ * (textures.slang:24-64). */
+int32_t cenote_probe_texture(cenote_scene* scene, uint32_t index, uint32_t mode, const float* uv, uint32_t n,
+                             float* rgba);
 
 /* ---- environment tables without device allocation --------------------------------- */
 

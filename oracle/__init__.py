@@ -42,13 +42,15 @@ def library() -> C.CDLL:
     lib = C.CDLL(str(LIB_PATH))
     P, U32, F, D = C.c_void_p, C.c_uint32, C.c_float, C.c_double
     sig = {
-        "oracle_scene_create": (P, [P, U32, P, U32, U32, P, P, U32, P]),
+        "oracle_scene_create": (P, [P, U32, P, U32, U32, P, P, U32, P, P, U32]),
         "oracle_scene_destroy": (None, [P]),
         "oracle_scene_light_count": (U32, [P]),
         "oracle_scene_lights": (None, [P, P]),
         "oracle_scene_select_prob": (F, [P]),
         "oracle_scene_env_power": (D, [P]),
         "oracle_scene_env_tables": (None, [P, P, P, P]),
+        "oracle_texture_decode": (C.c_int, [U32, U32, U32, P, P]),
+        "oracle_texture_sample": (C.c_int, [U32, U32, U32, P, U32, P, U32, P]),
         "oracle_render": (None, [P, U32, U32, U32, U32, U32, U32, U32, P, P, P, P, P]),
         "oracle_camera_basis": (None, [P, F, P, P, P]),
         "oracle_sampler": (None, [U32, U32, U32, P, P]),
@@ -118,6 +120,29 @@ def _camera(cam) -> _Camera:
     return c
 
 
+def texture_decode(tex) -> np.ndarray:
+    """Linear RGBA float texels (H, W, 4) of a scenes.Texture."""
+    out = np.zeros((tex.height, tex.width, 4), np.float32)
+    data = np.ascontiguousarray(tex.data)
+    if library().oracle_texture_decode(tex.format, tex.width, tex.height, _p(data), _p(out)) != 0:
+        raise ValueError("texture the oracle cannot decode")
+    return out
+
+
+def texture_sample(tex, uv, mode=0) -> np.ndarray:
+    u = np.ascontiguousarray(uv, np.float32).reshape(-1, 2)
+    out = np.zeros((len(u), 4), np.float32)
+    data = np.ascontiguousarray(tex.data)
+    if library().oracle_texture_sample(tex.format, tex.width, tex.height, _p(data), mode, _p(u), len(u), _p(out)) != 0:
+        raise ValueError("texture the oracle cannot decode")
+    return out
+
+
+class _Texture(C.Structure):
+    _fields_ = [("format", C.c_uint32), ("width", C.c_uint32), ("height", C.c_uint32), ("pad", C.c_uint32),
+                ("data", C.c_void_p)]
+
+
 class OracleScene:
     def __init__(self, spec):
         lib = library()
@@ -142,8 +167,17 @@ class OracleScene:
             deltas[i].anchor[:] = list(d.anchor)
             deltas[i].emission[:] = list(d.emission)
         tables = bsdf_tables()
+        textures = getattr(spec, "textures", [])
+        texs = (_Texture * max(1, len(textures)))()
+        for k, t in enumerate(textures):
+            data = np.ascontiguousarray(t.data)
+            keep.append(data)
+            texs[k].format, texs[k].width, texs[k].height = t.format, t.width, t.height
+            texs[k].data = _p(data)
         self._h = lib.oracle_scene_create(objs, len(spec.objects), C.byref(cam), env.width, env.height, _p(tex), deltas,
-                                          len(spec.delta_lights), _p(tables))
+                                          len(spec.delta_lights), _p(tables), texs, len(textures))
+        if not self._h:
+            raise ValueError("the oracle rejected the scene: a texture it cannot decode or a slot past the table")
 
     def render_sum(self, width, height, sample_begin, sample_count, max_bounces, light_sampling=0, threads=0,
                    out=None):

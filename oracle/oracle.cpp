@@ -17,6 +17,7 @@
 #include "lights_env.h"
 #include "openpbr.h"
 #include "rng.h"
+#include "textures.h"
 #include "trace.h"
 
 using namespace oracle;
@@ -53,6 +54,7 @@ struct Scene {
     V3f cam_pos, cam_look, cam_upv;       // Camera (scene/mod.rs:392-407)
     V3f cam_right, cam_up, cam_fwd;       // basis for the current target, scene/mod.rs:448-460
     float vfov = 40.0f, aperture = 0.0f, focus = 1.0f;
+    std::vector<Texture> textures;  // the bindless table, material slot order
 };
 
 // glam's Mat4::transform_point3 on the top three rows: ((x·p.x + y·p.y) + z·p.z) + w.
@@ -90,6 +92,67 @@ void invert_affine(const float m[3][4], float out[3][4]) {
 
 V3f mat_color(const float* f) { return {f[0], f[1], f[2]}; }
 
+// ---- textures (textures.slang:24-82, scene.slang:31-64) ---------------------
+
+struct F2v {
+    float x, y;
+};
+
+F2v interpolate_uv(const Instance& m, uint32_t prim, float b1, float b2) {
+    const float* uv0 = &m.uvs[2 * m.indices[3 * prim]];
+    const float* uv1 = &m.uvs[2 * m.indices[3 * prim + 1]];
+    const float* uv2 = &m.uvs[2 * m.indices[3 * prim + 2]];
+    return {uv0[0] + b1 * (uv1[0] - uv0[0]) + b2 * (uv2[0] - uv0[0]),
+            uv0[1] + b1 * (uv1[1] - uv0[1]) + b2 * (uv2[1] - uv0[1])};
+}
+
+void sample_texture(const Scene& s, uint32_t index, F2v uv, float out[4]) { s.textures[index].sample(uv.x, uv.y, out); }
+
+// Linear Rec.709 -> ACEScg, rows-dot-vector (textures.slang:37-45).
+V3f sample_color(const Scene& s, uint32_t index, F2v uv) {
+    float t[4];
+    sample_texture(s, index, uv, t);
+    return {0.613097400f * t[0] + 0.339523140f * t[1] + 0.047379450f * t[2],
+            0.070193730f * t[0] + 0.916353900f * t[1] + 0.013452399f * t[2],
+            0.020615594f * t[0] + 0.109569780f * t[1] + 0.869814660f * t[2]};
+}
+
+float sample_scalar(const Scene& s, uint32_t index, F2v uv) {
+    float t[4];
+    sample_texture(s, index, uv, t);
+    return t[0];
+}
+
+V3f sample_normal(const Scene& s, uint32_t index, F2v uv) {
+    float t[4];
+    sample_texture(s, index, uv, t);
+    float x = t[0] * 2.0f - 1.0f, y = t[1] * 2.0f - 1.0f;
+    return {x, y, std::sqrt(std::max(1.0f - (x * x + y * y), 0.0f))};
+}
+
+bool textured(const Material& m) {
+    return m.base_color_texture != TEXTURE_NONE || m.specular_roughness_texture != TEXTURE_NONE ||
+           m.metalness_texture != TEXTURE_NONE || m.emission_texture != TEXTURE_NONE;
+}
+
+Material resolve_material(const Scene& s, Material m, F2v uv) {  // textures.slang:70-82
+    if (m.base_color_texture != TEXTURE_NONE) wr3(m.base_color, sample_color(s, m.base_color_texture, uv));
+    if (m.specular_roughness_texture != TEXTURE_NONE)
+        m.specular_roughness = sample_scalar(s, m.specular_roughness_texture, uv);
+    if (m.metalness_texture != TEXTURE_NONE) m.metalness = sample_scalar(s, m.metalness_texture, uv);
+    if (m.emission_texture != TEXTURE_NONE)
+        wr3(m.emission, mat_color(m.emission) * sample_color(s, m.emission_texture, uv));
+    return m;
+}
+
+float opacity_at(const Scene& s, uint32_t inst, uint32_t prim, float b1, float b2) {  // scene.slang:56-64
+    const Instance& in = s.inst[inst];
+    float opacity = in.material.opacity;
+    if (in.material.opacity_texture != TEXTURE_NONE)
+        opacity *= sample_scalar(s, in.material.opacity_texture, interpolate_uv(in, prim, b1, b2));
+    return opacity;
+}
+
 // ---- kernels, restated ----------------------------------------------------
 
 struct Hit {
@@ -113,9 +176,7 @@ bool intersect(const Scene& s, V3f org, V3f dir, uint32_t mask, uint32_t pixel, 
         uint64_t key = hit_key(t.instance, t.primitive);
         if (!(tt < best_t || (tt == best_t && key < best_key))) return tmax;
         if (!t.opaque) {
-            const Instance& in = s.inst[t.instance];
-            float opacity = in.material.opacity;  // opacity maps are not in the oracle yet
-            (void)b1;
+            float opacity = opacity_at(s, t.instance, t.primitive, b1, b2);
             bool commit = crossings >= TRANSPARENT_CAP || hash_uniform(pixel, sample, bounce, crossings) < opacity;
             crossings++;
             if (!commit) return tmax;
@@ -152,7 +213,7 @@ float trace_shadow(const Scene& s, V3f org, V3f dir, float tmax, uint32_t light,
         if (!(tt < best_t || (tt == best_t && key < best_key))) return tm;
         bool target = t.instance == light && t.primitive == prim;
         if (!t.opaque && !target) {
-            atten *= 1.0f - s.inst[t.instance].material.opacity;
+            atten *= 1.0f - opacity_at(s, t.instance, t.primitive, b1, b2);
             if (atten < 1e-4f) { dead = true; return -1.0f; }
             return tm;
         }
@@ -225,6 +286,37 @@ Spawn spawn_point(const Instance& m, const Hit& hit, V3f ray_dir) {
     sp.normal = wn;
     sp.shading = sh;
     return sp;
+}
+
+// shade_surface.slang:183-231: the shading normal under a tangent-space
+// normal map, tangent frame from the triangle's positions and UVs.
+V3f mapped_shading_normal(const Scene& s, const Instance& m, const Hit& hit, F2v uv, uint32_t map,
+                          const Spawn& sp) {
+    uint32_t base = 3 * hit.primitive;
+    uint32_t i0 = m.indices[base], i1 = m.indices[base + 1], i2 = m.indices[base + 2];
+    float du1 = m.uvs[2 * i1] - m.uvs[2 * i0], dv1 = m.uvs[2 * i1 + 1] - m.uvs[2 * i0 + 1];
+    float du2 = m.uvs[2 * i2] - m.uvs[2 * i0], dv2 = m.uvs[2 * i2 + 1] - m.uvs[2 * i0 + 1];
+    float det = du1 * dv2 - dv1 * du2;
+    if (std::fabs(det) < 1e-12f) return sp.shading;
+    V3f e1 = fetch3(m.positions, i1) - fetch3(m.positions, i0);
+    V3f e2 = fetch3(m.positions, i2) - fetch3(m.positions, i0);
+    const auto& o = m.o2w;
+    V3f we1(dot(V3f(o[0][0], o[0][1], o[0][2]), e1), dot(V3f(o[1][0], o[1][1], o[1][2]), e1),
+            dot(V3f(o[2][0], o[2][1], o[2][2]), e1));
+    V3f we2(dot(V3f(o[0][0], o[0][1], o[0][2]), e2), dot(V3f(o[1][0], o[1][1], o[1][2]), e2),
+            dot(V3f(o[2][0], o[2][1], o[2][2]), e2));
+    V3f dpdu = (dv2 * we1 - dv1 * we2) / det;
+    V3f dpdv = (du1 * we2 - du2 * we1) / det;
+    V3f tangent = dpdu - sp.shading * dot(sp.shading, dpdu);
+    float len2 = dot(tangent, tangent);
+    if (!(len2 > 1e-20f)) return sp.shading;
+    tangent = tangent * (1.0f / std::sqrt(len2));
+    V3f bitangent = cross(sp.shading, tangent);
+    if (dot(bitangent, dpdv) < 0.0f) bitangent = -bitangent;
+    V3f t = sample_normal(s, map, uv);
+    V3f mapped = normalize(t.x * tangent + t.y * bitangent + t.z * sp.shading);
+    if (dot(mapped, sp.normal) < 0.0f) mapped = -mapped;
+    return mapped;
 }
 
 // raygen.slang:47-62
@@ -317,7 +409,10 @@ void trace_path(const Scene& s, uint32_t width, uint32_t height, uint32_t pixel,
         }
         // shade_surface.slang:235-521
         const Instance& mesh = s.inst[hit.instance];
-        const Material& mat = mesh.material;
+        F2v uv{0.0f, 0.0f};
+        const bool maps = textured(mesh.material) || mesh.material.normal_texture != TEXTURE_NONE;
+        if (maps) uv = interpolate_uv(mesh, hit.primitive, hit.b1, hit.b2);
+        const Material mat = textured(mesh.material) ? resolve_material(s, mesh.material, uv) : mesh.material;
         Spawn spawn = spawn_point(mesh, hit, dir);
         if (medium != MEDIUM_NONE) {
             const Material& interior = s.inst[medium].material;
@@ -342,7 +437,9 @@ void trace_path(const Scene& s, uint32_t width, uint32_t height, uint32_t pixel,
             }
             contribution = thr * mat_color(mat.emission) * weight;
         }
-        V3f shading = spawn.shading;  // normal maps are not in the oracle yet
+        V3f shading = spawn.shading;
+        if (mat.normal_texture != TEXTURE_NONE)
+            shading = mapped_shading_normal(s, mesh, hit, uv, mat.normal_texture, spawn);
         Frame<float> frame(shading);
         V3f wo = frame.to_local(-dir);
         MaterialT<float> mt = to_t<float>(mat);
@@ -391,6 +488,13 @@ void trace_path(const Scene& s, uint32_t width, uint32_t height, uint32_t pixel,
                 float u_list = (u_light - env_prob) / (1.0f - env_prob);
                 LightConnection cand = sample_lights(s.lights.data(), s.light_count, u_list, u_point.x,
                                                      u_point.y, spawn.position);
+                if (!cand.delta) {  // a textured emitter evaluates its map at the sampled point
+                    const Instance& em = s.inst[cand.instance];
+                    if (em.material.emission_texture != TEXTURE_NONE)
+                        cand.radiance = cand.radiance *
+                                        sample_color(s, em.material.emission_texture,
+                                                     interpolate_uv(em, cand.primitive, cand.bary_x, cand.bary_y));
+                }
                 V3f wl = frame.to_local(cand.direction);
                 bool through = dot(cand.direction, spawn.normal) < 0.0f;
                 if (cand.pdf > 0.0f && wl.z != 0.0f && (wl.z < 0.0f) == through) {
@@ -498,10 +602,33 @@ struct oracle_delta_light {
 
 void oracle_camera_basis(const oracle_camera* cam, float aspect, float* right, float* up, float* fwd);
 
+struct oracle_texture {  // mirrors cenote_texture in include/cenote_c.h
+    uint32_t format, width, height, pad;
+    const void* data;
+};
+
+// Returns null when a texture cannot be decoded or a material names a slot
+// past the table.
 void* oracle_scene_create(const oracle_object* objects, uint32_t n, const oracle_camera* cam,
                           uint32_t env_w, uint32_t env_h, const float* env_texels,
-                          const oracle_delta_light* deltas, uint32_t n_deltas, const float* bsdf_tables) {
+                          const oracle_delta_light* deltas, uint32_t n_deltas, const float* bsdf_tables,
+                          const oracle_texture* textures, uint32_t n_textures) {
     Scene* s = new Scene();
+    s->textures.resize(n_textures);
+    for (uint32_t k = 0; k < n_textures; ++k)
+        if (!s->textures[k].decode(textures[k].format, textures[k].width, textures[k].height, textures[k].data)) {
+            delete s;
+            return nullptr;
+        }
+    for (uint32_t i = 0; i < n; ++i) {
+        const Material& m = objects[i].material;
+        for (uint32_t slot : {m.base_color_texture, m.specular_roughness_texture, m.metalness_texture,
+                              m.emission_texture, m.opacity_texture, m.normal_texture})
+            if (slot != TEXTURE_NONE && slot >= n_textures) {
+                delete s;
+                return nullptr;
+            }
+    }
     s->tables.assign(bsdf_tables, bsdf_tables + TABLE_FLOATS);
     std::vector<TriangleLight> tri_lights;
     std::vector<Tri> tris;
@@ -647,6 +774,39 @@ void oracle_render(void* p, uint32_t width, uint32_t height, uint32_t sample_beg
 }
 
 // ---- probes ----------------------------------------------------------------
+
+// Decode a texture to linear RGBA floats (w·h·4); 0 on success.
+int oracle_texture_decode(uint32_t format, uint32_t w, uint32_t h, const void* data, float* out) {
+    Texture t;
+    if (!t.decode(format, w, h, data)) return -1;
+    std::memcpy(out, t.texels.data(), t.texels.size() * 4);
+    return 0;
+}
+
+// n taps at uv (n·2): mode 0 the filtered texel, 1 sampleColor, 2
+// sampleScalar, 3 sampleNormal (the modes of cenote_probe_texture).
+int oracle_texture_sample(uint32_t format, uint32_t w, uint32_t h, const void* data, uint32_t mode, const float* uv,
+                          uint32_t n, float* out) {
+    Scene s;
+    s.textures.resize(1);
+    if (!s.textures[0].decode(format, w, h, data)) return -1;
+    for (uint32_t i = 0; i < n; ++i) {
+        F2v c{uv[2 * i], uv[2 * i + 1]};
+        float* o = out + 4 * size_t(i);
+        o[0] = o[1] = o[2] = o[3] = 0.0f;
+        if (mode == 1) {
+            V3f v = sample_color(s, 0, c);
+            wr3(o, v);
+        } else if (mode == 2) {
+            o[0] = sample_scalar(s, 0, c);
+        } else if (mode == 3) {
+            wr3(o, sample_normal(s, 0, c));
+        } else {
+            sample_texture(s, 0, c, o);
+        }
+    }
+    return 0;
+}
 
 void oracle_sampler(uint32_t pixel, uint32_t dimension, uint32_t count, float* points, float* values) {
     for (uint32_t i = 0; i < count; ++i) {

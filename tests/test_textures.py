@@ -1,0 +1,270 @@
+"""Material textures: formats, BC blocks, sampling, and the shading slots.
+
+Known answers come from the published block layouts (BC1: RGB565 endpoints,
+2-bit indices, four-colour mode when c0 > c1; BC4: 8-bit endpoints, 3-bit
+indices, eight-value mode when r0 > r1; BC5 = two BC4 blocks) and from the
+sampling rules of crates/cenote/shaders/textures.slang:24-64 with the
+samplers of crates/cenote/src/gpu/image.rs:117-141 (bilinear, repeat, sRGB
+decoded per texel). GPU tests hold the texture unit's taps and the textured
+renders to the oracle.
+"""
+from __future__ import annotations
+
+import numpy as np
+import pytest
+
+import oracle
+from cenote_b200 import CenoteError, encode_texture, scenes, texture_bytes
+
+T = scenes
+
+
+def block_texture(fmt, block: bytes, w=4, h=4):
+    return T.Texture(fmt, w, h, np.frombuffer(block * ((w // 4) * (h // 4)), np.uint8).copy())
+
+
+def srgb(v):
+    return np.where(v <= 0.04045, v / 12.92, ((v + 0.055) / 1.055) ** 2.4)
+
+
+# ---- sizes and encoder -----------------------------------------------------------
+
+
+def test_texture_bytes():
+    assert texture_bytes(T.TEX_RGBA8_SRGB, 5, 3) == 60
+    assert texture_bytes(T.TEX_RGBA32F, 2, 2) == 64
+    assert texture_bytes(T.TEX_BC1_SRGB, 8, 4) == 16
+    assert texture_bytes(T.TEX_BC5_UNORM, 8, 8) == 64
+    assert texture_bytes(T.TEX_BC4_UNORM, 6, 4) == 0  # BC extents are multiples of 4
+    assert texture_bytes(99, 4, 4) == 0
+    assert texture_bytes(T.TEX_RGBA8_UNORM, 0, 4) == 0
+
+
+def test_encoder_rejects_non_bc_formats_and_sizes():
+    t = T.rgba8_texture(np.zeros((4, 4, 3)))
+    with pytest.raises(CenoteError):
+        encode_texture(T.TEX_RGBA8_SRGB, t)
+    with pytest.raises(CenoteError):
+        encode_texture(T.TEX_BC1_UNORM, T.rgba8_texture(np.zeros((6, 4, 3))))
+
+
+def psnr(a, b):
+    return 10 * np.log10(1.0 / np.mean((a - b) ** 2))
+
+
+def test_encoder_quality():
+    size = 64
+    grey = T.value_noise(size, 3)
+    # Colour on a line through RGB space: BC1's endpoints capture it closely.
+    line = np.stack([grey, 0.5 * grey + 0.2, 0.9 - 0.6 * grey], -1)
+    src = T.rgba8_texture(line, srgb=False)
+    ref = oracle.texture_decode(src)
+    bc1 = oracle.texture_decode(encode_texture(T.TEX_BC1_UNORM, src))
+    assert psnr(bc1[..., :3], ref[..., :3]) > 35  # RGB565 endpoints bound it near 37 dB
+    two = T.rgba8_texture(np.stack([grey, T.value_noise(size, 4), grey], -1), srgb=False)
+    ref2 = oracle.texture_decode(two)
+    assert psnr(oracle.texture_decode(encode_texture(T.TEX_BC4_UNORM, two))[..., 0], ref2[..., 0]) > 38
+    bc5 = oracle.texture_decode(encode_texture(T.TEX_BC5_UNORM, two))
+    assert psnr(bc5[..., :2], ref2[..., :2]) > 38
+    # A constant block survives exactly (up to the format's quantisation).
+    flat = T.rgba8_texture(np.full((8, 8, 3), 0.5), srgb=False)
+    d = oracle.texture_decode(encode_texture(T.TEX_BC4_UNORM, flat))
+    assert np.all(d[..., 0] == np.float32(128 / 255))
+
+
+# ---- block known answers ------------------------------------------------------------
+
+
+def test_bc1_four_and_three_colour_modes():
+    red, blue = 0xF800, 0x001F
+    idx = sum(k % 4 << (2 * k) for k in range(16))  # texel k uses palette entry k % 4
+    four = oracle.texture_decode(block_texture(T.TEX_BC1_UNORM, np.array([red, blue], "<u2").tobytes() +
+                                               np.array([idx], "<u4").tobytes()))
+    pal = np.array([[255, 0, 0], [0, 0, 255], [170, 0, 85], [85, 0, 170]]) / 255.0
+    for k in range(16):
+        assert np.allclose(four[k // 4, k % 4, :3], pal[k % 4], atol=1e-6)
+        assert four[k // 4, k % 4, 3] == 1.0
+    three = oracle.texture_decode(block_texture(T.TEX_BC1_UNORM, np.array([blue, red], "<u2").tobytes() +
+                                                np.array([idx], "<u4").tobytes()))
+    assert np.allclose(three[0, 2, :3], [127.5 / 255, 0, 127.5 / 255], atol=1e-6)
+    assert np.all(three[0, 3] == 0.0)  # transparent black
+    srgb_block = oracle.texture_decode(block_texture(T.TEX_BC1_SRGB, np.array([red, blue], "<u2").tobytes() +
+                                                     np.array([idx], "<u4").tobytes()))
+    assert np.allclose(srgb_block[0, 2, :3], srgb(pal[2]), atol=1e-6)
+
+
+def test_bc4_and_bc5_palettes():
+    bits = sum(k % 8 << (3 * k) for k in range(16))
+    idx = int(bits).to_bytes(6, "little")
+    eight = oracle.texture_decode(block_texture(T.TEX_BC4_UNORM, bytes([210, 70]) + idx))
+    expect = [210, 70] + [((7 - k) * 210 + k * 70) / 7 for k in range(1, 7)]
+    for k in range(16):
+        assert eight[k // 4, k % 4, 0] == pytest.approx(expect[k % 8] / 255, abs=1e-6)
+    six = oracle.texture_decode(block_texture(T.TEX_BC4_UNORM, bytes([70, 210]) + idx))
+    expect6 = [70, 210] + [((5 - k) * 70 + k * 210) / 5 for k in range(1, 5)] + [0, 255]
+    for k in range(16):
+        assert six[k // 4, k % 4, 0] == pytest.approx(expect6[k % 8] / 255, abs=1e-6)
+    bc5 = oracle.texture_decode(block_texture(T.TEX_BC5_UNORM, bytes([210, 70]) + idx + bytes([70, 210]) + idx))
+    assert np.allclose(bc5[..., 0], eight[..., 0]) and np.allclose(bc5[..., 1], six[..., 0])
+
+
+# ---- sampling ---------------------------------------------------------------------------
+
+
+def test_oracle_sampling_rules():
+    rng = np.random.default_rng(5)
+    px = rng.integers(0, 256, (4, 6, 4), dtype=np.uint8)
+    lin = T.Texture(T.TEX_RGBA8_UNORM, 6, 4, px)
+    s = T.Texture(T.TEX_RGBA8_SRGB, 6, 4, px)
+    centres = np.array([[(x + 0.5) / 6, (y + 0.5) / 4] for y in range(4) for x in range(6)])
+    # Texel centres return the texel; sRGB storage decodes colour, not alpha.
+    assert np.allclose(oracle.texture_sample(lin, centres), px.reshape(-1, 4) / 255.0, atol=1e-6)
+    dec = oracle.texture_sample(s, centres)
+    assert np.allclose(dec[:, :3], srgb(px.reshape(-1, 4)[:, :3] / 255.0), atol=1e-6)
+    assert np.allclose(dec[:, 3], px.reshape(-1, 4)[:, 3] / 255.0, atol=1e-6)
+    # Repeat addressing, and the bilinear midpoint of two texels.
+    assert np.allclose(oracle.texture_sample(lin, centres + 1.0), oracle.texture_sample(lin, centres), atol=1e-6)
+    assert np.allclose(oracle.texture_sample(lin, centres - 3.0), oracle.texture_sample(lin, centres), atol=1e-6)
+    mid = oracle.texture_sample(lin, [[1.0 / 6, 0.5 / 4]])[0]
+    assert np.allclose(mid, (px[0, 0] / 255.0 + px[0, 1] / 255.0) / 2, atol=1e-6)
+    # The seam: u = 0 blends the last and first columns.
+    seam = oracle.texture_sample(lin, [[0.0, 0.5 / 4]])[0]
+    assert np.allclose(seam, (px[0, 5] / 255.0 + px[0, 0] / 255.0) / 2, atol=1e-6)
+
+
+def test_oracle_slot_readers():
+    t = T.Texture(T.TEX_RGBA32F, 1, 1, np.array([[[0.25, 0.5, 0.75, 1.0]]], np.float32))
+    c = oracle.texture_sample(t, [[0.3, 0.7]], mode=1)[0, :3]
+    assert np.allclose(c, T.acescg((0.25, 0.5, 0.75)), atol=1e-6)
+    assert oracle.texture_sample(t, [[0.3, 0.7]], mode=2)[0, 0] == pytest.approx(0.25)
+    n = oracle.texture_sample(t, [[0.3, 0.7]], mode=3)[0, :3]
+    assert np.allclose(n, [-0.5, 0.0, np.sqrt(0.75)], atol=1e-6)
+
+
+def test_oracle_rejects_a_slot_past_the_table():
+    spec = T.cornell(16, 16, 1, 2)
+    spec.objects[0].material["base_color_texture"] = 0
+    with pytest.raises(ValueError):
+        oracle.OracleScene(spec)
+
+
+def test_oracle_textured_scene_guides_follow_the_maps():
+    # The wall's albedo guide is its RGBA32F map, colour-converted, at the hit.
+    spec = T.textured(64, 36, 2, 4)
+    g = oracle.OracleScene(spec).render_guides(64, 36, 0, 2, 4)
+    assert np.isfinite(g["beauty"]).all()
+    wall_px = g["albedo"][4, 32, :3] / 2
+    assert 0.0 <= wall_px.min() and wall_px.max() <= 1.0
+    # A flat normal map (exact 0.5, 0.5) leaves the render unchanged.
+    base = T.cornell(24, 24, 2, 4)
+    flat = T.cornell(24, 24, 2, 4)
+    flat.textures = [T.Texture(T.TEX_RGBA32F, 2, 2, np.tile(np.array([0.5, 0.5, 1, 1], np.float32), (2, 2, 1)))]
+    for o in flat.objects:
+        o.mesh.uvs = np.random.default_rng(1).random(o.mesh.uvs.shape).astype(np.float32)
+        o.material = o.material.copy()
+        o.material["normal_texture"] = 0
+    a = oracle.OracleScene(base).render_sum(24, 24, 0, 2, 4)
+    b = oracle.OracleScene(flat).render_sum(24, 24, 0, 2, 4)
+    assert np.abs(a - b).max() < 1e-3 * max(1.0, np.abs(a).max())
+
+
+def test_spec_archive_keeps_textures(tmp_path):
+    spec = T.textured(32, 18, 1, 2, size=16)
+    T.save_spec(tmp_path / "t.npz", spec)
+    back, _ = T.load_spec(tmp_path / "t.npz")
+    assert len(back.textures) == len(spec.textures)
+    for a, b in zip(spec.textures, back.textures):
+        assert (a.format, a.width, a.height) == (b.format, b.width, b.height)
+        assert np.array_equal(np.asarray(a.data), np.asarray(b.data))
+
+
+# ---- the texture unit against the oracle -----------------------------------------------
+
+
+FORMATS = ["rgba8_srgb", "rgba8_unorm", "rgba32f", "bc1_srgb", "bc1_unorm", "bc4", "bc5"]
+
+
+def make_texture(kind, size=32):
+    rng = np.random.default_rng(11)
+    rgb = np.stack([T.value_noise(size, k, octaves=3) for k in (1, 2, 3)], -1)
+    if kind == "rgba32f":
+        return T.Texture(T.TEX_RGBA32F, size, size,
+                         np.concatenate([rgb * 4.0, rng.random((size, size, 1))], -1).astype(np.float32))
+    src = T.rgba8_texture(rgb, srgb=kind.endswith("srgb"))
+    fmt = {"rgba8_srgb": None, "rgba8_unorm": None, "bc1_srgb": T.TEX_BC1_SRGB, "bc1_unorm": T.TEX_BC1_UNORM,
+           "bc4": T.TEX_BC4_UNORM, "bc5": T.TEX_BC5_UNORM}[kind]
+    return src if fmt is None else encode_texture(fmt, src)
+
+
+def probe_scene(ctx, tex):
+    from cenote_b200 import Scene
+
+    spec = T.cornell(8, 8, 1, 2)
+    spec.textures = [tex]
+    return Scene(ctx, spec)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("kind", FORMATS)
+def test_gpu_texture_taps_match_oracle(ctx, kind):
+    tex = make_texture(kind)
+    rng = np.random.default_rng(2)
+    uv = np.concatenate([rng.random((4000, 2)) * 3 - 1,                      # repeat addressing
+                         (np.stack(np.meshgrid(np.arange(32), np.arange(32)), -1).reshape(-1, 2) + 0.5) / 32])
+    sc = probe_scene(ctx, tex)
+    channels = {"bc4": 1, "bc5": 2}.get(kind, 4)
+    for mode in (0, 1, 2, 3):
+        got = sc.probe_texture(0, uv, mode)
+        ref = oracle.texture_sample(tex, uv, mode)
+        # sampleNormal's z = sqrt(1 - x^2 - y^2) amplifies tap error near the
+        # horizon: bound its x and y, which carry the tap itself.
+        c = channels if mode == 0 else {1: 3, 2: 1, 3: 2}[mode]
+        if mode == 1 and channels < 3:
+            continue
+        err = np.abs(got[:, :c] - ref[:, :c])
+        scale = 4.0 if kind == "rgba32f" else (2.0 if mode == 3 else 1.0)
+        # Hardware filtering keeps an 8-bit weight fraction and decodes BC
+        # palettes at its own precision: bounded, not bit-exact.
+        assert err.max() <= 0.02 * scale, (mode, err.max())
+        assert err.mean() <= 2e-3 * scale, (mode, err.mean())
+
+
+def gpu_render(ctx, spec, spp, max_bounces):
+    from cenote_b200 import Film, Renderer, Scene
+
+    scene = Scene(ctx, spec)
+    r = Renderer(ctx, max_bounces)
+    f = Film(ctx, spec.width, spec.height)
+    r.accumulate(scene, f, spp)
+    return f.all_averages()
+
+
+@pytest.mark.gpu
+def test_gpu_textured_render_matches_oracle(ctx):
+    from cenote_b200.metrics import rel_mse
+
+    spec = T.textured(96, 54, 16, 6)
+    got = gpu_render(ctx, spec, 16, 6)
+    ref = oracle.OracleScene(spec).render_guides(96, 54, 0, 16, 6)
+    ref = {k: v / 16 for k, v in ref.items()}
+    assert np.isfinite(got["beauty"]).all()
+    assert (got["beauty"][..., 3] == 1.0).all()
+    assert rel_mse(got["beauty"][..., :3], ref["beauty"][..., :3]) < 2e-3
+    assert rel_mse(got["albedo"][..., :3], ref["albedo"][..., :3]) < 2e-3
+    assert rel_mse(got["normal"][..., :3], ref["normal"][..., :3]) < 2e-3
+
+
+@pytest.mark.gpu
+def test_gpu_scene_rejects_bad_texture_slots(ctx):
+    from cenote_b200 import Scene
+
+    spec = T.cornell(8, 8, 1, 2)
+    spec.objects[0].material["base_color_texture"] = 3
+    with pytest.raises(CenoteError) as e:
+        Scene(ctx, spec)
+    assert e.value.code == -5
+    spec = T.cornell(8, 8, 1, 2)
+    spec.textures = [T.Texture(T.TEX_BC1_UNORM, 6, 4, np.zeros(16, np.uint8))]
+    with pytest.raises(CenoteError) as e:
+        Scene(ctx, spec)
+    assert e.value.code == -1
