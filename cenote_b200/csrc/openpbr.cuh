@@ -416,13 +416,40 @@ struct BsdfSample {
     uint32_t lobe;
 };
 
-// sampleBsdf, :821-884
+// The closure's value and pdf for one direction: the shading kernel needs both
+// for the next-event direction and for the scattered one, and evaluating
+// them together shares the half vector, D and G1 terms. (Inline: out of line
+// the closure moves to local memory, which costs more than the instruction
+// cache it saves.)
+struct EvalPdf {
+    float3 f;
+    float pdf;
+};
+
+__device__ __forceinline__ EvalPdf eval_pdf(const Closure& c, float3 wi, float3 wo) {
+    EvalPdf r;
+    r.f = eval_bsdf(c, wi, wo);
+    r.pdf = bsdf_pdf(c, wi, wo);
+    return r;
+}
+
+// sampleBsdf, :821-884, without its closing pdf evaluation: returns false
+// (no direction, pdf 0) where the reference returns pdf 0 early.
+__device__ __forceinline__ bool sample_bsdf_dir(const Closure& c, float3 wo, float u_lobe, float ux, float uy,
+                                                BsdfSample& r);
+
 __device__ __forceinline__ BsdfSample sample_bsdf(const Closure& c, float3 wo, float u_lobe, float ux, float uy) {
     BsdfSample r;
+    if (sample_bsdf_dir(c, wo, u_lobe, ux, uy, r)) r.pdf = bsdf_pdf(c, r.wi, wo);
+    return r;
+}
+
+__device__ __forceinline__ bool sample_bsdf_dir(const Closure& c, float3 wo, float u_lobe, float ux, float uy,
+                                                BsdfSample& r) {
     r.wi = f3(0.0f, 0.0f, 1.0f);
     r.pdf = 0.0f;
     r.lobe = LOBE_DIFFUSE;
-    if (c.w_total <= 0.0f) return r;
+    if (c.w_total <= 0.0f) return false;
     float pick = u_lobe * c.w_total;
     float3 wi;
     if (pick < c.w_fuzz) {
@@ -461,7 +488,7 @@ __device__ __forceinline__ BsdfSample sample_bsdf(const Closure& c, float3 wo, f
                 r.lobe = LOBE_TRANSMISSION;
                 float cc = dot(wo, h);
                 float cos2t = 1.0f - (1.0f - cc * cc) / (c.eta * c.eta);
-                if (cos2t <= 0.0f) return r;
+                if (cos2t <= 0.0f) return false;
                 wi = (cc / c.eta - sqrtf(cos2t)) * h - wo / c.eta;
             }
         }
@@ -473,8 +500,7 @@ __device__ __forceinline__ BsdfSample sample_bsdf(const Closure& c, float3 wo, f
         wi = f3(rr * cp, rr * sp, sqrtf(1.0f - ux));
     }
     r.wi = wi;
-    r.pdf = bsdf_pdf(c, wi, wo);
-    return r;
+    return true;
 }
 
 // Duff et al. frame, :888-909

@@ -15,61 +15,97 @@
 
 namespace cn {
 
-// Returns the attenuation (>= 0) when visible, -1 when occluded, -2 when a
-// traversal bound was exceeded.
-template <bool COUNT = false>
-__device__ __forceinline__ float shadow_query(const DeviceScene& scene, const Ray& ray, float tmax, uint32_t light,
-                                              uint32_t lprim, uint32_t leaf, uint32_t* visits = nullptr,
-                                              uint32_t* tests = nullptr) {
-    float atten = 1.0f;
-    bool occluded = false;
-    bool have_t = false;
-    float t_target = tmax;
+// The query's state, resumable step by step (a persistent kernel retires and
+// starts queries per lane; see Walk).
+struct ShadowQuery {
+    Walk w;
+    float atten, t_target, tm;
+    uint32_t light, lprim, leaf, best_inst, best_prim;
+    bool occluded, have_t, closest_fallback;
+};
+
+__device__ __forceinline__ void shadow_begin(const DeviceScene& scene, const Ray& ray, float tmax, uint32_t light,
+                                             uint32_t lprim, uint32_t leaf, ShadowQuery& q) {
+    q.atten = 1.0f;
+    q.occluded = false;
+    q.have_t = false;
+    q.t_target = tmax;
+    q.light = light;
+    q.lprim = lprim;
+    q.leaf = leaf;
     if (leaf != 0xffffffffu && leaf < scene.tri_count) {
         const float4* tp = scene.tris + 3u * leaf;
         float t, b1, b2;
         if (tri_hit(ray, __ldg(tp), __ldg(tp + 1), __ldg(tp + 2), tmax, t, b1, b2)) {
-            have_t = true;
-            t_target = t;
+            q.have_t = true;
+            q.t_target = t;
         }
     }
-    const bool closest_fallback = light != LIGHT_NONE && leaf == 0xffffffffu;
-    uint32_t best_inst = LIGHT_NONE, best_prim = 0;
-    float tm = t_target;
-    bool ok = traverse<COUNT>(scene, ray, tm, [&](uint32_t ti, float4 a, float4 b, float4 c, float& tcur) {
-        if (have_t && ti == leaf) return false;  // the target itself
+    q.closest_fallback = light != LIGHT_NONE && leaf == 0xffffffffu;
+    q.best_inst = LIGHT_NONE;
+    q.best_prim = 0;
+    q.tm = q.t_target;
+    walk_begin(q.w, ray);
+}
+
+template <bool COUNT = false>
+__device__ __forceinline__ int shadow_step(const DeviceScene& scene, const Ray& ray, ShadowQuery& q, uint2* stack,
+                                           uint32_t* visits = nullptr, uint32_t* tests = nullptr) {
+    if (scene.node_count == 0) return WALK_DONE;
+    return walk_step<COUNT>(scene, ray, q.tm, q.w, stack, [&](uint32_t ti, float4 a, float4 b, float4 c, float& tcur) {
+        if (q.have_t && ti == q.leaf) return false;  // the target itself
         float t, b1, b2;
         if (!tri_hit(ray, a, b, c, tcur, t, b1, b2)) return false;
         uint32_t inst = __float_as_uint(a.w), prim = __float_as_uint(b.w);
-        bool target = inst == light && prim == lprim;
-        if (closest_fallback) {
+        bool target = inst == q.light && prim == q.lprim;
+        if (q.closest_fallback) {
             // No leaf index for the target: the reference's closest-hit walk.
-            if (!(t < tcur || (t == tcur && (inst < best_inst || (inst == best_inst && prim < best_prim))))) return false;
-        } else if (have_t && t == t_target &&
-                   !(inst < light || (inst == light && prim < lprim))) {
+            if (!(t < tcur || (t == tcur && (inst < q.best_inst || (inst == q.best_inst && prim < q.best_prim)))))
+                return false;
+        } else if (q.have_t && t == q.t_target && !(inst < q.light || (inst == q.light && prim < q.lprim))) {
             return false;  // the target wins the tie
         }
         if (!(__float_as_uint(c.w) & TRI_OPAQUE) && !target) {
-            atten *= 1.0f - opacity_at(scene, inst, prim, b1, b2);
-            if (atten < 1e-4f) {
-                occluded = true;
+            q.atten *= 1.0f - opacity_at(scene, inst, prim, b1, b2);
+            if (q.atten < 1e-4f) {
+                q.occluded = true;
                 return true;
             }
             return false;
         }
-        if (!closest_fallback) {
-            occluded = true;  // an opaque occluder nearer than the target (or any, without one)
+        if (!q.closest_fallback) {
+            q.occluded = true;  // an opaque occluder nearer than the target (or any, without one)
             return true;
         }
         tcur = t;
-        best_inst = inst;
-        best_prim = prim;
+        q.best_inst = inst;
+        q.best_prim = prim;
         return false;
     }, visits, tests);
-    if (!ok) return -2.0f;
-    if (occluded) return -1.0f;
-    if (closest_fallback && !(best_inst == LIGHT_NONE || (best_inst == light && best_prim == lprim))) return -1.0f;
-    return atten;
+}
+
+// The attenuation (>= 0) when visible, -1 when occluded.
+__device__ __forceinline__ float shadow_result(const ShadowQuery& q) {
+    if (q.occluded) return -1.0f;
+    if (q.closest_fallback && !(q.best_inst == LIGHT_NONE || (q.best_inst == q.light && q.best_prim == q.lprim)))
+        return -1.0f;
+    return q.atten;
+}
+
+// The whole query for one ray: the attenuation (>= 0) when visible, -1 when
+// occluded, -2 when a traversal bound was exceeded.
+template <bool COUNT = false>
+__device__ __forceinline__ float shadow_query(const DeviceScene& scene, const Ray& ray, float tmax, uint32_t light,
+                                              uint32_t lprim, uint32_t leaf, uint32_t* visits = nullptr,
+                                              uint32_t* tests = nullptr) {
+    ShadowQuery q;
+    shadow_begin(scene, ray, tmax, light, lprim, leaf, q);
+    uint2 stack[TRAVERSAL_STACK];
+    for (;;) {
+        int st = shadow_step<COUNT>(scene, ray, q, stack, visits, tests);
+        if (st == WALK_OVERFLOW) return -2.0f;
+        if (st == WALK_DONE) return shadow_result(q);
+    }
 }
 
 }  // namespace cn

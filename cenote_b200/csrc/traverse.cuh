@@ -119,8 +119,7 @@ __device__ __forceinline__ uint32_t intersect_node(const WideNode* nodes, uint32
     uint32_t mask = 0;
 #pragma unroll
     for (int i = 0; i < 8; ++i) {
-        uint32_t meta = byte_of(n1.z, n1.w, i);
-        if (meta == 0) continue;
+        uint32_t meta = byte_of(n1.z, n1.w, i);  // 0 for an empty slot: contributes no bits
         float tnx = fmaf(float(byte_of(nx0, nx1, i)), aid.x, aor.x);
         float tny = fmaf(float(byte_of(ny0, ny1, i)), aid.y, aor.y);
         float tnz = fmaf(float(byte_of(nz0, nz1, i)), aid.z, aor.z);
@@ -149,59 +148,98 @@ __device__ __forceinline__ uint32_t intersect_node(const WideNode* nodes, uint32
 // triangle group is pushed and the lane keeps walking nodes, so warps test
 // triangles together instead of idling through each other's leaves
 // (Ylitie et al. 2017, postponement).
-constexpr uint32_t POSTPONE = 6;
+#ifndef CN_POSTPONE
+#define CN_POSTPONE 4
+#endif
+constexpr uint32_t POSTPONE = CN_POSTPONE;
 
+// The walk as a resumable state machine, so a persistent kernel can retire a
+// finished ray and start a new one in its lane while the warp's other lanes
+// are mid-walk (dynamic ray fetching, Aila & Laine, HPG 2009). The stack
+// lives with the caller.
+struct Walk {
+    uint2 g, t;      // the node group being expanded, the triangle group being tested
+    int sp;
+    uint32_t iter;
+    bool resumed;    // the triangle group came off the stack: never postpone it twice
+};
+
+enum : int { WALK_CONTINUE = 0, WALK_DONE = 1, WALK_OVERFLOW = -1 };
+
+__device__ __forceinline__ void walk_begin(Walk& w, const Ray& r) {
+    w.g = make_uint2(0u, (1u << (24u + r.oct_inv)) | 1u);  // the root: inner slot 0 of a virtual parent
+    w.t = make_uint2(0u, 0u);
+    w.sp = 0;
+    w.iter = 0;
+    w.resumed = false;
+}
+
+__device__ __forceinline__ uint32_t walk_bound(const DeviceScene& s) { return 4u * (s.node_count + s.tri_count) + 64u; }
+
+// One step: expand one node (or resume one postponed triangle group), then
+// test its triangles unless too few lanes of the warp would test alongside.
+// `visit` returning true stops the walk (WALK_DONE).
+template <bool COUNT = false, class Visit>
+__device__ __forceinline__ int walk_step(const DeviceScene& s, const Ray& r, float& tmax, Walk& w, uint2* stack,
+                                         Visit&& visit, uint32_t* visits = nullptr, uint32_t* tests = nullptr) {
+    if (++w.iter > walk_bound(s)) return WALK_OVERFLOW;
+    if (w.g.y & 0xff000000u) {
+        uint32_t pos = 31u - __clz(w.g.y & 0xff000000u);
+        w.g.y &= ~(1u << pos);
+        uint32_t slot = (pos - 24u) ^ r.oct_inv;
+        uint32_t ni = w.g.x + __popc(w.g.y & 0xffu & ((1u << slot) - 1u));
+        if (w.g.y & 0xff000000u) {
+            if (w.sp >= TRAVERSAL_STACK) return WALK_OVERFLOW;
+            stack[w.sp++] = w.g;
+        }
+        uint32_t bc, bt, im;
+        uint32_t hits = intersect_node(s.nodes, ni, r, tmax, bc, bt, im);
+        if (COUNT) ++*visits;
+        w.g = make_uint2(bc, (hits & 0xff000000u) | im);
+        w.t = make_uint2(bt, hits & 0x00ffffffu);
+        w.resumed = false;
+    } else {
+        w.t = w.g;  // a postponed triangle group came off the stack
+        w.g = make_uint2(0u, 0u);
+        w.resumed = true;
+    }
+    while (w.t.y & 0x00ffffffu) {
+        if (!w.resumed && uint32_t(__popc(__activemask())) < POSTPONE) {
+            if (w.sp >= TRAVERSAL_STACK) return WALK_OVERFLOW;
+            stack[w.sp++] = w.t;
+            break;
+        }
+        uint32_t k = __ffs(w.t.y) - 1u;
+        w.t.y &= w.t.y - 1u;
+        uint32_t ti = w.t.x + k;
+        const float4* tp = s.tris + 3u * ti;
+        float4 a = __ldg(tp), b = __ldg(tp + 1), c = __ldg(tp + 2);
+        if (COUNT) ++*tests;
+        if (visit(ti, a, b, c, tmax)) return WALK_DONE;
+    }
+    if (!(w.g.y & 0xff000000u)) {
+        if (w.sp == 0) return WALK_DONE;
+        w.g = stack[--w.sp];
+    }
+    return WALK_CONTINUE;
+}
+
+// The whole walk for one ray, handing each candidate triangle to
+// `visit(tri_index, v0, v1, v2, tmax&)`, which may shrink tmax and returns
+// true to stop. Returns false if a bound was exceeded (the caller flags an
+// overflow).
 template <bool COUNT = false, class Visit>
 __device__ __forceinline__ bool traverse(const DeviceScene& s, const Ray& r, float& tmax, Visit&& visit,
                                          uint32_t* visits = nullptr, uint32_t* tests = nullptr) {
     if (s.node_count == 0) return true;
     uint2 stack[TRAVERSAL_STACK];
-    int sp = 0;
-    uint2 g = make_uint2(0u, (1u << (24u + r.oct_inv)) | 1u);  // the root: inner slot 0 of a virtual parent
-    uint2 t = make_uint2(0u, 0u);
-    bool resumed;  // the triangle group came off the stack: never postpone it twice
-    const uint32_t max_iter = 4u * (s.node_count + s.tri_count) + 64u;
-    for (uint32_t iter = 0; iter < max_iter; ++iter) {
-        if (g.y & 0xff000000u) {
-            uint32_t pos = 31u - __clz(g.y & 0xff000000u);
-            g.y &= ~(1u << pos);
-            uint32_t slot = (pos - 24u) ^ r.oct_inv;
-            uint32_t ni = g.x + __popc(g.y & 0xffu & ((1u << slot) - 1u));
-            if (g.y & 0xff000000u) {
-                if (sp >= TRAVERSAL_STACK) return false;
-                stack[sp++] = g;
-            }
-            uint32_t bc, bt, im;
-            uint32_t hits = intersect_node(s.nodes, ni, r, tmax, bc, bt, im);
-            if (COUNT) ++*visits;
-            g = make_uint2(bc, (hits & 0xff000000u) | im);
-            t = make_uint2(bt, hits & 0x00ffffffu);
-            resumed = false;
-        } else {
-            t = g;  // a postponed triangle group came off the stack
-            g = make_uint2(0u, 0u);
-            resumed = true;
-        }
-        while (t.y & 0x00ffffffu) {
-            if (!resumed && uint32_t(__popc(__activemask())) < POSTPONE) {
-                if (sp >= TRAVERSAL_STACK) return false;
-                stack[sp++] = t;
-                break;
-            }
-            uint32_t k = __ffs(t.y) - 1u;
-            t.y &= t.y - 1u;
-            uint32_t ti = t.x + k;
-            const float4* tp = s.tris + 3u * ti;
-            float4 a = __ldg(tp), b = __ldg(tp + 1), c = __ldg(tp + 2);
-            if (COUNT) ++*tests;
-            if (visit(ti, a, b, c, tmax)) return true;
-        }
-        if (!(g.y & 0xff000000u)) {
-            if (sp == 0) return true;
-            g = stack[--sp];
-        }
+    Walk w;
+    walk_begin(w, r);
+    for (;;) {
+        int st = walk_step<COUNT>(s, r, tmax, w, stack, visit, visits, tests);
+        if (st == WALK_DONE) return true;
+        if (st == WALK_OVERFLOW) return false;
     }
-    return false;
 }
 
 }  // namespace cn

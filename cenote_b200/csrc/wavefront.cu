@@ -132,52 +132,106 @@ __global__ void __launch_bounds__(BLOCK) k_raygen(PathPool pool, WaveParams wp) 
 
 // ---- intersect (intersect.slang:47-88) -------------------------------------------
 
+// Dynamic ray fetching (Aila & Laine, HPG 2009): a lane whose ray finishes
+// does not wait for the warp's slowest ray. Each warp walks until at least
+// CN_REFILL_IDLE of its lanes are idle, then takes that many new rays with
+// one atomic and resumes; once the queue is drained it runs its last rays out.
+#ifndef CN_REFILL_IDLE
+#define CN_REFILL_IDLE 8
+#endif
+
+__device__ __forceinline__ uint32_t lanemask_lt() { return (1u << lane_id()) - 1u; }
+
+// Hand the warp's idle lanes their next work items: returns this lane's item
+// index (or ~0u) and sets `drained` (warp-uniform) once the queue is used up.
+__device__ __forceinline__ uint32_t refill(uint32_t* counter, uint32_t count, bool live, bool& drained) {
+    uint32_t idle = __ballot_sync(0xffffffffu, !live);
+    if (idle == 0) return ~0u;
+    uint32_t base = 0;
+    if (lane_id() == 0) base = atomicAdd(counter, uint32_t(__popc(idle)));
+    base = __shfl_sync(0xffffffffu, base, 0);
+    if (base + uint32_t(__popc(idle)) >= count) drained = true;
+    if (live) return ~0u;
+    uint32_t i = base + __popc(idle & lanemask_lt());
+    return i < count ? i : ~0u;
+}
+
 template <bool COUNT>
 __global__ void __launch_bounds__(BLOCK, CN_TRAV_MIN_BLOCKS) k_intersect(DeviceScene scene, PathPool pool, uint32_t bounce, uint32_t n0) {
     uint32_t visits = 0, tests = 0;
     const uint32_t count = min(bounce == 0 ? n0 : pool.counters[CTR_RAYS + bounce], pool.capacity);
     const uint32_t* queue = pool.queue[bounce & 1u];
     const uint32_t mask = bounce == 0 ? RAY_MASK_CAMERA : RAY_MASK_ALL;
-    for (;;) {
-        uint32_t base = warp_fetch(pool.counters + CTR_FETCH_ISECT + bounce);
-        if (base >= count) break;
-        uint32_t i = base + lane_id();
-        if (i >= count) continue;
-        uint32_t path = bounce == 0 ? i : queue[i];
-        float4 o = pool.org[path], d = pool.dir[path];
-        Ray ray = make_ray(xyz(o), xyz(d));
-        float tmax = 1e30f;
-        uint32_t best_inst = LIGHT_NONE, best_prim = 0;
-        float best_b1 = 0.0f, best_b2 = 0.0f;
-        uint32_t crossings = 0;
-        uint32_t pixel = 0, sample = 0;
-        if (scene.has_nonopaque) {
-            uint2 ps = pool.ps[path];
-            pixel = ps.x;
-            sample = ps.y;
+    uint32_t* fetch = pool.counters + CTR_FETCH_ISECT + bounce;
+    uint2 stack[TRAVERSAL_STACK];
+    Walk w;
+    Ray ray;
+    float tmax = 1e30f, best_b1 = 0.0f, best_b2 = 0.0f;
+    uint32_t path = 0, best_inst = LIGHT_NONE, best_prim = 0, crossings = 0, pixel = 0, sample = 0;
+    bool live = false, drained = false;
+    auto visit = [&](uint32_t, float4 a, float4 b, float4 c, float& tm) {
+        uint32_t flags = __float_as_uint(c.w);
+        if (!(flags & mask)) return false;
+        float t, b1, b2;
+        if (!tri_hit(ray, a, b, c, tm, t, b1, b2)) return false;
+        uint32_t inst = __float_as_uint(a.w), prim = __float_as_uint(b.w);
+        if (!(t < tm || (t == tm && (inst < best_inst || (inst == best_inst && prim < best_prim))))) return false;
+        if (!(flags & TRI_OPAQUE)) {
+            float opacity = opacity_at(scene, inst, prim, b1, b2);
+            bool commit = crossings >= TRANSPARENT_CAP || hash_uniform(pixel, sample, bounce, crossings) < opacity;
+            crossings++;
+            if (!commit) return false;
         }
-        bool ok = traverse<COUNT>(scene, ray, tmax, [&](uint32_t, float4 a, float4 b, float4 c, float& tm) {
-            uint32_t flags = __float_as_uint(c.w);
-            if (!(flags & mask)) return false;
-            float t, b1, b2;
-            if (!tri_hit(ray, a, b, c, tm, t, b1, b2)) return false;
-            uint32_t inst = __float_as_uint(a.w), prim = __float_as_uint(b.w);
-            if (!(t < tm || (t == tm && (inst < best_inst || (inst == best_inst && prim < best_prim))))) return false;
-            if (!(flags & TRI_OPAQUE)) {
-                float opacity = opacity_at(scene, inst, prim, b1, b2);
-                bool commit = crossings >= TRANSPARENT_CAP || hash_uniform(pixel, sample, bounce, crossings) < opacity;
-                crossings++;
-                if (!commit) return false;
+        tm = t;
+        best_inst = inst;
+        best_prim = prim;
+        best_b1 = b1;
+        best_b2 = b2;
+        return false;
+    };
+    for (;;) {
+        if (!drained) {
+            uint32_t i = refill(fetch, count, live, drained);
+            if (i != ~0u) {
+                path = bounce == 0 ? i : queue[i];
+                float4 o = pool.org[path], d = pool.dir[path];
+                ray = make_ray(xyz(o), xyz(d));
+                tmax = 1e30f;
+                best_inst = LIGHT_NONE;
+                best_prim = 0;
+                best_b1 = best_b2 = 0.0f;
+                crossings = 0;
+                if (scene.has_nonopaque) {
+                    uint2 ps = pool.ps[path];
+                    pixel = ps.x;
+                    sample = ps.y;
+                }
+                walk_begin(w, ray);
+                live = true;
+                if (scene.node_count == 0) {
+                    pool.hit[path] = make_uint4(LIGHT_NONE, 0u, 0u, 0u);
+                    live = false;
+                }
             }
-            tm = t;
-            best_inst = inst;
-            best_prim = prim;
-            best_b1 = b1;
-            best_b2 = b2;
-            return false;
-        }, &visits, &tests);
-        if (!ok) flag_overflow(pool.counters);
-        pool.hit[path] = make_uint4(best_inst, best_prim, __float_as_uint(best_b1), __float_as_uint(best_b2));
+        }
+        if (!__any_sync(0xffffffffu, live)) {
+            if (drained) break;
+            continue;
+        }
+        // Walk until enough lanes are idle to refill (all of them once drained).
+        const uint32_t want_idle = drained ? 32u : uint32_t(CN_REFILL_IDLE);
+        for (;;) {
+            if (live) {
+                int st = walk_step<COUNT>(scene, ray, tmax, w, stack, visit, &visits, &tests);
+                if (st != WALK_CONTINUE) {
+                    if (st == WALK_OVERFLOW) flag_overflow(pool.counters);
+                    pool.hit[path] =
+                        make_uint4(best_inst, best_prim, __float_as_uint(best_b1), __float_as_uint(best_b2));
+                    live = false;
+                }
+            }
+            if (uint32_t(__popc(__ballot_sync(0xffffffffu, !live))) >= want_idle) break;
+        }
     }
     if (COUNT) flush_counts(pool.counters, visits, tests);
 }
@@ -408,8 +462,9 @@ __global__ void __launch_bounds__(BLOCK, CN_SHADE_MIN_BLOCKS) k_shade(DeviceScen
                         if (cpdf > 0.0f && wl.z != 0.0f && (wl.z < 0.0f) == through) {
                             // A delta light has no competing BSDF strategy: weight 1.
                             bool mis = !cdelta && light_sampling == CENOTE_LIGHT_SAMPLING_MIS;
-                            float w = mis ? power_heuristic(nee, bsdf_pdf(cl, wl, wo)) : 1.0f;
-                            float3 unshadowed = thr * crad * eval_bsdf(cl, wl, wo) * fabsf(wl.z) * (w / nee);
+                            EvalPdf ep = eval_pdf(cl, wl, wo);
+                            float w = mis ? power_heuristic(nee, ep.pdf) : 1.0f;
+                            float3 unshadowed = thr * crad * ep.f * fabsf(wl.z) * (w / nee);
                             if (any_pos(unshadowed)) {
                                 float3 sorg = through ? sp.below : sp.position;
                                 push_shadow = true;
@@ -426,11 +481,17 @@ __global__ void __launch_bounds__(BLOCK, CN_SHADE_MIN_BLOCKS) k_shade(DeviceScen
                     }
                     float u_lobe = sample_1d(pixel, sample, bounce_dim(bounce, BSDF_LOBE));
                     float2 u = sample_2d(pixel, sample, bounce_dim(bounce, BSDF_DIR));
-                    BsdfSample sc = sample_bsdf(cl, wo, u_lobe, u.x, u.y);
+                    BsdfSample sc;
+                    float3 fsc = f3(0.0f);
+                    if (sample_bsdf_dir(cl, wo, u_lobe, u.x, u.y, sc)) {
+                        EvalPdf ep = eval_pdf(cl, sc.wi, wo);
+                        sc.pdf = ep.pdf;
+                        fsc = ep.f;
+                    }
                     float3 wiw = frame.to_world(sc.wi);
                     float3 scattered = f3(0.0f);
                     if (sc.pdf > 0.0f && sc.wi.z != 0.0f && (sc.wi.z > 0.0f) == (dot(wiw, sp.normal) > 0.0f))
-                        scattered = thr * eval_bsdf(cl, sc.wi, wo) * (fabsf(sc.wi.z) / sc.pdf);
+                        scattered = thr * fsc * (fabsf(sc.wi.z) / sc.pdf);
                     float survival = max3(scattered);
                     bool terminal = false;
                     if (survival <= 0.0f) {
@@ -492,25 +553,49 @@ __global__ void __launch_bounds__(BLOCK, CN_SHADE_MIN_BLOCKS) k_shade(DeviceScen
 template <bool COUNT>
 __global__ void __launch_bounds__(BLOCK, CN_TRAV_MIN_BLOCKS) k_shadow(DeviceScene scene, PathPool pool, uint32_t bounce) {
     const uint32_t count = min(pool.counters[CTR_SHADOWS + bounce], pool.capacity);
+    uint32_t* fetch = pool.counters + CTR_FETCH_SHADOW + bounce;
     uint32_t visits = 0, tests = 0;
+    uint2 stack[TRAVERSAL_STACK];
+    ShadowQuery q;
+    Ray ray;
+    float3 contrib = f3(0.0f);
+    uint32_t path = 0;
+    bool live = false, drained = false;
     for (;;) {
-        uint32_t base = warp_fetch(pool.counters + CTR_FETCH_SHADOW + bounce);
-        if (base >= count) break;
-        uint32_t i = base + lane_id();
-        if (i >= count) continue;
-        const float4* rec = reinterpret_cast<const float4*>(pool.shadows + i);
-        float4 q0 = rec[0], q1 = rec[1], q2 = rec[2], q3 = rec[3];
-        uint32_t path = __float_as_uint(q1.w);
-        uint32_t light = __float_as_uint(q2.w), lprim = __float_as_uint(q3.x);
-        Ray ray = make_ray(xyz(q0), xyz(q1));
-        float atten = shadow_query<COUNT>(scene, ray, q0.w, light, lprim, __float_as_uint(q3.y), &visits, &tests);
-        if (atten == -2.0f) {
-            flag_overflow(pool.counters);
+        if (!drained) {
+            uint32_t i = refill(fetch, count, live, drained);
+            if (i != ~0u) {
+                const float4* rec = reinterpret_cast<const float4*>(pool.shadows + i);
+                float4 q0 = rec[0], q1 = rec[1], q2 = rec[2], q3 = rec[3];
+                path = __float_as_uint(q1.w);
+                contrib = xyz(q2);
+                ray = make_ray(xyz(q0), xyz(q1));
+                shadow_begin(scene, ray, q0.w, __float_as_uint(q2.w), __float_as_uint(q3.x), __float_as_uint(q3.y), q);
+                live = true;
+            }
+        }
+        if (!__any_sync(0xffffffffu, live)) {
+            if (drained) break;
             continue;
         }
-        if (atten >= 0.0f) {
-            float4 r = pool.rad[path];
-            pool.rad[path] = make_float4(r.x + q2.x * atten, r.y + q2.y * atten, r.z + q2.z * atten, r.w);
+        const uint32_t want_idle = drained ? 32u : uint32_t(CN_REFILL_IDLE);
+        for (;;) {
+            if (live) {
+                int st = shadow_step<COUNT>(scene, ray, q, stack, &visits, &tests);
+                if (st == WALK_OVERFLOW) {
+                    flag_overflow(pool.counters);
+                    live = false;
+                } else if (st == WALK_DONE) {
+                    float atten = shadow_result(q);
+                    if (atten >= 0.0f) {
+                        float4 r = pool.rad[path];
+                        pool.rad[path] = make_float4(r.x + contrib.x * atten, r.y + contrib.y * atten,
+                                                     r.z + contrib.z * atten, r.w);
+                    }
+                    live = false;
+                }
+            }
+            if (uint32_t(__popc(__ballot_sync(0xffffffffu, !live))) >= want_idle) break;
         }
     }
     if (COUNT) flush_counts(pool.counters, visits, tests);

@@ -8,6 +8,7 @@
 #include <cmath>
 #include <cuda_runtime.h>
 
+#define __noinline__
 inline float __fadd_rn(float a, float b) { return a + b; }
 inline float __fsub_rn(float a, float b) { return a - b; }
 inline float __fmul_rn(float a, float b) { return a * b; }
@@ -21,6 +22,14 @@ inline float __uint_as_float(uint32_t u) { float f; std::memcpy(&f, &u, 4); retu
 inline uint32_t __float_as_uint(float f) { uint32_t u; std::memcpy(&u, &f, 4); return u; }
 inline int __clz(uint32_t x) { return x ? __builtin_clz(x) : 32; }
 inline int __popc(uint32_t x) { return __builtin_popcount(x); }
+// Byte select of the pair (y:x), selector nibbles 0-7 (the sign-replicate
+// bit is not used by the library).
+inline uint32_t __byte_perm(uint32_t x, uint32_t y, uint32_t s) {
+    uint64_t v = (uint64_t(y) << 32) | x;
+    uint32_t r = 0;
+    for (int k = 0; k < 4; ++k) r |= uint32_t((v >> (8 * ((s >> (4 * k)) & 7u))) & 0xffu) << (8 * k);
+    return r;
+}
 inline int __ffs(uint32_t x) { return __builtin_ffs(int(x)); }
 inline uint32_t min(uint32_t a, uint32_t b) { return a < b ? a : b; }
 template <class T> inline T __ldg(const T* p) { return *p; }
