@@ -37,12 +37,16 @@ WORKLOADS = {
                         "1280x720, 64 spp, 12 bounces"),
     "cornell": dict(scene="cornell", width=256, height=256, spp=16, max_bounces=8,
                     label="closed box (36 tris) + 0.5x0.5 emitter, 256x256, 16 spp, 8 bounces"),
+    "large": dict(scene="large", width=1920, height=1080, spp=64, max_bounces=16,
+                  label="fBm terrain 1024^2 grid (2.09 M tris, 64 tiles) + 500 glass/coat/fuzz instances (~2k tris "
+                        "each) + 4,096 lognormal(0,2) emitter triangles + 128 BC1/BC5 1024^2 textures, "
+                        "1920x1080, 64 spp, 16 bounces"),
 }
 
 
 def make_spec(w):
     from cenote_b200 import scenes
-    return scenes.chart() if w["scene"] == "chart" else scenes.cornell()
+    return {"chart": scenes.chart, "cornell": scenes.cornell, "large": scenes.large}[w["scene"]]()
 
 
 def measured_peaks():

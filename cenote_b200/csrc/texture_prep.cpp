@@ -16,6 +16,8 @@
 #include <cmath>
 #include <cstdint>
 #include <cstring>
+#include <thread>
+#include <vector>
 
 #include "../../include/cenote_c.h"
 #include "texture_prep.h"
@@ -203,24 +205,32 @@ bool texture_encode(uint32_t format, const uint8_t* rgba, uint32_t w, uint32_t h
     if (!bc1 && format != CENOTE_TEXTURE_BC4_UNORM && format != CENOTE_TEXTURE_BC5_UNORM) return false;
     const uint32_t bw = w / 4, bh = h / 4;
     const size_t block = format == CENOTE_TEXTURE_BC5_UNORM ? 16 : 8;
-    for (uint32_t by = 0; by < bh; ++by)
-        for (uint32_t bx = 0; bx < bw; ++bx) {
-            uint8_t* dst = out + block * (size_t(by) * bw + bx);
-            Rgb px[16];
-            uint8_t ch[2][16];
-            for (int t = 0; t < 16; ++t) {
-                const uint8_t* p = rgba + 4 * ((size_t(by) * 4 + t / 4) * w + bx * 4 + t % 4);
-                px[t] = {float(p[0]), float(p[1]), float(p[2])};
-                ch[0][t] = p[0];
-                ch[1][t] = p[1];
+    auto rows = [&](uint32_t by0, uint32_t by1) {
+        for (uint32_t by = by0; by < by1; ++by)
+            for (uint32_t bx = 0; bx < bw; ++bx) {
+                uint8_t* dst = out + block * (size_t(by) * bw + bx);
+                Rgb px[16];
+                uint8_t ch[2][16];
+                for (int t = 0; t < 16; ++t) {
+                    const uint8_t* p = rgba + 4 * ((size_t(by) * 4 + t / 4) * w + bx * 4 + t % 4);
+                    px[t] = {float(p[0]), float(p[1]), float(p[2])};
+                    ch[0][t] = p[0];
+                    ch[1][t] = p[1];
+                }
+                if (bc1) {
+                    encode_bc1_block(px, dst);
+                } else {
+                    encode_bc4_block(ch[0], dst);
+                    if (format == CENOTE_TEXTURE_BC5_UNORM) encode_bc4_block(ch[1], dst + 8);
+                }
             }
-            if (bc1) {
-                encode_bc1_block(px, dst);
-            } else {
-                encode_bc4_block(ch[0], dst);
-                if (format == CENOTE_TEXTURE_BC5_UNORM) encode_bc4_block(ch[1], dst + 8);
-            }
-        }
+    };
+    // Blocks are independent: split the block rows over the host's threads.
+    const uint32_t threads = std::max(1u, std::min(std::thread::hardware_concurrency(), std::max(1u, bh / 16)));
+    std::vector<std::thread> pool;
+    for (uint32_t k = 0; k < threads; ++k)
+        pool.emplace_back(rows, bh * k / threads, bh * (k + 1) / threads);
+    for (auto& t : pool) t.join();
     return true;
 }
 

@@ -321,13 +321,34 @@ class Texture:
 def rgba8_texture(rgb, srgb: bool = True, alpha=None) -> Texture:
     """An RGBA8 texture from float RGB in [0, 1] (H, W, 3), stored sRGB-encoded
     (colour) or linear (scalars, normal maps)."""
-    rgb = np.clip(np.asarray(rgb, np.float64), 0.0, 1.0)
+    rgb = np.clip(np.asarray(rgb, np.float32), np.float32(0), np.float32(1))
     if srgb:
-        rgb = np.where(rgb <= 0.0031308, rgb * 12.92, 1.055 * rgb ** (1 / 2.4) - 0.055)
+        rgb = np.where(rgb <= np.float32(0.0031308), rgb * np.float32(12.92),
+                       np.float32(1.055) * rgb ** np.float32(1 / 2.4) - np.float32(0.055))
     h, w = rgb.shape[:2]
-    a = np.ones((h, w)) if alpha is None else np.clip(alpha, 0, 1)
-    px = np.round(np.concatenate([rgb, a[..., None]], -1) * 255.0).astype(np.uint8)
-    return Texture(TEX_RGBA8_SRGB if srgb else TEX_RGBA8_UNORM, w, h, np.ascontiguousarray(px))
+    px = np.empty((h, w, 4), np.uint8)
+    px[..., :3] = (rgb * np.float32(255) + np.float32(0.5)).astype(np.uint8)
+    px[..., 3] = 255 if alpha is None else (np.clip(alpha, 0, 1) * 255 + 0.5).astype(np.uint8)
+    return Texture(TEX_RGBA8_SRGB if srgb else TEX_RGBA8_UNORM, w, h, px)
+
+
+def _lerp_axis(n: int, cells: int, wrap: bool):
+    """Lattice indices and smoothstep weights of n samples over `cells` cells."""
+    x = np.arange(n) * cells / n if wrap else np.linspace(0.0, cells, n, endpoint=False) + 0.5 * cells / n
+    i0 = np.floor(x).astype(int)
+    f = x - i0
+    i0 = i0 % cells if wrap else np.minimum(i0, cells - 1)
+    i1 = (i0 + 1) % cells if wrap else i0 + 1
+    return i0, i1, f * f * (3 - 2 * f)
+
+
+def _octave(lattice: np.ndarray, n: int, wrap: bool) -> np.ndarray:
+    """Separable smoothstep interpolation of a lattice to n x n: along x on
+    the lattice rows first, then one row gather along z."""
+    cells = lattice.shape[0] - (0 if wrap else 1)
+    i0, i1, f = _lerp_axis(n, cells, wrap)
+    rows_x = lattice[:, i0] * (1 - f)[None, :] + lattice[:, i1] * f[None, :]
+    return rows_x[i0] * (1 - f)[:, None] + rows_x[i1] * f[:, None]
 
 
 def value_noise(size: int, seed: int, octaves: int = 4, base: int = 8) -> np.ndarray:
@@ -338,15 +359,7 @@ def value_noise(size: int, seed: int, octaves: int = 4, base: int = 8) -> np.nda
     amp, total = 1.0, 0.0
     for o in range(octaves):
         cells = base << o
-        lattice = rng.random((cells, cells))
-        x = np.arange(size) * cells / size
-        i0 = np.floor(x).astype(int) % cells
-        i1 = (i0 + 1) % cells
-        f = x - np.floor(x)
-        f = f * f * (3 - 2 * f)
-        rows = lattice[i0][:, i0] * (1 - f)[None, :] + lattice[i0][:, i1] * f[None, :]
-        rows1 = lattice[i1][:, i0] * (1 - f)[None, :] + lattice[i1][:, i1] * f[None, :]
-        out += amp * (rows * (1 - f)[:, None] + rows1 * f[:, None])
+        out += amp * _octave(rng.random((cells, cells)), size, True)
         total += amp
         amp *= 0.5
     return out / total
@@ -552,3 +565,166 @@ def textured(width=160, height=90, spp=8, max_bounces=6, size=64, seed=7) -> Sce
     cam = Camera((0.0, 1.4, 4.0), (0.0, 0.6, 0.0), vfov_degrees=45.0)
     return SceneSpec("textured", objs, cam, Environment.constant((0.15, 0.18, 0.25)), width, height, spp,
                      max_bounces, textures=textures)
+
+
+# ---- the large scene --------------------------------------------------------------
+
+
+def fbm_heightfield(n: int, seed: int, octaves: int = 6) -> np.ndarray:
+    """Seeded fBm (value noise, lacunarity 2, gain 0.5) on an n x n grid, in [0, 1]."""
+    rng = np.random.default_rng(seed)
+    out = np.zeros((n, n))
+    amp, total = 1.0, 0.0
+    for o in range(octaves):
+        cells = 4 << o
+        out += amp * _octave(rng.random((cells + 1, cells + 1)), n, False)
+        total += amp
+        amp *= 0.5
+    return out / total
+
+
+def grid_mesh(heights: np.ndarray, x0: float, z0: float, cell: float, uv_scale: float) -> Mesh:
+    """A heightfield patch: vertices at (x0 + j·cell, h[i, j], z0 + i·cell),
+    two triangles per cell wound upward, smooth normals from central differences."""
+    h = np.asarray(heights, np.float64)
+    r, c = h.shape
+    jj, ii = np.meshgrid(np.arange(c), np.arange(r))
+    pos = np.stack([x0 + jj * cell, h, z0 + ii * cell], -1).reshape(-1, 3)
+    gx = np.gradient(h, cell, axis=1)
+    gz = np.gradient(h, cell, axis=0)
+    n = np.stack([-gx, np.ones_like(h), -gz], -1)
+    n /= np.linalg.norm(n, axis=-1, keepdims=True)
+    uv = np.stack([jj / (c - 1), ii / (r - 1)], -1).reshape(-1, 2) * uv_scale
+    a = (ii[:-1, :-1] * c + jj[:-1, :-1]).reshape(-1)
+    tris = np.concatenate([np.stack([a, a + c, a + 1], -1), np.stack([a + 1, a + c, a + c + 1], -1)])
+    return _mesh(pos, n.reshape(-1, 3), uv, tris)
+
+
+def torus(major: float, minor: float, nu: int = 32, nv: int = 32) -> Mesh:
+    u = np.arange(nu) * 2 * np.pi / nu
+    v = np.arange(nv) * 2 * np.pi / nv
+    uu, vv = np.meshgrid(u, v, indexing="ij")
+    cx, cz = np.cos(uu), np.sin(uu)
+    pos = np.stack([(major + minor * np.cos(vv)) * cx, minor * np.sin(vv), (major + minor * np.cos(vv)) * cz], -1)
+    nrm = np.stack([np.cos(vv) * cx, np.sin(vv), np.cos(vv) * cz], -1)
+    uv = np.stack([uu / (2 * np.pi), vv / (2 * np.pi)], -1)
+    i, j = np.meshgrid(np.arange(nu), np.arange(nv), indexing="ij")
+    a = (i * nv + j).reshape(-1)
+    b = (((i + 1) % nu) * nv + j).reshape(-1)
+    c = (i * nv + (j + 1) % nv).reshape(-1)
+    d = (((i + 1) % nu) * nv + (j + 1) % nv).reshape(-1)
+    tris = np.concatenate([np.stack([a, c, b], -1), np.stack([b, c, d], -1)])
+    return _mesh(pos.reshape(-1, 3), nrm.reshape(-1, 3), uv.reshape(-1, 2), tris)
+
+
+def uv_sphere(rings: int = 16, segments: int = 64) -> Mesh:
+    """Unit UV sphere, 2·rings·segments − 2·segments triangles."""
+    th = np.arange(rings + 1) * np.pi / rings
+    ph = np.arange(segments + 1) * 2 * np.pi / segments
+    t, p = np.meshgrid(th, ph, indexing="ij")
+    n = np.stack([np.sin(t) * np.cos(p), np.cos(t), np.sin(t) * np.sin(p)], -1).reshape(-1, 3)
+    uv = np.stack([p / (2 * np.pi), t / np.pi], -1).reshape(-1, 2)
+    row = segments + 1
+    tris = []
+    for r in range(rings):
+        for s in range(segments):
+            a = r * row + s
+            b = a + row
+            if r != 0:
+                tris.append((a, a + 1, b))
+            if r != rings - 1:
+                tris.append((a + 1, b + 1, b))
+    return _mesh(n, n.copy(), uv, np.asarray(tris))
+
+
+def superquadric(e: float = 0.3, rings: int = 16, segments: int = 64) -> Mesh:
+    """A rounded box (superellipsoid with exponent e), 1,920 triangles by default."""
+    sph = uv_sphere(rings, segments)
+    p = sph.positions.astype(np.float64)
+    q = np.sign(p) * np.abs(p) ** e
+    return _mesh(q, derive_flat_normals(q, sph.indices), sph.uvs, sph.indices)
+
+
+def derive_flat_normals(p, idx):
+    face = np.cross(p[idx[:, 1]] - p[idx[:, 0]], p[idx[:, 2]] - p[idx[:, 0]])
+    n = np.zeros_like(p)
+    for k in range(3):
+        np.add.at(n, idx[:, k], face)
+    ln = np.linalg.norm(n, axis=1, keepdims=True)
+    return np.where(ln > 0, n / np.maximum(ln, 1e-30), [0.0, 1.0, 0.0])
+
+
+def large(width=1920, height=1080, spp=64, max_bounces=16, grid=1024, instances=500, emitters=4096,
+          texture_size=1024, textures=128, seed=1) -> SceneSpec:
+    """The large scene: an fBm terrain of (grid−1)²·2 triangles (1024² grid:
+    2.09 M) in 8×8 tiles, each with its own BC1 base-colour and BC5 normal map
+    (128 seeded value-noise textures of texture_size²); `instances` copies of
+    three ~2k-triangle meshes — glass (IOR 1.5, absorption 0.2 per unit), a
+    clear-coated torus and a fuzz-covered rounded box — placed on the terrain;
+    `emitters` small emissive triangles whose powers are lognormal(0, 2); a
+    procedural sun-and-sky environment."""
+    from . import encode_texture
+
+    rng = np.random.default_rng(seed)
+    extent = 200.0
+    cell = extent / (grid - 1)
+    hf = fbm_heightfield(grid, seed) * 18.0
+    tiles = 8
+    per = (grid - 1) // tiles
+    objs, texs = [], []
+    ident = rows(np.eye(4))
+    for k in range(textures // 2):
+        col_noise = value_noise(texture_size, seed * 1000 + 2 * k, octaves=5, base=8)
+        hue = rng.random(3) * 0.4 + np.array([0.25, 0.25, 0.15])
+        col = np.clip(hue[None, None, :] * (0.5 + col_noise[..., None]), 0, 1)
+        texs.append(encode_texture(TEX_BC1_SRGB, rgba8_texture(col, srgb=True)))
+        bump = value_noise(texture_size, seed * 1000 + 2 * k + 1, octaves=5, base=16)
+        texs.append(encode_texture(TEX_BC5_UNORM, rgba8_texture(normal_map_from_height(bump, 8.0), srgb=False)))
+    for ti in range(tiles):
+        for tj in range(tiles):
+            r0, c0 = ti * per, tj * per
+            r1 = grid - 1 if ti == tiles - 1 else r0 + per
+            c1 = grid - 1 if tj == tiles - 1 else c0 + per
+            patch = hf[r0:r1 + 1, c0:c1 + 1]
+            mesh = grid_mesh(patch, -extent / 2 + c0 * cell, -extent / 2 + r0 * cell, cell, 8.0)
+            t = (ti * tiles + tj) % (textures // 2)
+            m = material(base_color=(1.0, 1.0, 1.0), specular_weight=1.0, specular_roughness=0.6)
+            m["base_color_texture"], m["normal_texture"] = 2 * t, 2 * t + 1
+            objs.append(Object(mesh, ident, m))
+
+    def height_at(x, z):
+        j = int(np.clip((x + extent / 2) / cell, 0, grid - 1))
+        i = int(np.clip((z + extent / 2) / cell, 0, grid - 1))
+        return float(hf[i, j])
+
+    glass = material(base_color=(1.0, 1.0, 1.0), specular_weight=1.0, specular_roughness=0.0, specular_ior=1.5,
+                     transmission_weight=1.0, transmission_color=np.exp(-0.2) * np.ones(3), transmission_depth=1.0)
+    coated = material(base_color=acescg((0.6, 0.1, 0.08)), specular_weight=1.0, specular_roughness=0.4,
+                      coat_weight=1.0, coat_roughness=0.05, coat_ior=1.5)
+    fuzzy = material(base_color=acescg((0.2, 0.3, 0.6)), specular_weight=0.5, specular_roughness=0.5,
+                     fuzz_weight=1.0, fuzz_color=(1.0, 0.9, 0.8), fuzz_roughness=0.5)
+    shapes = [(uv_sphere(16, 64), glass), (torus(1.0, 0.35, 32, 32), coated), (superquadric(0.35), fuzzy)]
+    span = extent * 0.35
+    for k in range(instances):
+        mesh, mat = shapes[k % 3]
+        x, z = rng.uniform(-span, span, 2)
+        s = rng.uniform(0.8, 2.5)
+        rot = rotate_y(rng.uniform(0, 360))
+        objs.append(Object(mesh, rows(translate(x, height_at(x, z) + s, z) @ rot @ scale(s)), mat))
+    powers = rng.lognormal(0.0, 2.0, emitters)
+    for k in range(emitters):
+        x, z = rng.uniform(-span, span, 2)
+        y = height_at(x, z) + rng.uniform(3.0, 12.0)
+        a = rng.uniform(0, 2 * np.pi)
+        size = 0.35
+        p0 = np.array([x, y, z])
+        p1 = p0 + size * np.array([np.cos(a), 0.0, np.sin(a)])
+        p2 = p0 + size * np.array([np.cos(a + 2.0), -0.3, np.sin(a + 2.0)])
+        tri = _mesh([p0, p1, p2], [np.cross(p1 - p0, p2 - p0) / np.linalg.norm(np.cross(p1 - p0, p2 - p0))] * 3,
+                    [[0, 0], [1, 0], [0, 1]], [[0, 1, 2]])
+        objs.append(Object(tri, ident, emitter(acescg((1.0, 0.85, 0.6)) * np.float32(powers[k] * 4.0))))
+    look = np.array([0.0, height_at(0.0, 0.0) + 2.0, 0.0])
+    eye = look + np.array([0.0, 28.0, 75.0])
+    cam = Camera(tuple(eye), tuple(look), vfov_degrees=45.0)
+    env = sky_hdri(1024, 512, sun_elevation_deg=25.0)
+    return SceneSpec("large", objs, cam, env, width, height, spp, max_bounces, textures=texs)
