@@ -115,7 +115,8 @@ EXPORTED_SYMBOLS = [
     "cenote_film_device_sums", "cenote_probe_sampler", "cenote_probe_bsdf", "cenote_probe_bsdf_sample",
     "cenote_probe_intersect", "cenote_probe_shadow", "cenote_probe_env_sample", "cenote_probe_env_pdf",
     "cenote_env_tables_static", "cenote_scene_create_textured", "cenote_texture_bytes", "cenote_texture_encode",
-    "cenote_probe_texture",
+    "cenote_probe_texture", "cenote_server_create", "cenote_server_destroy", "cenote_job_submit", "cenote_job_poll",
+    "cenote_job_wait", "cenote_job_result", "cenote_job_release", "cenote_server_stats",
 ]
 
 _lib = None
@@ -141,6 +142,14 @@ def library() -> C.CDLL:
         "cenote_texture_bytes": (C.c_uint64, [U32, U32, U32]),
         "cenote_texture_encode": (I32, [U32, P, U32, U32, P]),
         "cenote_probe_texture": (I32, [P, U32, U32, P, U32, P]),
+        "cenote_server_create": (I32, [P, C.c_uint64, P, P]),
+        "cenote_server_destroy": (None, [P]),
+        "cenote_job_submit": (I32, [P, P, U32, U32, U32, U32, P, P, P]),
+        "cenote_job_poll": (I32, [P, C.c_uint64, P]),
+        "cenote_job_wait": (I32, [P, C.c_uint64, C.c_double]),
+        "cenote_job_result": (I32, [P, C.c_uint64, P]),
+        "cenote_job_release": (I32, [P, C.c_uint64]),
+        "cenote_server_stats": (I32, [P, P]),
         "cenote_scene_destroy": (None, [P]),
         "cenote_scene_set_camera": (I32, [P, P]),
         "cenote_scene_prep_times": (I32, [P, P]),
@@ -529,6 +538,93 @@ class Renderer:
     def close(self) -> None:
         if getattr(self, "_h", None):
             library().cenote_renderer_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+# ---- serving ---------------------------------------------------------------------
+
+JOB_QUEUED, JOB_RUNNING, JOB_DONE, JOB_FAILED = 0, 1, 2, 3
+
+FRAME_FN = C.CFUNCTYPE(None, C.c_void_p, C.c_uint64, C.c_uint32, C.c_uint32, C.POINTER(C.c_float), C.c_uint32,
+                       C.c_uint32)
+
+
+class ServerOptions(C.Structure):
+    _fields_ = [("slots", C.c_uint32), ("frame_spp", C.c_uint32), ("max_active", C.c_uint32),
+                ("pool_paths", C.c_uint32), ("light_sampling", C.c_uint32), ("no_graphs", C.c_uint32)]
+
+
+class JobStatus(C.Structure):
+    _fields_ = [("state", C.c_uint32), ("samples", C.c_uint32), ("target", C.c_uint32), ("error", C.c_int32),
+                ("submit_ms", C.c_double), ("admit_ms", C.c_double), ("first_frame_ms", C.c_double),
+                ("done_ms", C.c_double)]
+
+
+class ServerCounters(C.Structure):
+    _fields_ = [("submitted", C.c_uint64), ("completed", C.c_uint64), ("failed", C.c_uint64),
+                ("queued", C.c_uint64), ("active", C.c_uint64), ("samples", C.c_uint64),
+                ("bytes_in_use", C.c_uint64), ("budget", C.c_uint64), ("wall_ms", C.c_double)]
+
+
+class Server:
+    """The serving loop (cenote_server_*): progressive jobs admitted by an HBM
+    budget, advanced in frame_spp chunks over `slots` streams. `on_frame(job,
+    samples, target, rgba)` runs on the server thread after every chunk."""
+
+    def __init__(self, ctx: Context, hbm_budget: int, slots: int = 0, frame_spp: int = 0, max_active: int = 0,
+                 pool_paths: int = 0, light_sampling: int = LIGHT_SAMPLING_MIS, graphs: bool = True, on_frame=None):
+        opt = ServerOptions(slots, frame_spp, max_active, pool_paths, light_sampling, 0 if graphs else 1)
+        h = C.c_void_p()
+        _check(library().cenote_server_create(ctx.handle, int(hbm_budget), C.byref(opt), C.byref(h)))
+        self._h = h
+        self.ctx = ctx
+        self._sizes = {}
+        self._on_frame = on_frame
+        self._fn = FRAME_FN(self._frame) if on_frame else None
+
+    def _frame(self, user, job, samples, target, rgba, w, h):
+        img = np.ctypeslib.as_array(rgba, shape=(h, w, 4)).copy()
+        self._on_frame(int(job), int(samples), int(target), img)
+
+    def submit(self, scene: Scene, width: int, height: int, target_spp: int, max_bounces: int) -> int:
+        job = C.c_uint64()
+        _check(library().cenote_job_submit(self._h, scene.handle, width, height, target_spp, max_bounces,
+                                           C.cast(self._fn, C.c_void_p) if self._fn else None, None, C.byref(job)))
+        self._sizes[job.value] = (width, height)
+        return job.value
+
+    def poll(self, job: int) -> JobStatus:
+        st = JobStatus()
+        _check(library().cenote_job_poll(self._h, job, C.byref(st)))
+        return st
+
+    def wait(self, job: int, timeout_ms: float = 600000.0) -> None:
+        _check(library().cenote_job_wait(self._h, job, timeout_ms))
+
+    def result(self, job: int) -> np.ndarray:
+        w, h = self._sizes[job]
+        out = np.zeros((h, w, 4), np.float32)
+        _check(library().cenote_job_result(self._h, job, _ptr(out)))
+        return out
+
+    def release(self, job: int) -> None:
+        _check(library().cenote_job_release(self._h, job))
+        self._sizes.pop(job, None)
+
+    def stats(self) -> dict:
+        st = ServerCounters()
+        _check(library().cenote_server_stats(self._h, C.byref(st)))
+        return {k: getattr(st, k) for k, _ in ServerCounters._fields_}
+
+    def close(self) -> None:
+        if getattr(self, "_h", None):
+            library().cenote_server_destroy(self._h)
             self._h = None
 
     def __del__(self):

@@ -18,6 +18,7 @@
 #include "../../include/cenote_c.h"
 #include "bvh_build.h"
 #include "records.h"
+#include "runtime.h"
 #include "texture_prep.h"
 #include "wavefront.h"
 
@@ -44,6 +45,7 @@ cudaError_t static_env_scratch(int device, double** out, size_t* max_texels, uin
 
 using namespace cn;
 
+
 namespace {
 
 // The BSDF lookup tables (ggx_energy.bin ++ ltc_sheen.bin, the layout of
@@ -52,65 +54,6 @@ const uint32_t kTables[] = {
 #include "tables_blob.inc"
 };
 static_assert(sizeof(kTables) == 16928 * 4, "BSDF tables are 16,928 floats");
-
-thread_local std::string g_error;
-
-int32_t fail(int32_t code, const std::string& msg) {
-    g_error = msg;
-    return code;
-}
-
-#define CN_CUDA(call)                                                                       \
-    do {                                                                                    \
-        cudaError_t e_ = (call);                                                            \
-        if (e_ != cudaSuccess)                                                              \
-            return fail(e_ == cudaErrorMemoryAllocation ? CENOTE_E_ALLOCATION : CENOTE_E_DEVICE, \
-                        std::string(#call ": ") + cudaGetErrorString(e_));                  \
-    } while (0)
-
-#define CN_CHECK(cond, code, msg) \
-    do {                          \
-        if (!(cond)) return fail((code), (msg)); \
-    } while (0)
-
-// Bounded wait: poll an event until it completes or `timeout_ms` passes.
-int32_t wait_stream(cudaStream_t s, cudaEvent_t ev, double timeout_ms) {
-    cudaError_t e = cudaEventRecord(ev, s);
-    if (e != cudaSuccess) return fail(CENOTE_E_DEVICE, std::string("cudaEventRecord: ") + cudaGetErrorString(e));
-    auto t0 = std::chrono::steady_clock::now();
-    for (;;) {
-        e = cudaEventQuery(ev);
-        if (e == cudaSuccess) return CENOTE_OK;
-        if (e != cudaErrorNotReady) return fail(CENOTE_E_DEVICE, std::string("device error: ") + cudaGetErrorString(e));
-        double ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
-        if (ms > timeout_ms) return fail(CENOTE_E_TIMEOUT, "device work did not finish within the wait bound");
-        std::this_thread::sleep_for(std::chrono::microseconds(ms < 5.0 ? 20 : 200));
-    }
-}
-
-struct DeviceBuffer {
-    void* ptr = nullptr;
-    size_t bytes = 0;
-    DeviceBuffer() = default;
-    DeviceBuffer(const DeviceBuffer&) = delete;
-    DeviceBuffer& operator=(const DeviceBuffer&) = delete;
-    ~DeviceBuffer() { release(); }
-    void release() {
-        if (ptr) cudaFree(ptr);
-        ptr = nullptr;
-        bytes = 0;
-    }
-    cudaError_t alloc(size_t n) {
-        release();
-        if (n == 0) n = 16;
-        bytes = n;
-        return cudaMalloc(&ptr, n);
-    }
-    template <class T>
-    T* as() const {
-        return static_cast<T*>(ptr);
-    }
-};
 
 struct V3 {
     float x, y, z;
@@ -247,6 +190,22 @@ float select_probability(double env_power, double light_power) {
 
 // Camera::basis (scene/mod.rs:448-460), scaled to the focal plane when the
 // lens is open (wavefront.rs:633-650).
+bool camera_valid(const cenote_camera& cam) {
+    V3 pos = v3(cam.position), look = v3(cam.look_at), up = v3(cam.up);
+    V3 d = look - pos;
+    float l = lengthv(d);
+    if (!(l > 0.0f) || !std::isfinite(l)) return false;
+    V3 c = crossv(d * (1.0f / l), up);
+    float cl = lengthv(c);
+    return cl > 0.0f && std::isfinite(cl) && cam.vfov_degrees > 0.0f && cam.vfov_degrees < 180.0f &&
+           !(cam.aperture_radius > 0.0f && !(cam.focus_distance > 0.0f));
+}
+
+}  // namespace
+
+namespace cn {
+// Camera::basis (crates/cenote/src/scene/mod.rs:448-460) for the wave's
+// aspect ratio, pre-scaled to the focal plane when the lens is open.
 void camera_basis(const cenote_camera& cam, float aspect, WaveParams& wp) {
     V3 pos = v3(cam.position), look = v3(cam.look_at), up = v3(cam.up);
     V3 d = look - pos;
@@ -267,166 +226,11 @@ void camera_basis(const cenote_camera& cam, float aspect, WaveParams& wp) {
     wp.cam_fwd = make_float3(fwd.x, fwd.y, fwd.z);
     wp.aperture = cam.aperture_radius;
 }
-
-bool camera_valid(const cenote_camera& cam) {
-    V3 pos = v3(cam.position), look = v3(cam.look_at), up = v3(cam.up);
-    V3 d = look - pos;
-    float l = lengthv(d);
-    if (!(l > 0.0f) || !std::isfinite(l)) return false;
-    V3 c = crossv(d * (1.0f / l), up);
-    float cl = lengthv(c);
-    return cl > 0.0f && std::isfinite(cl) && cam.vfov_degrees > 0.0f && cam.vfov_degrees < 180.0f &&
-           !(cam.aperture_radius > 0.0f && !(cam.focus_distance > 0.0f));
-}
-
-}  // namespace
-
-struct cenote_context {
-    // Handles made from this context hold a reference; the context is freed
-    // when cenote_context_destroy has been called and the last one is gone,
-    // so destroy order never leaves a dangling pointer.
-    std::atomic<int> refs{1};
-    int device = 0;
-    cudaStream_t stream = nullptr;
-    cudaEvent_t sync_ev = nullptr;
-    cudaEvent_t t0 = nullptr, t1 = nullptr;
-    LaunchShape shape{};
-    DeviceBuffer tables;
-    std::mutex mu;
-};
-
-struct cenote_scene {
-    cenote_context* ctx = nullptr;
-    DeviceScene ds{};
-    std::vector<std::unique_ptr<DeviceBuffer>> buffers;
-    cudaArray_t env_array = nullptr;
-    cudaTextureObject_t env_tex = 0;
-    cenote_camera camera{};
-    std::vector<LightRecord> lights;
-    uint32_t env_w = 1, env_h = 1;
-    double env_power = 0.0;
-    float select_prob = 0.0f;
-    float prep_ms[3] = {0, 0, 0};
-    uint64_t device_bytes = 0;
-    DeviceBuffer* env_marginal = nullptr;
-    DeviceBuffer* env_conditional = nullptr;
-    DeviceBuffer* env_pdfs = nullptr;
-    std::vector<cudaArray_t> tex_arrays;            // the bindless table's storage
-    std::vector<cudaTextureObject_t> tex_objects;
-
-    DeviceBuffer* add(size_t bytes, cudaError_t* err) {
-        buffers.push_back(std::make_unique<DeviceBuffer>());
-        *err = buffers.back()->alloc(bytes);
-        device_bytes += bytes;
-        return buffers.back().get();
-    }
-    ~cenote_scene() {
-        for (cudaTextureObject_t t : tex_objects) cudaDestroyTextureObject(t);
-        for (cudaArray_t a : tex_arrays) cudaFreeArray(a);
-        if (env_tex) cudaDestroyTextureObject(env_tex);
-        if (env_array) cudaFreeArray(env_array);
-    }
-};
-
-struct cenote_renderer {
-    cenote_context* ctx = nullptr;
-    uint32_t max_bounces = 8;
-    uint32_t light_sampling = 0;
-    uint32_t capacity_req = 0;
-    uint32_t samples_per_wave = 0;
-    uint32_t profiling = 0;
-    std::vector<cudaEvent_t> events;
-    PathPool pool{};
-    DeviceBuffer org, dir, thr, hit, ps, state, rad, q0, q1, shadows, counters, tally, scratch;
-    DeviceBuffer aov_albedo, aov_normal, aov_depth, aov_guide;
-    size_t pool_cap = 0, aov_cap = 0;
-    cenote_stats stats{};
-    unsigned long long tally_prev[5] = {0, 0, 0, 0, 0};
-
-    ~cenote_renderer() {
-        for (cudaEvent_t e : events) cudaEventDestroy(e);
-    }
-    cudaEvent_t event(size_t i) {
-        while (events.size() <= i) {
-            cudaEvent_t e;
-            if (cudaEventCreate(&e) != cudaSuccess) return nullptr;
-            events.push_back(e);
-        }
-        return events[i];
-    }
-
-    cudaError_t ensure(size_t cap) {
-        if (cap <= pool_cap) return cudaSuccess;
-        cudaError_t e;
-        if ((e = org.alloc(cap * 16)) || (e = dir.alloc(cap * 16)) || (e = thr.alloc(cap * 16)) ||
-            (e = hit.alloc(cap * 16)) || (e = ps.alloc(cap * 8)) || (e = state.alloc(cap * 4)) ||
-            (e = rad.alloc(cap * 16)) || (e = q0.alloc(cap * 4)) || (e = q1.alloc(cap * 4)) ||
-            (e = shadows.alloc(cap * sizeof(ShadowRay))))
-            return e;
-        pool.org = org.as<float4>();
-        pool.dir = dir.as<float4>();
-        pool.thr = thr.as<float4>();
-        pool.hit = hit.as<uint4>();
-        pool.ps = ps.as<uint2>();
-        pool.state = state.as<uint32_t>();
-        pool.rad = rad.as<float4>();
-        pool.queue[0] = q0.as<uint32_t>();
-        pool.queue[1] = q1.as<uint32_t>();
-        pool.shadows = shadows.as<ShadowRay>();
-        pool.capacity = uint32_t(cap);
-        pool_cap = cap;
-        return cudaSuccess;
-    }
-
-    // The guide lanes: allocated on the first wave that traces guides,
-    // detached (null) for waves that do not.
-    cudaError_t set_guides(bool on) {
-        if (on && aov_cap < pool_cap) {
-            cudaError_t e;
-            if ((e = aov_albedo.alloc(pool_cap * 16)) || (e = aov_normal.alloc(pool_cap * 16)) ||
-                (e = aov_depth.alloc(pool_cap * 4)) || (e = aov_guide.alloc(pool_cap * 16)))
-                return e;
-            aov_cap = pool_cap;
-        }
-        pool.aov_albedo = on ? aov_albedo.as<float4>() : nullptr;
-        pool.aov_normal = on ? aov_normal.as<float4>() : nullptr;
-        pool.aov_depth = on ? aov_depth.as<float>() : nullptr;
-        pool.aov_guide = on ? aov_guide.as<float4>() : nullptr;
-        return cudaSuccess;
-    }
-};
-
-struct cenote_film {
-    cenote_context* ctx = nullptr;
-    uint32_t width = 0, height = 0;
-    uint32_t samples = 0;
-    DeviceBuffer sum, avg;
-    DeviceBuffer albedo, normal, depth;  // guide sums (film.rs:95-112)
-    FilmTargets targets() {
-        return {sum.as<float4>(), albedo.as<float4>(), normal.as<float4>(), depth.as<float>()};
-    }
-};
-
-namespace {
-void free_context(cenote_context* ctx) {
-    cudaSetDevice(ctx->device);
-    if (ctx->stream) cudaStreamSynchronize(ctx->stream);
-    ctx->tables.release();
-    if (ctx->sync_ev) cudaEventDestroy(ctx->sync_ev);
-    if (ctx->t0) cudaEventDestroy(ctx->t0);
-    if (ctx->t1) cudaEventDestroy(ctx->t1);
-    if (ctx->stream) cudaStreamDestroy(ctx->stream);
-    delete ctx;
-}
-void retain(cenote_context* ctx) { ctx->refs.fetch_add(1); }
-void release(cenote_context* ctx) {
-    if (ctx->refs.fetch_sub(1) == 1) free_context(ctx);
-}
-}  // namespace
+}  // namespace cn
 
 extern "C" {
 
-const char* cenote_last_error(void) { return g_error.c_str(); }
+const char* cenote_last_error(void) { return cn::last_error(); }
 
 int32_t cenote_context_create(const cenote_options* options, cenote_context** out) {
     CN_CHECK(out, CENOTE_E_INVALID_ARGUMENT, "null output handle");
@@ -947,84 +751,30 @@ void* cenote_film_device_sums(cenote_film* film) { return film ? film->sum.ptr :
 
 namespace {
 
-// Trace `count` samples starting at `sample0` for every pixel; each wave's
-// samples go either into the film (ascending order) or, for a one-shot
-// render, into `oneshot` as raw RGBA.
+// The blocking form behind cenote_accumulate_n and cenote_render_once: plan,
+// enqueue on the context's stream, wait, then fold the counters and stage
+// timings into the renderer's stats.
 int32_t run_waves(cenote_renderer* r, cenote_scene* sc, uint32_t width, uint32_t height, uint32_t sample0,
                   uint32_t count, cenote_film* film, float4* oneshot) {
     cenote_context* ctx = r->ctx;
     const uint64_t pixels = uint64_t(width) * height;
-    uint32_t range = uint32_t(pixels);
-    uint32_t spw;
-    if (r->capacity_req && r->capacity_req < pixels) {
-        range = r->capacity_req;
-        spw = 1;
-    } else if (r->samples_per_wave) {
-        spw = r->samples_per_wave;
-    } else {
-        // Enough paths per wave to keep 148 SMs busy through the tail bounces.
-        uint64_t want = (uint64_t(1) << 22) / pixels;
-        spw = uint32_t(std::max<uint64_t>(1, std::min<uint64_t>(want, 64)));
-    }
-    if (oneshot) spw = 1;
-    spw = std::min(spw, count);
-    uint64_t need = uint64_t(range) * spw;
-    if (r->capacity_req) need = std::max<uint64_t>(need, std::min<uint64_t>(r->capacity_req, need));
-    CN_CHECK(need < (1ull << 31), CENOTE_E_INVALID_ARGUMENT, "wave too large");
-    CN_CUDA(r->ensure(need));
+    WavePlan plan = plan_waves(r, pixels, count, oneshot != nullptr);
+    CN_CHECK(plan.need < (1ull << 31), CENOTE_E_INVALID_ARGUMENT, "wave too large");
+    CN_CUDA(r->ensure(plan.need));
     // Films trace the guides (Renderer::accumulate); one-shot renders do not.
     CN_CUDA(r->set_guides(film != nullptr));
-
-    WaveParams wp{};
-    wp.width = width;
-    wp.height = height;
-    wp.max_bounces = r->max_bounces;
-    wp.light_sampling = r->light_sampling;
-    camera_basis(sc->camera, float(width) / float(height), wp);
 
     const bool timing = (r->profiling & CENOTE_PROFILE_TIMING) != 0;
     const bool counting = (r->profiling & CENOTE_PROFILE_COUNTS) != 0;
     // Stage event layout per wave: [begin, after raygen, (after isect, shade, shadow) × bounces, after film].
     const size_t per_wave = 3 + 3 * size_t(r->max_bounces);
-    size_t ev = 0;
-    uint32_t launches = 0, waves = 0;
-    auto mark = [&]() {
-        if (timing) cudaEventRecord(r->event(ev++), ctx->stream);
-    };
+    WaveCounts wc;
     CN_CUDA(cudaEventRecord(ctx->t0, ctx->stream));
-    for (uint32_t done = 0; done < count;) {
-        uint32_t s = std::min(spw, count - done);
-        for (uint64_t base = 0; base < pixels; base += range) {
-            wp.pixel_base = uint32_t(base);
-            wp.pixel_count = uint32_t(std::min<uint64_t>(range, pixels - base));
-            wp.samples = s;
-            wp.sample_base = sample0 + done;
-            const uint32_t n0 = wp.pixel_count * s;
-            mark();
-            launch_wave_begin(r->pool, wp, ctx->shape, ctx->stream);
-            mark();
-            for (uint32_t b = 0; b < r->max_bounces; ++b) {
-                launch_intersect(sc->ds, r->pool, b, n0, ctx->shape, counting, ctx->stream);
-                mark();
-                launch_shade(sc->ds, r->pool, b, wp, n0, ctx->shape, ctx->stream);
-                mark();
-                launch_shadow(sc->ds, r->pool, b, ctx->shape, counting, ctx->stream);
-                mark();
-            }
-            launch_tally(r->pool, r->tally.as<unsigned long long>(), n0, r->max_bounces, ctx->stream);
-            if (film)
-                launch_accumulate(r->pool, film->targets(), wp.pixel_base, wp.pixel_count, s,
-                                  film->samples == 0 && done == 0, ctx->stream);
-            else
-                launch_copy_rad(r->pool, oneshot, wp.pixel_base, wp.pixel_count, ctx->stream);
-            mark();
-            launches += 3 + 3 * r->max_bounces;
-            waves++;
-        }
-        done += s;
-    }
+    FilmTargets targets{};
+    if (film) targets = film->targets();
+    CN_CUDA(enqueue_waves(r, sc, width, height, sample0, count, r->max_bounces, plan, film ? &targets : nullptr,
+                          film && film->samples == 0, oneshot, nullptr, ctx->stream, timing, counting, &wc));
     CN_CUDA(cudaEventRecord(ctx->t1, ctx->stream));
-    CN_CUDA(cudaGetLastError());
     int32_t rc = wait_stream(ctx->stream, ctx->sync_ev, 600000.0);
     if (rc != CENOTE_OK) return rc;
     unsigned long long t[5];
@@ -1039,11 +789,11 @@ int32_t run_waves(cenote_renderer* r, cenote_scene* sc, uint32_t width, uint32_t
     st.triangle_tests = t[4] - r->tally_prev[4];
     st.samples = pixels * count;
     st.gpu_ms = ms;
-    st.kernel_launches = launches;
-    st.waves = waves;
-    st.samples_per_wave = spw;
+    st.kernel_launches = wc.launches;
+    st.waves = wc.waves;
+    st.samples_per_wave = plan.spw;
     if (timing) {
-        for (size_t w = 0; w + per_wave <= ev; w += per_wave) {
+        for (size_t w = 0; w + per_wave <= wc.events; w += per_wave) {
             auto el = [&](size_t a) {
                 float x = 0.0f;
                 cudaEventElapsedTime(&x, r->events[w + a], r->events[w + a + 1]);

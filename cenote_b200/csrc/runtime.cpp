@@ -1,0 +1,120 @@
+// Runtime helpers shared by the C ABI and the serving loop: errors, bounded
+// waits, and the wave planner/enqueuer over the kernels of wavefront.cu.
+#include <algorithm>
+#include <chrono>
+#include <thread>
+
+#include "runtime.h"
+
+namespace cn {
+
+void camera_basis(const cenote_camera& cam, float aspect, WaveParams& wp);
+
+namespace {
+
+thread_local std::string g_error;
+
+}  // namespace
+
+const char* last_error() { return g_error.c_str(); }
+
+
+int32_t fail(int32_t code, const std::string& msg) {
+    g_error = msg;
+    return code;
+}
+
+// Bounded wait: poll an event until it completes or `timeout_ms` passes.
+int32_t wait_stream(cudaStream_t s, cudaEvent_t ev, double timeout_ms) {
+    cudaError_t e = cudaEventRecord(ev, s);
+    if (e != cudaSuccess) return fail(CENOTE_E_DEVICE, std::string("cudaEventRecord: ") + cudaGetErrorString(e));
+    auto t0 = std::chrono::steady_clock::now();
+    for (;;) {
+        e = cudaEventQuery(ev);
+        if (e == cudaSuccess) return CENOTE_OK;
+        if (e != cudaErrorNotReady) return fail(CENOTE_E_DEVICE, std::string("device error: ") + cudaGetErrorString(e));
+        double ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+        if (ms > timeout_ms) return fail(CENOTE_E_TIMEOUT, "device work did not finish within the wait bound");
+        std::this_thread::sleep_for(std::chrono::microseconds(ms < 5.0 ? 20 : 200));
+    }
+}
+
+// How a call splits into waves: `range` pixels per wave, `spw` samples each.
+WavePlan plan_waves(const cenote_renderer* r, uint64_t pixels, uint32_t count, bool oneshot) {
+    WavePlan p{uint32_t(pixels), 1, 0};
+    if (r->capacity_req && r->capacity_req < pixels) {
+        p.range = r->capacity_req;
+        p.spw = 1;
+    } else if (r->samples_per_wave) {
+        p.spw = r->samples_per_wave;
+    } else {
+        // Enough paths per wave to keep 148 SMs busy through the tail bounces.
+        uint64_t want = (uint64_t(1) << 22) / pixels;
+        p.spw = uint32_t(std::max<uint64_t>(1, std::min<uint64_t>(want, 64)));
+    }
+    if (oneshot) p.spw = 1;
+    p.spw = std::max(1u, std::min(p.spw, count));
+    p.need = uint64_t(p.range) * p.spw;
+    if (r->capacity_req) p.need = std::max<uint64_t>(p.need, std::min<uint64_t>(r->capacity_req, p.need));
+    return p;
+}
+
+// Enqueue `count` samples from `sample0` for every pixel on `stream`, with no
+// host synchronisation (so a stream capture can record it): each wave's
+// samples go into the film in ascending order or, for a one-shot render,
+// into `oneshot` as raw RGBA. The pool must already hold `plan.need` paths
+// and the guide lanes must match `film`. `sample_offset` (device, may be
+// null) is added to every sample index. Timing marks are recorded only when
+// `timing` is set (never inside a capture).
+cudaError_t enqueue_waves(cenote_renderer* r, const cenote_scene* sc, uint32_t width, uint32_t height,
+                          uint32_t sample0, uint32_t count, uint32_t max_bounces, const WavePlan& plan,
+                          const FilmTargets* film, bool film_reset, float4* oneshot, const uint32_t* sample_offset,
+                          cudaStream_t stream, bool timing, bool counting, WaveCounts* wc) {
+    cenote_context* ctx = r->ctx;
+    const uint64_t pixels = uint64_t(width) * height;
+    WaveParams wp{};
+    wp.width = width;
+    wp.height = height;
+    wp.max_bounces = max_bounces;
+    wp.light_sampling = r->light_sampling;
+    wp.sample_offset = sample_offset;
+    camera_basis(sc->camera, float(width) / float(height), wp);
+    auto mark = [&]() {
+        if (timing) cudaEventRecord(r->event(wc->events++), stream);
+    };
+    for (uint32_t done = 0; done < count;) {
+        uint32_t s = std::min(plan.spw, count - done);
+        for (uint64_t base = 0; base < pixels; base += plan.range) {
+            wp.pixel_base = uint32_t(base);
+            wp.pixel_count = uint32_t(std::min<uint64_t>(plan.range, pixels - base));
+            wp.samples = s;
+            wp.sample_base = sample0 + done;
+            const uint32_t n0 = wp.pixel_count * s;
+            mark();
+            launch_wave_begin(r->pool, wp, ctx->shape, stream);
+            mark();
+            for (uint32_t b = 0; b < max_bounces; ++b) {
+                launch_intersect(sc->ds, r->pool, b, n0, ctx->shape, counting, stream);
+                mark();
+                launch_shade(sc->ds, r->pool, b, wp, n0, ctx->shape, stream);
+                mark();
+                launch_shadow(sc->ds, r->pool, b, ctx->shape, counting, stream);
+                mark();
+            }
+            launch_tally(r->pool, r->tally.as<unsigned long long>(), n0, max_bounces, stream);
+            if (film)
+                launch_accumulate(r->pool, *film, wp.pixel_base, wp.pixel_count, s, film_reset && done == 0,
+                                  stream);
+            else
+                launch_copy_rad(r->pool, oneshot, wp.pixel_base, wp.pixel_count, stream);
+            mark();
+            wc->launches += 3 + 3 * max_bounces;
+            wc->waves++;
+        }
+        done += s;
+    }
+    return cudaGetLastError();
+}
+
+
+}  // namespace cn

@@ -1,0 +1,248 @@
+// The library's runtime objects shared by the C ABI (capi.cpp) and the
+// serving loop (server.cpp): the opaque handle types, device buffers, the
+// status/error helpers, and the wave planner and enqueuer that drive the
+// kernels of wavefront.cu.
+#pragma once
+#include <atomic>
+#include <cstdint>
+#include <memory>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include <cuda_runtime.h>
+
+#include "../../include/cenote_c.h"
+#include "records.h"
+#include "wavefront.h"
+
+namespace cn {
+
+// Record `msg` as this thread's last error and return `code`.
+int32_t fail(int32_t code, const std::string& msg);
+// The calling thread's last error message (cenote_last_error).
+const char* last_error();
+
+#define CN_CUDA(call)                                                                       \
+    do {                                                                                    \
+        cudaError_t e_ = (call);                                                            \
+        if (e_ != cudaSuccess)                                                              \
+            return ::cn::fail(e_ == cudaErrorMemoryAllocation ? CENOTE_E_ALLOCATION : CENOTE_E_DEVICE, \
+                              std::string(#call ": ") + cudaGetErrorString(e_));            \
+    } while (0)
+
+#define CN_CHECK(cond, code, msg) \
+    do {                          \
+        if (!(cond)) return ::cn::fail((code), (msg)); \
+    } while (0)
+
+// Bounded wait: record `ev` on `s` and poll it until it completes or
+// `timeout_ms` passes (CENOTE_E_TIMEOUT).
+int32_t wait_stream(cudaStream_t s, cudaEvent_t ev, double timeout_ms);
+
+struct DeviceBuffer {
+    void* ptr = nullptr;
+    size_t bytes = 0;
+    DeviceBuffer() = default;
+    DeviceBuffer(const DeviceBuffer&) = delete;
+    DeviceBuffer& operator=(const DeviceBuffer&) = delete;
+    ~DeviceBuffer() { release(); }
+    void release() {
+        if (ptr) cudaFree(ptr);
+        ptr = nullptr;
+        bytes = 0;
+    }
+    cudaError_t alloc(size_t n) {
+        release();
+        if (n == 0) n = 16;
+        bytes = n;
+        return cudaMalloc(&ptr, n);
+    }
+    template <class T>
+    T* as() const {
+        return static_cast<T*>(ptr);
+    }
+};
+
+}  // namespace cn
+
+using cn::DeviceBuffer;
+using cn::DeviceScene;
+using cn::LightRecord;
+using cn::ShadowRay;
+using cn::LaunchShape;
+using cn::PathPool;
+using cn::FilmTargets;
+
+struct cenote_context {
+    // Handles made from this context hold a reference; the context is freed
+    // when cenote_context_destroy has been called and the last one is gone,
+    // so destroy order never leaves a dangling pointer.
+    std::atomic<int> refs{1};
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    cudaEvent_t sync_ev = nullptr;
+    cudaEvent_t t0 = nullptr, t1 = nullptr;
+    LaunchShape shape{};
+    cn::DeviceBuffer tables;
+    std::mutex mu;
+};
+
+struct cenote_scene {
+    cenote_context* ctx = nullptr;
+    DeviceScene ds{};
+    std::vector<std::unique_ptr<DeviceBuffer>> buffers;
+    cudaArray_t env_array = nullptr;
+    cudaTextureObject_t env_tex = 0;
+    cenote_camera camera{};
+    std::vector<LightRecord> lights;
+    uint32_t env_w = 1, env_h = 1;
+    double env_power = 0.0;
+    float select_prob = 0.0f;
+    float prep_ms[3] = {0, 0, 0};
+    uint64_t device_bytes = 0;
+    DeviceBuffer* env_marginal = nullptr;
+    DeviceBuffer* env_conditional = nullptr;
+    DeviceBuffer* env_pdfs = nullptr;
+    std::vector<cudaArray_t> tex_arrays;            // the bindless table's storage
+    std::vector<cudaTextureObject_t> tex_objects;
+
+    DeviceBuffer* add(size_t bytes, cudaError_t* err) {
+        buffers.push_back(std::make_unique<DeviceBuffer>());
+        *err = buffers.back()->alloc(bytes);
+        device_bytes += bytes;
+        return buffers.back().get();
+    }
+    ~cenote_scene() {
+        for (cudaTextureObject_t t : tex_objects) cudaDestroyTextureObject(t);
+        for (cudaArray_t a : tex_arrays) cudaFreeArray(a);
+        if (env_tex) cudaDestroyTextureObject(env_tex);
+        if (env_array) cudaFreeArray(env_array);
+    }
+};
+
+struct cenote_renderer {
+    cenote_context* ctx = nullptr;
+    uint32_t max_bounces = 8;
+    uint32_t light_sampling = 0;
+    uint32_t capacity_req = 0;
+    uint32_t samples_per_wave = 0;
+    uint32_t profiling = 0;
+    std::vector<cudaEvent_t> events;
+    PathPool pool{};
+    DeviceBuffer org, dir, thr, hit, ps, state, rad, q0, q1, shadows, counters, tally, scratch;
+    DeviceBuffer aov_albedo, aov_normal, aov_depth, aov_guide;
+    size_t pool_cap = 0, aov_cap = 0;
+    cenote_stats stats{};
+    unsigned long long tally_prev[5] = {0, 0, 0, 0, 0};
+
+    ~cenote_renderer() {
+        for (cudaEvent_t e : events) cudaEventDestroy(e);
+    }
+    cudaEvent_t event(size_t i) {
+        while (events.size() <= i) {
+            cudaEvent_t e;
+            if (cudaEventCreate(&e) != cudaSuccess) return nullptr;
+            events.push_back(e);
+        }
+        return events[i];
+    }
+
+    cudaError_t ensure(size_t cap) {
+        if (cap <= pool_cap) return cudaSuccess;
+        cudaError_t e;
+        if ((e = org.alloc(cap * 16)) || (e = dir.alloc(cap * 16)) || (e = thr.alloc(cap * 16)) ||
+            (e = hit.alloc(cap * 16)) || (e = ps.alloc(cap * 8)) || (e = state.alloc(cap * 4)) ||
+            (e = rad.alloc(cap * 16)) || (e = q0.alloc(cap * 4)) || (e = q1.alloc(cap * 4)) ||
+            (e = shadows.alloc(cap * sizeof(ShadowRay))))
+            return e;
+        pool.org = org.as<float4>();
+        pool.dir = dir.as<float4>();
+        pool.thr = thr.as<float4>();
+        pool.hit = hit.as<uint4>();
+        pool.ps = ps.as<uint2>();
+        pool.state = state.as<uint32_t>();
+        pool.rad = rad.as<float4>();
+        pool.queue[0] = q0.as<uint32_t>();
+        pool.queue[1] = q1.as<uint32_t>();
+        pool.shadows = shadows.as<ShadowRay>();
+        pool.capacity = uint32_t(cap);
+        pool_cap = cap;
+        return cudaSuccess;
+    }
+
+    // The guide lanes: allocated on the first wave that traces guides,
+    // detached (null) for waves that do not.
+    cudaError_t set_guides(bool on) {
+        if (on && aov_cap < pool_cap) {
+            cudaError_t e;
+            if ((e = aov_albedo.alloc(pool_cap * 16)) || (e = aov_normal.alloc(pool_cap * 16)) ||
+                (e = aov_depth.alloc(pool_cap * 4)) || (e = aov_guide.alloc(pool_cap * 16)))
+                return e;
+            aov_cap = pool_cap;
+        }
+        pool.aov_albedo = on ? aov_albedo.as<float4>() : nullptr;
+        pool.aov_normal = on ? aov_normal.as<float4>() : nullptr;
+        pool.aov_depth = on ? aov_depth.as<float>() : nullptr;
+        pool.aov_guide = on ? aov_guide.as<float4>() : nullptr;
+        return cudaSuccess;
+    }
+};
+
+struct cenote_film {
+    cenote_context* ctx = nullptr;
+    uint32_t width = 0, height = 0;
+    uint32_t samples = 0;
+    DeviceBuffer sum, avg;
+    DeviceBuffer albedo, normal, depth;  // guide sums (film.rs:95-112)
+    FilmTargets targets() {
+        return {sum.as<float4>(), albedo.as<float4>(), normal.as<float4>(), depth.as<float>()};
+    }
+};
+
+namespace cn {
+inline void free_context(cenote_context* ctx) {
+    cudaSetDevice(ctx->device);
+    if (ctx->stream) cudaStreamSynchronize(ctx->stream);
+    ctx->tables.release();
+    if (ctx->sync_ev) cudaEventDestroy(ctx->sync_ev);
+    if (ctx->t0) cudaEventDestroy(ctx->t0);
+    if (ctx->t1) cudaEventDestroy(ctx->t1);
+    if (ctx->stream) cudaStreamDestroy(ctx->stream);
+    delete ctx;
+}
+inline void retain(cenote_context* ctx) { ctx->refs.fetch_add(1); }
+inline void release(cenote_context* ctx) {
+    if (ctx->refs.fetch_sub(1) == 1) free_context(ctx);
+}
+}  // namespace cn
+
+
+namespace cn {
+
+// How a call splits into waves: `range` pixels per wave, `spw` samples each.
+struct WavePlan {
+    uint32_t range, spw;
+    uint64_t need;  // paths the pool must hold
+};
+
+struct WaveCounts {
+    uint32_t launches = 0, waves = 0;
+    size_t events = 0;
+};
+
+WavePlan plan_waves(const cenote_renderer* r, uint64_t pixels, uint32_t count, bool oneshot);
+
+// Enqueue `count` samples from `sample0` for every pixel on `stream`, with no
+// host synchronisation (so a stream capture can record it): each wave's
+// samples go into the film in ascending order or, for a one-shot render,
+// into `oneshot` as raw RGBA. The pool must already hold `plan.need` paths
+// and the guide lanes must match `film`. `sample_offset` (device, may be
+// null) is added to every sample index. Timing marks are recorded only when
+// `timing` is set (never inside a capture).
+cudaError_t enqueue_waves(cenote_renderer* r, const cenote_scene* sc, uint32_t width, uint32_t height,
+                          uint32_t sample0, uint32_t count, uint32_t max_bounces, const WavePlan& plan,
+                          const FilmTargets* film, bool film_reset, float4* oneshot, const uint32_t* sample_offset,
+                          cudaStream_t stream, bool timing, bool counting, WaveCounts* wc);
+
+}  // namespace cn

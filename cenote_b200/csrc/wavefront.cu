@@ -100,7 +100,7 @@ __global__ void __launch_bounds__(BLOCK) k_raygen(PathPool pool, WaveParams wp) 
     for (uint32_t p = blockIdx.x * blockDim.x + threadIdx.x; p < n; p += gridDim.x * blockDim.x) {
         uint32_t s = p / wp.pixel_count;
         uint32_t pixel = wp.pixel_base + (p - s * wp.pixel_count);
-        uint32_t sample = wp.sample_base + s;
+        uint32_t sample = wp.sample_base + s + (wp.sample_offset ? __ldg(wp.sample_offset) : 0u);
         float2 j = sample_2d(pixel, sample, CAMERA_JITTER);
         float xx = float(pixel % wp.width) + j.x, yy = float(pixel / wp.width) + j.y;
         float ux = xx / float(wp.width), uy = yy / float(wp.height);
@@ -682,6 +682,14 @@ __global__ void k_tally(const uint32_t* counters, unsigned long long* tally, uin
 }
 
 }  // namespace
+
+namespace {
+__global__ void k_advance(uint32_t* counter, uint32_t n) {
+    if (threadIdx.x == 0 && blockIdx.x == 0) *counter += n;
+}
+}  // namespace
+
+void launch_advance(uint32_t* counter, uint32_t n, cudaStream_t stream) { k_advance<<<1, 32, 0, stream>>>(counter, n); }
 
 void launch_tally(const PathPool& pool, unsigned long long* tally, uint32_t n0, uint32_t max_bounces,
                   cudaStream_t stream) {

@@ -53,6 +53,9 @@ struct WaveParams {
     uint32_t light_sampling;
     float3 cam_pos, cam_right, cam_up, cam_fwd;  // basis pre-scaled to the focal plane when the lens is open
     float aperture;
+    // When set, added to every sample index: a replayed CUDA graph reads its
+    // progress from device memory instead of baked launch parameters.
+    const uint32_t* sample_offset;
 };
 
 struct LaunchShape {
@@ -99,5 +102,7 @@ void launch_resolve1(const float* sum, float* avg, uint32_t pixels, float sample
 void launch_tally(const PathPool& pool, unsigned long long* tally, uint32_t n0, uint32_t max_bounces,
                   cudaStream_t stream);
 void launch_copy_rad(const PathPool& pool, float4* out, uint32_t pixel_base, uint32_t pixel_count, cudaStream_t stream);
+// *counter += n on the device (a graph's progress counter).
+void launch_advance(uint32_t* counter, uint32_t n, cudaStream_t stream);
 
 }  // namespace cn

@@ -728,3 +728,6 @@ def large(width=1920, height=1080, spp=64, max_bounces=16, grid=1024, instances=
     cam = Camera(tuple(eye), tuple(look), vfov_degrees=45.0)
     env = sky_hdri(1024, 512, sun_elevation_deg=25.0)
     return SceneSpec("large", objs, cam, env, width, height, spp, max_bounces, textures=texs)
+
+
+SCENES.update(textured=textured, large=large)

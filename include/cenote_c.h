@@ -299,6 +299,71 @@ int32_t cenote_probe_env_pdf(cenote_scene* scene, const float* directions, uint3
 int32_t cenote_probe_texture(cenote_scene* scene, uint32_t index, uint32_t mode, const float* uv, uint32_t n,
                              float* rgba);
 
+/* ---- serving: progressive jobs over one device ------------------------------------- */
+
+/* A request loop with no counterpart in the reference (which renders one
+ * view per render::Session, crates/cenote/src/render/session.rs:416): jobs
+ * of uneven scenes, sizes and sample counts are admitted in arrival order
+ * against an HBM budget, kept resident, and advanced in chunks of
+ * `frame_spp` samples over `slots` CUDA streams (each with its own path
+ * pool), a progressive frame after every chunk. A job's result is bitwise
+ * identical alone and in any mix. Scenes must outlive their jobs. */
+typedef struct cenote_server cenote_server;
+
+typedef struct cenote_server_options {
+    uint32_t slots;          /* concurrent streams, each with a path pool (0: 8) */
+    uint32_t frame_spp;      /* samples per progressive frame (0: 4) */
+    uint32_t max_active;     /* jobs resident at once (0: 64) */
+    uint32_t pool_paths;     /* path capacity per slot (0: 2^21) */
+    uint32_t light_sampling; /* CENOTE_LIGHT_SAMPLING_* */
+    uint32_t no_graphs;      /* 1: launch every chunk directly instead of replaying a captured graph */
+} cenote_server_options;
+
+#define CENOTE_JOB_QUEUED 0u
+#define CENOTE_JOB_RUNNING 1u
+#define CENOTE_JOB_DONE 2u
+#define CENOTE_JOB_FAILED 3u
+
+/* Called on the server thread after each chunk: `rgba` (width·height·4
+ * linear averages over `samples`) is valid only during the call. */
+typedef void (*cenote_frame_fn)(void* user, uint64_t job, uint32_t samples, uint32_t target_spp, const float* rgba,
+                                uint32_t width, uint32_t height);
+
+typedef struct cenote_job_status {
+    uint32_t state;   /* CENOTE_JOB_* */
+    uint32_t samples; /* completed */
+    uint32_t target;
+    int32_t error;    /* status code when FAILED */
+    /* Milliseconds on the server's clock; -1 until reached. */
+    double submit_ms, admit_ms, first_frame_ms, done_ms;
+} cenote_job_status;
+
+typedef struct cenote_server_counters {
+    uint64_t submitted, completed, failed, queued, active;
+    uint64_t samples;      /* pixel samples finished */
+    uint64_t bytes_in_use; /* resident bytes counted against the budget (pools + jobs) */
+    uint64_t budget;
+    double wall_ms;        /* since creation */
+} cenote_server_counters;
+
+/* `hbm_budget` bounds the pools and every resident job's film; the slots'
+ * pools are allocated here (CENOTE_E_BUDGET if they alone exceed it). */
+int32_t cenote_server_create(cenote_context* ctx, uint64_t hbm_budget, const cenote_server_options* options,
+                             cenote_server** out);
+/* Stops the loop after the chunks in flight; queued jobs are dropped. */
+void cenote_server_destroy(cenote_server* server);
+/* Queue a job (CENOTE_E_BUDGET if it could never fit); `fn` may be NULL. */
+int32_t cenote_job_submit(cenote_server* server, cenote_scene* scene, uint32_t width, uint32_t height,
+                          uint32_t target_spp, uint32_t max_bounces, cenote_frame_fn fn, void* user, uint64_t* job);
+int32_t cenote_job_poll(cenote_server* server, uint64_t job, cenote_job_status* status);
+/* Block until the job is done or failed, at most `timeout_ms` (CENOTE_E_TIMEOUT). */
+int32_t cenote_job_wait(cenote_server* server, uint64_t job, double timeout_ms);
+/* The finished job's averages (width·height·4 floats). */
+int32_t cenote_job_result(cenote_server* server, uint64_t job, float* rgba);
+/* Forget a finished job and its result. */
+int32_t cenote_job_release(cenote_server* server, uint64_t job);
+int32_t cenote_server_stats(cenote_server* server, cenote_server_counters* stats);
+
 /* ---- environment tables without device allocation --------------------------------- */
 
 /* The environment's sampling tables (the same bits cenote_scene_create
