@@ -116,7 +116,9 @@ EXPORTED_SYMBOLS = [
     "cenote_probe_intersect", "cenote_probe_shadow", "cenote_probe_env_sample", "cenote_probe_env_pdf",
     "cenote_env_tables_static", "cenote_scene_create_textured", "cenote_texture_bytes", "cenote_texture_encode",
     "cenote_probe_texture", "cenote_server_create", "cenote_server_destroy", "cenote_job_submit", "cenote_job_poll",
-    "cenote_job_wait", "cenote_job_result", "cenote_job_release", "cenote_server_stats",
+    "cenote_job_wait", "cenote_job_result", "cenote_job_release", "cenote_server_stats", "cenote_guide_create",
+    "cenote_guide_destroy", "cenote_guide_params", "cenote_guide_set_params", "cenote_guide_forward",
+    "cenote_guide_train_step",
 ]
 
 _lib = None
@@ -150,6 +152,12 @@ def library() -> C.CDLL:
         "cenote_job_result": (I32, [P, C.c_uint64, P]),
         "cenote_job_release": (I32, [P, C.c_uint64]),
         "cenote_server_stats": (I32, [P, P]),
+        "cenote_guide_create": (I32, [P, C.c_uint64, P]),
+        "cenote_guide_destroy": (None, [P]),
+        "cenote_guide_params": (I32, [P, P]),
+        "cenote_guide_set_params": (I32, [P, P]),
+        "cenote_guide_forward": (I32, [P, P, U32, P]),
+        "cenote_guide_train_step": (I32, [P, P, P, P, U32, F, P, P]),
         "cenote_scene_destroy": (None, [P]),
         "cenote_scene_set_camera": (I32, [P, P]),
         "cenote_scene_prep_times": (I32, [P, P]),
@@ -625,6 +633,59 @@ class Server:
     def close(self) -> None:
         if getattr(self, "_h", None):
             library().cenote_server_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+# ---- the learned guide ---------------------------------------------------------------
+
+GUIDE_IN, GUIDE_OUT, GUIDE_PARAMS = 96, 40, 17128
+
+
+class Guide:
+    """The directional guide's MLP (cenote_guide_*): tensor-core forward and
+    training step over host arrays."""
+
+    def __init__(self, ctx: Context, seed: int = 1):
+        h = C.c_void_p()
+        _check(library().cenote_guide_create(ctx.handle, seed, C.byref(h)))
+        self._h = h
+        self.ctx = ctx
+
+    def params(self) -> np.ndarray:
+        out = np.zeros(GUIDE_PARAMS, np.float32)
+        _check(library().cenote_guide_params(self._h, _ptr(out)))
+        return out
+
+    def set_params(self, p: np.ndarray) -> None:
+        p = np.ascontiguousarray(p, np.float32)
+        assert p.size == GUIDE_PARAMS
+        _check(library().cenote_guide_set_params(self._h, _ptr(p)))
+
+    def forward(self, feats: np.ndarray) -> np.ndarray:
+        x = np.ascontiguousarray(feats, np.float32).reshape(-1, GUIDE_IN)
+        out = np.zeros((len(x), GUIDE_OUT), np.float32)
+        _check(library().cenote_guide_forward(self._h, _ptr(x), len(x), _ptr(out)))
+        return out
+
+    def train_step(self, feats, dirs, weights, lr: float = 0.0, grads: bool = False):
+        x = np.ascontiguousarray(feats, np.float32).reshape(-1, GUIDE_IN)
+        d = np.ascontiguousarray(dirs, np.float32).reshape(-1, 3)
+        w = np.ascontiguousarray(weights, np.float32).reshape(-1)
+        loss = np.zeros(1, np.float32)
+        g = np.zeros(GUIDE_PARAMS, np.float32) if grads else None
+        _check(library().cenote_guide_train_step(self._h, _ptr(x), _ptr(d), _ptr(w), len(x), lr, _ptr(loss),
+                                                 _ptr(g) if grads else None))
+        return (float(loss[0]), g) if grads else float(loss[0])
+
+    def close(self) -> None:
+        if getattr(self, "_h", None):
+            library().cenote_guide_destroy(self._h)
             self._h = None
 
     def __del__(self):

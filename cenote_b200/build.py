@@ -19,8 +19,8 @@ CSRC = PKG / "csrc"
 OUT = PKG / "_build"
 LIB = PKG / "libcenote_b200.so"
 
-CU_SOURCES = ["wavefront.cu", "probes.cu", "env_build.cu"]
-CPP_SOURCES = ["capi.cpp", "runtime.cpp", "server.cpp", "bvh_build.cpp", "texture_prep.cpp"]
+CU_SOURCES = ["wavefront.cu", "probes.cu", "env_build.cu", "guide.cu"]
+CPP_SOURCES = ["capi.cpp", "runtime.cpp", "server.cpp", "guide_api.cpp", "bvh_build.cpp", "texture_prep.cpp"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
 

@@ -364,6 +364,28 @@ int32_t cenote_job_result(cenote_server* server, uint64_t job, float* rgba);
 int32_t cenote_job_release(cenote_server* server, uint64_t job);
 int32_t cenote_server_stats(cenote_server* server, cenote_server_counters* stats);
 
+/* ---- the learned directional guide ----------------------------------------------- */
+
+/* A small MLP (96 encoded inputs: position in 12 frequency bands, normal,
+ * outgoing direction; 3 hidden layers of 64 ReLU; 40 outputs = 8 von
+ * Mises-Fisher lobes of raw direction, concentration and weight logit) run
+ * and trained by tcgen05 tensor-core kernels in BF16 with FP32 accumulation.
+ * No counterpart in the reference. Parameters are 17,128 floats: W1 [64][96],
+ * b1, W2 [64][64], b2, W3 [64][64], b3, W4 [40][64], b4. */
+typedef struct cenote_guide cenote_guide;
+
+int32_t cenote_guide_create(cenote_context* ctx, uint64_t seed, cenote_guide** out);
+void cenote_guide_destroy(cenote_guide* guide);
+int32_t cenote_guide_params(cenote_guide* guide, float* params);
+int32_t cenote_guide_set_params(cenote_guide* guide, const float* params);
+/* outputs (n x 40) for features (n x 96, rounded to BF16 on the device). */
+int32_t cenote_guide_forward(cenote_guide* guide, const float* features, uint32_t n, float* outputs);
+/* One step on the loss mean_s -weights_s log q(dirs_s): the loss and, when
+ * `grads` is non-NULL, the gradient before the update; lr > 0 applies Adam
+ * (beta 0.9 / 0.999, eps 1e-8), lr = 0 only evaluates. */
+int32_t cenote_guide_train_step(cenote_guide* guide, const float* features, const float* dirs, const float* weights,
+                                uint32_t n, float lr, float* loss, float* grads);
+
 /* ---- environment tables without device allocation --------------------------------- */
 
 /* The environment's sampling tables (the same bits cenote_scene_create
