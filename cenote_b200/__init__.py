@@ -118,7 +118,7 @@ EXPORTED_SYMBOLS = [
     "cenote_probe_texture", "cenote_server_create", "cenote_server_destroy", "cenote_job_submit", "cenote_job_poll",
     "cenote_job_wait", "cenote_job_result", "cenote_job_release", "cenote_server_stats", "cenote_guide_create",
     "cenote_guide_destroy", "cenote_guide_params", "cenote_guide_set_params", "cenote_guide_forward",
-    "cenote_guide_train_step",
+    "cenote_guide_train_step", "cenote_renderer_set_guide",
 ]
 
 _lib = None
@@ -158,6 +158,7 @@ def library() -> C.CDLL:
         "cenote_guide_set_params": (I32, [P, P]),
         "cenote_guide_forward": (I32, [P, P, U32, P]),
         "cenote_guide_train_step": (I32, [P, P, P, P, U32, F, P, P]),
+        "cenote_renderer_set_guide": (I32, [P, P, F, U32, F]),
         "cenote_scene_destroy": (None, [P]),
         "cenote_scene_set_camera": (I32, [P, P]),
         "cenote_scene_prep_times": (I32, [P, P]),
@@ -534,6 +535,11 @@ class Renderer:
 
     def accumulate(self, scene: Scene, film: Film, count: int = 1) -> None:
         _check(library().cenote_accumulate_n(self._h, scene.handle, film.handle, count))
+
+    def set_guide(self, guide, fraction: float = 0.5, train_steps: int = 0, lr: float = 1e-2) -> None:
+        """Guided sampling with a Guide (None detaches); train_steps Adam steps per wave."""
+        self._guide = guide  # keep it alive while attached
+        _check(library().cenote_renderer_set_guide(self._h, guide._h if guide else None, fraction, train_steps, lr))
 
     def set_profiling(self, flags: int) -> None:
         _check(library().cenote_renderer_set_profiling(self._h, flags))

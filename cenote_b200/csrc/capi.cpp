@@ -456,6 +456,14 @@ int32_t cenote_scene_create_textured(cenote_context* ctx, const cenote_object* o
     }
     double light_power = 0.0;
     sc->lights = build_lights(tri_lights, deltas, delta_count, &light_power);
+    // World bounds of every triangle, for the learned guide's position encoding.
+    float bmin[3] = {1e30f, 1e30f, 1e30f}, bmax[3] = {-1e30f, -1e30f, -1e30f};
+    for (const BuildTri& t : tris)
+        for (int k = 0; k < 3; ++k)
+            for (int a = 0; a < 3; ++a) {
+                bmin[a] = std::min(bmin[a], t.v[k][a]);
+                bmax[a] = std::max(bmax[a], t.v[k][a]);
+            }
 
     auto t_bvh = std::chrono::steady_clock::now();
     WideBvh bvh = build_wide_bvh(tris, std::max(1u, std::thread::hardware_concurrency()));
@@ -588,6 +596,9 @@ int32_t cenote_scene_create_textured(cenote_context* ctx, const cenote_object* o
     ds.node_count = uint32_t(bvh.nodes.size());
     ds.tri_count = uint32_t(bvh.tris.size() / 12);
     ds.has_nonopaque = nonopaque ? 1u : 0u;
+    const float extent = std::max({bmax[0] - bmin[0], bmax[1] - bmin[1], bmax[2] - bmin[2], 1e-6f});
+    for (int a = 0; a < 3; ++a) ds.bbox_min[a] = tris.empty() ? 0.0f : bmin[a];
+    ds.bbox_inv = tris.empty() ? 1.0f : 1.0f / extent;
     ds.light_leaf = bleaf->as<uint32_t>();
     sc->prep_ms[2] = float(std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t_start).count());
     retain(ctx);
@@ -684,6 +695,19 @@ int32_t cenote_renderer_set_samples_per_wave(cenote_renderer* r, uint32_t spw) {
     return CENOTE_OK;
 }
 
+int32_t cenote_renderer_set_guide(cenote_renderer* r, cenote_guide* g, float fraction, uint32_t train_steps,
+                                  float lr) {
+    CN_CHECK(r, CENOTE_E_INVALID_ARGUMENT, "null renderer");
+    CN_CHECK(!g || g->ctx == r->ctx, CENOTE_E_INVALID_ARGUMENT, "guide from another context");
+    CN_CHECK(!g || (fraction >= 0.0f && fraction < 1.0f), CENOTE_E_INVALID_ARGUMENT, "fraction outside [0, 1)");
+    CN_CHECK(!g || (lr >= 0.0f && lr < 1.0f), CENOTE_E_INVALID_ARGUMENT, "learning rate outside [0, 1)");
+    r->guide = g;
+    r->guide_fraction = fraction;
+    r->guide_steps = train_steps;
+    r->guide_lr = lr;
+    return CENOTE_OK;
+}
+
 int32_t cenote_renderer_set_profiling(cenote_renderer* r, uint32_t flags) {
     CN_CHECK(r, CENOTE_E_INVALID_ARGUMENT, "null renderer");
     CN_CHECK((flags & ~3u) == 0, CENOTE_E_INVALID_ARGUMENT, "unknown profiling flag");
@@ -763,6 +787,8 @@ int32_t run_waves(cenote_renderer* r, cenote_scene* sc, uint32_t width, uint32_t
     CN_CUDA(r->ensure(plan.need));
     // Films trace the guides (Renderer::accumulate); one-shot renders do not.
     CN_CUDA(r->set_guides(film != nullptr));
+    CN_CUDA(r->set_learned_guide(r->guide != nullptr));
+    if (r->guide) CN_CUDA(r->guide->ensure(cenote_renderer::GUIDE_BATCH));
 
     const bool timing = (r->profiling & CENOTE_PROFILE_TIMING) != 0;
     const bool counting = (r->profiling & CENOTE_PROFILE_COUNTS) != 0;

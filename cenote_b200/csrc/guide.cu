@@ -25,7 +25,9 @@
 #include <cuda_runtime.h>
 
 #include "guide.h"
+#include "records.h"
 #include "umma.cuh"
+#include "wavefront.h"
 
 namespace cn {
 namespace guide {
@@ -458,6 +460,186 @@ __global__ void k_cast(const float* __restrict__ p, __nv_bfloat16* __restrict__ 
     if (i < OUT_PAD) b4[i] = i < OUT ? p[P_B4 + i] : 0.0f;
 }
 
+// ---- in the wavefront ------------------------------------------------------------------------
+
+__device__ __forceinline__ float3 ld3(const float* p, uint32_t v) {
+    return make_float3(__ldg(p + 3 * v), __ldg(p + 3 * v + 1), __ldg(p + 3 * v + 2));
+}
+
+// A hit's world position and geometric normal turned against the ray: the
+// guide's inputs (the shading kernel records the same quantities).
+__device__ void hit_frame(const DeviceScene& s, uint4 h, float3 dir, float3& pos, float3& nrm) {
+    const GeomRecord& g = s.geometry[h.x];
+    const uint32_t prim = h.y;
+    const float b1 = __uint_as_float(h.z), b2 = __uint_as_float(h.w);
+    uint32_t i0 = __ldg(g.indices + 3 * prim), i1 = __ldg(g.indices + 3 * prim + 1), i2 = __ldg(g.indices + 3 * prim + 2);
+    float3 v0 = ld3(g.positions, i0), v1 = ld3(g.positions, i1), v2 = ld3(g.positions, i2);
+    float3 e1 = make_float3(v1.x - v0.x, v1.y - v0.y, v1.z - v0.z), e2 = make_float3(v2.x - v0.x, v2.y - v0.y, v2.z - v0.z);
+    float3 op = make_float3(v0.x + b1 * e1.x + b2 * e2.x, v0.y + b1 * e1.y + b2 * e2.y, v0.z + b1 * e1.z + b2 * e2.z);
+    float3 on = make_float3(e1.y * e2.z - e1.z * e2.y, e1.z * e2.x - e1.x * e2.z, e1.x * e2.y - e1.y * e2.x);
+    pos = make_float3(g.o2w[0][0] * op.x + g.o2w[0][1] * op.y + g.o2w[0][2] * op.z + g.o2w[0][3],
+                      g.o2w[1][0] * op.x + g.o2w[1][1] * op.y + g.o2w[1][2] * op.z + g.o2w[1][3],
+                      g.o2w[2][0] * op.x + g.o2w[2][1] * op.y + g.o2w[2][2] * op.z + g.o2w[2][3]);
+    float3 wn = make_float3(g.w2o[0][0] * on.x + g.w2o[1][0] * on.y + g.w2o[2][0] * on.z,
+                            g.w2o[0][1] * on.x + g.w2o[1][1] * on.y + g.w2o[2][1] * on.z,
+                            g.w2o[0][2] * on.x + g.w2o[1][2] * on.y + g.w2o[2][2] * on.z);
+    float inv = rsqrtf(wn.x * wn.x + wn.y * wn.y + wn.z * wn.z);
+    wn = make_float3(wn.x * inv, wn.y * inv, wn.z * inv);
+    if (wn.x * dir.x + wn.y * dir.y + wn.z * dir.z > 0.0f) wn = make_float3(-wn.x, -wn.y, -wn.z);
+    nrm = wn;
+}
+
+__device__ __forceinline__ float3 unit_pos(const DeviceScene& s, float3 p) {
+    return make_float3((p.x - s.bbox_min[0]) * s.bbox_inv, (p.y - s.bbox_min[1]) * s.bbox_inv,
+                       (p.z - s.bbox_min[2]) * s.bbox_inv);
+}
+
+__global__ void __launch_bounds__(TILE, 1) k_infer_paths(Net net, DeviceScene scene, PathPool pool, uint32_t bounce,
+                                                         uint32_t n0, int* err) {
+    extern __shared__ __align__(1024) uint8_t smem[];
+    uint32_t* slot = reinterpret_cast<uint32_t*>(smem + FwdSmem::SLOT);
+    int* sflag = reinterpret_cast<int*>(smem + FwdSmem::FLAG);
+    const uint32_t count = min(bounce == 0 ? n0 : pool.counters[CTR_RAYS + bounce], pool.capacity);
+    const uint32_t* queue = pool.queue[bounce & 1u];
+    if (threadIdx.x == 0) {
+        umma::mbar_init(reinterpret_cast<uint64_t*>(smem + FwdSmem::BAR), 1);
+        *sflag = 0;
+    }
+    if (threadIdx.x < 32) umma::tmem_alloc(slot, 64);
+    load_net(smem, net);
+    umma::fence_before_sync();
+    __syncthreads();
+    umma::fence_after_sync();
+    const uint32_t tmem = *slot;
+    uint32_t phase = 0;
+    float feat[IN], o[OUT];
+    for (uint32_t tile = blockIdx.x; tile * TILE < count; tile += gridDim.x) {
+        const uint32_t i = tile * TILE + threadIdx.x;
+        uint32_t path = 0;
+        bool hit = false;
+        if (i < count) {
+            path = bounce == 0 ? i : queue[i];
+            uint4 h = pool.hit[path];
+            hit = h.x != LIGHT_NONE;
+            if (hit) {
+                float4 d4 = pool.dir[path];
+                float3 dir = make_float3(d4.x, d4.y, d4.z);
+                float3 p, n;
+                hit_frame(scene, h, dir, p, n);
+                encode(unit_pos(scene, p), n, make_float3(-dir.x, -dir.y, -dir.z), feat);
+            }
+        }
+        if (!hit)
+            for (uint32_t c = 0; c < IN; ++c) feat[c] = 0.0f;
+        if (!forward_tile(smem, tmem, phase, feat, o, nullptr)) {
+            if (threadIdx.x == 0) atomicExch(err, 1);
+            break;
+        }
+        if (hit) {
+            float* dst = pool.guide_out + size_t(path) * OUT;
+            for (uint32_t c = 0; c < OUT; c += 4) *reinterpret_cast<float4*>(dst + c) = make_float4(o[c], o[c + 1], o[c + 2], o[c + 3]);
+        }
+    }
+    umma::fence_before_sync();
+    __syncthreads();
+    if (threadIdx.x < 32) {
+        umma::tmem_dealloc(tmem, 64);
+        umma::tmem_relinquish();
+    }
+}
+
+__device__ __forceinline__ float lum(float3 c) { return 0.2722287f * c.x + 0.6740818f * c.y + 0.0536895f * c.z; }
+
+__global__ void k_resolve_records(Record* recs, const uint32_t* count, uint32_t capacity, const float4* rad) {
+    const uint32_t n = min(*count, capacity);
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        Record r = recs[i];
+        float c = 0.0f;
+        if (r.q2.w >= 0.0f && r.q0.w > 0.0f) {
+            float4 f = rad[__float_as_uint(r.q3.w)];
+            float L = (lum(make_float3(f.x, f.y, f.z)) - r.q2.w) / fmaxf(r.q1.w, 1e-12f);
+            c = fmaxf(L, 0.0f) / r.q0.w;
+            if (!isfinite(c)) c = 0.0f;
+        }
+        recs[i].q0.w = c;
+    }
+}
+
+// Training forward over records: inputs encoded from each record.
+__global__ void __launch_bounds__(TILE, 1) k_forward_records(Net net, const Record* __restrict__ recs,
+                                                             const uint32_t* count, uint32_t capacity, uint32_t offset,
+                                                             uint32_t rows, float3 bmin, float binv,
+                                                             float* __restrict__ out, __nv_bfloat16* __restrict__ save,
+                                                             float* sums, int* err) {
+    extern __shared__ __align__(1024) uint8_t smem[];
+    uint32_t* slot = reinterpret_cast<uint32_t*>(smem + FwdSmem::SLOT);
+    int* sflag = reinterpret_cast<int*>(smem + FwdSmem::FLAG);
+    const uint32_t n = min(*count, capacity);
+    if (threadIdx.x == 0) {
+        umma::mbar_init(reinterpret_cast<uint64_t*>(smem + FwdSmem::BAR), 1);
+        *sflag = 0;
+    }
+    if (threadIdx.x < 32) umma::tmem_alloc(slot, 64);
+    load_net(smem, net);
+    umma::fence_before_sync();
+    __syncthreads();
+    umma::fence_after_sync();
+    const uint32_t tmem = *slot;
+    uint32_t phase = 0;
+    float feat[IN], o[OUT];
+    float wsum = 0.0f;
+    for (uint32_t tile = blockIdx.x; n > 0 && tile * TILE < rows; tile += gridDim.x) {
+        const uint32_t r = tile * TILE + threadIdx.x;
+        if (r < rows) {
+            const Record rc = recs[(offset + r) % n];
+            float3 p = make_float3((rc.q0.x - bmin.x) * binv, (rc.q0.y - bmin.y) * binv, (rc.q0.z - bmin.z) * binv);
+            encode(p, make_float3(rc.q1.x, rc.q1.y, rc.q1.z), make_float3(rc.q2.x, rc.q2.y, rc.q2.z), feat);
+            wsum += rc.q0.w;
+        } else {
+            for (uint32_t c = 0; c < IN; ++c) feat[c] = 0.0f;
+        }
+        if (!forward_tile(smem, tmem, phase, feat, o, r < rows ? save + size_t(r) * ACT : nullptr)) {
+            if (threadIdx.x == 0) atomicExch(err, 1);
+            break;
+        }
+        if (r < rows)
+            for (uint32_t c = 0; c < OUT; ++c) out[size_t(r) * OUT + c] = o[c];
+    }
+    for (int k = 16; k > 0; k >>= 1) wsum += __shfl_xor_sync(0xffffffffu, wsum, k);
+    if ((threadIdx.x & 31) == 0) atomicAdd(sums, wsum);
+    umma::fence_before_sync();
+    __syncthreads();
+    if (threadIdx.x < 32) {
+        umma::tmem_dealloc(tmem, 64);
+        umma::tmem_relinquish();
+    }
+}
+
+// Loss over records: weights normalised by the batch mean and clamped at 20
+// (one bright sample must not dominate a step), then averaged.
+__global__ void k_loss_records(const float* __restrict__ out, const Record* __restrict__ recs, const uint32_t* count,
+                               uint32_t capacity, uint32_t offset, uint32_t rows, const float* sums,
+                               __nv_bfloat16* __restrict__ dz4, float* loss) {
+    const uint32_t n = min(*count, capacity);
+    const float mean = sums[0] / float(rows);
+    float acc = 0.0f;
+    for (uint32_t r = blockIdx.x * blockDim.x + threadIdx.x; r < rows; r += gridDim.x * blockDim.x) {
+        float c = 0.0f;
+        float3 w = make_float3(0.0f, 0.0f, 1.0f);
+        if (n > 0 && mean > 0.0f) {
+            const Record rc = recs[(offset + r) % n];
+            c = fminf(rc.q0.w / mean, 20.0f) / float(rows);
+            w = make_float3(rc.q3.x, rc.q3.y, rc.q3.z);
+        }
+        MixtureGrad g = mixture_grad(out + size_t(r) * OUT, w, c);
+        acc += -c * g.log_q;
+        for (uint32_t k = 0; k < OUT_PAD; ++k)
+            dz4[size_t(r) * OUT_PAD + k] = __float2bfloat16_rn(k < OUT ? g.d[k] : 0.0f);
+    }
+    for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
+    if ((threadIdx.x & 31) == 0) atomicAdd(loss, acc);
+}
+
 }  // namespace
 
 // ---- host launchers ----------------------------------------------------------------------
@@ -477,6 +659,10 @@ static Net view(const Buffers& b) {
 
 cudaError_t configure(int device, int* sms) {
     cudaError_t e = cudaFuncSetAttribute(k_forward, cudaFuncAttributeMaxDynamicSharedMemorySize, FwdSmem::BYTES);
+    if (e == cudaSuccess)
+        e = cudaFuncSetAttribute(k_infer_paths, cudaFuncAttributeMaxDynamicSharedMemorySize, FwdSmem::BYTES);
+    if (e == cudaSuccess)
+        e = cudaFuncSetAttribute(k_forward_records, cudaFuncAttributeMaxDynamicSharedMemorySize, FwdSmem::BYTES);
     if (e == cudaSuccess)
         e = cudaFuncSetAttribute(k_backward, cudaFuncAttributeMaxDynamicSharedMemorySize, BwdSmem::BYTES);
     if (e == cudaSuccess) e = cudaDeviceGetAttribute(sms, cudaDevAttrMultiProcessorCount, device);
@@ -516,6 +702,32 @@ void launch_adam(const Buffers& b, float lr, uint32_t step, cudaStream_t s) {
     const float c1 = 1.0f / (1.0f - powf(b1, float(step)));
     const float c2 = 1.0f / (1.0f - powf(b2, float(step)));
     k_adam<<<(PARAMS + 255) / 256, 256, 0, s>>>(b.params, b.grad, b.m, b.v, PARAMS, lr, b1, b2, eps, c1, c2);
+}
+
+void launch_infer_paths(const Buffers& b, const DeviceScene& scene, const PathPool& pool, uint32_t bounce,
+                        uint32_t n0, int sms, cudaStream_t s) {
+    // Twice the SM count: a second CTA per SM hides the first's tensor-core waits.
+    k_infer_paths<<<2 * sms, TILE, FwdSmem::BYTES, s>>>(view(b), scene, pool, bounce, n0, b.err);
+}
+
+void launch_resolve_records(Record* recs, const uint32_t* count, uint32_t capacity, const float4* rad, cudaStream_t s) {
+    k_resolve_records<<<148 * 4, 256, 0, s>>>(recs, count, capacity, rad);
+}
+
+void launch_train_records(const Buffers& b, const TrainScratch& t, const Record* recs, const uint32_t* count,
+                          uint32_t capacity, uint32_t offset, float3 bbox_min, float bbox_inv, float lr,
+                          uint32_t step, int sms, cudaStream_t s) {
+    cudaMemsetAsync(t.sums, 0, 8, s);
+    uint32_t tiles = (t.rows + TILE - 1) / TILE;
+    int grid = int(tiles < uint32_t(sms) ? tiles : uint32_t(sms));
+    k_forward_records<<<grid, TILE, FwdSmem::BYTES, s>>>(view(b), recs, count, capacity, offset, t.rows, bbox_min,
+                                                         bbox_inv, t.out, t.save, t.sums, b.err);
+    int lgrid = int((t.rows + 255) / 256);
+    if (lgrid > 148 * 8) lgrid = 148 * 8;
+    k_loss_records<<<lgrid, 256, 0, s>>>(t.out, recs, count, capacity, offset, t.rows, t.sums, t.dz4, t.sums + 1);
+    launch_backward(b, t.save, t.dz4, t.rows, sms, s);
+    launch_adam(b, lr, step, s);
+    launch_cast(b, s);
 }
 
 }  // namespace guide

@@ -2,6 +2,7 @@
 // head (shared by the training kernels and guided sampling in the shading
 // kernel) and the launchers of guide.cu.
 #pragma once
+#include <cmath>
 #include <cstdint>
 #include <cuda_bf16.h>
 #include <cuda_runtime.h>
@@ -64,6 +65,107 @@ struct MixtureGrad {
     float log_q;
 };
 
+// ---- inputs ------------------------------------------------------------------------------
+
+// The encoded inputs of one vertex: position p (in [0,1]^3 of the scene's
+// bounds) in FREQS sine/cosine bands per axis, then n, wo and p; zero padded.
+__host__ __device__ inline void encode(float3 p, float3 n, float3 wo, float* f) {
+    const float c[3] = {p.x, p.y, p.z};
+    uint32_t k = 0;
+    for (uint32_t b = 0; b < FREQS; ++b) {
+        const float s = 3.14159265f * float(1u << b);
+        for (int a = 0; a < 3; ++a) {
+            float sv, cv;
+#ifdef __CUDA_ARCH__
+            __sincosf(s * c[a], &sv, &cv);
+#else
+            sv = sinf(s * c[a]);
+            cv = cosf(s * c[a]);
+#endif
+            f[k++] = sv;
+            f[k++] = cv;
+        }
+    }
+    f[k++] = n.x;
+    f[k++] = n.y;
+    f[k++] = n.z;
+    f[k++] = wo.x;
+    f[k++] = wo.y;
+    f[k++] = wo.z;
+    f[k++] = p.x;
+    f[k++] = p.y;
+    f[k++] = p.z;
+    while (k < IN) f[k++] = 0.0f;
+}
+
+// One training record: a guided-mode surface vertex, 64 bytes.
+//   q0 = (position, pdf of the sampled direction; the target weight once resolved)
+//   q1 = (shading normal, luminance of the throughput after the scatter)
+//   q2 = (outgoing direction, luminance of the path's radiance before the next vertex; < 0 until known)
+//   q3 = (sampled direction, path index as bits)
+struct Record {
+    float4 q0, q1, q2, q3;
+};
+
+// ---- the mixture at a vertex, from its raw outputs -------------------------------------------
+#ifdef __CUDACC__
+
+// Lobe weights by softmax of the logits (o[5i + 4]).
+__device__ inline void lobe_weights(const float* o, float* w) {
+    float m = -1e30f;
+    for (int i = 0; i < LOBES; ++i) m = fmaxf(m, o[5 * i + 4]);
+    float s = 0.0f;
+    for (int i = 0; i < LOBES; ++i) {
+        w[i] = __expf(o[5 * i + 4] - m);
+        s += w[i];
+    }
+    for (int i = 0; i < LOBES; ++i) w[i] /= s;
+}
+
+__device__ inline float mixture_pdf(const float* o, float3 d) {
+    float w[LOBES];
+    lobe_weights(o, w);
+    float q = 0.0f;
+    for (int i = 0; i < LOBES; ++i) {
+        Lobe L = lobe(o + 5 * i);
+        q += w[i] * vmf_pdf(L.kappa, L.mu.x * d.x + L.mu.y * d.y + L.mu.z * d.z);
+    }
+    return q;
+}
+
+// A direction from the mixture: lobe by u_lobe, then the vMF around its mean
+// (inverse-cdf cos theta = 1 + log(u + (1 - u) e^{-2 kappa}) / kappa).
+__device__ inline float3 mixture_sample(const float* o, float u_lobe, float u1, float u2) {
+    float w[LOBES];
+    lobe_weights(o, w);
+    int pick = LOBES - 1;
+    float acc = 0.0f;
+    for (int i = 0; i < LOBES; ++i) {
+        acc += w[i];
+        if (u_lobe < acc) {
+            pick = i;
+            break;
+        }
+    }
+    Lobe L = lobe(o + 5 * pick);
+    float ct = 1.0f + logf(u1 + (1.0f - u1) * __expf(-2.0f * L.kappa)) / L.kappa;
+    ct = fminf(fmaxf(ct, -1.0f), 1.0f);
+    float st = sqrtf(fmaxf(0.0f, 1.0f - ct * ct));
+    float sp, cp;
+    __sincosf(6.283185307f * u2, &sp, &cp);
+    // Frame around mu (Duff et al. 2017).
+    float3 n = L.mu;
+    float sg = n.z >= 0.0f ? 1.0f : -1.0f;
+    float a = -1.0f / (sg + n.z);
+    float b = n.x * n.y * a;
+    float3 t = make_float3(1.0f + sg * n.x * n.x * a, sg * b, -sg * n.x);
+    float3 bt = make_float3(b, sg + n.y * n.y * a, -n.y);
+    return make_float3(st * cp * t.x + st * sp * bt.x + ct * n.x, st * cp * t.y + st * sp * bt.y + ct * n.y,
+                       st * cp * t.z + st * sp * bt.z + ct * n.z);
+}
+
+#endif  // __CUDACC__
+
 // ---- launchers (guide.cu) -----------------------------------------------------------------
 
 cudaError_t configure(int device, int* sms);
@@ -79,6 +181,33 @@ void launch_backward(const Buffers& b, const __nv_bfloat16* save, const __nv_bfl
                      cudaStream_t s);
 // One Adam step (beta 0.9 / 0.999), zeroing the gradient.
 void launch_adam(const Buffers& b, float lr, uint32_t step, cudaStream_t s);
+
+}  // namespace guide
+
+struct DeviceScene;
+struct PathPool;
+
+namespace guide {
+
+// The 40 mixture outputs of every hit path of `bounce` into pool.guide_out.
+void launch_infer_paths(const Buffers& b, const DeviceScene& scene, const PathPool& pool, uint32_t bounce,
+                        uint32_t n0, int sms, cudaStream_t s);
+// Turn the wave's records into target weights L / pdf (L from the paths'
+// final radiance and the snapshot the next vertex took).
+void launch_resolve_records(Record* recs, const uint32_t* count, uint32_t capacity, const float4* rad, cudaStream_t s);
+
+// Scratch of the training steps (device).
+struct TrainScratch {
+    float* out;            // [rows][OUT]
+    __nv_bfloat16* save;   // [rows][ACT]
+    __nv_bfloat16* dz4;    // [rows][OUT_PAD]
+    float* sums;           // [2]: batch weight sum, loss
+    uint32_t rows;
+};
+// One step on `rows` records starting at `offset` (wrapping over the count).
+void launch_train_records(const Buffers& b, const TrainScratch& t, const Record* recs, const uint32_t* count,
+                          uint32_t capacity, uint32_t offset, float3 bbox_min, float bbox_inv, float lr,
+                          uint32_t step, int sms, cudaStream_t s);
 
 }  // namespace guide
 }  // namespace cn

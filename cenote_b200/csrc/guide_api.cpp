@@ -10,31 +10,6 @@
 
 using namespace cn;
 
-struct cenote_guide {
-    cenote_context* ctx = nullptr;
-    DeviceBuffer params, grad, m, v, w1, w2, w3, w4, b4, err, loss;
-    DeviceBuffer feats, out, save, dz4, dirs, weights;
-    size_t cap = 0;
-    uint32_t step = 0;
-    int sms = 148;
-
-    guide::Buffers view() {
-        return {params.as<float>(), grad.as<float>(), m.as<float>(), v.as<float>(), w1.as<__nv_bfloat16>(),
-                w2.as<__nv_bfloat16>(), w3.as<__nv_bfloat16>(), w4.as<__nv_bfloat16>(), b4.as<float>(),
-                err.as<int>()};
-    }
-    cudaError_t ensure(size_t n) {
-        if (n <= cap) return cudaSuccess;
-        cudaError_t e;
-        if ((e = feats.alloc(n * guide::IN * 4)) || (e = out.alloc(n * guide::OUT * 4)) ||
-            (e = save.alloc(n * guide::ACT * 2)) || (e = dz4.alloc(n * guide::OUT_PAD * 2)) ||
-            (e = dirs.alloc(n * 12)) || (e = weights.alloc(n * 4)))
-            return e;
-        cap = n;
-        return cudaSuccess;
-    }
-};
-
 namespace {
 
 // Initial weights: uniform in +-sqrt(6 / fan_in) (He et al. 2015, for ReLU

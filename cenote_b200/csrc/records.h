@@ -100,6 +100,8 @@ struct DeviceScene {
     const unsigned long long* textures;  // cudaTextureObject_t per bindless slot
     uint32_t texture_count;
     uint32_t pad2;
+    float bbox_min[3];    // world bounds of every triangle, for the guide's position encoding
+    float bbox_inv;       // 1 / the bounds' largest extent
 };
 
 // One queued shadow ray: 64 bytes, four 16-byte lanes.

@@ -82,6 +82,17 @@ cudaError_t enqueue_waves(cenote_renderer* r, const cenote_scene* sc, uint32_t w
     auto mark = [&]() {
         if (timing) cudaEventRecord(r->event(wc->events++), stream);
     };
+    // The learned guide: mixture outputs after each intersect, training records
+    // from the shading kernel, then Adam steps on the wave's records.
+    const bool guided = r->guide && r->pool.guide_out;
+    if (guided) {
+        const double per_wave = double(std::min<uint64_t>(plan.range, pixels)) * plan.spw * 3.0;
+        GuideRecordSink sk{r->g_records.ptr, r->g_count.as<uint32_t>(), cenote_renderer::GUIDE_RECORDS,
+                           float(std::min(1.0, cenote_renderer::GUIDE_RECORDS / std::max(1.0, per_wave))),
+                           r->guide_fraction, 0};
+        cudaError_t e = cudaMemcpyAsync(r->g_sink.ptr, &sk, sizeof sk, cudaMemcpyHostToDevice, stream);
+        if (e != cudaSuccess) return e;
+    }
     for (uint32_t done = 0; done < count;) {
         uint32_t s = std::min(plan.spw, count - done);
         for (uint64_t base = 0; base < pixels; base += plan.range) {
@@ -91,11 +102,13 @@ cudaError_t enqueue_waves(cenote_renderer* r, const cenote_scene* sc, uint32_t w
             wp.sample_base = sample0 + done;
             const uint32_t n0 = wp.pixel_count * s;
             mark();
+            if (guided) cudaMemsetAsync(r->g_count.ptr, 0, 4, stream);
             launch_wave_begin(r->pool, wp, ctx->shape, stream);
             mark();
             for (uint32_t b = 0; b < max_bounces; ++b) {
                 launch_intersect(sc->ds, r->pool, b, n0, ctx->shape, counting, stream);
                 mark();
+                if (guided) guide::launch_infer_paths(r->guide->view(), sc->ds, r->pool, b, n0, r->guide->sms, stream);
                 launch_shade(sc->ds, r->pool, b, wp, n0, ctx->shape, stream);
                 mark();
                 launch_shadow(sc->ds, r->pool, b, ctx->shape, counting, stream);
@@ -108,6 +121,19 @@ cudaError_t enqueue_waves(cenote_renderer* r, const cenote_scene* sc, uint32_t w
             else
                 launch_copy_rad(r->pool, oneshot, wp.pixel_base, wp.pixel_count, stream);
             mark();
+            if (guided) {
+                guide::Record* recs = r->g_records.as<guide::Record>();
+                const uint32_t* cnt = r->g_count.as<uint32_t>();
+                guide::launch_resolve_records(recs, cnt, cenote_renderer::GUIDE_RECORDS, r->pool.rad, stream);
+                const float3 bmin = make_float3(sc->ds.bbox_min[0], sc->ds.bbox_min[1], sc->ds.bbox_min[2]);
+                for (uint32_t k = 0; k < r->guide_steps; ++k) {
+                    r->guide->step++;
+                    guide::launch_train_records(r->guide->view(), r->guide->scratch(cenote_renderer::GUIDE_BATCH), recs,
+                                                cnt, cenote_renderer::GUIDE_RECORDS, k * cenote_renderer::GUIDE_BATCH,
+                                                bmin, sc->ds.bbox_inv, r->guide_lr, r->guide->step, r->guide->sms,
+                                                stream);
+                }
+            }
             wc->launches += 3 + 3 * max_bounces;
             wc->waves++;
         }

@@ -13,6 +13,7 @@
 #include <cuda_runtime.h>
 
 #include "../../include/cenote_c.h"
+#include "guide.h"
 #include "records.h"
 #include "wavefront.h"
 
@@ -73,6 +74,8 @@ using cn::ShadowRay;
 using cn::LaunchShape;
 using cn::PathPool;
 using cn::FilmTargets;
+using cn::GuideRecordSink;
+namespace guide = cn::guide;
 
 struct cenote_context {
     // Handles made from this context hold a reference; the context is freed
@@ -133,6 +136,15 @@ struct cenote_renderer {
     DeviceBuffer org, dir, thr, hit, ps, state, rad, q0, q1, shadows, counters, tally, scratch;
     DeviceBuffer aov_albedo, aov_normal, aov_depth, aov_guide;
     size_t pool_cap = 0, aov_cap = 0;
+    // The learned guide (cenote_renderer_set_guide): per-path mixture outputs
+    // and open records, the wave's training records and its sink.
+    cenote_guide* guide = nullptr;
+    float guide_fraction = 0.5f, guide_lr = 1e-2f;
+    uint32_t guide_steps = 0;
+    DeviceBuffer g_out, g_rec, g_records, g_count, g_sink;
+    size_t g_cap = 0;
+    static constexpr uint32_t GUIDE_RECORDS = 1u << 20;
+    static constexpr uint32_t GUIDE_BATCH = 65536;
     cenote_stats stats{};
     unsigned long long tally_prev[5] = {0, 0, 0, 0, 0};
 
@@ -171,6 +183,25 @@ struct cenote_renderer {
         return cudaSuccess;
     }
 
+    // The learned guide's lanes, sized with the pool; detached without a guide.
+    cudaError_t set_learned_guide(bool on) {
+        if (on && g_cap < pool_cap) {
+            cudaError_t e;
+            if ((e = g_out.alloc(pool_cap * guide::OUT * 4)) || (e = g_rec.alloc(pool_cap * 4))) return e;
+            g_cap = pool_cap;
+        }
+        if (on && !g_records.ptr) {
+            cudaError_t e;
+            if ((e = g_records.alloc(size_t(GUIDE_RECORDS) * sizeof(guide::Record))) || (e = g_count.alloc(16)) ||
+                (e = g_sink.alloc(sizeof(GuideRecordSink))))
+                return e;
+        }
+        pool.guide_out = on ? g_out.as<float>() : nullptr;
+        pool.guide_rec = on ? g_rec.as<uint32_t>() : nullptr;
+        pool.sink = on ? g_sink.as<GuideRecordSink>() : nullptr;
+        return cudaSuccess;
+    }
+
     // The guide lanes: allocated on the first wave that traces guides,
     // detached (null) for waves that do not.
     cudaError_t set_guides(bool on) {
@@ -185,6 +216,34 @@ struct cenote_renderer {
         pool.aov_normal = on ? aov_normal.as<float4>() : nullptr;
         pool.aov_depth = on ? aov_depth.as<float>() : nullptr;
         pool.aov_guide = on ? aov_guide.as<float4>() : nullptr;
+        return cudaSuccess;
+    }
+};
+
+struct cenote_guide {
+    cenote_context* ctx = nullptr;
+    DeviceBuffer params, grad, m, v, w1, w2, w3, w4, b4, err, loss;
+    DeviceBuffer feats, out, save, dz4, dirs, weights;
+    size_t cap = 0;
+    uint32_t step = 0;
+    int sms = 148;
+
+    guide::Buffers view() {
+        return {params.as<float>(), grad.as<float>(), m.as<float>(), v.as<float>(), w1.as<__nv_bfloat16>(),
+                w2.as<__nv_bfloat16>(), w3.as<__nv_bfloat16>(), w4.as<__nv_bfloat16>(), b4.as<float>(),
+                err.as<int>()};
+    }
+    guide::TrainScratch scratch(uint32_t rows) {
+        return {out.as<float>(), save.as<__nv_bfloat16>(), dz4.as<__nv_bfloat16>(), loss.as<float>(), rows};
+    }
+    cudaError_t ensure(size_t n) {
+        if (n <= cap) return cudaSuccess;
+        cudaError_t e;
+        if ((e = feats.alloc(n * guide::IN * 4)) || (e = out.alloc(n * guide::OUT * 4)) ||
+            (e = save.alloc(n * guide::ACT * 2)) || (e = dz4.alloc(n * guide::OUT_PAD * 2)) ||
+            (e = dirs.alloc(n * 12)) || (e = weights.alloc(n * 4)))
+            return e;
+        cap = n;
         return cudaSuccess;
     }
 };

@@ -18,6 +18,7 @@
 //    the two, so the per-path write stays single and ordered.
 #include "wavefront.h"
 
+#include "guide.h"
 #include "lights_env.cuh"
 #include "openpbr.cuh"
 #include "sampler.cuh"
@@ -122,6 +123,7 @@ __global__ void __launch_bounds__(BLOCK) k_raygen(PathPool pool, WaveParams wp) 
         pool.ps[p] = make_uint2(pixel, sample);
         pool.state[p] = MEDIUM_NONE;
         pool.rad[p] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+        if (pool.guide_rec) pool.guide_rec[p] = ~0u;
         if (pool.aov_albedo) {
             pool.aov_albedo[p] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
             pool.aov_normal[p] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
@@ -316,7 +318,19 @@ __device__ __forceinline__ void record_guides(const PathPool& pool, uint32_t pat
     pool.aov_normal[path] = make_float4(b.x + w.x * n.x, b.y + w.y * n.y, b.z + w.z * n.z, b.w);
 }
 
-template <bool AOV>
+__device__ __forceinline__ float luminance(float3 c) { return 0.2722287f * c.x + 0.6740818f * c.y + 0.0536895f * c.z; }
+
+// The path's open training record learns the radiance gathered so far (the
+// next vertex's snapshot; everything after it is the record's target).
+__device__ __forceinline__ void close_record(const PathPool& pool, uint32_t path, float4 rad) {
+    uint32_t rec = pool.guide_rec[path];
+    if (rec != ~0u) {
+        reinterpret_cast<guide::Record*>(pool.sink->records)[rec].q2.w = luminance(xyz(rad));
+        pool.guide_rec[path] = ~0u;
+    }
+}
+
+template <bool AOV, bool GUIDE>
 __global__ void __launch_bounds__(BLOCK, CN_SHADE_MIN_BLOCKS) k_shade(DeviceScene scene, PathPool pool, uint32_t bounce,
                                                  uint32_t max_bounces, uint32_t light_sampling, uint32_t n0) {
     const uint32_t count = min(bounce == 0 ? n0 : pool.counters[CTR_RAYS + bounce], pool.capacity);
@@ -337,6 +351,7 @@ __global__ void __launch_bounds__(BLOCK, CN_SHADE_MIN_BLOCKS) k_shade(DeviceScen
             float4 t4 = pool.thr[path];
             float3 thr = xyz(t4);
             float4 rad = pool.rad[path];
+            if (GUIDE) close_record(pool, path, rad);
             if (h.x == LIGHT_NONE) {
                 // shade_miss.slang:29-75
                 float weight = 1.0f;
@@ -406,6 +421,15 @@ __global__ void __launch_bounds__(BLOCK, CN_SHADE_MIN_BLOCKS) k_shade(DeviceScen
                 Frame frame(sp.shading);
                 float3 wo = frame.to_local(-dir);
                 Closure cl = resolve_closure(scene.bsdf_tables, mat, wo, medium == inst);
+                // The learned guide's share of the one-sample MIS with BSDF
+                // sampling: none on near-specular vertices, where the BSDF is the
+                // better proposal and a broad mixture would waste its samples.
+                float g_alpha = 0.0f;
+                const float* g_out = nullptr;
+                if (GUIDE) {
+                    g_out = pool.guide_out + size_t(path) * guide::OUT;
+                    if (cl.w_diffuse + cl.w_fuzz > 0.0f || cl.alpha > 0.05f) g_alpha = pool.sink->fraction;
+                }
                 // Guides (shade_surface.slang:322-340): camera rays are fully
                 // open; the first hit records camera-plane depth.
                 float3 guide = f3(0.0f), aov_alb = f3(0.0f);
@@ -463,7 +487,10 @@ __global__ void __launch_bounds__(BLOCK, CN_SHADE_MIN_BLOCKS) k_shade(DeviceScen
                             // A delta light has no competing BSDF strategy: weight 1.
                             bool mis = !cdelta && light_sampling == CENOTE_LIGHT_SAMPLING_MIS;
                             EvalPdf ep = eval_pdf(cl, wl, wo);
-                            float w = mis ? power_heuristic(nee, ep.pdf) : 1.0f;
+                            float p_scatter = ep.pdf;
+                            if (GUIDE && g_alpha > 0.0f)
+                                p_scatter = g_alpha * guide::mixture_pdf(g_out, cdir) + (1.0f - g_alpha) * ep.pdf;
+                            float w = mis ? power_heuristic(nee, p_scatter) : 1.0f;
                             float3 unshadowed = thr * crad * ep.f * fabsf(wl.z) * (w / nee);
                             if (any_pos(unshadowed)) {
                                 float3 sorg = through ? sp.below : sp.position;
@@ -483,10 +510,25 @@ __global__ void __launch_bounds__(BLOCK, CN_SHADE_MIN_BLOCKS) k_shade(DeviceScen
                     float2 u = sample_2d(pixel, sample, bounce_dim(bounce, BSDF_DIR));
                     BsdfSample sc;
                     float3 fsc = f3(0.0f);
-                    if (sample_bsdf_dir(cl, wo, u_lobe, u.x, u.y, sc)) {
+                    bool have;
+                    if (GUIDE && g_alpha > 0.0f && u_lobe < g_alpha) {
+                        // A direction from the guide's mixture (the pick's leftover
+                        // chooses the lobe); lobe labels follow the hemisphere.
+                        float3 d = guide::mixture_sample(g_out, u_lobe / g_alpha, u.x, u.y);
+                        sc.wi = frame.to_local(d);
+                        sc.pdf = 0.0f;
+                        sc.lobe = sc.wi.z < 0.0f ? LOBE_TRANSMISSION : LOBE_DIFFUSE;
+                        have = true;
+                    } else {
+                        const float ub = g_alpha > 0.0f ? (u_lobe - g_alpha) / (1.0f - g_alpha) : u_lobe;
+                        have = sample_bsdf_dir(cl, wo, ub, u.x, u.y, sc);
+                    }
+                    if (have) {
                         EvalPdf ep = eval_pdf(cl, sc.wi, wo);
                         sc.pdf = ep.pdf;
                         fsc = ep.f;
+                        if (GUIDE && g_alpha > 0.0f)
+                            sc.pdf = g_alpha * guide::mixture_pdf(g_out, frame.to_world(sc.wi)) + (1.0f - g_alpha) * ep.pdf;
                     }
                     float3 wiw = frame.to_world(sc.wi);
                     float3 scattered = f3(0.0f);
@@ -520,6 +562,19 @@ __global__ void __launch_bounds__(BLOCK, CN_SHADE_MIN_BLOCKS) k_shade(DeviceScen
                         pool.thr[path] = f4(scattered, sc.pdf);
                         pool.state[path] = (sc.lobe << 24) | (medium & 0xffffffu);
                         push_ray = true;
+                        if (GUIDE && g_alpha > 0.0f && pool.sink->records &&
+                            hash_uniform(pixel, sample, bounce, 0x6a09u) < pool.sink->rate) {
+                            uint32_t idx = atomicAdd(pool.sink->count, 1u);
+                            if (idx < pool.sink->capacity) {
+                                guide::Record rc;
+                                rc.q0 = f4(sp.position, sc.pdf);
+                                rc.q1 = f4(sp.normal, luminance(scattered));
+                                rc.q2 = f4(-dir, -1.0f);
+                                rc.q3 = f4(wiw, __uint_as_float(path));
+                                reinterpret_cast<guide::Record*>(pool.sink->records)[idx] = rc;
+                                pool.guide_rec[path] = idx;
+                            }
+                        }
                         if (any_pos(contribution))
                             pool.rad[path] =
                                 make_float4(rad.x + contribution.x, rad.y + contribution.y, rad.z + contribution.z, rad.w);
@@ -704,7 +759,7 @@ LaunchShape launch_shape(int device) {
     int occ = 0;
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_intersect<false>, BLOCK, 0);
     ls.grid_isect = sms * (occ > 0 ? occ : 4);
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_shade<true>, BLOCK, 0);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_shade<true, false>, BLOCK, 0);
     ls.grid_shade = sms * (occ > 0 ? occ : 4);
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_shadow<false>, BLOCK, 0);
     ls.grid_shadow = sms * (occ > 0 ? occ : 4);
@@ -725,10 +780,14 @@ void launch_intersect(const DeviceScene& scene, const PathPool& pool, uint32_t b
 
 void launch_shade(const DeviceScene& scene, const PathPool& pool, uint32_t bounce, const WaveParams& wp, uint32_t n0,
                   const LaunchShape& ls, cudaStream_t stream) {
-    if (pool.aov_albedo)
-        k_shade<true><<<ls.grid_shade, BLOCK, 0, stream>>>(scene, pool, bounce, wp.max_bounces, wp.light_sampling, n0);
-    else
-        k_shade<false><<<ls.grid_shade, BLOCK, 0, stream>>>(scene, pool, bounce, wp.max_bounces, wp.light_sampling, n0);
+    const bool aov = pool.aov_albedo != nullptr, guided = pool.guide_out != nullptr;
+    auto args = [&](auto kernel) {
+        kernel<<<ls.grid_shade, BLOCK, 0, stream>>>(scene, pool, bounce, wp.max_bounces, wp.light_sampling, n0);
+    };
+    if (aov && guided) args(k_shade<true, true>);
+    else if (aov) args(k_shade<true, false>);
+    else if (guided) args(k_shade<false, true>);
+    else args(k_shade<false, false>);
 }
 
 void launch_shadow(const DeviceScene& scene, const PathPool& pool, uint32_t bounce, const LaunchShape& ls,

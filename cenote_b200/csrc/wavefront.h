@@ -38,10 +38,26 @@ struct PathPool {
     float4* aov_normal;
     float* aov_depth;
     float4* aov_guide;
+    // The learned guide (all null without one): 40 raw mixture outputs per
+    // path for the current bounce, the path's open training record (~0u: none),
+    // and the wave's record buffer with its counter.
+    float* guide_out;
+    uint32_t* guide_rec;
+    struct GuideRecordSink* sink;
     uint32_t* queue[2];   // ray queues, ping-pong by bounce parity
     ShadowRay* shadows;
     uint32_t* counters;
     uint32_t capacity;
+};
+
+// Where guided vertices record themselves for training.
+struct GuideRecordSink {
+    void* records;        // guide::Record[capacity]
+    uint32_t* count;
+    uint32_t capacity;
+    float rate;           // probability that a guided vertex records
+    float fraction;       // the guide's share of the one-sample MIS
+    uint32_t pad;
 };
 
 struct WaveParams {

@@ -385,6 +385,16 @@ int32_t cenote_guide_forward(cenote_guide* guide, const float* features, uint32_
  * (beta 0.9 / 0.999, eps 1e-8), lr = 0 only evaluates. */
 int32_t cenote_guide_train_step(cenote_guide* guide, const float* features, const float* dirs, const float* weights,
                                 uint32_t n, float lr, float* loss, float* grads);
+/* Guided sampling in a renderer (NULL detaches): every surface vertex that is
+ * not near-specular draws its direction from the guide's mixture with
+ * probability `fraction`, else from the BSDF, and weighs by the combined pdf
+ * (one-sample MIS, so the estimate stays unbiased whatever the network says);
+ * next-event MIS uses the same combined pdf. With train_steps > 0 the renderer
+ * records a sample of its guided vertices each wave and runs that many Adam
+ * steps (batch 65,536, learning rate `lr`) on them after the wave. The guide
+ * must outlive its use by the renderer. */
+int32_t cenote_renderer_set_guide(cenote_renderer* renderer, cenote_guide* guide, float fraction,
+                                  uint32_t train_steps, float lr);
 
 /* ---- environment tables without device allocation --------------------------------- */
 
