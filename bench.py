@@ -169,6 +169,71 @@ def run_reference(args, w):
     print(json.dumps(line), flush=True)
 
 
+def run_guiding(args):
+    """Learned guiding on the large scene: device time for plain and guided
+    sampling to reach relMSE <= 0.01 against a plain render of
+    `--reference-spp` samples, accumulating 4 spp at a time (the guide trains
+    online from a seeded random initialisation, one Adam step of 65,536
+    records after every 4-spp wave over the first 256 spp, then stays
+    frozen)."""
+    from cenote_b200 import Context, Film, Guide, Renderer, Scene, scenes
+    from cenote_b200.metrics import rel_mse
+    if int(os.environ.get("RANK", "0")) != 0:
+        return
+    W, H = args.width, args.height
+    B = 16 if args.scene == "large" else 8
+    ctx = Context(0)
+    spec = scenes.SCENES[args.scene](W, H, 64, B)
+    scene = Scene(ctx, spec)
+    ref_r = Renderer(ctx, B)
+    ref_f = Film(ctx, W, H)
+    t0 = time.perf_counter()
+    done = 0
+    # The reference draws sample indices from 2^24 on, so it shares no samples
+    # with the renders it judges.
+    while done < args.reference_spp:
+        n = min(512, args.reference_spp - done)
+        ref_r.accumulate_range(scene, ref_f, (1 << 24) + done, n)
+        done += n
+    ref_s = time.perf_counter() - t0
+    ref = ref_f.averages()[..., :3]
+    target, chunk, cap = 0.01, 4, 4096
+
+    def run(guided):
+        r = Renderer(ctx, B, samples_per_wave=chunk)
+        g = None
+        if guided:
+            g = Guide(ctx, seed=11)
+            r.set_guide(g, 0.5, 1, 5e-3)
+        f = Film(ctx, W, H)
+        ms, spp, err, curve = 0.0, 0, float("inf"), []
+        while spp < cap:
+            if guided and spp == 256:
+                r.set_guide(g, 0.5, 0, 5e-3)  # the guide trained long enough: freeze it
+            r.accumulate(scene, f, chunk)
+            ms += r.stats()["gpu_ms"]
+            spp += chunk
+            err = rel_mse(f.averages()[..., :3], ref)
+            if spp in (16, 64, 256, 1024) or err <= target:
+                curve.append({"spp": spp, "ms": round(ms, 2), "rel_mse": err})
+            if err <= target:
+                break
+        return {"ms": ms, "spp": spp, "rel_mse": err, "reached": err <= target, "curve": curve}
+
+    plain = run(False)
+    guided = run(True)
+    line = {
+        "metric": "device time to relMSE <= 0.01, guided / plain", "value": guided["ms"] / plain["ms"],
+        "unit": "ratio", "higher_is_better": False, "n_gpus": 1, "scaling": "none", "vs_baseline": None,
+        "dtype": "f32 (guide MLP bf16 with f32 accumulation)", "data": "synthetic (procedural scene, seeded)",
+        "config": {"workload": f"{args.scene} at {W}x{H}, {B} bounces, reference {args.reference_spp} spp plain; "
+                               "4-spp chunks; guide: 8 vMF lobes, 3x64 hidden, one-sample MIS weight 0.5, "
+                               "1 Adam step (lr 5e-3, batch 65,536) per wave for the first 256 spp, then frozen"},
+        "plain": plain, "guided": guided, "reference_s": ref_s,
+    }
+    print(json.dumps(line), flush=True)
+
+
 def run_serving(args):
     """The batched-serving workload: a seeded Poisson stream (200 jobs/s) of
     progressive render jobs drawn uniformly from the closed box, the material
@@ -240,13 +305,20 @@ def main():
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="chart", choices=list(WORKLOADS) + ["serving"])
+    ap.add_argument("--workload", default="chart", choices=list(WORKLOADS) + ["serving", "guiding"])
     ap.add_argument("--jobs", type=int, default=256, help="serving: jobs in the Poisson stream")
+    ap.add_argument("--width", type=int, default=480, help="guiding: image width")
+    ap.add_argument("--height", type=int, default=270, help="guiding: image height")
+    ap.add_argument("--reference-spp", type=int, default=16384, help="guiding: spp of the plain reference")
+    ap.add_argument("--scene", default="large", choices=["large", "ceiling_box"], help="guiding: the scene")
     ap.add_argument("--spp", type=int, default=0, help="override the workload's spp (profiling runs)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     args = ap.parse_args()
     if args.workload == "serving":
         run_serving(args)
+        return
+    if args.workload == "guiding":
+        run_guiding(args)
         return
     w = dict(WORKLOADS[args.workload])
     if args.spp:

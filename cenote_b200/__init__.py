@@ -118,7 +118,7 @@ EXPORTED_SYMBOLS = [
     "cenote_probe_texture", "cenote_server_create", "cenote_server_destroy", "cenote_job_submit", "cenote_job_poll",
     "cenote_job_wait", "cenote_job_result", "cenote_job_release", "cenote_server_stats", "cenote_guide_create",
     "cenote_guide_destroy", "cenote_guide_params", "cenote_guide_set_params", "cenote_guide_forward",
-    "cenote_guide_train_step", "cenote_renderer_set_guide",
+    "cenote_guide_train_step", "cenote_renderer_set_guide", "cenote_accumulate_range",
 ]
 
 _lib = None
@@ -159,6 +159,7 @@ def library() -> C.CDLL:
         "cenote_guide_forward": (I32, [P, P, U32, P]),
         "cenote_guide_train_step": (I32, [P, P, P, P, U32, F, P, P]),
         "cenote_renderer_set_guide": (I32, [P, P, F, U32, F]),
+        "cenote_accumulate_range": (I32, [P, P, P, U32, U32]),
         "cenote_scene_destroy": (None, [P]),
         "cenote_scene_set_camera": (I32, [P, P]),
         "cenote_scene_prep_times": (I32, [P, P]),
@@ -535,6 +536,10 @@ class Renderer:
 
     def accumulate(self, scene: Scene, film: Film, count: int = 1) -> None:
         _check(library().cenote_accumulate_n(self._h, scene.handle, film.handle, count))
+
+    def accumulate_range(self, scene: Scene, film: Film, first_sample: int, count: int) -> None:
+        """Accumulate samples first_sample .. first_sample + count - 1 (independent of the film's count)."""
+        _check(library().cenote_accumulate_range(self._h, scene.handle, film.handle, first_sample, count))
 
     def set_guide(self, guide, fraction: float = 0.5, train_steps: int = 0, lr: float = 1e-2) -> None:
         """Guided sampling with a Guide (None detaches); train_steps Adam steps per wave."""

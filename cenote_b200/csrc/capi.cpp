@@ -853,6 +853,19 @@ int32_t cenote_accumulate_n(cenote_renderer* r, cenote_scene* scene, cenote_film
     return rc;
 }
 
+int32_t cenote_accumulate_range(cenote_renderer* r, cenote_scene* scene, cenote_film* film, uint32_t first_sample,
+                                uint32_t count) {
+    CN_CHECK(r && scene && film, CENOTE_E_INVALID_ARGUMENT, "null argument");
+    CN_CHECK(r->ctx == scene->ctx && r->ctx == film->ctx, CENOTE_E_INVALID_ARGUMENT, "handles from different contexts");
+    CN_CHECK(uint64_t(first_sample) + count <= 0xffffffffull, CENOTE_E_INVALID_ARGUMENT, "sample index overflow");
+    if (count == 0) return CENOTE_OK;
+    std::lock_guard<std::mutex> lock(r->ctx->mu);
+    CN_CUDA(cudaSetDevice(r->ctx->device));
+    int32_t rc = run_waves(r, scene, film->width, film->height, first_sample, count, film, nullptr);
+    if (rc == CENOTE_OK) film->samples += count;
+    return rc;
+}
+
 int32_t cenote_accumulate(cenote_renderer* r, cenote_scene* scene, cenote_film* film) {
     return cenote_accumulate_n(r, scene, film, 1);
 }

@@ -730,4 +730,17 @@ def large(width=1920, height=1080, spp=64, max_bounces=16, grid=1024, instances=
     return SceneSpec("large", objs, cam, env, width, height, spp, max_bounces, textures=texs)
 
 
-SCENES.update(textured=textured, large=large)
+def ceiling_box(width=256, height=256, spp=16, max_bounces=8) -> SceneSpec:
+    """The closed box with its emitter turned to face the ceiling, 0.4 below
+    it: light reaches the room only by a bounce off the ceiling, so next-event
+    estimation from most surfaces finds the lamp's back face and the
+    directional distribution of incident light is sharply peaked."""
+    spec = cornell(width, height, spp, max_bounces)
+    lamp = spec.objects[-1]
+    q = quad([(-0.25, 1.6, -0.25), (-0.25, 1.6, 0.25), (0.25, 1.6, 0.25), (0.25, 1.6, -0.25)])
+    spec.objects[-1] = Object(q, lamp.transform, lamp.material)
+    spec.name = "ceiling_box"
+    return spec
+
+
+SCENES.update(textured=textured, large=large, ceiling_box=ceiling_box)

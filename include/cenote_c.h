@@ -256,6 +256,12 @@ uint32_t cenote_film_samples(cenote_film* film);
 int32_t cenote_accumulate(cenote_renderer* r, cenote_scene* scene, cenote_film* film);
 /* `count` consecutive accumulate calls in one submission (bitwise identical). */
 int32_t cenote_accumulate_n(cenote_renderer* r, cenote_scene* scene, cenote_film* film, uint32_t count);
+/* Accumulate the samples first_sample .. first_sample + count - 1 of every
+ * pixel (Wavefront::trace's explicit sample index, wavefront.rs:568) instead
+ * of the film's own count: independent estimates of one image, e.g. a
+ * reference that shares no samples with the render it judges. */
+int32_t cenote_accumulate_range(cenote_renderer* r, cenote_scene* scene, cenote_film* film, uint32_t first_sample,
+                                uint32_t count);
 /* Film::averages: sums / samples into host memory; any pointer may be NULL.
  * beauty/albedo/normal are w·h·4 floats, depth w·h floats. */
 int32_t cenote_film_averages(cenote_film* film, float* beauty, float* albedo, float* normal, float* depth);

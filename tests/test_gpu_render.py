@@ -264,3 +264,23 @@ def test_ray_counts_are_reported(ctx):
     ref.render_sum(64, 64, 0, 4, 8)
     # Identical sample sequences: the ray counts agree to rounding-induced path splits.
     assert abs(int(st["extension_rays"]) - int(ref.last_ray_counts[0])) / ref.last_ray_counts[0] < 0.01
+
+
+def test_accumulate_range_matches_the_film_sequence(ctx):
+    spec = scenes.cornell(32, 24, 4, 6)
+    s = Scene(ctx, spec)
+    r = Renderer(ctx, 6)
+    a, b, c = Film(ctx, 32, 24), Film(ctx, 32, 24), Film(ctx, 32, 24)
+    r.accumulate(s, a, 6)
+    r.accumulate_range(s, b, 0, 6)
+    assert np.array_equal(a.sums(), b.sums()) and b.samples == 6
+    # Samples 6..9 continue the sequence where the film left off.
+    r.accumulate(s, a, 4)
+    r.accumulate_range(s, c, 0, 6)
+    r.accumulate_range(s, c, 6, 4)
+    assert np.array_equal(a.sums(), c.sums())
+    # A disjoint range is a different, equally valid estimate.
+    d = Film(ctx, 32, 24)
+    r.accumulate_range(s, d, 1 << 20, 10)
+    assert not np.array_equal(a.sums(), d.sums())
+    assert abs(d.sums()[..., 0].mean() / a.sums()[..., 0].mean() - 1.0) < 0.2
