@@ -118,7 +118,8 @@ EXPORTED_SYMBOLS = [
     "cenote_probe_texture", "cenote_server_create", "cenote_server_destroy", "cenote_job_submit", "cenote_job_poll",
     "cenote_job_wait", "cenote_job_result", "cenote_job_release", "cenote_server_stats", "cenote_guide_create",
     "cenote_guide_destroy", "cenote_guide_params", "cenote_guide_set_params", "cenote_guide_forward",
-    "cenote_guide_train_step", "cenote_renderer_set_guide", "cenote_accumulate_range",
+    "cenote_guide_train_step", "cenote_renderer_set_guide", "cenote_accumulate_range", "cenote_film_tonemap",
+    "cenote_film_tonemap_device", "cenote_film_restore",
 ]
 
 _lib = None
@@ -160,6 +161,9 @@ def library() -> C.CDLL:
         "cenote_guide_train_step": (I32, [P, P, P, P, U32, F, P, P]),
         "cenote_renderer_set_guide": (I32, [P, P, F, U32, F]),
         "cenote_accumulate_range": (I32, [P, P, P, U32, U32]),
+        "cenote_film_tonemap": (I32, [P, F, P]),
+        "cenote_film_tonemap_device": (I32, [P, F, P]),
+        "cenote_film_restore": (I32, [P, P, U32]),
         "cenote_scene_destroy": (None, [P]),
         "cenote_scene_set_camera": (I32, [P, P]),
         "cenote_scene_prep_times": (I32, [P, P]),
@@ -489,6 +493,24 @@ class Film:
     def averages_into(self, ptr: int) -> None:
         """Resolve into caller memory at `ptr` (pinned host memory for speed)."""
         _check(library().cenote_film_averages(self._h, ptr, None, None, None))
+
+    def tonemap(self, exposure_stops: float = 0.0) -> np.ndarray:
+        """The display frame (tonemap.slang): uint8 (H, W, 4), sRGB-encoded."""
+        out = np.zeros((self.height, self.width), np.uint32)
+        _check(library().cenote_film_tonemap(self._h, exposure_stops, _ptr(out)))
+        return out.view(np.uint8).reshape(self.height, self.width, 4)
+
+    def tonemap_device(self, exposure_stops: float, ptr: int) -> None:
+        """Write the display frame (H*W packed RGBA8 words) to device memory at
+        `ptr`, ordered on the context's stream; returns without waiting."""
+        _check(library().cenote_film_tonemap_device(self._h, exposure_stops, ptr))
+
+    def set_sums(self, beauty_sum: np.ndarray, samples: int) -> None:
+        """Resume from saved beauty sums (H, W, 4) holding `samples` samples."""
+        s = np.ascontiguousarray(beauty_sum, np.float32)
+        if s.shape != (self.height, self.width, 4):
+            raise CenoteError(-1, f"sums of shape {s.shape} for a {self.width}x{self.height} film")
+        _check(library().cenote_film_restore(self._h, _ptr(s), samples))
 
     def sums(self) -> np.ndarray:
         out = np.zeros((self.height, self.width, 4), np.float32)

@@ -4,11 +4,15 @@
     python -m cenote_b200.cli render [SCENE] [--spp N] [--width W] [--height H]
                                      [--depth D] [--out render.exr] [--frames K]
 
-SCENE is a built-in workload (cornell, chart) or a pbrt-v4 file (.pbrt, the
-subset cenote_b200.pbrt imports). Unset flags take the scene's own settings.
+SCENE is a built-in workload (cornell, chart, textured, large, ceiling_box), a
+scene file in the reference's change-set format (.ron, cenote_b200.scene_file)
+or a pbrt-v4 file (.pbrt, the subset cenote_b200.pbrt imports). Unset flags take the scene's own settings.
 Accumulates SPP samples and writes the linear averages as one multi-layer
 EXR: beauty R/G/B/A, the denoiser guides albedo.R/G/B and normal.X/Y/Z, depth Z
 (crates/cenote-cli/src/main.rs:196-216).
+--png additionally writes the display frame the reference's viewer presents
+(crates/cenote/shaders/tonemap.slang: exposure --exposure stops, ACES fit, sRGB)
+as an 8-bit PNG, tonemapped on the device.
 --frames repeats the render (profiling); --samples-per-wave fixes how many
 samples of every pixel one wave carries; --stats prints the renderer's counters.
 """
@@ -16,8 +20,10 @@ from __future__ import annotations
 
 import argparse
 import json
+import struct
 import sys
 import time
+import zlib
 
 import numpy as np
 
@@ -29,9 +35,25 @@ def load_scene(name: str):
     if name.endswith(".pbrt"):
         from .pbrt import import_pbrt
         return import_pbrt(name)
+    if name.endswith(".ron"):
+        from .scene_file import load_scene_file
+        return load_scene_file(name)
     if name in scenes.SCENES:
         return scenes.SCENES[name]()
-    raise SystemExit(f"unknown scene {name!r}: use one of {sorted(scenes.SCENES)} or a .pbrt file")
+    raise SystemExit(f"unknown scene {name!r}: use one of {sorted(scenes.SCENES)}, a .ron or a .pbrt file")
+
+
+def write_png(path: str, rgba8: np.ndarray) -> None:
+    """An 8-bit RGBA PNG (no filtering) from uint8 (H, W, 4)."""
+    h, w = rgba8.shape[:2]
+    raw = b"".join(b"\x00" + rgba8[y].tobytes() for y in range(h))
+
+    def chunk(tag: bytes, data: bytes) -> bytes:
+        return struct.pack(">I", len(data)) + tag + data + struct.pack(">I", zlib.crc32(tag + data) & 0xFFFFFFFF)
+
+    with open(path, "wb") as f:
+        f.write(b"\x89PNG\r\n\x1a\n" + chunk(b"IHDR", struct.pack(">IIBBBBB", w, h, 8, 6, 0, 0, 0)) +
+                chunk(b"IDAT", zlib.compress(raw, 6)) + chunk(b"IEND", b""))
 
 
 def render(args) -> int:
@@ -54,6 +76,8 @@ def render(args) -> int:
     if args.out:
         av = film.all_averages()
         write_aov_exr(args.out, av["beauty"], av["albedo"], av["normal"], av["depth"])
+    if args.png:
+        write_png(args.png, film.tonemap(args.exposure))
     st = renderer.stats()
     msg = (f"wrote {args.out} ({width}x{height}, {spp} spp, depth {depth}; layers: beauty, albedo, normal, Z) "
            f"in {dt * 1e3:.1f} ms/frame, "
@@ -78,6 +102,8 @@ def main(argv=None) -> int:
     r.add_argument("--device", type=int, default=0)
     r.add_argument("--samples-per-wave", type=int, default=0, help="0 = automatic")
     r.add_argument("--stats", action="store_true")
+    r.add_argument("--png", default="", help="also write the tonemapped display frame here")
+    r.add_argument("--exposure", type=float, default=0.0, help="display exposure in stops (--png)")
     args = ap.parse_args(argv)
     for v in (args.spp, args.width, args.height, args.samples_per_wave):
         if v < 0:

@@ -914,6 +914,32 @@ int32_t cenote_film_averages(cenote_film* film, float* beauty, float* albedo, fl
     return wait_stream(film->ctx->stream, film->ctx->sync_ev, 600000.0);
 }
 
+int32_t cenote_film_tonemap_device(cenote_film* film, float exposure_stops, void* rgba8) {
+    CN_CHECK(film && rgba8, CENOTE_E_INVALID_ARGUMENT, "null argument");
+    CN_CHECK(film->samples > 0, CENOTE_E_INVALID_ARGUMENT, "tonemapping an empty film");
+    CN_CUDA(cudaSetDevice(film->ctx->device));
+    const uint32_t px = film->width * film->height;
+    launch_resolve(film->sum.as<float4>(), film->avg.as<float4>(), px, float(film->samples), film->ctx->stream);
+    launch_tonemap(film->avg.as<float4>(), static_cast<uint32_t*>(rgba8), px, std::exp2(exposure_stops),
+                   film->ctx->stream);
+    CN_CUDA(cudaGetLastError());
+    return CENOTE_OK;
+}
+
+int32_t cenote_film_tonemap(cenote_film* film, float exposure_stops, uint32_t* rgba8) {
+    CN_CHECK(film && rgba8, CENOTE_E_INVALID_ARGUMENT, "null argument");
+    CN_CHECK(film->samples > 0, CENOTE_E_INVALID_ARGUMENT, "tonemapping an empty film");
+    std::lock_guard<std::mutex> lock(film->ctx->mu);
+    CN_CUDA(cudaSetDevice(film->ctx->device));
+    const size_t px = size_t(film->width) * film->height;
+    DeviceBuffer out;
+    CN_CUDA(out.alloc(px * 4));
+    int32_t rc = cenote_film_tonemap_device(film, exposure_stops, out.ptr);
+    if (rc != CENOTE_OK) return rc;
+    CN_CUDA(cudaMemcpyAsync(rgba8, out.ptr, px * 4, cudaMemcpyDeviceToHost, film->ctx->stream));
+    return wait_stream(film->ctx->stream, film->ctx->sync_ev, 600000.0);
+}
+
 int32_t cenote_film_sums(cenote_film* film, float* beauty_sum) {
     CN_CHECK(film && beauty_sum, CENOTE_E_INVALID_ARGUMENT, "null argument");
     std::lock_guard<std::mutex> lock(film->ctx->mu);
@@ -921,6 +947,19 @@ int32_t cenote_film_sums(cenote_film* film, float* beauty_sum) {
     CN_CUDA(cudaMemcpyAsync(beauty_sum, film->sum.ptr, size_t(film->width) * film->height * 16, cudaMemcpyDeviceToHost,
                             film->ctx->stream));
     return wait_stream(film->ctx->stream, film->ctx->sync_ev, 600000.0);
+}
+
+int32_t cenote_film_restore(cenote_film* film, const float* beauty_sum, uint32_t samples) {
+    CN_CHECK(film && beauty_sum, CENOTE_E_INVALID_ARGUMENT, "null argument");
+    CN_CHECK(samples > 0, CENOTE_E_INVALID_ARGUMENT, "a restored film holds at least one sample");
+    std::lock_guard<std::mutex> lock(film->ctx->mu);
+    int32_t rc = cenote_film_reset(film);
+    if (rc != CENOTE_OK) return rc;
+    CN_CUDA(cudaMemcpyAsync(film->sum.ptr, beauty_sum, size_t(film->width) * film->height * 16, cudaMemcpyHostToDevice,
+                            film->ctx->stream));
+    rc = wait_stream(film->ctx->stream, film->ctx->sync_ev, 600000.0);
+    if (rc == CENOTE_OK) film->samples = samples;
+    return rc;
 }
 
 // ---- probes ------------------------------------------------------------------------------

@@ -713,6 +713,42 @@ __global__ void k_resolve(const float4* __restrict__ sum, float4* __restrict__ a
     }
 }
 
+// The display transform of crates/cenote/shaders/tonemap.slang:16-99 into
+// packed RGBA8: exposure, ACEScg -> linear Rec.709, Stephen Hill's analytic
+// RRT+ODT fit (BakingLab; its published matrices and rational curve), sRGB
+// transfer, round to 8 bits (R in the low byte). Each matrix row is summed
+// left to right.
+__device__ __forceinline__ float3 mat3_row_sum(const float m[3][3], float3 v) {
+    return f3((m[0][0] * v.x + m[0][1] * v.y) + m[0][2] * v.z, (m[1][0] * v.x + m[1][1] * v.y) + m[1][2] * v.z,
+              (m[2][0] * v.x + m[2][1] * v.y) + m[2][2] * v.z);
+}
+
+__device__ __forceinline__ uint32_t quantize8(float c) {
+    return uint32_t(rintf(fminf(fmaxf(c, 0.0f), 1.0f) * 255.0f));
+}
+
+__device__ __forceinline__ float srgb_encode(float c) {
+    return c <= 0.0031308f ? 12.92f * c : 1.055f * powf(c, 1.0f / 2.4f) - 0.055f;
+}
+
+__global__ void k_tonemap(const float4* __restrict__ avg, uint32_t* __restrict__ out, uint32_t n, float exposure) {
+    const float SRGB_FROM_ACESCG[3][3] = {{1.705050993f, -0.621792121f, -0.083258872f},
+                                          {-0.130256418f, 1.140804737f, -0.010548319f},
+                                          {-0.024003357f, -0.128968976f, 1.152972333f}};
+    const float IN[3][3] = {{0.59719f, 0.35458f, 0.04823f}, {0.07600f, 0.90834f, 0.01566f}, {0.02840f, 0.13383f, 0.83777f}};
+    const float OUT[3][3] = {{1.60475f, -0.53108f, -0.07367f}, {-0.10208f, 1.10813f, -0.00605f},
+                             {-0.00327f, -0.07276f, 1.07602f}};
+    for (uint32_t p = blockIdx.x * blockDim.x + threadIdx.x; p < n; p += gridDim.x * blockDim.x) {
+        float4 a = avg[p];
+        float3 v = mat3_row_sum(IN, mat3_row_sum(SRGB_FROM_ACESCG, f3(a.x * exposure, a.y * exposure, a.z * exposure)));
+        float3 num = v * (v + f3(0.0245786f)) - f3(0.000090537f);
+        float3 den = v * (0.983729f * v + f3(0.4329510f)) + f3(0.238081f);
+        float3 d = saturate3(mat3_row_sum(OUT, num / den));
+        out[p] = quantize8(srgb_encode(d.x)) | quantize8(srgb_encode(d.y)) << 8 | quantize8(srgb_encode(d.z)) << 16 |
+                 255u << 24;
+    }
+}
+
 __global__ void k_resolve1(const float* __restrict__ sum, float* __restrict__ avg, uint32_t n, float samples) {
     for (uint32_t p = blockIdx.x * blockDim.x + threadIdx.x; p < n; p += gridDim.x * blockDim.x) avg[p] = sum[p] / samples;
 }
@@ -815,6 +851,12 @@ void launch_accumulate(const PathPool& pool, const FilmTargets& film, uint32_t p
         k_accumulate<true><<<grid, 256, 0, stream>>>(pool, film, pixel_base, pixel_count, samples, reset ? 1u : 0u);
     else
         k_accumulate<false><<<grid, 256, 0, stream>>>(pool, film, pixel_base, pixel_count, samples, reset ? 1u : 0u);
+}
+
+void launch_tonemap(const float4* avg, uint32_t* out, uint32_t pixels, float exposure_scale, cudaStream_t stream) {
+    int grid = int((pixels + 255) / 256);
+    if (grid > 148 * 16) grid = 148 * 16;
+    k_tonemap<<<grid, 256, 0, stream>>>(avg, out, pixels, exposure_scale);
 }
 
 void launch_resolve1(const float* sum, float* avg, uint32_t pixels, float samples, cudaStream_t stream) {

@@ -113,6 +113,8 @@ void launch_accumulate(const PathPool& pool, const FilmTargets& film, uint32_t p
                        uint32_t samples, bool reset, cudaStream_t stream);
 void launch_resolve(const float4* sum, float4* avg, uint32_t pixels, float samples, cudaStream_t stream);
 void launch_resolve1(const float* sum, float* avg, uint32_t pixels, float samples, cudaStream_t stream);
+// The display transform (tonemap.slang): linear ACEScg averages -> sRGB RGBA8.
+void launch_tonemap(const float4* avg, uint32_t* out, uint32_t pixels, float exposure_scale, cudaStream_t stream);
 // tally[0] += extension rays, [1] += shadow rays, [2] |= overflow,
 // [3] += node visits, [4] += triangle tests.
 void launch_tally(const PathPool& pool, unsigned long long* tally, uint32_t n0, uint32_t max_bounces,

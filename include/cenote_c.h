@@ -265,10 +265,21 @@ int32_t cenote_accumulate_range(cenote_renderer* r, cenote_scene* scene, cenote_
 /* Film::averages: sums / samples into host memory; any pointer may be NULL.
  * beauty/albedo/normal are w·h·4 floats, depth w·h floats. */
 int32_t cenote_film_averages(cenote_film* film, float* beauty, float* albedo, float* normal, float* depth);
+/* The display frame (crates/cenote/shaders/tonemap.slang, headless): the
+ * beauty average exposed by 2^exposure_stops, through the ACES RRT+ODT fit
+ * and the sRGB transfer, packed RGBA8 (R in the low byte), w·h words into
+ * host memory. The _device form writes device memory on the context's stream
+ * and returns without waiting (a serving preview). */
+int32_t cenote_film_tonemap(cenote_film* film, float exposure_stops, uint32_t* rgba8);
+int32_t cenote_film_tonemap_device(cenote_film* film, float exposure_stops, void* rgba8);
 /* The raw running beauty sums (w·h·4 floats). */
 int32_t cenote_film_sums(cenote_film* film, float* beauty_sum);
 /* Device pointer to the beauty sums (float4 per pixel). */
 void* cenote_film_device_sums(cenote_film* film);
+/* Resume accumulation from a checkpoint: the film takes `beauty_sum` (w·h·4
+ * floats, as cenote_film_sums returned them) and `samples`; the guide sums
+ * restart at zero. */
+int32_t cenote_film_restore(cenote_film* film, const float* beauty_sum, uint32_t samples);
 
 /* ---- probes (test entry points; rng_test.slang and friends) ------------------------- */
 
