@@ -120,6 +120,7 @@ EXPORTED_SYMBOLS = [
     "cenote_guide_destroy", "cenote_guide_params", "cenote_guide_set_params", "cenote_guide_forward",
     "cenote_guide_train_step", "cenote_renderer_set_guide", "cenote_accumulate_range", "cenote_film_tonemap",
     "cenote_film_tonemap_device", "cenote_film_restore",
+    "cenote_scene_add_delta_light",
 ]
 
 _lib = None
@@ -164,6 +165,7 @@ def library() -> C.CDLL:
         "cenote_film_tonemap": (I32, [P, F, P]),
         "cenote_film_tonemap_device": (I32, [P, F, P]),
         "cenote_film_restore": (I32, [P, P, U32]),
+        "cenote_scene_add_delta_light": (I32, [P, P]),
         "cenote_scene_destroy": (None, [P]),
         "cenote_scene_set_camera": (I32, [P, P]),
         "cenote_scene_prep_times": (I32, [P, P]),
@@ -373,6 +375,15 @@ class Scene:
     def set_camera(self, cam: scenes.Camera) -> None:
         c = _c_camera(cam)
         _check(library().cenote_scene_set_camera(self._h, C.byref(c)))
+
+    def add_delta_light(self, light: "scenes.DeltaLight") -> None:
+        """Append a point or distant light; the light list and its alias
+        table are rebuilt as if the scene had been created with it."""
+        d = DeltaLightC()
+        d.kind = light.kind
+        d.anchor[:] = list(light.anchor)
+        d.emission[:] = list(light.emission)
+        _check(library().cenote_scene_add_delta_light(self._h, C.byref(d)))
 
     def prep_times_ms(self):
         out = np.zeros(3, np.float32)

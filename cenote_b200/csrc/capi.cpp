@@ -136,24 +136,15 @@ double record_power(const LightRecord& r) {
 
 // Walker/Vose over f64 shares: stable small/large partition, both popped
 // from the back, leftovers keep threshold 1.
-std::vector<LightRecord> build_lights(const std::vector<TriLight>& tris, const cenote_delta_light* deltas,
-                                      uint32_t n_deltas, double* total_out) {
-    std::vector<LightRecord> recs;
-    recs.reserve(tris.size() + n_deltas);
-    for (const TriLight& t : tris)
-        recs.push_back(make_record(KIND_TRIANGLE, t.c[0], t.c[1] - t.c[0], t.c[2] - t.c[0], t.emission, t.instance,
-                                   t.primitive));
-    for (uint32_t i = 0; i < n_deltas; ++i)
-        recs.push_back(make_record(deltas[i].kind, v3(deltas[i].anchor), {0, 0, 0}, {0, 0, 0}, v3(deltas[i].emission),
-                                   LIGHT_NONE, 0));
+// Fills every record's pdf and alias entry from its power; returns the total.
+double alias_lights(std::vector<LightRecord>& recs) {
     std::vector<double> power(recs.size());
     double total = 0.0;
     for (size_t i = 0; i < recs.size(); ++i) {
         power[i] = record_power(recs[i]);
         total += power[i];
     }
-    *total_out = total;
-    if (total <= 0.0) return recs;
+    if (total <= 0.0) return total;
     for (size_t i = 0; i < recs.size(); ++i) {
         double sel = power[i] / total;
         if (recs[i].kind == KIND_TRIANGLE) {
@@ -179,6 +170,23 @@ std::vector<LightRecord> build_lights(const std::vector<TriLight>& tris, const c
         share[rich] -= 1.0 - share[poor];
         (share[rich] < 1.0 ? small : large).push_back(rich);
     }
+    return total;
+}
+
+LightRecord delta_record(const cenote_delta_light& d) {
+    return make_record(d.kind, v3(d.anchor), {0, 0, 0}, {0, 0, 0}, v3(d.emission), LIGHT_NONE, 0);
+}
+
+// lights.rs:175-227: triangle records first, then the delta lights, in order.
+std::vector<LightRecord> build_lights(const std::vector<TriLight>& tris, const cenote_delta_light* deltas,
+                                      uint32_t n_deltas, double* total_out) {
+    std::vector<LightRecord> recs;
+    recs.reserve(tris.size() + n_deltas);
+    for (const TriLight& t : tris)
+        recs.push_back(make_record(KIND_TRIANGLE, t.c[0], t.c[1] - t.c[0], t.c[2] - t.c[0], t.emission, t.instance,
+                                   t.primitive));
+    for (uint32_t i = 0; i < n_deltas; ++i) recs.push_back(delta_record(deltas[i]));
+    *total_out = alias_lights(recs);
     return recs;
 }
 
@@ -618,6 +626,42 @@ void cenote_scene_destroy(cenote_scene* scene) {
 int32_t cenote_scene_set_camera(cenote_scene* scene, const cenote_camera* camera) {
     CN_CHECK(scene && camera && camera_valid(*camera), CENOTE_E_INVALID_ARGUMENT, "degenerate camera");
     scene->camera = *camera;
+    return CENOTE_OK;
+}
+
+int32_t cenote_scene_add_delta_light(cenote_scene* scene, const cenote_delta_light* light) {
+    CN_CHECK(scene && light, CENOTE_E_INVALID_ARGUMENT, "null argument");
+    CN_CHECK(light->kind == KIND_DISTANT || light->kind == KIND_POINT, CENOTE_E_INVALID_ARGUMENT,
+             "unknown delta-light kind");
+    for (int a = 0; a < 3; ++a)
+        CN_CHECK(std::isfinite(light->anchor[a]) && std::isfinite(light->emission[a]), CENOTE_E_INVALID_ARGUMENT,
+                 "non-finite delta light");
+    std::lock_guard<std::mutex> lock(scene->ctx->mu);
+    CN_CUDA(cudaSetDevice(scene->ctx->device));
+    // The records rebuilt from scratch: the same list a scene created with the
+    // light among its deltas holds, bit for bit.
+    std::vector<LightRecord> recs = scene->lights;
+    for (LightRecord& r : recs) {
+        r.pdf = 0.0f;
+        r.alias_threshold = 1.0f;
+        r.alias_index = 0;
+    }
+    recs.push_back(delta_record(*light));
+    const double power = alias_lights(recs);
+    cudaError_t err = cudaSuccess;
+    // A new buffer: launches already queued (and graphs already captured)
+    // keep reading the old one, which the scene keeps until it is destroyed.
+    DeviceBuffer* b = scene->add(recs.size() * sizeof(LightRecord), &err);
+    CN_CUDA(err);
+    CN_CUDA(cudaMemcpyAsync(b->ptr, recs.data(), recs.size() * sizeof(LightRecord), cudaMemcpyHostToDevice,
+                            scene->ctx->stream));
+    int32_t rc = wait_stream(scene->ctx->stream, scene->ctx->sync_ev, 600000.0);
+    if (rc != CENOTE_OK) return rc;
+    scene->lights = std::move(recs);
+    scene->select_prob = select_probability(scene->env_power, power);
+    scene->ds.lights = b->as<LightRecord>();
+    scene->ds.light_count = uint32_t(scene->lights.size());
+    scene->ds.select_prob = scene->select_prob;
     return CENOTE_OK;
 }
 

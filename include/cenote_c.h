@@ -214,6 +214,11 @@ int32_t cenote_scene_create_textured(cenote_context* ctx, const cenote_object* o
                                      const cenote_delta_light* deltas, uint32_t delta_count,
                                      const cenote_texture* textures, uint32_t texture_count, cenote_scene** out);
 void cenote_scene_destroy(cenote_scene* scene);
+/* Append a delta light (lights.rs:57-73) to a built scene: the light list,
+ * its alias table and the environment/light selection probability are rebuilt
+ * as if the scene had been created with it last among `deltas`. Renders
+ * already queued, and serving jobs already admitted, keep the old list. */
+int32_t cenote_scene_add_delta_light(cenote_scene* scene, const cenote_delta_light* light);
 /* Replace the camera (the viewer's orbit control writes Scene::camera_mut). */
 int32_t cenote_scene_set_camera(cenote_scene* scene, const cenote_camera* camera);
 /* Scene-prep timings (ms): [0] BVH build, [1] env tables on the GPU, [2] total. */
