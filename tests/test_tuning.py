@@ -1,0 +1,99 @@
+"""The launch knobs: material sort before shading, wave size, refill threshold,
+and the autotuner that picks them per scene.
+
+Every knob only reorders or regroups work: each path's arithmetic and random
+numbers are keyed by its pixel and sample, never by its queue slot, and
+equal-distance hits resolve by (instance, primitive) whatever the traversal
+order, so every setting must give the same film bit for bit, and the same ray
+counts.
+"""
+from __future__ import annotations
+
+import numpy as np
+import pytest
+
+from cenote_b200 import SORT_ALL, SORT_NONE, SORT_SECONDARY, scenes
+
+pytestmark = pytest.mark.gpu
+
+
+def run(ctx, spec, mode, spp, bounces, spw=0):
+    from cenote_b200 import Film, Renderer, Scene
+
+    r = Renderer(ctx, bounces, samples_per_wave=spw, material_sort=mode)
+    f = Film(ctx, spec.width, spec.height)
+    r.accumulate(Scene(ctx, spec), f, spp)
+    st = r.stats()
+    return f.all_averages(), (st["extension_rays"], st["shadow_rays"], st["overflow"])
+
+
+@pytest.mark.parametrize("name", ["cornell", "chart", "textured"])
+def test_every_sort_mode_gives_the_same_film(ctx, name):
+    spec = {"cornell": lambda: scenes.cornell(64, 64, 8, 8), "chart": lambda: scenes.chart(96, 54, 4, 8),
+            "textured": lambda: scenes.textured(64, 48, 4, 6)}[name]()
+    base, counts = run(ctx, spec, SORT_NONE, spec.spp, spec.max_bounces)
+    assert counts[2] == 0
+    for mode in (SORT_ALL, SORT_SECONDARY):
+        got, c = run(ctx, spec, mode, spec.spp, spec.max_bounces, spw=2)
+        assert c == counts
+        for k in base:
+            assert np.array_equal(got[k], base[k], equal_nan=True), (mode, k)
+
+
+def test_sorted_render_once_matches(ctx):
+    from cenote_b200 import Renderer, Scene
+
+    spec = scenes.cornell(40, 30, 1, 8)
+    scene = Scene(ctx, spec)
+    a = Renderer(ctx, 8).render(scene, 40, 30, 3)
+    b = Renderer(ctx, 8, material_sort=SORT_ALL).render(scene, 40, 30, 3)
+    assert np.array_equal(a, b)
+
+
+def test_unknown_mode_is_refused(ctx):
+    from cenote_b200 import CenoteError, Renderer
+
+    with pytest.raises(CenoteError):
+        Renderer(ctx, 4).set_material_sort(3)
+
+
+def test_tuning_knobs_leave_the_film_unchanged(ctx):
+    from cenote_b200 import Film, Renderer, Scene
+
+    spec = scenes.chart(96, 54, 4, 8)
+    scene = Scene(ctx, spec)
+    films = []
+    for knobs in [(SORT_NONE, 0, 0), (SORT_ALL, 1, 4), (SORT_SECONDARY, 4, 16), (SORT_ALL, 2, 32)]:
+        r = Renderer(ctx, 8)
+        r.set_tuning(*knobs)
+        f = Film(ctx, spec.width, spec.height)
+        r.accumulate(scene, f, 4)
+        films.append(f.averages())
+    for f in films[1:]:
+        assert np.array_equal(f, films[0])
+
+
+def test_autotune_picks_a_valid_setting_and_keeps_it(ctx):
+    from cenote_b200 import Film, Renderer, Scene
+
+    spec = scenes.cornell(128, 96, 8, 8)
+    scene = Scene(ctx, spec)
+    r = Renderer(ctx, 8)
+    t = r.autotune(scene, spec.width, spec.height)
+    assert t["material_sort"] in (SORT_NONE, SORT_ALL, SORT_SECONDARY)
+    assert t["refill_idle"] in (0, 4, 8, 16) and t["ms_per_sample"] > 0
+    kept = r.tuning()
+    assert {k: kept[k] for k in ("material_sort", "samples_per_wave", "refill_idle")} == \
+        {k: t[k] for k in ("material_sort", "samples_per_wave", "refill_idle")}
+    f, g = Film(ctx, spec.width, spec.height), Film(ctx, spec.width, spec.height)
+    r.accumulate(scene, f, 8)
+    Renderer(ctx, 8).accumulate(scene, g, 8)
+    assert np.array_equal(f.averages(), g.averages())
+
+
+def test_bad_tuning_is_refused(ctx):
+    from cenote_b200 import CenoteError, Renderer
+
+    r = Renderer(ctx, 4)
+    with pytest.raises(CenoteError):
+        r.set_tuning(SORT_ALL, 0, 33)
