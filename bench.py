@@ -313,6 +313,9 @@ def main():
     ap.add_argument("--scene", default="large", choices=["large", "ceiling_box"], help="guiding: the scene")
     ap.add_argument("--spp", type=int, default=0, help="override the workload's spp (profiling runs)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--material-sort", type=int, default=None, choices=[0, 1, 2],
+                    help="fix the material sort (0 off, 1 every bounce, 2 from the first bounce on) "
+                         "instead of autotuning the launch knobs")
     args = ap.parse_args()
     if args.workload == "serving":
         run_serving(args)
@@ -347,6 +350,13 @@ def main():
     prep_wall_ms = (time.perf_counter() - t0) * 1e3
     prep = scene.prep_times_ms()
     r = Renderer(ctx, maxb)
+    t_tune = time.perf_counter()
+    if args.material_sort is None:
+        tuning = r.autotune(scene, W, H)  # per-scene launch knobs, outside the timed region
+    else:
+        r.set_tuning(args.material_sort)
+        tuning = r.tuning()
+    tune_s = time.perf_counter() - t_tune
     film = Film(ctx, W, H)
     stream = torch.cuda.ExternalStream(ctx.stream)
 
@@ -448,6 +458,13 @@ def main():
                    "l2": "256 MB buffer written between timed steps (L2 flush); the path pool per wave also "
                          "exceeds L2",
                    "samples_per_wave": counts["samples_per_wave"], "waves_per_step": counts["waves"],
+                   "tuning": {"material_sort": ["off", "every bounce", "secondary bounces"][tuning["material_sort"]],
+                              "samples_per_wave": tuning["samples_per_wave"] or "automatic",
+                              "refill_idle": tuning["refill_idle"] or 8,
+                              "top_nodes_in_shared_memory": tuning["top_nodes"],
+                              "l2_persisting_bvh": bool(tuning["l2_window"]),
+                              "chosen_by": "autotuner" if args.material_sort is None else "flag",
+                              "autotune_s": round(tune_s, 3)},
                    "guides": "albedo, normal and depth traced and accumulated every sample, as Renderer::accumulate does"},
         "e2e": {"value": e2e_value, "unit": "Msamples/s", "ms_per_step": e2e_step,
                 "h2d_bytes_per_step": 48, "d2h_bytes_per_step": W * H * 16},

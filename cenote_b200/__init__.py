@@ -82,6 +82,11 @@ class DeltaLightC(C.Structure):
     _fields_ = [("kind", C.c_uint32), ("anchor", C.c_float * 3), ("emission", C.c_float * 3)]
 
 
+class TuningC(C.Structure):
+    _fields_ = [("material_sort", C.c_uint32), ("samples_per_wave", C.c_uint32), ("refill_idle", C.c_uint32),
+                ("top_nodes", C.c_uint32), ("l2_window", C.c_uint32), ("ms_per_sample", C.c_float)]
+
+
 class Options(C.Structure):
     _fields_ = [("device", C.c_int32)]
 
@@ -120,7 +125,8 @@ EXPORTED_SYMBOLS = [
     "cenote_guide_destroy", "cenote_guide_params", "cenote_guide_set_params", "cenote_guide_forward",
     "cenote_guide_train_step", "cenote_renderer_set_guide", "cenote_accumulate_range", "cenote_film_tonemap",
     "cenote_film_tonemap_device", "cenote_film_restore",
-    "cenote_scene_add_delta_light",
+    "cenote_scene_add_delta_light", "cenote_renderer_set_material_sort", "cenote_renderer_set_tuning",
+    "cenote_renderer_get_tuning", "cenote_renderer_autotune",
 ]
 
 _lib = None
@@ -166,6 +172,10 @@ def library() -> C.CDLL:
         "cenote_film_tonemap_device": (I32, [P, F, P]),
         "cenote_film_restore": (I32, [P, P, U32]),
         "cenote_scene_add_delta_light": (I32, [P, P]),
+        "cenote_renderer_set_material_sort": (I32, [P, U32]),
+        "cenote_renderer_set_tuning": (I32, [P, P]),
+        "cenote_renderer_get_tuning": (I32, [P, P]),
+        "cenote_renderer_autotune": (I32, [P, P, U32, U32, P]),
         "cenote_scene_destroy": (None, [P]),
         "cenote_scene_set_camera": (I32, [P, P]),
         "cenote_scene_prep_times": (I32, [P, P]),
@@ -543,17 +553,22 @@ class Film:
             pass
 
 
+SORT_NONE, SORT_ALL, SORT_SECONDARY = 0, 1, 2
+
+
 class Renderer:
     """Renderer::with_max_bounces + LightSampling: the wavefront engine."""
 
     def __init__(self, ctx: Context, max_bounces: int = 8, light_sampling: int = LIGHT_SAMPLING_MIS,
-                 capacity: int = 0, samples_per_wave: int = 0):
+                 capacity: int = 0, samples_per_wave: int = 0, material_sort: int | None = None):
         h = C.c_void_p()
         _check(library().cenote_renderer_create(ctx.handle, max_bounces, light_sampling, capacity, C.byref(h)))
         self._h = h
         self.ctx = ctx
         if samples_per_wave:
             self.set_samples_per_wave(samples_per_wave)
+        if material_sort is not None:
+            self.set_material_sort(material_sort)
 
     @property
     def handle(self):
@@ -561,6 +576,26 @@ class Renderer:
 
     def set_samples_per_wave(self, n: int) -> None:
         _check(library().cenote_renderer_set_samples_per_wave(self._h, n))
+
+    def set_material_sort(self, mode: int) -> None:
+        """SORT_NONE, SORT_ALL or SORT_SECONDARY: shade each bounce's paths in material order."""
+        _check(library().cenote_renderer_set_material_sort(self._h, mode))
+
+    def tuning(self) -> dict:
+        t = TuningC()
+        _check(library().cenote_renderer_get_tuning(self._h, C.byref(t)))
+        return {name: getattr(t, name) for name, _ in TuningC._fields_}
+
+    def set_tuning(self, material_sort: int, samples_per_wave: int = 0, refill_idle: int = 0,
+                   top_nodes: int = 0, l2_window: int = 0) -> None:
+        t = TuningC(material_sort, samples_per_wave, refill_idle, top_nodes, l2_window, 0.0)
+        _check(library().cenote_renderer_set_tuning(self._h, C.byref(t)))
+
+    def autotune(self, scene: Scene, width: int, height: int) -> dict:
+        """Time the launch knobs on `scene` at width x height, keep the fastest and return it."""
+        t = TuningC()
+        _check(library().cenote_renderer_autotune(self._h, scene.handle, width, height, C.byref(t)))
+        return {name: getattr(t, name) for name, _ in TuningC._fields_}
 
     def render(self, scene: Scene, width: int, height: int, sample: int = 0) -> np.ndarray:
         out = np.zeros((height, width, 4), np.float32)

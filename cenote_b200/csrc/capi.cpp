@@ -259,6 +259,8 @@ int32_t cenote_context_create(const cenote_options* options, cenote_context** ou
     CN_CUDA(cudaEventCreate(&ctx->t0));
     CN_CUDA(cudaEventCreate(&ctx->t1));
     ctx->shape = launch_shape(dev);
+    ctx->l2_persist_max = size_t(prop.persistingL2CacheMaxSize);
+    ctx->l2_window_max = size_t(prop.accessPolicyMaxWindowSize);
     CN_CUDA(ctx->tables.alloc(sizeof(kTables)));
     CN_CUDA(cudaMemcpy(ctx->tables.ptr, kTables, sizeof(kTables), cudaMemcpyHostToDevice));
     *out = ctx.release();
@@ -752,6 +754,38 @@ int32_t cenote_renderer_set_guide(cenote_renderer* r, cenote_guide* g, float fra
     return CENOTE_OK;
 }
 
+int32_t cenote_renderer_set_material_sort(cenote_renderer* r, uint32_t mode) {
+    CN_CHECK(r, CENOTE_E_INVALID_ARGUMENT, "null renderer");
+    CN_CHECK(mode <= CENOTE_SORT_SECONDARY, CENOTE_E_INVALID_ARGUMENT, "unknown material-sort mode");
+    r->material_sort = mode;
+    return CENOTE_OK;
+}
+
+int32_t cenote_renderer_set_tuning(cenote_renderer* r, const cenote_tuning* t) {
+    CN_CHECK(r && t, CENOTE_E_INVALID_ARGUMENT, "null argument");
+    CN_CHECK(t->material_sort <= CENOTE_SORT_SECONDARY, CENOTE_E_INVALID_ARGUMENT, "unknown material-sort mode");
+    CN_CHECK(t->refill_idle <= 32, CENOTE_E_INVALID_ARGUMENT, "refill threshold above a warp");
+    CN_CHECK(t->top_nodes <= TOP_NODES_MAX, CENOTE_E_INVALID_ARGUMENT, "more top-level nodes than shared memory holds");
+    CN_CHECK(t->l2_window <= 1, CENOTE_E_INVALID_ARGUMENT, "l2_window is 0 or 1");
+    r->material_sort = t->material_sort;
+    r->samples_per_wave = t->samples_per_wave;
+    r->refill_idle = t->refill_idle;
+    r->top_nodes = t->top_nodes;
+    r->l2_window = t->l2_window;
+    return CENOTE_OK;
+}
+
+int32_t cenote_renderer_get_tuning(cenote_renderer* r, cenote_tuning* out) {
+    CN_CHECK(r && out, CENOTE_E_INVALID_ARGUMENT, "null argument");
+    out->material_sort = r->material_sort;
+    out->samples_per_wave = r->samples_per_wave;
+    out->refill_idle = r->refill_idle;
+    out->top_nodes = r->top_nodes;
+    out->l2_window = r->l2_window;
+    out->ms_per_sample = r->tuned_ms_per_sample;
+    return CENOTE_OK;
+}
+
 int32_t cenote_renderer_set_profiling(cenote_renderer* r, uint32_t flags) {
     CN_CHECK(r, CENOTE_E_INVALID_ARGUMENT, "null renderer");
     CN_CHECK((flags & ~3u) == 0, CENOTE_E_INVALID_ARGUMENT, "unknown profiling flag");
@@ -822,9 +856,47 @@ namespace {
 // The blocking form behind cenote_accumulate_n and cenote_render_once: plan,
 // enqueue on the context's stream, wait, then fold the counters and stage
 // timings into the renderer's stats.
+// While alive, the scene's wide BVH nodes are a persisting access-policy
+// window on the context's stream: the waves' streaming path state does not
+// evict them from L2. The window is cleared and the persisting lines are
+// released on exit.
+struct L2Window {
+    cudaStream_t stream = nullptr;
+    L2Window(cenote_context* ctx, const cenote_scene* sc, bool on) {
+        const size_t bytes = std::min(size_t(sc->ds.node_count) * sizeof(WideNode), ctx->l2_window_max);
+        if (!on || bytes == 0 || ctx->l2_persist_max == 0) return;
+        const size_t want = std::min(bytes, ctx->l2_persist_max);
+        if (ctx->l2_set_aside < want) {
+            if (cudaDeviceSetLimit(cudaLimitPersistingL2CacheSize, want) != cudaSuccess) {
+                cudaGetLastError();
+                return;
+            }
+            ctx->l2_set_aside = want;
+        }
+        cudaStreamAttrValue a{};
+        a.accessPolicyWindow.base_ptr = const_cast<WideNode*>(sc->ds.nodes);
+        a.accessPolicyWindow.num_bytes = bytes;
+        a.accessPolicyWindow.hitRatio = std::min(1.0f, float(ctx->l2_set_aside) / float(bytes));
+        a.accessPolicyWindow.hitProp = cudaAccessPropertyPersisting;
+        a.accessPolicyWindow.missProp = cudaAccessPropertyStreaming;
+        if (cudaStreamSetAttribute(ctx->stream, cudaStreamAttributeAccessPolicyWindow, &a) == cudaSuccess)
+            stream = ctx->stream;
+        else
+            cudaGetLastError();
+    }
+    ~L2Window() {
+        if (!stream) return;
+        cudaStreamAttrValue a{};
+        a.accessPolicyWindow.num_bytes = 0;
+        cudaStreamSetAttribute(stream, cudaStreamAttributeAccessPolicyWindow, &a);
+        cudaCtxResetPersistingL2Cache();
+    }
+};
+
 int32_t run_waves(cenote_renderer* r, cenote_scene* sc, uint32_t width, uint32_t height, uint32_t sample0,
                   uint32_t count, cenote_film* film, float4* oneshot) {
     cenote_context* ctx = r->ctx;
+    L2Window l2(ctx, sc, r->l2_window != 0);
     const uint64_t pixels = uint64_t(width) * height;
     WavePlan plan = plan_waves(r, pixels, count, oneshot != nullptr);
     CN_CHECK(plan.need < (1ull << 31), CENOTE_E_INVALID_ARGUMENT, "wave too large");
@@ -885,6 +957,79 @@ int32_t run_waves(cenote_renderer* r, cenote_scene* sc, uint32_t width, uint32_t
 }
 
 }  // namespace
+
+int32_t cenote_renderer_autotune(cenote_renderer* r, cenote_scene* scene, uint32_t width, uint32_t height,
+                                 cenote_tuning* out) {
+    CN_CHECK(r && scene && width > 0 && height > 0, CENOTE_E_INVALID_ARGUMENT, "null handle or empty target");
+    CN_CHECK(r->ctx == scene->ctx, CENOTE_E_INVALID_ARGUMENT, "handles from different contexts");
+    cenote_film* film = nullptr;
+    int32_t rc = cenote_film_create(r->ctx, width, height, &film);
+    if (rc != CENOTE_OK) return rc;
+    std::unique_ptr<cenote_film, void (*)(cenote_film*)> hold(film, cenote_film_destroy);
+    std::lock_guard<std::mutex> lock(r->ctx->mu);
+    CN_CUDA(cudaSetDevice(r->ctx->device));
+    const uint64_t pixels = uint64_t(width) * height;
+    // The automatic wave size (plan_waves), its half, and 2x, 4x and 8x,
+    // bounded by 64 M paths (about 16 GB of path state).
+    const uint32_t auto_spw = uint32_t(std::max<uint64_t>(1, std::min<uint64_t>((uint64_t(1) << 24) / pixels, 64)));
+    const uint32_t spw_cap = uint32_t(std::max<uint64_t>(1, std::min<uint64_t>((uint64_t(1) << 26) / pixels, 256)));
+    const uint32_t spws[5] = {0, std::max(1u, auto_spw / 2), std::min(spw_cap, auto_spw * 2),
+                              std::min(spw_cap, auto_spw * 4), std::min(spw_cap, auto_spw * 8)};
+    // Probe length: two waves of the largest candidate, at most ~128 M samples.
+    uint32_t probe = std::max(2u, 2 * spws[4]);
+    while (probe > 2 && pixels * probe > (uint64_t(1) << 27)) probe /= 2;
+    const uint32_t saved_profiling = r->profiling;
+    r->profiling = 0;
+    cenote_tuning best{r->material_sort, r->samples_per_wave, r->refill_idle, r->top_nodes, r->l2_window, 0.0f};
+    auto apply = [&](const cenote_tuning& t) {
+        r->material_sort = t.material_sort;
+        r->samples_per_wave = t.samples_per_wave;
+        r->refill_idle = t.refill_idle;
+        r->top_nodes = t.top_nodes;
+        r->l2_window = t.l2_window;
+    };
+    // Device time of `probe` samples, the better of two runs (the first run of
+    // a new wave size also allocates).
+    auto measure = [&](const cenote_tuning& t, float* ms) -> int32_t {
+        apply(t);
+        float m = 1e30f;
+        for (int k = 0; k < 2; ++k) {
+            int32_t e = run_waves(r, scene, width, height, 1u << 30, probe, film, nullptr);
+            if (e != CENOTE_OK) return e;
+            m = std::min(m, r->stats.gpu_ms);
+        }
+        *ms = m;
+        return CENOTE_OK;
+    };
+    float best_ms = 0.0f;
+    rc = measure(best, &best_ms);
+    for (int knob = 0; knob < 5 && rc == CENOTE_OK; ++knob) {
+        for (int c = 0; c < (knob == 1 ? 5 : (knob == 4 ? 2 : 3)) && rc == CENOTE_OK; ++c) {
+            cenote_tuning t = best;
+            if (knob == 0) t.material_sort = uint32_t(c);
+            if (knob == 1) t.samples_per_wave = spws[c];
+            if (knob == 2) t.refill_idle = c == 0 ? 4u : (c == 1 ? 8u : 16u);
+            if (knob == 3) t.top_nodes = c == 0 ? 0u : (c == 1 ? 80u : TOP_NODES_MAX);
+            if (knob == 4) t.l2_window = uint32_t(c);
+            if (t.material_sort == best.material_sort && t.samples_per_wave == best.samples_per_wave &&
+                t.refill_idle == best.refill_idle && t.top_nodes == best.top_nodes && t.l2_window == best.l2_window)
+                continue;
+            float ms = 0.0f;
+            rc = measure(t, &ms);
+            if (rc == CENOTE_OK && ms < best_ms) {
+                best = t;
+                best_ms = ms;
+            }
+        }
+    }
+    r->profiling = saved_profiling;
+    apply(best);
+    if (rc != CENOTE_OK) return rc;
+    best.ms_per_sample = best_ms / float(probe);
+    r->tuned_ms_per_sample = best.ms_per_sample;
+    if (out) *out = best;
+    return CENOTE_OK;
+}
 
 int32_t cenote_accumulate_n(cenote_renderer* r, cenote_scene* scene, cenote_film* film, uint32_t count) {
     CN_CHECK(r && scene && film, CENOTE_E_INVALID_ARGUMENT, "null argument");

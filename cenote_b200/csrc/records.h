@@ -102,6 +102,11 @@ struct DeviceScene {
     uint32_t pad2;
     float bbox_min[3];    // world bounds of every triangle, for the guide's position encoding
     float bbox_inv;       // 1 / the bounds' largest extent
+    // Set inside a traversal kernel (0 elsewhere): nodes 0..top_count-1 (the
+    // BVH's top levels: the builder lays nodes out breadth first) are staged
+    // in the block's shared memory at shared-window address top_smem.
+    uint32_t top_count;
+    uint32_t top_smem;
 };
 
 // One queued shadow ray: 64 bytes, four 16-byte lanes.

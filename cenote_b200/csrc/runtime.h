@@ -89,6 +89,8 @@ struct cenote_context {
     LaunchShape shape{};
     cn::DeviceBuffer tables;
     std::mutex mu;
+    // L2 persistence (this context's own set-aside; nothing outlives it).
+    size_t l2_persist_max = 0, l2_window_max = 0, l2_set_aside = 0;
 };
 
 struct cenote_scene {
@@ -134,6 +136,15 @@ struct cenote_renderer {
     std::vector<cudaEvent_t> events;
     PathPool pool{};
     DeviceBuffer org, dir, thr, hit, ps, state, rad, q0, q1, shadows, counters, tally, scratch;
+    // Material sort before shading: CENOTE_SORT_NONE, _ALL or _SECONDARY
+    // (every bounce by default: 1.1x on the material chart, 1.6x on the
+    // textured 2 M-triangle terrain, measured on a B200).
+    uint32_t material_sort = 1;
+    uint32_t refill_idle = 0;  // 0: the kernels' default
+    uint32_t top_nodes = 0;    // BVH nodes staged in shared memory by the traversal kernels
+    uint32_t l2_window = 0;    // mark the BVH nodes persisting in L2 during this renderer's waves
+    float tuned_ms_per_sample = 0.0f;
+    DeviceBuffer sort_order, sort_keys, sort_bins;
     DeviceBuffer aov_albedo, aov_normal, aov_depth, aov_guide;
     size_t pool_cap = 0, aov_cap = 0;
     // The learned guide (cenote_renderer_set_guide): per-path mixture outputs
@@ -166,7 +177,8 @@ struct cenote_renderer {
         if ((e = org.alloc(cap * 16)) || (e = dir.alloc(cap * 16)) || (e = thr.alloc(cap * 16)) ||
             (e = hit.alloc(cap * 16)) || (e = ps.alloc(cap * 8)) || (e = state.alloc(cap * 4)) ||
             (e = rad.alloc(cap * 16)) || (e = q0.alloc(cap * 4)) || (e = q1.alloc(cap * 4)) ||
-            (e = shadows.alloc(cap * sizeof(ShadowRay))))
+            (e = shadows.alloc(cap * sizeof(ShadowRay))) || (e = sort_order.alloc(cap * 4)) ||
+            (e = sort_keys.alloc(cap * 4)) || (e = sort_bins.alloc(cn::SORT_BINS * 4)))
             return e;
         pool.org = org.as<float4>();
         pool.dir = dir.as<float4>();
@@ -178,6 +190,9 @@ struct cenote_renderer {
         pool.queue[0] = q0.as<uint32_t>();
         pool.queue[1] = q1.as<uint32_t>();
         pool.shadows = shadows.as<ShadowRay>();
+        pool.order = nullptr;  // set per bounce by the wave loop when sorting
+        pool.sort_keys = sort_keys.as<uint32_t>();
+        pool.sort_bins = sort_bins.as<uint32_t>();
         pool.capacity = uint32_t(cap);
         pool_cap = cap;
         return cudaSuccess;

@@ -95,10 +95,47 @@ __device__ __forceinline__ uint32_t byte_of(uint32_t lo4, uint32_t hi4, int i) {
 
 // Intersect the eight children of node `ni`. Returns the hit mask; fills the
 // node's child/triangle base indices and inner mask.
-__device__ __forceinline__ uint32_t intersect_node(const WideNode* nodes, uint32_t ni, const Ray& r, float tmax,
+__device__ __forceinline__ uint4 ld_shared4(uint32_t addr) {
+    uint4 v;
+#ifdef __CUDA_ARCH__
+    asm("ld.shared.v4.u32 {%0, %1, %2, %3}, [%4];" : "=r"(v.x), "=r"(v.y), "=r"(v.z), "=r"(v.w) : "r"(addr));
+#else
+    v = make_uint4(0u, 0u, 0u, 0u);
+#endif
+    return v;
+}
+
+// Copy the first `limit` nodes (at most the scene's) into `smem` for the
+// whole block and record them in `s`; every thread of the block must call it.
+__device__ __forceinline__ void stage_top_levels(DeviceScene& s, uint4* smem, uint32_t limit) {
+#ifdef __CUDA_ARCH__
+    const uint32_t n = min(s.node_count, limit);
+    const uint4* src = reinterpret_cast<const uint4*>(s.nodes);
+    for (uint32_t k = threadIdx.x; k < 5u * n; k += blockDim.x) smem[k] = __ldg(src + k);
+    __syncthreads();
+    s.top_count = n;
+    s.top_smem = uint32_t(__cvta_generic_to_shared(smem));
+#endif
+}
+
+__device__ __forceinline__ uint32_t intersect_node(const DeviceScene& s, uint32_t ni, const Ray& r, float tmax,
                                                    uint32_t& base_child, uint32_t& base_tri, uint32_t& imask) {
-    const uint4* q = reinterpret_cast<const uint4*>(nodes + ni);
-    uint4 n0 = __ldg(q), n1 = __ldg(q + 1), n2 = __ldg(q + 2), n3 = __ldg(q + 3), n4 = __ldg(q + 4);
+    uint4 n0, n1, n2, n3, n4;
+    if (ni < s.top_count) {
+        const uint32_t a = s.top_smem + 80u * ni;
+        n0 = ld_shared4(a);
+        n1 = ld_shared4(a + 16u);
+        n2 = ld_shared4(a + 32u);
+        n3 = ld_shared4(a + 48u);
+        n4 = ld_shared4(a + 64u);
+    } else {
+        const uint4* q = reinterpret_cast<const uint4*>(s.nodes + ni);
+        n0 = __ldg(q);
+        n1 = __ldg(q + 1);
+        n2 = __ldg(q + 2);
+        n3 = __ldg(q + 3);
+        n4 = __ldg(q + 4);
+    }
     float3 p = f3(__uint_as_float(n0.x), __uint_as_float(n0.y), __uint_as_float(n0.z));
     float sx = __uint_as_float((n0.w & 0xffu) << 23);
     float sy = __uint_as_float(((n0.w >> 8) & 0xffu) << 23);
@@ -193,7 +230,7 @@ __device__ __forceinline__ int walk_step(const DeviceScene& s, const Ray& r, flo
             stack[w.sp++] = w.g;
         }
         uint32_t bc, bt, im;
-        uint32_t hits = intersect_node(s.nodes, ni, r, tmax, bc, bt, im);
+        uint32_t hits = intersect_node(s, ni, r, tmax, bc, bt, im);
         if (COUNT) ++*visits;
         w.g = make_uint2(bc, (hits & 0xff000000u) | im);
         w.t = make_uint2(bt, hits & 0x00ffffffu);

@@ -160,6 +160,8 @@ __device__ __forceinline__ uint32_t refill(uint32_t* counter, uint32_t count, bo
 
 template <bool COUNT>
 __global__ void __launch_bounds__(BLOCK, CN_TRAV_MIN_BLOCKS) k_intersect(DeviceScene scene, PathPool pool, uint32_t bounce, uint32_t n0) {
+    extern __shared__ uint4 top_levels[];
+    stage_top_levels(scene, top_levels, min(pool.top_nodes, TOP_NODES_MAX));  // as the launch sized it
     uint32_t visits = 0, tests = 0;
     const uint32_t count = min(bounce == 0 ? n0 : pool.counters[CTR_RAYS + bounce], pool.capacity);
     const uint32_t* queue = pool.queue[bounce & 1u];
@@ -221,7 +223,7 @@ __global__ void __launch_bounds__(BLOCK, CN_TRAV_MIN_BLOCKS) k_intersect(DeviceS
             continue;
         }
         // Walk until enough lanes are idle to refill (all of them once drained).
-        const uint32_t want_idle = drained ? 32u : uint32_t(CN_REFILL_IDLE);
+        const uint32_t want_idle = drained ? 32u : (pool.refill_idle ? pool.refill_idle : uint32_t(CN_REFILL_IDLE));
         for (;;) {
             if (live) {
                 int st = walk_step<COUNT>(scene, ray, tmax, w, stack, visit, &visits, &tests);
@@ -344,7 +346,7 @@ __global__ void __launch_bounds__(BLOCK, CN_SHADE_MIN_BLOCKS) k_shade(DeviceScen
         uint32_t path = 0;
         ShadowRay sr;
         if (i < count) {
-            path = bounce == 0 ? i : queue[i];
+            path = pool.order ? pool.order[i] : (bounce == 0 ? i : queue[i]);
             uint4 h = pool.hit[path];
             float4 d4 = pool.dir[path];
             float3 dir = xyz(d4);
@@ -607,6 +609,8 @@ __global__ void __launch_bounds__(BLOCK, CN_SHADE_MIN_BLOCKS) k_shade(DeviceScen
 
 template <bool COUNT>
 __global__ void __launch_bounds__(BLOCK, CN_TRAV_MIN_BLOCKS) k_shadow(DeviceScene scene, PathPool pool, uint32_t bounce) {
+    extern __shared__ uint4 top_levels[];
+    stage_top_levels(scene, top_levels, min(pool.top_nodes, TOP_NODES_MAX));  // as the launch sized it
     const uint32_t count = min(pool.counters[CTR_SHADOWS + bounce], pool.capacity);
     uint32_t* fetch = pool.counters + CTR_FETCH_SHADOW + bounce;
     uint32_t visits = 0, tests = 0;
@@ -633,7 +637,7 @@ __global__ void __launch_bounds__(BLOCK, CN_TRAV_MIN_BLOCKS) k_shadow(DeviceScen
             if (drained) break;
             continue;
         }
-        const uint32_t want_idle = drained ? 32u : uint32_t(CN_REFILL_IDLE);
+        const uint32_t want_idle = drained ? 32u : (pool.refill_idle ? pool.refill_idle : uint32_t(CN_REFILL_IDLE));
         for (;;) {
             if (live) {
                 int st = shadow_step<COUNT>(scene, ray, q, stack, &visits, &tests);
@@ -758,6 +762,87 @@ __global__ void k_copy_rad(const float4* __restrict__ rad, float4* __restrict__ 
         out[base + p] = rad[p];
 }
 
+// ---- material sort -----------------------------------------------------------------
+// Shading in key order keeps a warp on one material: one closure path, one
+// set of textures, neighbouring vertices. Keys are counted with one atomic
+// per distinct key per warp (__match_any_sync), the counts become offsets in
+// one block, and the scatter hands each key's paths consecutive slots.
+
+__device__ __forceinline__ uint32_t sort_count(const PathPool& pool, uint32_t bounce, uint32_t n0) {
+    return min(bounce == 0 ? n0 : pool.counters[CTR_RAYS + bounce], pool.capacity);
+}
+
+__global__ void __launch_bounds__(BLOCK) k_sort_keys(PathPool pool, uint32_t bounce, uint32_t n0) {
+    const uint32_t count = sort_count(pool, bounce, n0);
+    const uint32_t* queue = pool.queue[bounce & 1u];
+    const uint32_t* hit_inst = reinterpret_cast<const uint32_t*>(pool.hit);
+    const uint32_t stride = gridDim.x * blockDim.x;
+    for (uint32_t base = blockIdx.x * blockDim.x + (threadIdx.x & ~31u); base < count; base += stride) {
+        const uint32_t i = base + lane_id();
+        const bool valid = i < count;
+        uint32_t key = 0xffffffffu;
+        if (valid) {
+            const uint32_t path = bounce == 0 ? i : queue[i];
+            const uint32_t inst = hit_inst[4u * size_t(path)];
+            key = inst == LIGHT_NONE ? 0u : 1u + inst % (SORT_BINS - 1u);
+            pool.sort_keys[i] = key;
+        }
+        const uint32_t peers = __match_any_sync(0xffffffffu, key);
+        if (valid && lane_id() == uint32_t(__ffs(peers) - 1)) atomicAdd(pool.sort_bins + key, uint32_t(__popc(peers)));
+    }
+}
+
+// One block of 1024 threads: exclusive prefix sums of the SORT_BINS counts.
+__global__ void __launch_bounds__(1024) k_sort_scan(uint32_t* bins) {
+    constexpr uint32_t PER = SORT_BINS / 1024u;
+    __shared__ uint32_t warp_sums[32];
+    uint32_t v[PER], local = 0;
+#pragma unroll
+    for (uint32_t k = 0; k < PER; ++k) {
+        v[k] = bins[threadIdx.x * PER + k];
+        local += v[k];
+    }
+    uint32_t incl = local;
+    for (int o = 1; o < 32; o <<= 1) {
+        uint32_t y = __shfl_up_sync(0xffffffffu, incl, o);
+        if (lane_id() >= uint32_t(o)) incl += y;
+    }
+    if (lane_id() == 31u) warp_sums[threadIdx.x >> 5] = incl;
+    __syncthreads();
+    if (threadIdx.x < 32) {
+        uint32_t w = warp_sums[threadIdx.x], wi = w;
+        for (int o = 1; o < 32; o <<= 1) {
+            uint32_t y = __shfl_up_sync(0xffffffffu, wi, o);
+            if (lane_id() >= uint32_t(o)) wi += y;
+        }
+        warp_sums[threadIdx.x] = wi - w;
+    }
+    __syncthreads();
+    uint32_t run = warp_sums[threadIdx.x >> 5] + incl - local;
+#pragma unroll
+    for (uint32_t k = 0; k < PER; ++k) {
+        bins[threadIdx.x * PER + k] = run;
+        run += v[k];
+    }
+}
+
+__global__ void __launch_bounds__(BLOCK) k_sort_scatter(PathPool pool, uint32_t bounce, uint32_t n0) {
+    const uint32_t count = sort_count(pool, bounce, n0);
+    const uint32_t* queue = pool.queue[bounce & 1u];
+    const uint32_t stride = gridDim.x * blockDim.x;
+    for (uint32_t base = blockIdx.x * blockDim.x + (threadIdx.x & ~31u); base < count; base += stride) {
+        const uint32_t i = base + lane_id();
+        const bool valid = i < count;
+        const uint32_t key = valid ? pool.sort_keys[i] : 0xffffffffu;
+        const uint32_t peers = __match_any_sync(0xffffffffu, key);
+        const uint32_t leader = uint32_t(__ffs(peers) - 1);
+        uint32_t slot = 0;
+        if (valid && lane_id() == leader) slot = atomicAdd(pool.sort_bins + key, uint32_t(__popc(peers)));
+        slot = __shfl_sync(0xffffffffu, slot, leader);
+        if (valid) pool.order[slot + __popc(peers & ((1u << lane_id()) - 1u))] = bounce == 0 ? i : queue[i];
+    }
+}
+
 // Fold one wave's queue counters into the renderer's running totals:
 // tally[0] += extension rays, tally[1] += shadow rays, tally[2] |= overflow.
 __global__ void k_tally(const uint32_t* counters, unsigned long long* tally, uint32_t n0, uint32_t max_bounces) {
@@ -793,11 +878,11 @@ LaunchShape launch_shape(int device) {
     LaunchShape ls;
     ls.block = BLOCK;
     int occ = 0;
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_intersect<false>, BLOCK, 0);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_intersect<false>, BLOCK, TOP_NODES_MAX * 80u);
     ls.grid_isect = sms * (occ > 0 ? occ : 4);
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_shade<true, false>, BLOCK, 0);
     ls.grid_shade = sms * (occ > 0 ? occ : 4);
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_shadow<false>, BLOCK, 0);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_shadow<false>, BLOCK, TOP_NODES_MAX * 80u);
     ls.grid_shadow = sms * (occ > 0 ? occ : 4);
     ls.grid_stream = sms * 8;
     return ls;
@@ -810,8 +895,9 @@ void launch_wave_begin(const PathPool& pool, const WaveParams& wp, const LaunchS
 
 void launch_intersect(const DeviceScene& scene, const PathPool& pool, uint32_t bounce, uint32_t n0,
                       const LaunchShape& ls, bool count_visits, cudaStream_t stream) {
-    if (count_visits) k_intersect<true><<<ls.grid_isect, BLOCK, 0, stream>>>(scene, pool, bounce, n0);
-    else k_intersect<false><<<ls.grid_isect, BLOCK, 0, stream>>>(scene, pool, bounce, n0);
+    const size_t smem = size_t(min(pool.top_nodes, TOP_NODES_MAX)) * 80u;
+    if (count_visits) k_intersect<true><<<ls.grid_isect, BLOCK, smem, stream>>>(scene, pool, bounce, n0);
+    else k_intersect<false><<<ls.grid_isect, BLOCK, smem, stream>>>(scene, pool, bounce, n0);
 }
 
 void launch_shade(const DeviceScene& scene, const PathPool& pool, uint32_t bounce, const WaveParams& wp, uint32_t n0,
@@ -828,8 +914,9 @@ void launch_shade(const DeviceScene& scene, const PathPool& pool, uint32_t bounc
 
 void launch_shadow(const DeviceScene& scene, const PathPool& pool, uint32_t bounce, const LaunchShape& ls,
                    bool count_visits, cudaStream_t stream) {
-    if (count_visits) k_shadow<true><<<ls.grid_shadow, BLOCK, 0, stream>>>(scene, pool, bounce);
-    else k_shadow<false><<<ls.grid_shadow, BLOCK, 0, stream>>>(scene, pool, bounce);
+    const size_t smem = size_t(min(pool.top_nodes, TOP_NODES_MAX)) * 80u;
+    if (count_visits) k_shadow<true><<<ls.grid_shadow, BLOCK, smem, stream>>>(scene, pool, bounce);
+    else k_shadow<false><<<ls.grid_shadow, BLOCK, smem, stream>>>(scene, pool, bounce);
 }
 
 void launch_wave(const DeviceScene& scene, const PathPool& pool, const WaveParams& wp, const LaunchShape& ls,
@@ -851,6 +938,15 @@ void launch_accumulate(const PathPool& pool, const FilmTargets& film, uint32_t p
         k_accumulate<true><<<grid, 256, 0, stream>>>(pool, film, pixel_base, pixel_count, samples, reset ? 1u : 0u);
     else
         k_accumulate<false><<<grid, 256, 0, stream>>>(pool, film, pixel_base, pixel_count, samples, reset ? 1u : 0u);
+}
+
+void launch_material_sort(const PathPool& pool, uint32_t bounce, uint32_t n0, const LaunchShape& ls,
+                          cudaStream_t stream) {
+    if (!pool.order || !pool.sort_keys || !pool.sort_bins) return;  // the caller's pool view carries all three
+    cudaMemsetAsync(pool.sort_bins, 0, SORT_BINS * sizeof(uint32_t), stream);
+    k_sort_keys<<<ls.grid_stream, BLOCK, 0, stream>>>(pool, bounce, n0);
+    k_sort_scan<<<1, 1024, 0, stream>>>(pool.sort_bins);
+    k_sort_scatter<<<ls.grid_stream, BLOCK, 0, stream>>>(pool, bounce, n0);
 }
 
 void launch_tonemap(const float4* avg, uint32_t* out, uint32_t pixels, float exposure_scale, cudaStream_t stream) {

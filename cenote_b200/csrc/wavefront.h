@@ -44,11 +44,23 @@ struct PathPool {
     float* guide_out;
     uint32_t* guide_rec;
     struct GuideRecordSink* sink;
+    // Material sort (null when off): the shading order of the bounce's paths,
+    // each queue entry's key, and SORT_BINS key counts turned into offsets.
+    uint32_t* order;
+    uint32_t* sort_keys;
+    uint32_t* sort_bins;
     uint32_t* queue[2];   // ray queues, ping-pong by bounce parity
     ShadowRay* shadows;
     uint32_t* counters;
     uint32_t capacity;
+    // Idle lanes before a traversal warp refills with new rays (1..32; 0 =
+    // the built-in default): a per-scene tuning knob.
+    uint32_t refill_idle;
+    // BVH nodes each traversal block stages in shared memory (0..TOP_NODES_MAX).
+    uint32_t top_nodes;
 };
+
+constexpr uint32_t TOP_NODES_MAX = 320;  // 25.6 KB per 128-thread block: 8 blocks still fit an SM
 
 // Where guided vertices record themselves for training.
 struct GuideRecordSink {
@@ -73,6 +85,10 @@ struct WaveParams {
     // progress from device memory instead of baked launch parameters.
     const uint32_t* sample_offset;
 };
+
+// Keys of the material sort: 0 for a miss, else 1 + the hit's instance (its
+// material slot) folded into SORT_BINS - 1 buckets.
+constexpr uint32_t SORT_BINS = 2048;
 
 struct LaunchShape {
     int grid_isect, grid_shade, grid_shadow, grid_stream;
@@ -114,6 +130,11 @@ void launch_accumulate(const PathPool& pool, const FilmTargets& film, uint32_t p
 void launch_resolve(const float4* sum, float4* avg, uint32_t pixels, float samples, cudaStream_t stream);
 void launch_resolve1(const float* sum, float* avg, uint32_t pixels, float samples, cudaStream_t stream);
 // The display transform (tonemap.slang): linear ACEScg averages -> sRGB RGBA8.
+// Counting sort of bounce `bounce`'s queue by material key into pool.order
+// (keys, then one-block scan, then scatter); the shading kernel then reads
+// its paths in that order.
+void launch_material_sort(const PathPool& pool, uint32_t bounce, uint32_t n0, const LaunchShape& ls,
+                          cudaStream_t stream);
 void launch_tonemap(const float4* avg, uint32_t* out, uint32_t pixels, float exposure_scale, cudaStream_t stream);
 // tally[0] += extension rays, [1] += shadow rays, [2] |= overflow,
 // [3] += node visits, [4] += triangle tests.

@@ -244,6 +244,36 @@ void cenote_renderer_destroy(cenote_renderer* r);
  * one-sample waves. Results are bitwise identical for every setting. */
 int32_t cenote_renderer_set_samples_per_wave(cenote_renderer* r, uint32_t samples_per_wave);
 int32_t cenote_renderer_stats(cenote_renderer* r, cenote_stats* out);
+/* Material sort before shading: the bounce's paths are counting-sorted by
+ * the hit's material slot (misses first) and shaded in that order. Only the
+ * order of work changes: without online guide training (whose batches follow
+ * the order records are made in) the results are bitwise the same. */
+#define CENOTE_SORT_NONE 0u
+#define CENOTE_SORT_ALL 1u
+#define CENOTE_SORT_SECONDARY 2u /* every bounce but the camera rays' */
+/* A new renderer sorts every bounce (CENOTE_SORT_ALL). */
+int32_t cenote_renderer_set_material_sort(cenote_renderer* r, uint32_t mode);
+/* The per-scene launch knobs. None changes a result: every setting renders
+ * the same film bit for bit. */
+typedef struct cenote_tuning {
+    uint32_t material_sort;    /* CENOTE_SORT_* */
+    uint32_t samples_per_wave; /* samples of every pixel one wave carries (0 = automatic); sets the queue capacity */
+    uint32_t refill_idle;      /* idle lanes (1..32) before a traversal warp takes new rays (0 = default 8) */
+    uint32_t top_nodes;        /* BVH top-level nodes staged in shared memory per traversal block (0..320) */
+    uint32_t l2_window;        /* 1: the BVH nodes are a persisting L2 access-policy window during the waves */
+    float ms_per_sample;       /* autotune: device time of one sample of every pixel at the chosen setting */
+} cenote_tuning;
+int32_t cenote_renderer_set_tuning(cenote_renderer* r, const cenote_tuning* tuning);
+int32_t cenote_renderer_get_tuning(cenote_renderer* r, cenote_tuning* out);
+/* Time candidate settings on `scene` at width x height (a scratch film, a few
+ * hundred ms of device time at 1080p) by coordinate descent over the sort
+ * mode, samples per wave, refill threshold, shared-memory top levels and
+ * the L2 persistence window;
+ * apply the fastest to `r` and
+ * report it in `out` (nullable). The renderer's stats afterwards describe the
+ * last probe. */
+int32_t cenote_renderer_autotune(cenote_renderer* r, cenote_scene* scene, uint32_t width, uint32_t height,
+                                 cenote_tuning* out);
 int32_t cenote_renderer_set_profiling(cenote_renderer* r, uint32_t flags);
 
 /* Renderer::render: one wave at sample index `sample`, RGBA f32 row-major,

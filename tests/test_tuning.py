@@ -63,7 +63,8 @@ def test_tuning_knobs_leave_the_film_unchanged(ctx):
     spec = scenes.chart(96, 54, 4, 8)
     scene = Scene(ctx, spec)
     films = []
-    for knobs in [(SORT_NONE, 0, 0), (SORT_ALL, 1, 4), (SORT_SECONDARY, 4, 16), (SORT_ALL, 2, 32)]:
+    for knobs in [(SORT_NONE, 0, 0, 0, 0), (SORT_ALL, 1, 4, 80, 1), (SORT_SECONDARY, 4, 16, 320, 0),
+                  (SORT_ALL, 2, 32, 1, 1), (SORT_NONE, 3, 8, 7, 0)]:
         r = Renderer(ctx, 8)
         r.set_tuning(*knobs)
         f = Film(ctx, spec.width, spec.height)
@@ -81,10 +82,10 @@ def test_autotune_picks_a_valid_setting_and_keeps_it(ctx):
     r = Renderer(ctx, 8)
     t = r.autotune(scene, spec.width, spec.height)
     assert t["material_sort"] in (SORT_NONE, SORT_ALL, SORT_SECONDARY)
-    assert t["refill_idle"] in (0, 4, 8, 16) and t["ms_per_sample"] > 0
+    assert t["refill_idle"] in (0, 4, 8, 16) and t["top_nodes"] in (0, 80, 320) and t["ms_per_sample"] > 0
     kept = r.tuning()
-    assert {k: kept[k] for k in ("material_sort", "samples_per_wave", "refill_idle")} == \
-        {k: t[k] for k in ("material_sort", "samples_per_wave", "refill_idle")}
+    knobs = ("material_sort", "samples_per_wave", "refill_idle", "top_nodes", "l2_window")
+    assert {k: kept[k] for k in knobs} == {k: t[k] for k in knobs}
     f, g = Film(ctx, spec.width, spec.height), Film(ctx, spec.width, spec.height)
     r.accumulate(scene, f, 8)
     Renderer(ctx, 8).accumulate(scene, g, 8)
@@ -97,3 +98,7 @@ def test_bad_tuning_is_refused(ctx):
     r = Renderer(ctx, 4)
     with pytest.raises(CenoteError):
         r.set_tuning(SORT_ALL, 0, 33)
+    with pytest.raises(CenoteError):
+        r.set_tuning(SORT_ALL, 0, 8, 321)
+    with pytest.raises(CenoteError):
+        r.set_tuning(SORT_ALL, 0, 8, 0, 2)
