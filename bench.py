@@ -313,6 +313,8 @@ def main():
     ap.add_argument("--scene", default="large", choices=["large", "ceiling_box"], help="guiding: the scene")
     ap.add_argument("--spp", type=int, default=0, help="override the workload's spp (profiling runs)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--bvh", default="host", choices=["host", "gpu"],
+                    help="BVH builder: host binned SAH or GPU PLOC (scene prep, outside the timed region)")
     ap.add_argument("--material-sort", type=int, default=None, choices=[0, 1, 2],
                     help="fix the material sort (0 off, 1 every bounce, 2 from the first bounce on) "
                          "instead of autotuning the launch knobs")
@@ -332,7 +334,8 @@ def main():
 
     import torch
     import torch.distributed as dist
-    from cenote_b200 import PROFILE_COUNTS, PROFILE_TIMING, Context, Film, Renderer, Scene, scenes
+    from cenote_b200 import (BVH_GPU_PLOC, BVH_HOST_SAH, PROFILE_COUNTS, PROFILE_TIMING, Context, Film, Renderer,
+                             Scene, scenes)
 
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -345,6 +348,7 @@ def main():
     spec = make_spec(w)
     W, H, spp, maxb = w["width"], w["height"], w["spp"], w["max_bounces"]
     ctx = Context(local)
+    ctx.set_bvh_builder(BVH_GPU_PLOC if args.bvh == "gpu" else BVH_HOST_SAH)
     t0 = time.perf_counter()
     scene = Scene(ctx, spec)
     prep_wall_ms = (time.perf_counter() - t0) * 1e3
@@ -472,8 +476,8 @@ def main():
         "rays_per_s": (rays[0] + rays[1]) * world / (ms / 1e3),
         "extension_rays_per_step": rays[0] / args.steps, "shadow_rays_per_step": rays[1] / args.steps,
         "stage_ms_per_step": {k: v / args.steps for k, v in stage.items()},
-        "scene_prep_ms": {"bvh": float(prep[0]), "env_tables": float(prep[1]), "total": float(prep[2]),
-                          "wall": prep_wall_ms},
+        "scene_prep_ms": {"bvh": float(prep[0]), "bvh_builder": "GPU PLOC" if args.bvh == "gpu" else "host binned SAH",
+                          "env_tables": float(prep[1]), "total": float(prep[2]), "wall": prep_wall_ms},
         "roofline": {
             "kernel": "traversal (k_intersect + k_shadow)", "bound": "hbm",
             "achieved": achieved, "peak": peak, "unit": "GB/s",

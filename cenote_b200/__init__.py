@@ -126,7 +126,7 @@ EXPORTED_SYMBOLS = [
     "cenote_guide_train_step", "cenote_renderer_set_guide", "cenote_accumulate_range", "cenote_film_tonemap",
     "cenote_film_tonemap_device", "cenote_film_restore",
     "cenote_scene_add_delta_light", "cenote_renderer_set_material_sort", "cenote_renderer_set_tuning",
-    "cenote_renderer_get_tuning", "cenote_renderer_autotune",
+    "cenote_renderer_get_tuning", "cenote_renderer_autotune", "cenote_context_set_bvh_builder",
 ]
 
 _lib = None
@@ -176,6 +176,7 @@ def library() -> C.CDLL:
         "cenote_renderer_set_tuning": (I32, [P, P]),
         "cenote_renderer_get_tuning": (I32, [P, P]),
         "cenote_renderer_autotune": (I32, [P, P, U32, U32, P]),
+        "cenote_context_set_bvh_builder": (I32, [P, U32]),
         "cenote_scene_destroy": (None, [P]),
         "cenote_scene_set_camera": (I32, [P, P]),
         "cenote_scene_prep_times": (I32, [P, P]),
@@ -241,6 +242,9 @@ def _c_camera(cam: scenes.Camera) -> CameraC:
     return c
 
 
+BVH_HOST_SAH, BVH_GPU_PLOC = 0, 1
+
+
 class Context:
     """One CUDA device and the stream every handle made from it shares."""
 
@@ -261,6 +265,10 @@ class Context:
 
     def synchronize(self) -> None:
         _check(library().cenote_synchronize(self._h))
+
+    def set_bvh_builder(self, builder: int) -> None:
+        """BVH_HOST_SAH or BVH_GPU_PLOC for scenes created from now on."""
+        _check(library().cenote_context_set_bvh_builder(self._h, builder))
 
     def close(self) -> None:
         if self._h:

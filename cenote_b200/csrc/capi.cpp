@@ -17,6 +17,7 @@
 
 #include "../../include/cenote_c.h"
 #include "bvh_build.h"
+#include "bvh_gpu.h"
 #include "records.h"
 #include "runtime.h"
 #include "texture_prep.h"
@@ -273,6 +274,13 @@ void cenote_context_destroy(cenote_context* ctx) {
 
 void* cenote_context_stream(cenote_context* ctx) { return ctx ? static_cast<void*>(ctx->stream) : nullptr; }
 
+int32_t cenote_context_set_bvh_builder(cenote_context* ctx, uint32_t builder) {
+    CN_CHECK(ctx, CENOTE_E_INVALID_ARGUMENT, "null context");
+    CN_CHECK(builder <= CENOTE_BVH_GPU_PLOC, CENOTE_E_INVALID_ARGUMENT, "unknown BVH builder");
+    ctx->bvh_builder = builder;
+    return CENOTE_OK;
+}
+
 int32_t cenote_synchronize(cenote_context* ctx) {
     CN_CHECK(ctx, CENOTE_E_INVALID_ARGUMENT, "null context");
     return wait_stream(ctx->stream, ctx->sync_ev, 600000.0);
@@ -476,32 +484,58 @@ int32_t cenote_scene_create_textured(cenote_context* ctx, const cenote_object* o
             }
 
     auto t_bvh = std::chrono::steady_clock::now();
-    WideBvh bvh = build_wide_bvh(tris, std::max(1u, std::thread::hardware_concurrency()));
-    sc->prep_ms[0] = float(std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t_bvh).count());
-    DeviceBuffer* bnodes = sc->add(bvh.nodes.size() * sizeof(WideNode), &err);
-    CN_CUDA(err);
-    DeviceBuffer* btris = sc->add(bvh.tris.size() * 4, &err);
-    CN_CUDA(err);
-    if (!bvh.nodes.empty()) {
-        CN_CUDA(cudaMemcpyAsync(bnodes->ptr, bvh.nodes.data(), bvh.nodes.size() * sizeof(WideNode),
-                                cudaMemcpyHostToDevice, ctx->stream));
-        CN_CUDA(cudaMemcpyAsync(btris->ptr, bvh.tris.data(), bvh.tris.size() * 4, cudaMemcpyHostToDevice, ctx->stream));
-    }
-    // Each emissive triangle's leaf index, for the shadow query's target test.
-    std::vector<uint32_t> light_leaf(std::max<size_t>(1, sc->lights.size()), 0xffffffffu);
-    for (size_t leaf = 0; leaf < bvh.tris.size() / 12; ++leaf) {
-        uint32_t inst, prim;
-        std::memcpy(&inst, &bvh.tris[12 * leaf + 3], 4);
-        std::memcpy(&prim, &bvh.tris[12 * leaf + 7], 4);
-        if (geoms[inst].light != LIGHT_NONE) light_leaf[geoms[inst].light + prim] = uint32_t(leaf);
-    }
-    DeviceBuffer* bleaf = sc->add(light_leaf.size() * 4, &err);
-    CN_CUDA(err);
-    CN_CUDA(cudaMemcpyAsync(bleaf->ptr, light_leaf.data(), light_leaf.size() * 4, cudaMemcpyHostToDevice, ctx->stream));
+    DeviceBuffer* bnodes = nullptr;
+    DeviceBuffer* btris = nullptr;
+    uint32_t node_count = 0;
+    const uint32_t tri_count = uint32_t(tris.size());
     DeviceBuffer* bgeo = sc->add(geoms.size() * sizeof(GeomRecord), &err);
     CN_CUDA(err);
     CN_CUDA(cudaMemcpyAsync(bgeo->ptr, geoms.data(), geoms.size() * sizeof(GeomRecord), cudaMemcpyHostToDevice,
                             ctx->stream));
+    DeviceBuffer* bleaf = sc->add(std::max<size_t>(1, sc->lights.size()) * 4, &err);
+    CN_CUDA(err);
+    CN_CUDA(cudaMemsetAsync(bleaf->ptr, 0xff, std::max<size_t>(1, sc->lights.size()) * 4, ctx->stream));
+    if (ctx->bvh_builder == CENOTE_BVH_GPU_PLOC && !tris.empty()) {
+        // Triangles in input order, identity in the w lanes; the device
+        // builds the binary tree, collapses it and lays out the leaves.
+        std::vector<float> packed(tris.size() * 12);
+        for (size_t i = 0; i < tris.size(); ++i) {
+            float* rec = &packed[12 * i];
+            for (int k = 0; k < 3; ++k)
+                for (int a = 0; a < 3; ++a) rec[4 * k + a] = tris[i].v[k][a];
+            std::memcpy(&rec[3], &tris[i].instance, 4);
+            std::memcpy(&rec[7], &tris[i].primitive, 4);
+            std::memcpy(&rec[11], &tris[i].flags, 4);
+        }
+        DeviceBuffer staged;
+        CN_CUDA(staged.alloc(packed.size() * 4));
+        CN_CUDA(cudaMemcpyAsync(staged.ptr, packed.data(), packed.size() * 4, cudaMemcpyHostToDevice, ctx->stream));
+        GpuBvh g{};
+        CN_CUDA(build_wide_bvh_gpu(staged.as<float4>(), tri_count, &g, ctx->stream));
+        bnodes = sc->adopt(g.nodes, size_t(g.node_count) * sizeof(WideNode));
+        btris = sc->adopt(g.tris, size_t(tri_count) * 48);
+        node_count = g.node_count;
+    } else {
+        WideBvh bvh = build_wide_bvh(tris, std::max(1u, std::thread::hardware_concurrency()));
+        bnodes = sc->add(bvh.nodes.size() * sizeof(WideNode), &err);
+        CN_CUDA(err);
+        btris = sc->add(bvh.tris.size() * 4, &err);
+        CN_CUDA(err);
+        if (!bvh.nodes.empty()) {
+            CN_CUDA(cudaMemcpyAsync(bnodes->ptr, bvh.nodes.data(), bvh.nodes.size() * sizeof(WideNode),
+                                    cudaMemcpyHostToDevice, ctx->stream));
+            CN_CUDA(cudaMemcpyAsync(btris->ptr, bvh.tris.data(), bvh.tris.size() * 4, cudaMemcpyHostToDevice,
+                                    ctx->stream));
+        }
+        node_count = uint32_t(bvh.nodes.size());
+        // wait for the uploads before the host vectors go
+        CN_CUDA(cudaStreamSynchronize(ctx->stream));
+    }
+    // Each emissive triangle's leaf index, for the shadow query's target test.
+    launch_light_leaves(btris->as<float4>(), tri_count, bgeo->as<GeomRecord>(), bleaf->as<uint32_t>(), ctx->stream);
+    CN_CUDA(cudaGetLastError());
+    CN_CUDA(cudaStreamSynchronize(ctx->stream));
+    sc->prep_ms[0] = float(std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t_bvh).count());
     DeviceBuffer* bmat = sc->add(mats.size() * sizeof(Material), &err);
     CN_CUDA(err);
     CN_CUDA(cudaMemcpyAsync(bmat->ptr, mats.data(), mats.size() * sizeof(Material), cudaMemcpyHostToDevice, ctx->stream));
@@ -603,8 +637,8 @@ int32_t cenote_scene_create_textured(cenote_context* ctx, const cenote_object* o
     ds.env_h = eh;
     ds.select_prob = sc->select_prob;
     ds.light_count = uint32_t(sc->lights.size());
-    ds.node_count = uint32_t(bvh.nodes.size());
-    ds.tri_count = uint32_t(bvh.tris.size() / 12);
+    ds.node_count = node_count;
+    ds.tri_count = tri_count;
     ds.has_nonopaque = nonopaque ? 1u : 0u;
     const float extent = std::max({bmax[0] - bmin[0], bmax[1] - bmin[1], bmax[2] - bmin[2], 1e-6f});
     for (int a = 0; a < 3; ++a) ds.bbox_min[a] = tris.empty() ? 0.0f : bmin[a];

@@ -91,6 +91,7 @@ struct cenote_context {
     std::mutex mu;
     // L2 persistence (this context's own set-aside; nothing outlives it).
     size_t l2_persist_max = 0, l2_window_max = 0, l2_set_aside = 0;
+    uint32_t bvh_builder = CENOTE_BVH_HOST_SAH;  // for scenes created from now on
 };
 
 struct cenote_scene {
@@ -112,7 +113,15 @@ struct cenote_scene {
     std::vector<cudaArray_t> tex_arrays;            // the bindless table's storage
     std::vector<cudaTextureObject_t> tex_objects;
 
-    DeviceBuffer* add(size_t bytes, cudaError_t* err) {
+    // Take ownership of memory cudaMalloc'd elsewhere (the GPU BVH build).
+    DeviceBuffer* adopt(void* p, size_t bytes) {
+        buffers.push_back(std::make_unique<DeviceBuffer>());
+        buffers.back()->ptr = p;
+        buffers.back()->bytes = bytes;
+        device_bytes += bytes;
+        return buffers.back().get();
+    }
+        DeviceBuffer* add(size_t bytes, cudaError_t* err) {
         buffers.push_back(std::make_unique<DeviceBuffer>());
         *err = buffers.back()->alloc(bytes);
         device_bytes += bytes;
