@@ -299,6 +299,47 @@ def run_serving(args):
     server.close()
 
 
+def run_knob_sweep(args, w):
+    """The launch knobs one at a time around the autotuner's choice: device
+    ms per sample of every pixel (the better of 3 runs of 16 spp) for each
+    value of each knob, the others held at the tuned setting. One JSON line."""
+    from cenote_b200 import BVH_GPU_PLOC, BVH_HOST_SAH, Context, Film, Renderer, Scene
+
+    ctx = Context(0)
+    ctx.set_bvh_builder(BVH_GPU_PLOC if args.bvh == "gpu" else BVH_HOST_SAH)
+    scene = Scene(ctx, make_spec(w))
+    W, H = w["width"], w["height"]
+    r = Renderer(ctx, w["max_bounces"])
+    t0 = time.perf_counter()
+    best = r.autotune(scene, W, H)
+    tune_s = time.perf_counter() - t0
+    film = Film(ctx, W, H)
+    spp = 16
+
+    def timed(knobs):
+        r.set_tuning(*knobs)
+        ms = []
+        for _ in range(3):
+            r.accumulate(scene, film, spp)
+            ms.append(r.stats()["gpu_ms"])
+        return round(min(ms) / spp, 4)
+
+    names = ("material_sort", "samples_per_wave", "refill_idle", "top_nodes", "l2_window")
+    base = tuple(best[k] for k in names)
+    values = ((0, 1, 2), (0, 4, 8, 16), (4, 8, 16, 32), (0, 80, 320), (0, 1))
+    sweep = {"tuned": timed(base)}
+    for i, vals in enumerate(values):
+        for v in vals:
+            k = list(base)
+            k[i] = v
+            sweep[f"{names[i]}={v}"] = timed(tuple(k))
+    line = {"metric": "device ms per sample of every pixel, one knob varied", "unit": "ms", "workload": w["label"],
+            "autotuned": {k: best[k] for k in names}, "autotune_s": round(tune_s, 2),
+            "samples_per_call": spp, "note": "samples_per_wave above 16 equals 16 at 16 spp per call",
+            "sweep": sweep}
+    print(json.dumps(line), flush=True)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -315,9 +356,14 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--bvh", default="host", choices=["host", "gpu"],
                     help="BVH builder: host binned SAH or GPU PLOC (scene prep, outside the timed region)")
+    ap.add_argument("--tuning", default="",
+                    help="pin the launch knobs instead of autotuning: sort,samples_per_wave,refill,top_nodes,l2 "
+                         "(profiling runs that must not record the tuner's probes)")
     ap.add_argument("--material-sort", type=int, default=None, choices=[0, 1, 2],
                     help="fix the material sort (0 off, 1 every bounce, 2 from the first bounce on) "
                          "instead of autotuning the launch knobs")
+    ap.add_argument("--sweep-knobs", action="store_true",
+                    help="instead of the bench: time each launch knob around the autotuned setting")
     args = ap.parse_args()
     if args.workload == "serving":
         run_serving(args)
@@ -328,6 +374,9 @@ def main():
     w = dict(WORKLOADS[args.workload])
     if args.spp:
         w["spp"] = args.spp
+    if args.sweep_knobs:
+        run_knob_sweep(args, w)
+        return
     if args.impl == "reference":
         run_reference(args, w)
         return
@@ -355,7 +404,10 @@ def main():
     prep = scene.prep_times_ms()
     r = Renderer(ctx, maxb)
     t_tune = time.perf_counter()
-    if args.material_sort is None:
+    if args.tuning:
+        r.set_tuning(*[int(x) for x in args.tuning.split(",")])
+        tuning = r.tuning()
+    elif args.material_sort is None:
         tuning = r.autotune(scene, W, H)  # per-scene launch knobs, outside the timed region
     else:
         r.set_tuning(args.material_sort)
@@ -452,6 +504,12 @@ def main():
     achieved = alg_bytes_frame / (trav_ms_frame / 1e3) / 1e9 if trav_ms_frame > 0 else None
     peak, peak_kind = measured_peaks()
     traffic = committed_traffic(args.workload)
+    # DRAM bytes per traversal launch from the committed capture of a smaller
+    # wave, scaled by paths per wave: the BVH is L2-resident, so DRAM traffic
+    # is the per-ray path-state traffic and grows with the rays per launch.
+    wave_paths = W * H * min(counts["samples_per_wave"], spp)
+    traffic_per_launch = (traffic["bytes_per_launch_captured"] * wave_paths / traffic["captured_paths_per_wave"]
+                          if traffic and "captured_paths_per_wave" in traffic else None)
 
     line = {
         "metric": "Msamples/s", "value": value, "unit": "Msamples/s", "n_gpus": world, "steps": args.steps,
@@ -467,7 +525,7 @@ def main():
                               "refill_idle": tuning["refill_idle"] or 8,
                               "top_nodes_in_shared_memory": tuning["top_nodes"],
                               "l2_persisting_bvh": bool(tuning["l2_window"]),
-                              "chosen_by": "autotuner" if args.material_sort is None else "flag",
+                              "chosen_by": "autotuner" if args.material_sort is None and not args.tuning else "flag",
                               "autotune_s": round(tune_s, 3)},
                    "guides": "albedo, normal and depth traced and accumulated every sample, as Renderer::accumulate does"},
         "e2e": {"value": e2e_value, "unit": "Msamples/s", "ms_per_step": e2e_step,
@@ -482,7 +540,7 @@ def main():
             "kernel": "traversal (k_intersect + k_shadow)", "bound": "hbm",
             "achieved": achieved, "peak": peak, "unit": "GB/s",
             "frac": (achieved / peak) if achieved else None, "peak_source": peak_kind,
-            "traffic": traffic["bytes_per_launch"] if traffic else None,
+            "traffic": traffic_per_launch,
             "algorithmic_bytes_per_launch": alg_bytes_frame / max(1, trav_launches),
             "launch_ms": trav_ms_frame / max(1, trav_launches),
             "nodes_per_ray": counts["node_visits"] / max(1, ext + shd),

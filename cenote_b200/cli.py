@@ -14,7 +14,9 @@ EXR: beauty R/G/B/A, the denoiser guides albedo.R/G/B and normal.X/Y/Z, depth Z
 (crates/cenote/shaders/tonemap.slang: exposure --exposure stops, ACES fit, sRGB)
 as an 8-bit PNG, tonemapped on the device.
 --frames repeats the render (profiling); --samples-per-wave fixes how many
-samples of every pixel one wave carries; --stats prints the renderer's counters.
+samples of every pixel one wave carries; --tuning pins the launch knobs
+(sort,samples_per_wave,refill,top_nodes,l2) and --autotune picks them on the
+scene first; --stats prints the renderer's counters.
 """
 from __future__ import annotations
 
@@ -67,6 +69,13 @@ def render(args) -> int:
     scene = Scene(ctx, spec)
     prep = time.perf_counter() - t0
     renderer = Renderer(ctx, depth, samples_per_wave=args.samples_per_wave)
+    if args.tuning:
+        knobs = [int(x) for x in args.tuning.split(",")]
+        if args.samples_per_wave and len(knobs) > 1:
+            knobs[1] = args.samples_per_wave
+        renderer.set_tuning(*knobs)
+    elif args.autotune:
+        renderer.autotune(scene, width, height)
     film = Film(ctx, width, height)
     t0 = time.perf_counter()
     for _ in range(max(1, args.frames)):
@@ -102,6 +111,8 @@ def main(argv=None) -> int:
     r.add_argument("--device", type=int, default=0)
     r.add_argument("--samples-per-wave", type=int, default=0, help="0 = automatic")
     r.add_argument("--stats", action="store_true")
+    r.add_argument("--tuning", default="", help="launch knobs: sort,samples_per_wave,refill,top_nodes,l2")
+    r.add_argument("--autotune", action="store_true", help="time the launch knobs on the scene first")
     r.add_argument("--png", default="", help="also write the tonemapped display frame here")
     r.add_argument("--exposure", type=float, default=0.0, help="display exposure in stops (--png)")
     args = ap.parse_args(argv)

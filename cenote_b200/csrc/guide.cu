@@ -565,6 +565,15 @@ __global__ void k_resolve_records(Record* recs, const uint32_t* count, uint32_t 
     }
 }
 
+// Row r of the batch starting at `offset`: a prime stride (above any record
+// count, hence coprime to it) walks the wave's records as a permutation, so
+// every batch spans the whole wave. Records arrive in shading order, which the
+// material sort groups by material: contiguous batches would each see one or
+// two materials.
+__device__ __forceinline__ uint32_t batch_record(uint32_t offset, uint32_t r, uint32_t n) {
+    return uint32_t((uint64_t(offset) + uint64_t(r) * 2654435761ull) % n);
+}
+
 // Training forward over records: inputs encoded from each record.
 __global__ void __launch_bounds__(TILE, 1) k_forward_records(Net net, const Record* __restrict__ recs,
                                                              const uint32_t* count, uint32_t capacity, uint32_t offset,
@@ -591,7 +600,7 @@ __global__ void __launch_bounds__(TILE, 1) k_forward_records(Net net, const Reco
     for (uint32_t tile = blockIdx.x; n > 0 && tile * TILE < rows; tile += gridDim.x) {
         const uint32_t r = tile * TILE + threadIdx.x;
         if (r < rows) {
-            const Record rc = recs[(offset + r) % n];
+            const Record rc = recs[batch_record(offset, r, n)];
             float3 p = make_float3((rc.q0.x - bmin.x) * binv, (rc.q0.y - bmin.y) * binv, (rc.q0.z - bmin.z) * binv);
             encode(p, make_float3(rc.q1.x, rc.q1.y, rc.q1.z), make_float3(rc.q2.x, rc.q2.y, rc.q2.z), feat);
             wsum += rc.q0.w;
@@ -627,7 +636,7 @@ __global__ void k_loss_records(const float* __restrict__ out, const Record* __re
         float c = 0.0f;
         float3 w = make_float3(0.0f, 0.0f, 1.0f);
         if (n > 0 && mean > 0.0f) {
-            const Record rc = recs[(offset + r) % n];
+            const Record rc = recs[batch_record(offset, r, n)];
             c = fminf(rc.q0.w / mean, 20.0f) / float(rows);
             w = make_float3(rc.q3.x, rc.q3.y, rc.q3.z);
         }

@@ -33,10 +33,11 @@ namespace {
 constexpr int BLOCK = 128;
 
 // Minimum resident 128-thread blocks per SM for the shading kernel: the
-// register cap that trades spills against occupancy (5 → 96 registers,
-// measured fastest on the 1280x720 chart: 421 vs 414 at 4 and 391 uncapped).
+// register cap that trades spills against occupancy (6 → 80 registers; with
+// material-sorted waves of 30-60 M paths, 6 measured 2 % faster than 5 on the
+// textured terrain and level on the chart; 4 and uncapped were slower).
 #ifndef CN_SHADE_MIN_BLOCKS
-#define CN_SHADE_MIN_BLOCKS 5
+#define CN_SHADE_MIN_BLOCKS 6
 #endif
 // The same for the traversal kernels (8 → 64 registers).
 #ifndef CN_TRAV_MIN_BLOCKS

@@ -8,11 +8,14 @@ as the checker; the shipped library never imports, links or runs it.
 
 Parity pins: every host table is checked against the reference's own tests
 (lights.rs:320-475, environment.rs:258-324, color.rs:39-59), restated in
-tests/test_oracle_golden.py. The image path has no reference render that can be
-produced here (the reference is Rust + Vulkan; no cargo, slangc or Vulkan
-device exists on this machine or the GPU box), so image-level parity is pinned
-to the restatement and the reference's physical tests (furnaces, analytic
-lights, MIS agreement), not to reference pixels.
+tests/test_oracle_golden.py. The reference cannot be run here (Rust + Vulkan; no
+cargo, slangc or Vulkan device on this machine or the GPU box), but it commits
+its own 64-spp renders of two pbrt scenes
+(crates/cenote-pbrt/tests/golden/{cornell-box,veach-mis}.exr): imported with
+cenote_b200.pbrt and rendered here with the same Sobol-Burley samples, the
+oracle reproduces those pixels' noise (tests/test_corpus.py), which pins the
+image path to reference pixels, alongside the reference's physical tests
+(furnaces, analytic lights, MIS agreement).
 """
 from __future__ import annotations
 
