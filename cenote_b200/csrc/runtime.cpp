@@ -110,20 +110,18 @@ cudaError_t enqueue_waves(cenote_renderer* r, const cenote_scene* sc, uint32_t w
             launch_wave_begin(r->pool, wp, ctx->shape, stream);
             mark();
             for (uint32_t b = 0; b < max_bounces; ++b) {
-                launch_intersect(sc->ds, r->pool, b, n0, ctx->shape, counting, stream);
-                mark();
-                if (guided) guide::launch_infer_paths(r->guide->view(), sc->ds, r->pool, b, n0, r->guide->sms, stream);
                 const bool sort = r->material_sort == CENOTE_SORT_ALL ||
                                   (r->material_sort == CENOTE_SORT_SECONDARY && b > 0);
+                const PathPool view = sort ? r->sorted_view() : r->pool;
+                if (sort) launch_sort_begin(view, stream);
+                launch_intersect(sc->ds, view, b, n0, ctx->shape, counting, stream);
+                mark();
+                if (guided) guide::launch_infer_paths(r->guide->view(), sc->ds, r->pool, b, n0, r->guide->sms, stream);
                 if (sort) {
-                    PathPool sorted = r->pool;
-                    sorted.order = r->sort_order.as<uint32_t>();
-                    launch_material_sort(sorted, b, n0, ctx->shape, stream);
-                    launch_shade(sc->ds, sorted, b, wp, n0, ctx->shape, stream);
-                    wc->launches += 3;
-                } else {
-                    launch_shade(sc->ds, r->pool, b, wp, n0, ctx->shape, stream);
+                    launch_material_sort(view, b, n0, ctx->shape, stream);
+                    wc->launches += 2;
                 }
+                launch_shade(sc->ds, view, b, wp, n0, ctx->shape, stream);
                 mark();
                 launch_shadow(sc->ds, r->pool, b, ctx->shape, counting, stream);
                 mark();

@@ -199,9 +199,11 @@ struct cenote_renderer {
         pool.queue[0] = q0.as<uint32_t>();
         pool.queue[1] = q1.as<uint32_t>();
         pool.shadows = shadows.as<ShadowRay>();
-        pool.order = nullptr;  // set per bounce by the wave loop when sorting
-        pool.sort_keys = sort_keys.as<uint32_t>();
-        pool.sort_bins = sort_bins.as<uint32_t>();
+        // Null here: the wave loop passes a view with all three set to the
+        // bounces it sorts.
+        pool.order = nullptr;
+        pool.sort_keys = nullptr;
+        pool.sort_bins = nullptr;
         pool.capacity = uint32_t(cap);
         pool_cap = cap;
         return cudaSuccess;
@@ -228,7 +230,16 @@ struct cenote_renderer {
 
     // The guide lanes: allocated on the first wave that traces guides,
     // detached (null) for waves that do not.
-    cudaError_t set_guides(bool on) {
+    // The pool as the bounces that sort see it.
+    PathPool sorted_view() const {
+        PathPool p = pool;
+        p.order = sort_order.as<uint32_t>();
+        p.sort_keys = sort_keys.as<uint32_t>();
+        p.sort_bins = sort_bins.as<uint32_t>();
+        return p;
+    }
+
+        cudaError_t set_guides(bool on) {
         if (on && aov_cap < pool_cap) {
             cudaError_t e;
             if ((e = aov_albedo.alloc(pool_cap * 16)) || (e = aov_normal.alloc(pool_cap * 16)) ||

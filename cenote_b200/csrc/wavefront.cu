@@ -173,7 +173,22 @@ __global__ void __launch_bounds__(BLOCK, CN_TRAV_MIN_BLOCKS) k_intersect(DeviceS
     Ray ray;
     float tmax = 1e30f, best_b1 = 0.0f, best_b2 = 0.0f;
     uint32_t path = 0, best_inst = LIGHT_NONE, best_prim = 0, crossings = 0, pixel = 0, sample = 0;
-    bool live = false, drained = false;
+    uint32_t qi = 0;          // the ray's queue position (the material sort's key slot)
+    bool live = false, drained = false, finished = false;
+    // Material sort (when this bounce sorts): each finished ray's key goes to
+    // its queue slot and into the key counts, one atomic per distinct key per
+    // warp. Called where the whole warp is converged.
+    auto flush_keys = [&]() {
+        if (!pool.sort_keys) return;
+        if (__ballot_sync(0xffffffffu, finished) == 0u) return;
+        const uint32_t key = finished ? (best_inst == LIGHT_NONE ? 0u : 1u + best_inst % (SORT_BINS - 1u)) : 0xffffffffu;
+        const uint32_t peers = __match_any_sync(0xffffffffu, key);
+        if (finished) {
+            pool.sort_keys[qi] = key;
+            if (lane_id() == uint32_t(__ffs(peers) - 1)) atomicAdd(pool.sort_bins + key, uint32_t(__popc(peers)));
+        }
+        finished = false;
+    };
     auto visit = [&](uint32_t, float4 a, float4 b, float4 c, float& tm) {
         uint32_t flags = __float_as_uint(c.w);
         if (!(flags & mask)) return false;
@@ -198,6 +213,7 @@ __global__ void __launch_bounds__(BLOCK, CN_TRAV_MIN_BLOCKS) k_intersect(DeviceS
         if (!drained) {
             uint32_t i = refill(fetch, count, live, drained);
             if (i != ~0u) {
+                qi = i;
                 path = bounce == 0 ? i : queue[i];
                 float4 o = pool.org[path], d = pool.dir[path];
                 ray = make_ray(xyz(o), xyz(d));
@@ -216,9 +232,11 @@ __global__ void __launch_bounds__(BLOCK, CN_TRAV_MIN_BLOCKS) k_intersect(DeviceS
                 if (scene.node_count == 0) {
                     pool.hit[path] = make_uint4(LIGHT_NONE, 0u, 0u, 0u);
                     live = false;
+                    finished = true;
                 }
             }
         }
+        flush_keys();
         if (!__any_sync(0xffffffffu, live)) {
             if (drained) break;
             continue;
@@ -233,8 +251,10 @@ __global__ void __launch_bounds__(BLOCK, CN_TRAV_MIN_BLOCKS) k_intersect(DeviceS
                     pool.hit[path] =
                         make_uint4(best_inst, best_prim, __float_as_uint(best_b1), __float_as_uint(best_b2));
                     live = false;
+                    finished = true;
                 }
             }
+            flush_keys();
             if (uint32_t(__popc(__ballot_sync(0xffffffffu, !live))) >= want_idle) break;
         }
     }
@@ -765,32 +785,13 @@ __global__ void k_copy_rad(const float4* __restrict__ rad, float4* __restrict__ 
 
 // ---- material sort -----------------------------------------------------------------
 // Shading in key order keeps a warp on one material: one closure path, one
-// set of textures, neighbouring vertices. Keys are counted with one atomic
-// per distinct key per warp (__match_any_sync), the counts become offsets in
-// one block, and the scatter hands each key's paths consecutive slots.
+// set of textures, neighbouring vertices. k_intersect writes each ray's key
+// and counts it (one atomic per distinct key per warp, __match_any_sync) as
+// the ray finishes, the counts become offsets in one block, and the scatter
+// hands each key's paths consecutive slots.
 
 __device__ __forceinline__ uint32_t sort_count(const PathPool& pool, uint32_t bounce, uint32_t n0) {
     return min(bounce == 0 ? n0 : pool.counters[CTR_RAYS + bounce], pool.capacity);
-}
-
-__global__ void __launch_bounds__(BLOCK) k_sort_keys(PathPool pool, uint32_t bounce, uint32_t n0) {
-    const uint32_t count = sort_count(pool, bounce, n0);
-    const uint32_t* queue = pool.queue[bounce & 1u];
-    const uint32_t* hit_inst = reinterpret_cast<const uint32_t*>(pool.hit);
-    const uint32_t stride = gridDim.x * blockDim.x;
-    for (uint32_t base = blockIdx.x * blockDim.x + (threadIdx.x & ~31u); base < count; base += stride) {
-        const uint32_t i = base + lane_id();
-        const bool valid = i < count;
-        uint32_t key = 0xffffffffu;
-        if (valid) {
-            const uint32_t path = bounce == 0 ? i : queue[i];
-            const uint32_t inst = hit_inst[4u * size_t(path)];
-            key = inst == LIGHT_NONE ? 0u : 1u + inst % (SORT_BINS - 1u);
-            pool.sort_keys[i] = key;
-        }
-        const uint32_t peers = __match_any_sync(0xffffffffu, key);
-        if (valid && lane_id() == uint32_t(__ffs(peers) - 1)) atomicAdd(pool.sort_bins + key, uint32_t(__popc(peers)));
-    }
 }
 
 // One block of 1024 threads: exclusive prefix sums of the SORT_BINS counts.
@@ -941,11 +942,13 @@ void launch_accumulate(const PathPool& pool, const FilmTargets& film, uint32_t p
         k_accumulate<false><<<grid, 256, 0, stream>>>(pool, film, pixel_base, pixel_count, samples, reset ? 1u : 0u);
 }
 
+void launch_sort_begin(const PathPool& pool, cudaStream_t stream) {
+    if (pool.sort_bins) cudaMemsetAsync(pool.sort_bins, 0, SORT_BINS * sizeof(uint32_t), stream);
+}
+
 void launch_material_sort(const PathPool& pool, uint32_t bounce, uint32_t n0, const LaunchShape& ls,
                           cudaStream_t stream) {
     if (!pool.order || !pool.sort_keys || !pool.sort_bins) return;  // the caller's pool view carries all three
-    cudaMemsetAsync(pool.sort_bins, 0, SORT_BINS * sizeof(uint32_t), stream);
-    k_sort_keys<<<ls.grid_stream, BLOCK, 0, stream>>>(pool, bounce, n0);
     k_sort_scan<<<1, 1024, 0, stream>>>(pool.sort_bins);
     k_sort_scatter<<<ls.grid_stream, BLOCK, 0, stream>>>(pool, bounce, n0);
 }

@@ -130,9 +130,12 @@ void launch_accumulate(const PathPool& pool, const FilmTargets& film, uint32_t p
 void launch_resolve(const float4* sum, float4* avg, uint32_t pixels, float samples, cudaStream_t stream);
 void launch_resolve1(const float* sum, float* avg, uint32_t pixels, float samples, cudaStream_t stream);
 // The display transform (tonemap.slang): linear ACEScg averages -> sRGB RGBA8.
-// Counting sort of bounce `bounce`'s queue by material key into pool.order
-// (keys, then one-block scan, then scatter); the shading kernel then reads
-// its paths in that order.
+// Counting sort of bounce `bounce`'s queue by material key into pool.order.
+// launch_sort_begin clears the key counts before the bounce's intersect,
+// which (given a pool view with sort_keys set) writes and counts every ray's
+// key; launch_material_sort then turns the counts into offsets and scatters
+// the paths; the shading kernel reads them in that order.
+void launch_sort_begin(const PathPool& pool, cudaStream_t stream);
 void launch_material_sort(const PathPool& pool, uint32_t bounce, uint32_t n0, const LaunchShape& ls,
                           cudaStream_t stream);
 void launch_tonemap(const float4* avg, uint32_t* out, uint32_t pixels, float exposure_scale, cudaStream_t stream);
