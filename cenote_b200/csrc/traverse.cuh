@@ -21,6 +21,7 @@
 
 namespace cn {
 
+
 constexpr int TRAVERSAL_STACK = 32;
 
 struct Ray {
@@ -153,10 +154,17 @@ __device__ __forceinline__ uint32_t intersect_node(const DeviceScene& s, uint32_
     if (r.idir.y < 0.0f) { uint32_t t0 = ny0, t1 = ny1; ny0 = fy0; ny1 = fy1; fy0 = t0; fy1 = t1; }
     if (r.idir.z < 0.0f) { uint32_t t0 = nz0, t1 = nz1; nz0 = fz0; nz1 = fz1; fz0 = t0; fz1 = t1; }
     const float tlimit = tmax * 1.00002f;  // cull only nodes clearly beyond the current hit
+    // An inner child's meta byte is 0b001_11sss (bit 24 + slot); XOR its slot
+    // with the ray's octant for all eight children at once: bit 3 of a byte
+    // is set where its bits 3 and 4 both are (inner children only: leaf
+    // offsets stop at 23), moved to bit 0 and multiplied by the octant (at
+    // most 7, so no carry crosses a byte).
+    const uint32_t ml = n1.z ^ ((((n1.z >> 1) & n1.z & 0x08080808u) >> 3) * r.oct_inv);
+    const uint32_t mh = n1.w ^ ((((n1.w >> 1) & n1.w & 0x08080808u) >> 3) * r.oct_inv);
     uint32_t mask = 0;
 #pragma unroll
     for (int i = 0; i < 8; ++i) {
-        uint32_t meta = byte_of(n1.z, n1.w, i);  // 0 for an empty slot: contributes no bits
+        uint32_t meta = byte_of(ml, mh, i);  // 0 for an empty slot: contributes no bits
         float tnx = fmaf(float(byte_of(nx0, nx1, i)), aid.x, aor.x);
         float tny = fmaf(float(byte_of(ny0, ny1, i)), aid.y, aor.y);
         float tnz = fmaf(float(byte_of(nz0, nz1, i)), aid.z, aor.z);
@@ -166,10 +174,7 @@ __device__ __forceinline__ uint32_t intersect_node(const DeviceScene& s, uint32_
         float t0 = fmaxf(fmaxf(tnx, tny), fmaxf(tnz, 0.0f));
         float t1 = fminf(fminf(tfx, tfy), fminf(tfz, tlimit)) * 1.0000004f;
         if (t0 <= t1) {
-            uint32_t bits = meta >> 5;
-            uint32_t bit_index = meta & 0x1fu;
-            if ((meta & 0x18u) == 0x18u) bit_index ^= r.oct_inv;
-            mask |= bits << bit_index;
+            mask |= (meta >> 5) << (meta & 0x1fu);
         }
     }
     return mask;
