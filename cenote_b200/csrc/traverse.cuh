@@ -51,9 +51,12 @@ __device__ __forceinline__ Ray make_ray(float3 org, float3 dir) {
     r.kx = kx;
     r.ky = ky;
     r.kz = kz;
-    r.sx = __fdiv_rn(comp(dir, kx), dz);
-    r.sy = __fdiv_rn(comp(dir, ky), dz);
-    r.sz = __fdiv_rn(1.0f, dz);
+    // The shear constants (Woop et al. 2013) from the reciprocal already
+    // taken: any per-ray constants keep the test watertight, as long as every
+    // triangle of the ray uses the same ones.
+    r.sz = comp(r.idir, kz);
+    r.sx = __fmul_rn(comp(dir, kx), r.sz);
+    r.sy = __fmul_rn(comp(dir, ky), r.sz);
     r.oct_inv = (dir.x >= 0.0f ? 4u : 0u) | (dir.y >= 0.0f ? 2u : 0u) | (dir.z >= 0.0f ? 1u : 0u);
     return r;
 }

@@ -36,9 +36,9 @@ inline RayPre ray_pre(V3f org, V3f dir) {
     r.kx = r.kz + 1 == 3 ? 0 : r.kz + 1;
     r.ky = r.kx + 1 == 3 ? 0 : r.kx + 1;
     if (dir[r.kz] < 0.0f) std::swap(r.kx, r.ky);
-    r.sx = dir[r.kx] / dir[r.kz];
-    r.sy = dir[r.ky] / dir[r.kz];
     r.sz = 1.0f / dir[r.kz];
+    r.sx = dir[r.kx] * r.sz;
+    r.sy = dir[r.ky] * r.sz;
     return r;
 }
 
