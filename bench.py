@@ -324,9 +324,9 @@ def run_knob_sweep(args, w):
             ms.append(r.stats()["gpu_ms"])
         return round(min(ms) / spp, 4)
 
-    names = ("material_sort", "samples_per_wave", "refill_idle", "top_nodes", "l2_window")
+    names = ("material_sort", "samples_per_wave", "refill_idle", "top_nodes", "l2_window", "per_lane_triangles")
     base = tuple(best[k] for k in names)
-    values = ((0, 1, 2), (0, 4, 8, 16), (4, 8, 16, 32), (0, 80, 320), (0, 1))
+    values = ((0, 1, 2), (0, 4, 8, 16), (4, 8, 16, 32), (0, 80, 320), (0, 1), (0, 1))
     sweep = {"tuned": timed(base)}
     for i, vals in enumerate(values):
         for v in vals:
@@ -357,7 +357,8 @@ def main():
     ap.add_argument("--bvh", default="host", choices=["host", "gpu"],
                     help="BVH builder: host binned SAH or GPU PLOC (scene prep, outside the timed region)")
     ap.add_argument("--tuning", default="",
-                    help="pin the launch knobs instead of autotuning: sort,samples_per_wave,refill,top_nodes,l2 "
+                    help="pin the launch knobs instead of autotuning: sort,samples_per_wave,refill,top_nodes,l2"
+                         "[,per_lane_triangles] "
                          "(profiling runs that must not record the tuner's probes)")
     ap.add_argument("--material-sort", type=int, default=None, choices=[0, 1, 2],
                     help="fix the material sort (0 off, 1 every bounce, 2 from the first bounce on) "
@@ -525,6 +526,7 @@ def main():
                               "refill_idle": tuning["refill_idle"] or 8,
                               "top_nodes_in_shared_memory": tuning["top_nodes"],
                               "l2_persisting_bvh": bool(tuning["l2_window"]),
+                              "triangle_tests": "per lane" if tuning["per_lane_triangles"] else "warp queue",
                               "chosen_by": "autotuner" if args.material_sort is None and not args.tuning else "flag",
                               "autotune_s": round(tune_s, 3)},
                    "guides": "albedo, normal and depth traced and accumulated every sample, as Renderer::accumulate does"},

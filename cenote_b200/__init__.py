@@ -84,7 +84,8 @@ class DeltaLightC(C.Structure):
 
 class TuningC(C.Structure):
     _fields_ = [("material_sort", C.c_uint32), ("samples_per_wave", C.c_uint32), ("refill_idle", C.c_uint32),
-                ("top_nodes", C.c_uint32), ("l2_window", C.c_uint32), ("ms_per_sample", C.c_float)]
+                ("top_nodes", C.c_uint32), ("l2_window", C.c_uint32), ("per_lane_triangles", C.c_uint32),
+                ("ms_per_sample", C.c_float)]
 
 
 class Options(C.Structure):
@@ -118,7 +119,7 @@ EXPORTED_SYMBOLS = [
     "cenote_renderer_stats", "cenote_renderer_set_profiling", "cenote_render_once", "cenote_film_create", "cenote_film_destroy", "cenote_film_reset",
     "cenote_film_samples", "cenote_accumulate", "cenote_accumulate_n", "cenote_film_averages", "cenote_film_sums",
     "cenote_film_device_sums", "cenote_probe_sampler", "cenote_probe_bsdf", "cenote_probe_bsdf_sample",
-    "cenote_probe_intersect", "cenote_probe_shadow", "cenote_probe_env_sample", "cenote_probe_env_pdf",
+    "cenote_probe_intersect", "cenote_probe_intersect_queued", "cenote_probe_shadow", "cenote_probe_env_sample", "cenote_probe_env_pdf",
     "cenote_env_tables_static", "cenote_scene_create_textured", "cenote_texture_bytes", "cenote_texture_encode",
     "cenote_probe_texture", "cenote_server_create", "cenote_server_destroy", "cenote_job_submit", "cenote_job_poll",
     "cenote_job_wait", "cenote_job_result", "cenote_job_release", "cenote_server_stats", "cenote_guide_create",
@@ -202,6 +203,7 @@ def library() -> C.CDLL:
         "cenote_probe_bsdf": (I32, [P, P, P, P, U32, U32, P, P]),
         "cenote_probe_bsdf_sample": (I32, [P, P, P, P, U32, U32, P, P, P]),
         "cenote_probe_intersect": (I32, [P, P, P, U32, P, P]),
+        "cenote_probe_intersect_queued": (I32, [P, P, P, U32, P, P]),
         "cenote_probe_shadow": (I32, [P, P, P, P, P, U32, P]),
         "cenote_probe_env_sample": (I32, [P, P, U32, P, P, P]),
         "cenote_probe_env_pdf": (I32, [P, P, U32, P]),
@@ -431,13 +433,15 @@ class Scene:
                                                  C.byref(power), C.byref(sel)))
         return marginal, conditional, pdfs, power.value, sel.value
 
-    def probe_intersect(self, origins: np.ndarray, directions: np.ndarray):
+    def probe_intersect(self, origins: np.ndarray, directions: np.ndarray, queued: bool = False):
+        """Closest hits; `queued` walks them through the warp triangle queue."""
         o = np.ascontiguousarray(origins, np.float32)
         d = np.ascontiguousarray(directions, np.float32)
         n = len(o)
         hits = np.zeros((n, 4), np.uint32)
         t = np.zeros(n, np.float32)
-        _check(library().cenote_probe_intersect(self._h, _ptr(o), _ptr(d), n, _ptr(hits), _ptr(t)))
+        fn = library().cenote_probe_intersect_queued if queued else library().cenote_probe_intersect
+        _check(fn(self._h, _ptr(o), _ptr(d), n, _ptr(hits), _ptr(t)))
         return hits, t
 
     def probe_shadow(self, origins, directions, tmax, targets):
@@ -595,8 +599,8 @@ class Renderer:
         return {name: getattr(t, name) for name, _ in TuningC._fields_}
 
     def set_tuning(self, material_sort: int, samples_per_wave: int = 0, refill_idle: int = 0,
-                   top_nodes: int = 0, l2_window: int = 0) -> None:
-        t = TuningC(material_sort, samples_per_wave, refill_idle, top_nodes, l2_window, 0.0)
+                   top_nodes: int = 0, l2_window: int = 0, per_lane_triangles: int = 0) -> None:
+        t = TuningC(material_sort, samples_per_wave, refill_idle, top_nodes, l2_window, per_lane_triangles, 0.0)
         _check(library().cenote_renderer_set_tuning(self._h, C.byref(t)))
 
     def autotune(self, scene: Scene, width: int, height: int) -> dict:

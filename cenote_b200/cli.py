@@ -111,7 +111,8 @@ def main(argv=None) -> int:
     r.add_argument("--device", type=int, default=0)
     r.add_argument("--samples-per-wave", type=int, default=0, help="0 = automatic")
     r.add_argument("--stats", action="store_true")
-    r.add_argument("--tuning", default="", help="launch knobs: sort,samples_per_wave,refill,top_nodes,l2")
+    r.add_argument("--tuning", default="",
+                   help="launch knobs: sort,samples_per_wave,refill,top_nodes,l2[,per_lane_triangles]")
     r.add_argument("--autotune", action="store_true", help="time the launch knobs on the scene first")
     r.add_argument("--png", default="", help="also write the tonemapped display frame here")
     r.add_argument("--exposure", type=float, default=0.0, help="display exposure in stops (--png)")

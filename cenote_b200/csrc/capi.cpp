@@ -34,6 +34,8 @@ void probe_bsdf_sample(const float* tables, const Material& m, const float3* wo,
                        uint32_t exiting, float3* wi, float* pdf, uint32_t* lobe, cudaStream_t s);
 void probe_intersect(const DeviceScene& scene, const float3* org, const float3* dir, uint32_t n, uint4* hits, float* t,
                      uint32_t* flag, cudaStream_t s);
+void probe_intersect_queued(const DeviceScene& scene, const float3* org, const float3* dir, uint32_t n, uint4* hits,
+                            float* t, uint32_t* flag, cudaStream_t s);
 void probe_shadow(const DeviceScene& scene, const float3* org, const float3* dir, const float* tmax,
                   const uint2* targets, uint32_t n, float* out, uint32_t* flag, cudaStream_t s);
 void probe_env_sample(const DeviceScene& scene, const float2* u, uint32_t n, float3* dir, float* pdf, uint2* rc,
@@ -801,11 +803,13 @@ int32_t cenote_renderer_set_tuning(cenote_renderer* r, const cenote_tuning* t) {
     CN_CHECK(t->refill_idle <= 32, CENOTE_E_INVALID_ARGUMENT, "refill threshold above a warp");
     CN_CHECK(t->top_nodes <= TOP_NODES_MAX, CENOTE_E_INVALID_ARGUMENT, "more top-level nodes than shared memory holds");
     CN_CHECK(t->l2_window <= 1, CENOTE_E_INVALID_ARGUMENT, "l2_window is 0 or 1");
+    CN_CHECK(t->per_lane_triangles <= 1, CENOTE_E_INVALID_ARGUMENT, "per_lane_triangles is 0 or 1");
     r->material_sort = t->material_sort;
     r->samples_per_wave = t->samples_per_wave;
     r->refill_idle = t->refill_idle;
     r->top_nodes = t->top_nodes;
     r->l2_window = t->l2_window;
+    r->per_lane_triangles = t->per_lane_triangles;
     return CENOTE_OK;
 }
 
@@ -816,6 +820,7 @@ int32_t cenote_renderer_get_tuning(cenote_renderer* r, cenote_tuning* out) {
     out->refill_idle = r->refill_idle;
     out->top_nodes = r->top_nodes;
     out->l2_window = r->l2_window;
+    out->per_lane_triangles = r->per_lane_triangles;
     out->ms_per_sample = r->tuned_ms_per_sample;
     return CENOTE_OK;
 }
@@ -1014,13 +1019,15 @@ int32_t cenote_renderer_autotune(cenote_renderer* r, cenote_scene* scene, uint32
     while (probe > 2 && pixels * probe > (uint64_t(1) << 27)) probe /= 2;
     const uint32_t saved_profiling = r->profiling;
     r->profiling = 0;
-    cenote_tuning best{r->material_sort, r->samples_per_wave, r->refill_idle, r->top_nodes, r->l2_window, 0.0f};
+    cenote_tuning best{r->material_sort, r->samples_per_wave, r->refill_idle, r->top_nodes,
+                       r->l2_window,        r->per_lane_triangles, 0.0f};
     auto apply = [&](const cenote_tuning& t) {
         r->material_sort = t.material_sort;
         r->samples_per_wave = t.samples_per_wave;
         r->refill_idle = t.refill_idle;
         r->top_nodes = t.top_nodes;
         r->l2_window = t.l2_window;
+        r->per_lane_triangles = t.per_lane_triangles;
     };
     // Device time of `probe` samples, the better of two runs (the first run of
     // a new wave size also allocates).
@@ -1037,16 +1044,21 @@ int32_t cenote_renderer_autotune(cenote_renderer* r, cenote_scene* scene, uint32
     };
     float best_ms = 0.0f;
     rc = measure(best, &best_ms);
-    for (int knob = 0; knob < 5 && rc == CENOTE_OK; ++knob) {
-        for (int c = 0; c < (knob == 1 ? 5 : (knob == 4 ? 2 : 3)) && rc == CENOTE_OK; ++c) {
+    // An all-opaque scene chooses between the warp triangle queue and per-lane
+    // tests; fractional opacity always tests per lane.
+    const int knobs = scene->ds.has_nonopaque ? 5 : 6;
+    for (int knob = 0; knob < knobs && rc == CENOTE_OK; ++knob) {
+        for (int c = 0; c < (knob == 1 ? 5 : (knob >= 4 ? 2 : 3)) && rc == CENOTE_OK; ++c) {
             cenote_tuning t = best;
             if (knob == 0) t.material_sort = uint32_t(c);
             if (knob == 1) t.samples_per_wave = spws[c];
             if (knob == 2) t.refill_idle = c == 0 ? 4u : (c == 1 ? 8u : 16u);
             if (knob == 3) t.top_nodes = c == 0 ? 0u : (c == 1 ? 80u : TOP_NODES_MAX);
             if (knob == 4) t.l2_window = uint32_t(c);
+            if (knob == 5) t.per_lane_triangles = uint32_t(c);
             if (t.material_sort == best.material_sort && t.samples_per_wave == best.samples_per_wave &&
-                t.refill_idle == best.refill_idle && t.top_nodes == best.top_nodes && t.l2_window == best.l2_window)
+                t.refill_idle == best.refill_idle && t.top_nodes == best.top_nodes && t.l2_window == best.l2_window &&
+                t.per_lane_triangles == best.per_lane_triangles)
                 continue;
             float ms = 0.0f;
             rc = measure(t, &ms);
@@ -1259,8 +1271,8 @@ int32_t cenote_probe_bsdf_sample(cenote_context* ctx, const cenote_material* m, 
                           });
 }
 
-int32_t cenote_probe_intersect(cenote_scene* sc, const float* origins, const float* directions, uint32_t n,
-                               uint32_t* hits, float* t) {
+static int32_t probe_closest(cenote_scene* sc, const float* origins, const float* directions, uint32_t n,
+                             uint32_t* hits, float* t, bool queued) {
     CN_CHECK(sc && origins && directions && hits && t, CENOTE_E_INVALID_ARGUMENT, "null argument");
     if (n == 0) return CENOTE_OK;
     cenote_context* ctx = sc->ctx;
@@ -1270,12 +1282,23 @@ int32_t cenote_probe_intersect(cenote_scene* sc, const float* origins, const flo
     int32_t rc = with_device_io(ctx, {{origins, size_t(n) * 12}, {directions, size_t(n) * 12}},
                                 {{hits, size_t(n) * 16}, {t, size_t(n) * 4}, {&flag, 4}},
                                 [&](std::vector<void*>& i, std::vector<void*>& o) {
-                                    probe_intersect(sc->ds, static_cast<float3*>(i[0]), static_cast<float3*>(i[1]), n,
-                                                    static_cast<uint4*>(o[0]), static_cast<float*>(o[1]),
-                                                    static_cast<uint32_t*>(o[2]), ctx->stream);
+                                    auto probe = queued ? probe_intersect_queued : probe_intersect;
+                                    probe(sc->ds, static_cast<float3*>(i[0]), static_cast<float3*>(i[1]), n,
+                                          static_cast<uint4*>(o[0]), static_cast<float*>(o[1]),
+                                          static_cast<uint32_t*>(o[2]), ctx->stream);
                                 });
     if (rc == CENOTE_OK && flag) return fail(CENOTE_E_OVERFLOW, "traversal bound exceeded");
     return rc;
+}
+
+int32_t cenote_probe_intersect(cenote_scene* sc, const float* origins, const float* directions, uint32_t n,
+                               uint32_t* hits, float* t) {
+    return probe_closest(sc, origins, directions, n, hits, t, false);
+}
+
+int32_t cenote_probe_intersect_queued(cenote_scene* sc, const float* origins, const float* directions, uint32_t n,
+                                      uint32_t* hits, float* t) {
+    return probe_closest(sc, origins, directions, n, hits, t, true);
 }
 
 int32_t cenote_probe_shadow(cenote_scene* sc, const float* origins, const float* directions, const float* tmax,

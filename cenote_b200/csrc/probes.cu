@@ -10,6 +10,7 @@
 #include "shadow.cuh"
 #include "textures.cuh"
 #include "traverse.cuh"
+#include "trqueue.cuh"
 
 namespace cn {
 namespace {
@@ -66,6 +67,50 @@ __global__ void k_probe_intersect(DeviceScene scene, const float3* org, const fl
     tout[i] = bi == LIGHT_NONE ? -1.0f : tmax;
 }
 
+// The queued closest-hit walk (trqueue.cuh) over n rays: each warp walks its
+// own contiguous share of the rays, refilling idle lanes as the wavefront
+// kernel does.
+struct ProbeSource {
+    const float3* org;
+    const float3* dir;
+    uint4* hits;
+    float* tout;
+    uint32_t cursor, end;  // the warp's next ray and the end of its share (warp-uniform)
+    __device__ __forceinline__ uint32_t next(bool live, bool& drained) {
+        const uint32_t idle = __ballot_sync(0xffffffffu, !live);
+        const uint32_t lane = threadIdx.x & 31u;
+        const uint32_t i = cursor + __popc(idle & ((1u << lane) - 1u));
+        cursor += __popc(idle);
+        if (cursor >= end) drained = true;
+        return (!live && i < end) ? i : ~0u;
+    }
+    __device__ __forceinline__ void ray(uint32_t i, float3& o, float3& d) const {
+        o = org[i];
+        d = dir[i];
+    }
+    __device__ __forceinline__ void emit(uint32_t i, uint4 h, float t) const {
+        hits[i] = h;
+        tout[i] = h.x == LIGHT_NONE ? -1.0f : t;
+    }
+    __device__ __forceinline__ void step(bool, uint32_t, uint32_t) const {}
+    __device__ __forceinline__ uint32_t want_idle(bool drained) const { return drained ? 32u : 8u; }
+};
+
+constexpr uint32_t PROBE_RAYS_PER_WARP = 256;
+
+__global__ void __launch_bounds__(128) k_probe_intersect_queued(DeviceScene scene, const float3* org,
+                                                                const float3* dir, uint32_t n, uint4* hits,
+                                                                float* tout, uint32_t* flag) {
+    __shared__ TriQueueSmem tqs[4];
+    const uint32_t warp = blockIdx.x * 4u + (threadIdx.x >> 5);
+    const uint32_t begin = warp * PROBE_RAYS_PER_WARP;
+    if (begin >= n) return;  // whole warps only
+    ProbeSource src{org, dir, hits, tout, begin, min(n, begin + PROBE_RAYS_PER_WARP)};
+    bool overflow = false;
+    queued_closest<false>(scene, tqs[threadIdx.x >> 5], src, RAY_MASK_ALL, overflow, nullptr, nullptr);
+    if (overflow) atomicOr(flag, 1u);
+}
+
 __global__ void k_probe_shadow(DeviceScene scene, const float3* org, const float3* dir, const float* tmaxs,
                                const uint2* targets, uint32_t n, float* out, uint32_t* flag) {
     uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -79,7 +124,8 @@ __global__ void k_probe_shadow(DeviceScene scene, const float3* org, const float
         uint32_t first = scene.geometry[light].light;
         if (first != LIGHT_NONE) leaf = scene.light_leaf[first + lprim];
     }
-    float a = shadow_query(scene, ray, tmaxs[i], light, lprim, leaf);
+    uint2 stack[TRAVERSAL_STACK];
+    float a = shadow_query(scene, ray, tmaxs[i], light, lprim, leaf, stack);
     if (a == -2.0f) atomicOr(flag, 1u);
     out[i] = a < 0.0f ? -1.0f : a;
 }
@@ -139,6 +185,11 @@ void probe_bsdf_sample(const float* tables, const Material& m, const float3* wo,
 void probe_intersect(const DeviceScene& scene, const float3* org, const float3* dir, uint32_t n, uint4* hits, float* t,
                      uint32_t* flag, cudaStream_t s) {
     k_probe_intersect<<<blocks(n), 128, 0, s>>>(scene, org, dir, n, hits, t, flag);
+}
+void probe_intersect_queued(const DeviceScene& scene, const float3* org, const float3* dir, uint32_t n, uint4* hits,
+                            float* t, uint32_t* flag, cudaStream_t s) {
+    const uint32_t grid = (n + 4u * PROBE_RAYS_PER_WARP - 1u) / (4u * PROBE_RAYS_PER_WARP);
+    k_probe_intersect_queued<<<grid, 128, 0, s>>>(scene, org, dir, n, hits, t, flag);
 }
 void probe_shadow(const DeviceScene& scene, const float3* org, const float3* dir, const float* tmax,
                   const uint2* targets, uint32_t n, float* out, uint32_t* flag, cudaStream_t s) {

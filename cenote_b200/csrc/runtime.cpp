@@ -76,6 +76,7 @@ cudaError_t enqueue_waves(cenote_renderer* r, const cenote_scene* sc, uint32_t w
     const uint64_t pixels = uint64_t(width) * height;
     r->pool.refill_idle = r->refill_idle;
     r->pool.top_nodes = r->top_nodes;
+    r->pool.per_lane_triangles = r->per_lane_triangles;
     WaveParams wp{};
     wp.width = width;
     wp.height = height;

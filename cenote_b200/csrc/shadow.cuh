@@ -93,14 +93,14 @@ __device__ __forceinline__ float shadow_result(const ShadowQuery& q) {
 }
 
 // The whole query for one ray: the attenuation (>= 0) when visible, -1 when
-// occluded, -2 when a traversal bound was exceeded.
+// occluded, -2 when a traversal bound was exceeded. `stack` holds
+// TRAVERSAL_STACK entries.
 template <bool COUNT = false>
 __device__ __forceinline__ float shadow_query(const DeviceScene& scene, const Ray& ray, float tmax, uint32_t light,
-                                              uint32_t lprim, uint32_t leaf, uint32_t* visits = nullptr,
+                                              uint32_t lprim, uint32_t leaf, uint2* stack, uint32_t* visits = nullptr,
                                               uint32_t* tests = nullptr) {
     ShadowQuery q;
     shadow_begin(scene, ray, tmax, light, lprim, leaf, q);
-    uint2 stack[TRAVERSAL_STACK];
     for (;;) {
         int st = shadow_step<COUNT>(scene, ray, q, stack, visits, tests);
         if (st == WALK_OVERFLOW) return -2.0f;

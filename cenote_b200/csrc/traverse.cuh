@@ -221,6 +221,29 @@ __device__ __forceinline__ void walk_begin(Walk& w, const Ray& r) {
 
 __device__ __forceinline__ uint32_t walk_bound(const DeviceScene& s) { return 4u * (s.node_count + s.tri_count) + 64u; }
 
+// Take the nearest pending inner child of the node group w.g (which must
+// have one), push what remains of the group and intersect the child: w.g
+// becomes its inner children, w.t its hit leaves' triangles. Returns false
+// when the stack is full.
+template <bool COUNT = false>
+__device__ __forceinline__ bool expand_node(const DeviceScene& s, const Ray& r, float tmax, Walk& w, uint2* stack,
+                                            uint32_t* visits) {
+    uint32_t pos = 31u - __clz(w.g.y & 0xff000000u);
+    w.g.y &= ~(1u << pos);
+    uint32_t slot = (pos - 24u) ^ r.oct_inv;
+    uint32_t ni = w.g.x + __popc(w.g.y & 0xffu & ((1u << slot) - 1u));
+    if (w.g.y & 0xff000000u) {
+        if (w.sp >= TRAVERSAL_STACK) return false;
+        stack[w.sp++] = w.g;
+    }
+    uint32_t bc, bt, im;
+    uint32_t hits = intersect_node(s, ni, r, tmax, bc, bt, im);
+    if (COUNT) ++*visits;
+    w.g = make_uint2(bc, (hits & 0xff000000u) | im);
+    w.t = make_uint2(bt, hits & 0x00ffffffu);
+    return true;
+}
+
 // One step: expand one node (or resume one postponed triangle group), then
 // test its triangles unless too few lanes of the warp would test alongside.
 // `visit` returning true stops the walk (WALK_DONE).
@@ -229,19 +252,7 @@ __device__ __forceinline__ int walk_step(const DeviceScene& s, const Ray& r, flo
                                          Visit&& visit, uint32_t* visits = nullptr, uint32_t* tests = nullptr) {
     if (++w.iter > walk_bound(s)) return WALK_OVERFLOW;
     if (w.g.y & 0xff000000u) {
-        uint32_t pos = 31u - __clz(w.g.y & 0xff000000u);
-        w.g.y &= ~(1u << pos);
-        uint32_t slot = (pos - 24u) ^ r.oct_inv;
-        uint32_t ni = w.g.x + __popc(w.g.y & 0xffu & ((1u << slot) - 1u));
-        if (w.g.y & 0xff000000u) {
-            if (w.sp >= TRAVERSAL_STACK) return WALK_OVERFLOW;
-            stack[w.sp++] = w.g;
-        }
-        uint32_t bc, bt, im;
-        uint32_t hits = intersect_node(s, ni, r, tmax, bc, bt, im);
-        if (COUNT) ++*visits;
-        w.g = make_uint2(bc, (hits & 0xff000000u) | im);
-        w.t = make_uint2(bt, hits & 0x00ffffffu);
+        if (!expand_node<COUNT>(s, r, tmax, w, stack, visits)) return WALK_OVERFLOW;
         w.resumed = false;
     } else {
         w.t = w.g;  // a postponed triangle group came off the stack

@@ -25,6 +25,7 @@
 #include "shadow.cuh"
 #include "textures.cuh"
 #include "traverse.cuh"
+#include "trqueue.cuh"
 
 namespace cn {
 
@@ -258,6 +259,56 @@ __global__ void __launch_bounds__(BLOCK, CN_TRAV_MIN_BLOCKS) k_intersect(DeviceS
             if (uint32_t(__popc(__ballot_sync(0xffffffffu, !live))) >= want_idle) break;
         }
     }
+    if (COUNT) flush_counts(pool.counters, visits, tests);
+}
+
+// The closest-hit stage for scenes whose triangles are all opaque: the same
+// persistent, refilling grid as k_intersect, with the triangle tests shared
+// by the warp through its triangle queue (trqueue.cuh). Hits are bitwise
+// those of k_intersect.
+struct IsectSource {
+    const PathPool& pool;
+    const uint32_t* queue;
+    uint32_t* fetch;
+    uint32_t count, bounce;
+    __device__ __forceinline__ uint32_t path_of(uint32_t i) const { return bounce == 0 ? i : queue[i]; }
+    __device__ __forceinline__ uint32_t next(bool live, bool& drained) { return refill(fetch, count, live, drained); }
+    __device__ __forceinline__ void ray(uint32_t i, float3& o, float3& d) const {
+        const uint32_t path = path_of(i);
+        o = xyz(pool.org[path]);
+        d = xyz(pool.dir[path]);
+    }
+    __device__ __forceinline__ void emit(uint32_t i, uint4 hit, float) const { pool.hit[path_of(i)] = hit; }
+    // Material sort: each finished ray's key goes to its queue slot and into
+    // the key counts, one atomic per distinct key per warp.
+    __device__ __forceinline__ void step(bool finished, uint32_t i, uint32_t inst) const {
+        if (!pool.sort_keys) return;
+        if (__ballot_sync(0xffffffffu, finished) == 0u) return;
+        const uint32_t key = finished ? (inst == LIGHT_NONE ? 0u : 1u + inst % (SORT_BINS - 1u)) : 0xffffffffu;
+        const uint32_t peers = __match_any_sync(0xffffffffu, key);
+        if (finished) {
+            pool.sort_keys[i] = key;
+            if (lane_id() == uint32_t(__ffs(peers) - 1)) atomicAdd(pool.sort_bins + key, uint32_t(__popc(peers)));
+        }
+    }
+    __device__ __forceinline__ uint32_t want_idle(bool drained) const {
+        return drained ? 32u : (pool.refill_idle ? pool.refill_idle : uint32_t(CN_REFILL_IDLE));
+    }
+};
+
+template <bool COUNT>
+__global__ void __launch_bounds__(BLOCK, CN_TRAV_MIN_BLOCKS)
+    k_intersect_queued(DeviceScene scene, PathPool pool, uint32_t bounce, uint32_t n0) {
+    extern __shared__ uint4 top_levels[];
+    __shared__ TriQueueSmem tqs[BLOCK / 32];
+    stage_top_levels(scene, top_levels, min(pool.top_nodes, TOP_NODES_MAX));
+    uint32_t visits = 0, tests = 0;
+    IsectSource src{pool, pool.queue[bounce & 1u], pool.counters + CTR_FETCH_ISECT + bounce,
+                    min(bounce == 0 ? n0 : pool.counters[CTR_RAYS + bounce], pool.capacity), bounce};
+    bool overflow = false;
+    queued_closest<COUNT>(scene, tqs[threadIdx.x >> 5], src, bounce == 0 ? RAY_MASK_CAMERA : RAY_MASK_ALL, overflow,
+                          &visits, &tests);
+    if (overflow) flag_overflow(pool.counters);
     if (COUNT) flush_counts(pool.counters, visits, tests);
 }
 
@@ -681,6 +732,73 @@ __global__ void __launch_bounds__(BLOCK, CN_TRAV_MIN_BLOCKS) k_shadow(DeviceScen
     if (COUNT) flush_counts(pool.counters, visits, tests);
 }
 
+// The shadow stage for scenes whose triangles are all opaque: k_shadow's
+// persistent, refilling grid with the triangle tests shared by the warp
+// through its triangle queue (trqueue.cuh). Radiance is bitwise k_shadow's.
+struct ShadowSource {
+    const DeviceScene& scene;
+    const PathPool& pool;
+    uint32_t* fetch;
+    uint32_t count;
+    __device__ __forceinline__ uint32_t next(bool live, bool& drained) { return refill(fetch, count, live, drained); }
+    __device__ __forceinline__ bool begin(uint32_t i, Ray& ray, AnyQuery& a) const {
+        const float4* rec = reinterpret_cast<const float4*>(pool.shadows + i);
+        const float4 q0 = rec[0], q1 = rec[1], q2 = rec[2], q3 = rec[3];
+        ray = make_ray(xyz(q0), xyz(q1));
+        const uint32_t light = __float_as_uint(q2.w), leaf = __float_as_uint(q3.y);
+        a.occluded = false;
+        a.light = light;
+        a.lprim = __float_as_uint(q3.x);
+        a.tm = q0.w;
+        a.leaf = 0xffffffffu;
+        if (light != LIGHT_NONE && leaf == 0xffffffffu) return false;  // no leaf: the closest-hit query
+        if (leaf < scene.tri_count) {
+            const float4* tp = scene.tris + 3u * leaf;
+            float t, b1, b2;
+            if (tri_hit(ray, __ldg(tp), __ldg(tp + 1), __ldg(tp + 2), q0.w, t, b1, b2)) {
+                a.tm = t;
+                a.leaf = leaf;
+            }
+        }
+        return true;
+    }
+    __device__ __forceinline__ void add(uint32_t i, float atten) const {
+        const float4* rec = reinterpret_cast<const float4*>(pool.shadows + i);
+        const uint32_t path = __float_as_uint(rec[1].w);
+        const float4 c = rec[2], r = pool.rad[path];
+        pool.rad[path] = make_float4(r.x + c.x * atten, r.y + c.y * atten, r.z + c.z * atten, r.w);
+    }
+    __device__ __forceinline__ void closest(uint32_t i, uint2* stack) const {
+        const float4* rec = reinterpret_cast<const float4*>(pool.shadows + i);
+        const float4 q0 = rec[0], q1 = rec[1], q2 = rec[2], q3 = rec[3];
+        const float atten = shadow_query(scene, make_ray(xyz(q0), xyz(q1)), q0.w, __float_as_uint(q2.w),
+                                         __float_as_uint(q3.x), __float_as_uint(q3.y), stack);
+        if (atten == -2.0f) flag_overflow(pool.counters);
+        else if (atten >= 0.0f) add(i, atten);
+    }
+    __device__ __forceinline__ void emit(uint32_t i, bool visible) const {
+        if (visible) add(i, 1.0f);
+    }
+    __device__ __forceinline__ uint32_t want_idle(bool drained) const {
+        return drained ? 32u : (pool.refill_idle ? pool.refill_idle : uint32_t(CN_REFILL_IDLE));
+    }
+};
+
+template <bool COUNT>
+__global__ void __launch_bounds__(BLOCK, CN_TRAV_MIN_BLOCKS)
+    k_shadow_queued(DeviceScene scene, PathPool pool, uint32_t bounce) {
+    extern __shared__ uint4 top_levels[];
+    __shared__ TriQueueSmem tqs[BLOCK / 32];
+    stage_top_levels(scene, top_levels, min(pool.top_nodes, TOP_NODES_MAX));
+    uint32_t visits = 0, tests = 0;
+    ShadowSource src{scene, pool, pool.counters + CTR_FETCH_SHADOW + bounce,
+                     min(pool.counters[CTR_SHADOWS + bounce], pool.capacity)};
+    bool overflow = false;
+    queued_any<COUNT>(scene, tqs[threadIdx.x >> 5], src, overflow, &visits, &tests);
+    if (overflow) flag_overflow(pool.counters);
+    if (COUNT) flush_counts(pool.counters, visits, tests);
+}
+
 // ---- film --------------------------------------------------------------------------
 
 __device__ __forceinline__ bool finite4(float4 v) {
@@ -882,10 +1000,20 @@ LaunchShape launch_shape(int device) {
     int occ = 0;
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_intersect<false>, BLOCK, TOP_NODES_MAX * 80u);
     ls.grid_isect = sms * (occ > 0 ? occ : 4);
+    // The queued kernel's own shared memory leaves fewer blocks room for the
+    // staged top levels: size its grid for the launch's dynamic shared memory.
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_intersect_queued<false>, BLOCK, 0);
+    ls.grid_isect_queued = sms * (occ > 0 ? occ : 4);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_intersect_queued<false>, BLOCK, TOP_NODES_MAX * 80u);
+    ls.grid_isect_queued_top = sms * (occ > 0 ? occ : 4);
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_shade<true, false>, BLOCK, 0);
     ls.grid_shade = sms * (occ > 0 ? occ : 4);
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_shadow<false>, BLOCK, TOP_NODES_MAX * 80u);
     ls.grid_shadow = sms * (occ > 0 ? occ : 4);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_shadow_queued<false>, BLOCK, 0);
+    ls.grid_shadow_queued = sms * (occ > 0 ? occ : 4);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_shadow_queued<false>, BLOCK, TOP_NODES_MAX * 80u);
+    ls.grid_shadow_queued_top = sms * (occ > 0 ? occ : 4);
     ls.grid_stream = sms * 8;
     return ls;
 }
@@ -898,8 +1026,15 @@ void launch_wave_begin(const PathPool& pool, const WaveParams& wp, const LaunchS
 void launch_intersect(const DeviceScene& scene, const PathPool& pool, uint32_t bounce, uint32_t n0,
                       const LaunchShape& ls, bool count_visits, cudaStream_t stream) {
     const size_t smem = size_t(min(pool.top_nodes, TOP_NODES_MAX)) * 80u;
-    if (count_visits) k_intersect<true><<<ls.grid_isect, BLOCK, smem, stream>>>(scene, pool, bounce, n0);
-    else k_intersect<false><<<ls.grid_isect, BLOCK, smem, stream>>>(scene, pool, bounce, n0);
+    if (!scene.has_nonopaque && !pool.per_lane_triangles) {
+        const int grid = smem ? ls.grid_isect_queued_top : ls.grid_isect_queued;
+        if (count_visits) k_intersect_queued<true><<<grid, BLOCK, smem, stream>>>(scene, pool, bounce, n0);
+        else k_intersect_queued<false><<<grid, BLOCK, smem, stream>>>(scene, pool, bounce, n0);
+    } else if (count_visits) {
+        k_intersect<true><<<ls.grid_isect, BLOCK, smem, stream>>>(scene, pool, bounce, n0);
+    } else {
+        k_intersect<false><<<ls.grid_isect, BLOCK, smem, stream>>>(scene, pool, bounce, n0);
+    }
 }
 
 void launch_shade(const DeviceScene& scene, const PathPool& pool, uint32_t bounce, const WaveParams& wp, uint32_t n0,
@@ -917,8 +1052,15 @@ void launch_shade(const DeviceScene& scene, const PathPool& pool, uint32_t bounc
 void launch_shadow(const DeviceScene& scene, const PathPool& pool, uint32_t bounce, const LaunchShape& ls,
                    bool count_visits, cudaStream_t stream) {
     const size_t smem = size_t(min(pool.top_nodes, TOP_NODES_MAX)) * 80u;
-    if (count_visits) k_shadow<true><<<ls.grid_shadow, BLOCK, smem, stream>>>(scene, pool, bounce);
-    else k_shadow<false><<<ls.grid_shadow, BLOCK, smem, stream>>>(scene, pool, bounce);
+    if (!scene.has_nonopaque && !pool.per_lane_triangles) {
+        const int grid = smem ? ls.grid_shadow_queued_top : ls.grid_shadow_queued;
+        if (count_visits) k_shadow_queued<true><<<grid, BLOCK, smem, stream>>>(scene, pool, bounce);
+        else k_shadow_queued<false><<<grid, BLOCK, smem, stream>>>(scene, pool, bounce);
+    } else if (count_visits) {
+        k_shadow<true><<<ls.grid_shadow, BLOCK, smem, stream>>>(scene, pool, bounce);
+    } else {
+        k_shadow<false><<<ls.grid_shadow, BLOCK, smem, stream>>>(scene, pool, bounce);
+    }
 }
 
 void launch_wave(const DeviceScene& scene, const PathPool& pool, const WaveParams& wp, const LaunchShape& ls,

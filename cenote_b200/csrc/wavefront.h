@@ -58,6 +58,9 @@ struct PathPool {
     uint32_t refill_idle;
     // BVH nodes each traversal block stages in shared memory (0..TOP_NODES_MAX).
     uint32_t top_nodes;
+    // 1: traversal lanes test their own triangles even in an all-opaque scene
+    // (0: the warp triangle queue, trqueue.cuh).
+    uint32_t per_lane_triangles;
 };
 
 constexpr uint32_t TOP_NODES_MAX = 320;  // 25.6 KB per 128-thread block: 8 blocks still fit an SM
@@ -91,7 +94,8 @@ struct WaveParams {
 constexpr uint32_t SORT_BINS = 2048;
 
 struct LaunchShape {
-    int grid_isect, grid_shade, grid_shadow, grid_stream;
+    int grid_isect, grid_isect_queued, grid_isect_queued_top, grid_shade, grid_shadow, grid_shadow_queued,
+        grid_shadow_queued_top, grid_stream;
     int block;
 };
 

@@ -267,14 +267,17 @@ typedef struct cenote_tuning {
     uint32_t refill_idle;      /* idle lanes (1..32) before a traversal warp takes new rays (0 = default 8) */
     uint32_t top_nodes;        /* BVH top-level nodes staged in shared memory per traversal block (0..320) */
     uint32_t l2_window;        /* 1: the BVH nodes are a persisting L2 access-policy window during the waves */
+    uint32_t per_lane_triangles; /* 1: each traversal lane tests its own triangles; 0: a warp shares its
+                                  * pending triangle tests through a queue (scenes whose triangles are all
+                                  * opaque; scenes with fractional opacity always test per lane) */
     float ms_per_sample;       /* autotune: device time of one sample of every pixel at the chosen setting */
 } cenote_tuning;
 int32_t cenote_renderer_set_tuning(cenote_renderer* r, const cenote_tuning* tuning);
 int32_t cenote_renderer_get_tuning(cenote_renderer* r, cenote_tuning* out);
 /* Time candidate settings on `scene` at width x height (a scratch film, a few
  * hundred ms of device time at 1080p) by coordinate descent over the sort
- * mode, samples per wave, refill threshold, shared-memory top levels and
- * the L2 persistence window;
+ * mode, samples per wave, refill threshold, shared-memory top levels, the
+ * L2 persistence window and per-lane or queued triangle tests;
  * apply the fastest to `r` and
  * report it in `out` (nullable). The renderer's stats afterwards describe the
  * last probe. */
@@ -340,6 +343,11 @@ int32_t cenote_probe_bsdf_sample(cenote_context* ctx, const cenote_material* mat
  * b1 bits, b2 bits) per ray, instance 0xffffffff on a miss; t = hit distance. */
 int32_t cenote_probe_intersect(cenote_scene* scene, const float* origins, const float* directions, uint32_t n,
                                uint32_t* hits, float* t);
+/* The same query through the warp triangle queue the wavefront uses for
+ * all-opaque scenes (every lane of a warp tests the warp's pending
+ * triangles); results equal cenote_probe_intersect's bit for bit. */
+int32_t cenote_probe_intersect_queued(cenote_scene* scene, const float* origins, const float* directions,
+                                      uint32_t n, uint32_t* hits, float* t);
 /* Shadow query: attenuation ≥ 0 when the (instance, primitive) target — or
  * nothing, for target instance 0xffffffff — is the closest hit within tmax;
  * -1 when occluded. */

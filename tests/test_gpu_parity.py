@@ -132,11 +132,12 @@ def random_rays(spec, n, seed):
     return org, d
 
 
+@pytest.mark.parametrize("queued", [False, True], ids=["per_lane", "warp_queue"])
 @pytest.mark.parametrize("which", ["cornell", "chart_small"])
-def test_closest_hits_bit_exact(request, which):
+def test_closest_hits_bit_exact(request, which, queued):
     spec, dev, ref = request.getfixturevalue(which)
     org, d = random_rays(spec, 200000, seed=5)
-    hits, t = dev.probe_intersect(org, d)
+    hits, t = dev.probe_intersect(org, d, queued=queued)
     rh, rt = ref.intersect(org, d)
     assert np.array_equal(hits, rh)
     assert np.array_equal(t.view(np.uint32), rt.view(np.uint32))

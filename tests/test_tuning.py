@@ -63,8 +63,8 @@ def test_tuning_knobs_leave_the_film_unchanged(ctx):
     spec = scenes.chart(96, 54, 4, 8)
     scene = Scene(ctx, spec)
     films = []
-    for knobs in [(SORT_NONE, 0, 0, 0, 0), (SORT_ALL, 1, 4, 80, 1), (SORT_SECONDARY, 4, 16, 320, 0),
-                  (SORT_ALL, 2, 32, 1, 1), (SORT_NONE, 3, 8, 7, 0)]:
+    for knobs in [(SORT_NONE, 0, 0, 0, 0, 0), (SORT_ALL, 1, 4, 80, 1, 1), (SORT_SECONDARY, 4, 16, 320, 0, 0),
+                  (SORT_ALL, 2, 32, 1, 1, 0), (SORT_NONE, 3, 8, 7, 0, 1), (SORT_ALL, 0, 8, 0, 0, 1)]:
         r = Renderer(ctx, 8)
         r.set_tuning(*knobs)
         f = Film(ctx, spec.width, spec.height)
@@ -84,7 +84,7 @@ def test_autotune_picks_a_valid_setting_and_keeps_it(ctx):
     assert t["material_sort"] in (SORT_NONE, SORT_ALL, SORT_SECONDARY)
     assert t["refill_idle"] in (0, 4, 8, 16) and t["top_nodes"] in (0, 80, 320) and t["ms_per_sample"] > 0
     kept = r.tuning()
-    knobs = ("material_sort", "samples_per_wave", "refill_idle", "top_nodes", "l2_window")
+    knobs = ("material_sort", "samples_per_wave", "refill_idle", "top_nodes", "l2_window", "per_lane_triangles")
     assert {k: kept[k] for k in knobs} == {k: t[k] for k in knobs}
     f, g = Film(ctx, spec.width, spec.height), Film(ctx, spec.width, spec.height)
     r.accumulate(scene, f, 8)
@@ -102,3 +102,5 @@ def test_bad_tuning_is_refused(ctx):
         r.set_tuning(SORT_ALL, 0, 8, 321)
     with pytest.raises(CenoteError):
         r.set_tuning(SORT_ALL, 0, 8, 0, 2)
+    with pytest.raises(CenoteError):
+        r.set_tuning(SORT_ALL, 0, 8, 0, 0, 2)
