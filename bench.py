@@ -239,11 +239,13 @@ def run_serving(args):
     progressive render jobs drawn uniformly from the closed box, the material
     chart and the large scene, at a resolution uniform in {256², 640x360,
     1280x720, 1920x1080} and a target spp log-uniform in 1..256, admitted
-    against a 160 GB budget with a frame every 4 spp. Reports time to first
-    frame and time to target spp (p50/p99 over jobs, submission to event, on
-    the server's clock) and the aggregate samples/s from the first submission
-    to the last completion."""
-    from cenote_b200 import JOB_DONE, Context, Scene, Server, scenes
+    against a 160 GB budget with a frame every 4 spp. With --concurrency C
+    the same job draws run as a closed loop instead: C jobs in flight, each
+    completion submitting the next. Reports time to first frame and time to
+    target spp (p50/p99 over jobs, submission to event, on the server's clock)
+    and the aggregate samples/s from the first submission to the last
+    completion."""
+    from cenote_b200 import JOB_DONE, JOB_FAILED, Context, Scene, Server, scenes
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return
@@ -268,11 +270,25 @@ def run_serving(args):
     ids = []
     with ClockSampler(0) as clocks:
         t0 = time.perf_counter()
-        for at, n, w, h, spp in jobs:
-            delay = at - (time.perf_counter() - t0)
-            if delay > 0:
-                time.sleep(delay)
-            ids.append(server.submit(resident[n], w, h, spp, specs[n][1]))
+        if args.concurrency:
+            # Closed loop: `concurrency` jobs in flight, each completion
+            # submitting the stream's next job at once.
+            pending = list(jobs)
+            live = []
+            while pending or live:
+                while pending and len(live) < args.concurrency:
+                    _, n, w, h, spp = pending.pop(0)
+                    j = server.submit(resident[n], w, h, spp, specs[n][1])
+                    ids.append(j)
+                    live.append(j)
+                time.sleep(0.0005)
+                live = [j for j in live if server.poll(j).state not in (JOB_DONE, JOB_FAILED)]
+        else:
+            for at, n, w, h, spp in jobs:
+                delay = at - (time.perf_counter() - t0)
+                if delay > 0:
+                    time.sleep(delay)
+                ids.append(server.submit(resident[n], w, h, spp, specs[n][1]))
         for j in ids:
             server.wait(j, 1800000.0)
     st = [server.poll(j) for j in ids]
@@ -285,7 +301,9 @@ def run_serving(args):
         "metric": "p99 time to first frame (batched serving)", "value": pct(ttff, 99), "unit": "ms",
         "higher_is_better": False, "n_gpus": 1, "scaling": "none", "vs_baseline": None, "dtype": "f32",
         "data": "synthetic (procedural scenes, seeded job stream)",
-        "config": {"workload": f"{args.jobs} jobs, Poisson 200/s, scenes {{closed box, material chart, large}}, "
+        "config": {"workload": (f"{args.jobs} jobs, closed loop with {args.concurrency} jobs in flight"
+                                if args.concurrency else f"{args.jobs} jobs, Poisson 200/s")
+                               + ", scenes {closed box, material chart, large}, "
                                "resolutions {256^2, 640x360, 1280x720, 1920x1080}, spp log-uniform 1..256, "
                                "160 GB budget, 8 slots, 64 resident jobs, a frame every 4 spp"},
         "time_to_first_frame_ms": {"p50": pct(ttff, 50), "p99": pct(ttff, 99), "max": float(ttff.max())},
@@ -348,6 +366,8 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="chart", choices=list(WORKLOADS) + ["serving", "guiding"])
     ap.add_argument("--jobs", type=int, default=256, help="serving: jobs in the Poisson stream")
+    ap.add_argument("--concurrency", type=int, default=0,
+                    help="serving: keep this many jobs in flight (closed loop) instead of the Poisson arrivals")
     ap.add_argument("--width", type=int, default=480, help="guiding: image width")
     ap.add_argument("--height", type=int, default=270, help="guiding: image height")
     ap.add_argument("--reference-spp", type=int, default=16384, help="guiding: spp of the plain reference")

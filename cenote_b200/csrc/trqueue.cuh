@@ -10,9 +10,11 @@
 // per-warp FIFO in shared memory and keeps walking; once the FIFO holds a
 // warp's worth of triangles (or no lane has nodes left), a round hands one
 // (ray, triangle) pair to every lane: a warp scan of the entries' bit counts
-// maps lane j to its entry and bit, the owner's ray comes over shuffles, and each owner's candidates reduce to the lexicographic minimum
-// of (t, instance, primitive) with warp reductions. A lane whose walk has
-// ended waits for its queued triangles before it takes a new ray.
+// maps lane j to its entry and bit, the owner's ray comes over shuffles, and
+// each owner's candidates reduce to the lexicographic minimum of (t,
+// instance, primitive) through shared-memory atomic minima (any-hit queries:
+// an OR of occluders). A lane whose walk has ended waits for its queued
+// triangles before it takes a new ray.
 //
 // Results are bitwise those of the per-lane walk: the watertight test of a
 // (ray, triangle) pair is the same arithmetic wherever it runs, and both
@@ -31,7 +33,6 @@ namespace cn {
 
 constexpr uint32_t TQ_CAP = 64;  // FIFO entries per warp (a power of two, at least 2 x 32)
 constexpr uint32_t TQ_FULL = 0xffffffffu;
-
 
 // One warp's queue in shared memory (896 bytes), small enough that a full SM
 // of traversal blocks leaves the L1 cache (which holds the walks' stacks and
