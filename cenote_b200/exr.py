@@ -1,12 +1,14 @@
-"""Minimal OpenEXR scanline writer/reader: FLOAT channels, no compression or
-RLE (compression 0/1), one scanline per block — enough for the renderer's
+"""Minimal OpenEXR scanline writer/reader: the writer stores FLOAT or HALF
+channels uncompressed, one scanline per block — enough for the renderer's
 linear output (crates/cenote/src/output.rs writes the same channel set:
-R, G, B, A, albedo.*, normal.*, Z) and for reading the reference's RLE
-goldens. Written from the OpenEXR file-layout document.
+R, G, B, A, albedo.*, normal.*, Z); the reader also takes RLE, ZIPS and ZIP
+(16-line) blocks and single-level tiles, enough for the reference's goldens
+and the corpus's sky images. Written from the OpenEXR file-layout document.
 """
 from __future__ import annotations
 
 import struct
+import zlib
 
 import numpy as np
 
@@ -81,19 +83,32 @@ def _rle_decode(src: bytes, n: int) -> bytes:
         else:
             out += src[i:i + 1] * (c + 1)
             i += 1
-    # predictor + interleave reversal (OpenEXR RLE/ZIP pre-processing)
-    buf = bytearray(out)
-    for k in range(1, len(buf)):
-        buf[k] = (buf[k - 1] + buf[k] - 128) & 0xFF
+    return _unpredict(bytes(out))
+
+
+def _unpredict(data: bytes) -> bytes:
+    """Reverse OpenEXR's RLE/ZIP pre-processing: the byte-delta predictor,
+    then the split of even and odd bytes into two halves."""
+    t = np.frombuffer(data, np.uint8).astype(np.int64)
+    if len(t) == 0:
+        return b""
+    d = t - 128
+    d[0] = t[0]
+    buf = (np.cumsum(d) & 0xFF).astype(np.uint8)
     half = (len(buf) + 1) // 2
-    res = bytearray(len(buf))
+    res = np.empty(len(buf), np.uint8)
     res[0::2] = buf[:half]
     res[1::2] = buf[half:]
-    return bytes(res)
+    return res.tobytes()
+
+
+def _zip_decode(src: bytes) -> bytes:
+    return _unpredict(zlib.decompress(src))
 
 
 def read_exr(path) -> dict[str, np.ndarray]:
-    """FLOAT scanline images, compression none or RLE."""
+    """Scanline or single-level tiled images of HALF, FLOAT or UINT channels,
+    compression none, RLE, ZIPS or ZIP."""
     raw = open(path, "rb").read()
     assert struct.unpack("<i", raw[:4])[0] == MAGIC
     pos = 8
@@ -126,6 +141,10 @@ def read_exr(path) -> dict[str, np.ndarray]:
         expect = sum(sizes[t] for _, t in chans) * rows * cols
         if comp == 1 and n < expect:
             payload = _rle_decode(payload, expect)
+        elif comp in (2, 3) and n < expect:
+            payload = _zip_decode(payload)
+        elif comp not in (0, 1, 2, 3):
+            raise ValueError(f"{path}: EXR compression {comp} is not read")
         p = 0
         for r in range(rows):
             for name, t in chans:
@@ -147,8 +166,10 @@ def read_exr(path) -> dict[str, np.ndarray]:
             cols, rows = min(tx, w - cx * tx), min(ty, h - cy * ty)
             unpack(raw[off + 20:off + 20 + n], n, rows, cols, cy * ty, cx * tx)
         return out
-    offsets = struct.unpack(f"<{h}Q", raw[pos:pos + 8 * h])
+    lines = 16 if comp == 3 else 1  # scanlines per block
+    blocks = (h + lines - 1) // lines
+    offsets = struct.unpack(f"<{blocks}Q", raw[pos:pos + 8 * blocks])
     for off in offsets:
         y, n = struct.unpack("<ii", raw[off:off + 8])
-        unpack(raw[off + 8:off + 8 + n], n, 1, w, y - y0, 0)
+        unpack(raw[off + 8:off + 8 + n], n, min(lines, h - (y - y0)), w, y - y0, 0)
     return out

@@ -18,8 +18,17 @@ a corpus scene renders here as it does there:
   (crates/cenote/src/scene/description.rs:313-340) and colours enter through
   Rec.709 -> ACEScg (crates/cenote/src/scene/lower.rs:316-373);
 * `trianglemesh` verbatim (flipped per ReverseOrientation XOR a mirroring
-  transform), `sphere` tessellated 32 rings x 64 segments (shape.rs:108-154),
-  missing normals derived smooth and area-weighted;
+  transform), `plymesh` read as stored (map/mod.rs:579-598: no flip), `sphere`
+  tessellated 32 rings x 64 segments (shape.rs:108-154), missing normals
+  derived smooth and area-weighted;
+* `imagemap` textures on colour slots (map/mod.rs:1223-1258, 1300-1358):
+  the image feeds the slot, whose constant becomes 1;
+* an image `infinite` light: its square equal-area octahedral EXR resampled
+  to the equirect sky the renderer reads, orientation and `scale` baked in
+  (crates/cenote-pbrt/src/env.rs:36-176, map/mod.rs:853-907); an image-less
+  one becomes a constant sky;
+* media (`MakeNamedMedium`, `MediumInterface`) are ignored with a warning, as
+  the reference's importer ignores them (map/mod.rs:402-408);
 * `Integrator` maxdepth -> bounce cap, `Sampler` pixelsamples -> spp, `Film`
   resolution.
 
@@ -182,16 +191,43 @@ def sphere_mesh(radius: float) -> scenes.Mesh:
                        np.array(tris, np.uint32))
 
 
+def _cross32(a: np.ndarray, b: np.ndarray) -> np.ndarray:
+    f = np.float32
+    return np.stack([a[:, 1] * b[:, 2] - b[:, 1] * a[:, 2], a[:, 2] * b[:, 0] - b[:, 2] * a[:, 0],
+                     a[:, 0] * b[:, 1] - b[:, 0] * a[:, 1]], -1).astype(f)
+
+
 def derive_normals(positions: np.ndarray, indices: np.ndarray) -> np.ndarray:
-    """Smooth, area-weighted vertex normals from the winding."""
-    p = positions.astype(np.float64)
-    face = np.cross(p[indices[:, 1]] - p[indices[:, 0]], p[indices[:, 2]] - p[indices[:, 0]])
+    """Smooth, area-weighted vertex normals from the winding, in the
+    reference's f32 arithmetic (crates/cenote/src/scene/lower.rs:532-550):
+    each face's unnormalised cross product adds onto its corners in triangle
+    order, then each sum is scaled by the reciprocal of its length; a vertex
+    whose sum cannot normalise takes +Y."""
+    f = np.float32
+    p = np.asarray(positions, f)
+    idx = np.asarray(indices, np.int64).reshape(-1, 3)
+    face = _cross32(p[idx[:, 1]] - p[idx[:, 0]], p[idx[:, 2]] - p[idx[:, 0]])
     n = np.zeros_like(p)
-    for k in range(3):
-        np.add.at(n, indices[:, k], face)
-    length = np.linalg.norm(n, axis=1, keepdims=True)
-    n = np.where(length > 0, n / np.maximum(length, 1e-300), np.array([0.0, 0.0, 1.0]))
-    return n.astype(np.float32)
+    np.add.at(n, idx.ravel(), np.repeat(face, 3, axis=0))  # f32, corners in triangle order
+    dot = ((n[:, 0] * n[:, 0] + n[:, 1] * n[:, 1]) + n[:, 2] * n[:, 2]).astype(f)
+    with np.errstate(divide="ignore", invalid="ignore", over="ignore"):
+        rcp = (f(1.0) / np.sqrt(dot)).astype(f)
+    ok = np.isfinite(rcp) & (rcp > 0)
+    out = np.where(ok[:, None], n * np.where(ok, rcp, f(0.0))[:, None], np.array([0.0, 1.0, 0.0], f))
+    return out.astype(f)
+
+
+def _inverse3_f32(m: np.ndarray) -> np.ndarray:
+    """A 3x3 inverse as glam's Mat3::inverse computes it in f32: the columns'
+    cross products over the determinant."""
+    f = np.float32
+    c = np.asarray(m, f).T  # c[k] = column k
+    t0 = _cross32(c[1][None], c[2][None])[0]
+    t1 = _cross32(c[2][None], c[0][None])[0]
+    t2 = _cross32(c[0][None], c[1][None])[0]
+    det = f((c[2][0] * t2[0] + c[2][1] * t2[1]) + c[2][2] * t2[2])
+    inv = f(1.0) / det
+    return np.stack([t0 * inv, t1 * inv, t2 * inv], 0).astype(f)  # rows = the transposed columns
 
 
 class _State:
@@ -248,8 +284,98 @@ def _lower(d) -> np.ndarray:
     return m
 
 
+def _sphere_to_square(d: np.ndarray) -> np.ndarray:
+    """Clarberg's equal-area sphere -> square map (env.rs:103-128), f32:
+    +z at the square's centre, -z at its corners. d: (N, 3) unit vectors."""
+    f = np.float32
+    x, y, z = np.abs(d[:, 0]), np.abs(d[:, 1]), np.abs(d[:, 2])
+    r = np.sqrt(np.maximum(f(1.0) - z, f(0.0)))
+    a, b = np.maximum(x, y), np.minimum(x, y)
+    with np.errstate(divide="ignore", invalid="ignore"):
+        b = np.where(a == 0, f(0.0), b / np.where(a == 0, f(1.0), a)).astype(f)
+    phi = (np.arctan(b.astype(np.float64)).astype(f) * f(2.0 / math.pi)).astype(f)
+    phi = np.where(x < y, f(1.0) - phi, phi)
+    v = phi * r
+    u = r - v
+    neg = d[:, 2] < 0
+    u, v = np.where(neg, f(1.0) - v, u), np.where(neg, f(1.0) - u, v)
+    u = np.copysign(u, d[:, 0])
+    v = np.copysign(v, d[:, 1])
+    return np.stack([f(0.5) * (u + f(1.0)), f(0.5) * (v + f(1.0))], -1).astype(f)
+
+
+def _wrap_square(x: np.ndarray, y: np.ndarray):
+    """Mirror taps back into the square across the octahedron's seams
+    (env.rs:130-150, pbrt's WrapEqualAreaSquare)."""
+    f = np.float32
+    lo, hi = x < 0, x > 1
+    x = np.where(lo, -x, np.where(hi, f(2.0) - x, x))
+    y = np.where(lo | hi, f(1.0) - y, y)
+    lo, hi = y < 0, y > 1
+    x = np.where(lo | hi, f(1.0) - x, x)
+    y = np.where(lo, -y, np.where(hi, f(2.0) - y, y))
+    return x.astype(f), y.astype(f)
+
+
+def resample_octahedral(texels: np.ndarray, world_from_light: np.ndarray, scale: float) -> np.ndarray:
+    """A square equal-area octahedral sky (S, S, 3), linear Rec.709, as the
+    equirect image (S, 2S, 3) the renderer's environment reads (row 0 the +Y
+    zenith, the horizontal centre facing -Z), radiance times `scale`, each
+    direction mapped into the light's frame first (env.rs:36-77, 88-100,
+    152-176), in f32."""
+    f = np.float32
+    size = texels.shape[0]
+    if texels.shape[1] != size:
+        raise ValueError(f"an infinite light's image is {texels.shape[1]}x{size}: pbrt-v4 skies are square "
+                         "equal-area octahedral images")
+    ow = min(2 * size, 4096)
+    oh = ow // 2
+    light_from_world = _inverse3_f32(world_from_light)
+    u = ((np.arange(ow, dtype=f) + f(0.5)) / f(ow)).astype(f)
+    v = ((np.arange(oh, dtype=f) + f(0.5)) / f(oh)).astype(f)
+    uu, vv = np.meshgrid(u, v)
+    phi = (f(2.0 * math.pi) * (uu - f(0.5))).astype(f)
+    theta = (f(math.pi) * vv).astype(f)
+    # f32 sines and cosines correctly rounded (through f64), as the C
+    # library's sinf/cosf return them.
+    t64, p64 = theta.astype(np.float64), phi.astype(np.float64)
+    st, ct = np.sin(t64).astype(f), np.cos(t64).astype(f)
+    d = np.stack([st * np.sin(p64).astype(f), ct, -st * np.cos(p64).astype(f)], -1).reshape(-1, 3).astype(f)
+    m = light_from_world
+    ld = np.stack([(m[r, 0] * d[:, 0] + m[r, 1] * d[:, 1]) + m[r, 2] * d[:, 2] for r in range(3)], -1).astype(f)
+    dot = ((ld[:, 0] * ld[:, 0] + ld[:, 1] * ld[:, 1]) + ld[:, 2] * ld[:, 2]).astype(f)
+    ld = (ld * (f(1.0) / np.sqrt(dot)).astype(f)[:, None]).astype(f)
+    uv = _sphere_to_square(ld)
+    sz = f(size)
+    px, py = (uv[:, 0] * sz - f(0.5)).astype(f), (uv[:, 1] * sz - f(0.5)).astype(f)
+    x0, y0 = np.floor(px).astype(f), np.floor(py).astype(f)
+    fx, fy = (px - x0).astype(f), (py - y0).astype(f)
+    flat = np.asarray(texels, f).reshape(-1, 3)
+    out = np.zeros((len(px), 3), f)
+    for dx, dy, w in ((0, 0, (f(1) - fx) * (f(1) - fy)), (1, 0, fx * (f(1) - fy)), (0, 1, (f(1) - fx) * fy),
+                      (1, 1, fx * fy)):
+        tx, ty = _wrap_square(((x0 + f(dx) + f(0.5)) / sz).astype(f), ((y0 + f(dy) + f(0.5)) / sz).astype(f))
+        ix = np.minimum((tx * sz).astype(np.int64), size - 1)
+        iy = np.minimum((ty * sz).astype(np.int64), size - 1)
+        out = (out + w.astype(f)[:, None] * flat[iy * size + ix]).astype(f)
+    return (out * f(scale)).astype(f).reshape(oh, ow, 3)
+
+
+def sky_environment(octahedral: np.ndarray, world_from_light: np.ndarray, scale: float) -> scenes.Environment:
+    """The renderer's environment for an image infinite light: the
+    octahedral sky resampled to equirect, then to ACEScg."""
+    return scenes.environment_rec709(resample_octahedral(np.asarray(octahedral, np.float32), world_from_light, scale))
+
+
 class PbrtImport:
-    def __init__(self):
+    def __init__(self, base: Path | None = None):
+        self.base = Path(base) if base is not None else Path(".")
+        self.textures = []       # scenes.Texture, the bindless table
+        self.named_textures = {}  # name -> (path, encoding)
+        self.texture_slots = {}   # (path, srgb) -> table index
+        self.environment = scenes.Environment.constant((0.0, 0.0, 0.0))
+        self.sky = False
+        self.sky_source = None  # (octahedral Rec.709 texels, world_from_light, scale) of an image sky
         self.warnings = []
         self.named = {}
         self.objects = []
@@ -268,8 +394,35 @@ class PbrtImport:
         r = 0.0 if r is None else max(float(r), 0.0)
         return r ** (0.25 if remap else 0.5)
 
+    def _texture_slot(self, name: str, color: bool) -> int:
+        """The table index of named imagemap texture `name` (an 8-bit PNG)."""
+        from .scene_file import read_png
+        path, encoding = self.named_textures[name]
+        srgb = color if encoding is None else encoding == "sRGB"
+        key = (str(path), srgb)
+        if key not in self.texture_slots:
+            img = read_png(path)
+            if img.shape[2] == 1:
+                img = np.repeat(img, 3, 2)
+            if img.shape[2] == 2:
+                img = np.concatenate([np.repeat(img[..., :1], 3, 2), img[..., 1:]], 2)
+            if img.shape[2] == 3:
+                img = np.concatenate([img, np.full(img.shape[:2] + (1,), 255, np.uint8)], 2)
+            self.textures.append(scenes.Texture(scenes.TEX_RGBA8_SRGB if srgb else scenes.TEX_RGBA8_UNORM,
+                                                img.shape[1], img.shape[0], np.ascontiguousarray(img)))
+            self.texture_slots[key] = len(self.textures) - 1
+        return self.texture_slots[key]
+
     def _material(self, ty, p: _Params):
         refl = p.values("reflectance")
+        if ty == "diffuse" and p.type_of("reflectance") == "texture":
+            name = str(refl[0])
+            if name in self.named_textures:
+                d = _openpbr(base_color=(1.0, 1.0, 1.0), specular_weight=0.0)
+                d["base_color_texture"] = self._texture_slot(name, True)
+                return d
+            self.warnings.append(f'unknown texture "{name}": mid-grey used')
+            return _openpbr(base_color=(0.5, 0.5, 0.5), specular_weight=0.0)
         if ty == "diffuse":
             return _openpbr(base_color=tuple(refl) if refl else (0.5, 0.5, 0.5), specular_weight=0.0)
         if ty == "coateddiffuse":
@@ -377,6 +530,17 @@ class PbrtImport:
                     self.warnings.append(f"area light {names} is not supported")
             elif d == "Shape":
                 self._shape(names[0], p, st)
+            elif d == "Texture":
+                if len(names) >= 3 and names[2] == "imagemap" and p.get_one("filename") is not None:
+                    enc = p.get_one("encoding")
+                    self.named_textures[names[0]] = (self.base / str(p.get_one("filename")),
+                                                     enc if enc in ("sRGB", "linear") else None)
+                else:
+                    self.warnings.append(f"texture {names} is not supported")
+            elif d == "LightSource":
+                self._light(names[0] if names else "", p, st)
+            elif d in ("MakeNamedMedium", "MediumInterface"):
+                self.warnings.append(f"{d}: participating media are not supported, ignored")
             elif d in ("WorldEnd", "PixelFilter", "ColorSpace", "Option"):
                 pass
             else:
@@ -384,6 +548,26 @@ class PbrtImport:
         if not in_world or self.camera is None:
             raise ValueError("pbrt file has no WorldBegin / Camera")
         return self
+
+    def _light(self, ty, p: _Params, st: _State):
+        if ty != "infinite":
+            self.warnings.append(f'light "{ty}" is not supported')
+            return
+        if self.sky:
+            self.warnings.append("one environment is rendered: a further infinite light is skipped")
+            return
+        scale = float(p.get_one("scale", 1.0))
+        if p.get_one("filename") is not None:
+            from .exr import read_exr
+            ch = read_exr(self.base / str(p.get_one("filename")))
+            src = np.stack([ch["R"], ch["G"], ch["B"]], -1).astype(np.float32)
+            world_from_light = (self.conjugation @ st.ctm)[:3, :3].astype(np.float32)
+            self.sky_source = (src, world_from_light, scale)
+            self.environment = sky_environment(src, world_from_light, scale)
+        else:
+            rgb = np.asarray(p.values("L") or (1.0, 1.0, 1.0), np.float32) * np.float32(scale)
+            self.environment = scenes.environment_rec709(np.tile(rgb.reshape(1, 1, 3), (1, 2, 1)))
+        self.sky = True
 
     def _shape(self, ty, p: _Params, st: _State):
         flip = st.reverse ^ (np.linalg.det(st.ctm[:3, :3]) < 0)
@@ -402,6 +586,14 @@ class PbrtImport:
             if nrm is None:
                 nrm = derive_normals(pos, idx)
             mesh = scenes.Mesh(pos, nrm, uv, idx)
+        elif ty == "plymesh":
+            from .scene_file import read_ply
+            if flip:
+                self.warnings.append("ReverseOrientation on a plymesh is ignored")
+            pos, nrm, uv, idx = read_ply(self.base / str(p.get_one("filename")))
+            nrm = derive_normals(pos, idx) if nrm is None else nrm
+            uv = np.zeros((len(pos), 2), np.float32) if uv is None else uv
+            mesh = scenes.Mesh(pos, nrm, uv, idx)
         elif ty == "sphere":
             mesh = sphere_mesh(float(p.get_one("radius", 1.0)))
         else:
@@ -411,22 +603,28 @@ class PbrtImport:
         if st.area is not None:
             base = dict(base, emission_color=st.area[0], emission_luminance=st.area[1])
         xf = scenes.rows(self.conjugation @ st.ctm)
-        self.objects.append(scenes.Object(mesh, xf, _lower(base)))
+        slot = base.get("base_color_texture")
+        mat = _lower({k: v for k, v in base.items() if k != "base_color_texture"})
+        if slot is not None:
+            mat["base_color_texture"] = slot
+        self.objects.append(scenes.Object(mesh, xf, mat))
 
     def spec(self, name="pbrt") -> scenes.SceneSpec:
         w, h = self.res
-        return scenes.SceneSpec(name, self.objects, self.camera, scenes.Environment.constant((0.0, 0.0, 0.0)), w, h,
-                                self.spp, self.max_bounces)
+        return scenes.SceneSpec(name, self.objects, self.camera, self.environment, w, h, self.spp, self.max_bounces,
+                                textures=list(self.textures))
 
 
 def import_pbrt(path, width=None, height=None) -> scenes.SceneSpec:
     """Import a pbrt-v4 file; width/height override its Film resolution."""
-    return import_pbrt_text(Path(path).read_text(), width, height, Path(path).parent.name)
+    return import_pbrt_text(Path(path).read_text(), width, height, Path(path).parent.name, Path(path).parent)
 
 
-def import_pbrt_text(text: str, width=None, height=None, name="pbrt") -> scenes.SceneSpec:
-    imp = PbrtImport().run_text(text)
+def import_pbrt_text(text: str, width=None, height=None, name="pbrt", base=None) -> scenes.SceneSpec:
+    """Import pbrt-v4 text; files it names resolve against `base`."""
+    imp = PbrtImport(base).run_text(text)
     spec = imp.spec(name)
+    spec.sky_source = imp.sky_source
     if width:
         spec.width = width
     if height:

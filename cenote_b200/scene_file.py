@@ -399,14 +399,7 @@ def lower(sf: SceneFile, width=None, height=None) -> scenes.SceneSpec:
         if e.get("path") is not None:
             from .exr import read_exr
             ch = read_exr(sf.path(e["path"]))
-            rgb = np.stack([ch["R"], ch["G"], ch["B"]], -1).reshape(-1, 3).astype(np.float32)
-            m = scenes._ACESCG_FROM_REC709
-            # Summed left to right in f32, as scenes.acescg does for colours.
-            ac = np.stack([(m[r, 0] * rgb[:, 0] + m[r, 1] * rgb[:, 1]) + m[r, 2] * rgb[:, 2] for r in range(3)], -1)
-            ac = np.maximum(ac, np.float32(0.0))
-            h, w = ch["R"].shape
-            tex = np.concatenate([ac.reshape(h, w, 3), np.ones((h, w, 1), np.float32)], -1).astype(np.float32)
-            env = scenes.Environment(w, h, np.ascontiguousarray(tex))
+            env = scenes.environment_rec709(np.stack([ch["R"], ch["G"], ch["B"]], -1))
     deltas = []
     for name in sorted(sf.objects["Light"]):
         light = sf.objects["Light"][name].get("light")

@@ -296,6 +296,20 @@ class Environment:
         return Environment(1, 1, t)
 
 
+def environment_rec709(rgb: np.ndarray) -> Environment:
+    """An environment from linear Rec.709 texels (H, W, 3), row 0 the +Y
+    zenith: converted to ACEScg as the reference's environment loader does,
+    each channel summed left to right in f32 as `acescg` does for colours,
+    negatives clamped to zero."""
+    h, w = rgb.shape[:2]
+    c = np.asarray(rgb, np.float32).reshape(-1, 3)
+    m = _ACESCG_FROM_REC709
+    ac = np.stack([(m[r, 0] * c[:, 0] + m[r, 1] * c[:, 1]) + m[r, 2] * c[:, 2] for r in range(3)], -1)
+    ac = np.maximum(ac, np.float32(0.0))
+    tex = np.concatenate([ac.reshape(h, w, 3), np.ones((h, w, 1), np.float32)], -1).astype(np.float32)
+    return Environment(w, h, np.ascontiguousarray(tex))
+
+
 @dataclass
 class DeltaLight:
     kind: int  # 1 distant (anchor = unit travel direction), 2 point (anchor = position)

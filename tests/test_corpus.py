@@ -18,16 +18,27 @@ import pytest
 
 from cenote_b200 import scenes
 from cenote_b200.metrics import flip_ldr_linear, flip_map, rel_mse, to_ldr8
-from cenote_b200.pbrt import FLIP_Z, import_pbrt_text
+from cenote_b200.pbrt import FLIP_Z, _sphere_to_square, import_pbrt_text, resample_octahedral, sky_environment
 
 GOLDEN = pathlib.Path(__file__).parent / "golden"
-CORPUS = ["cornell_box", "veach_mis"]
-MAX_MEAN_FLIP = 0.01   # corpus.rs:41
-MAX_REL_MSE = 1e-4     # a second, independent 64-spp render scores 4e-3 (cornell) and 0.4 (veach)
+CORPUS = ["cornell_box", "veach_mis", "teapot_full"]
+# (mean LDR-FLIP, relMSE) bars against the reference's own 64-spp render.
+# cornell-box and veach-mis hold the reference's bar (corpus.rs:41) and a
+# relMSE far below a second, independent 64-spp render's (4e-3 and 0.4): the
+# same samples reproduce the same noise. teapot-full's double glass (65
+# bounces of refraction) amplifies the ulp-level differences between the
+# reference's hardware ray-triangle hits and the watertight test, and its
+# floor texture is BC7-compressed and its sky hardware-filtered there, so
+# its bars sit between the same-sample render (FLIP 0.023, relMSE 2.3e-3)
+# and an independent one (0.115, 0.068).
+BARS = {"cornell_box": (0.01, 1e-4), "veach_mis": (0.01, 1e-4), "teapot_full": (0.035, 6e-3)}
 
 
 def load(name):
     spec, extra = scenes.load_spec(GOLDEN / f"corpus_{name}.npz")
+    if "sky_octahedral" in extra:
+        spec.environment = sky_environment(extra["sky_octahedral"].astype(np.float32), extra["sky_world_from_light"],
+                                           float(extra["sky_scale"]))
     return spec, extra["golden"]
 
 
@@ -74,8 +85,22 @@ def test_oracle_reproduces_reference_corpus_render(name):
     spec, golden = load(name)
     img = oracle.OracleScene(spec).render_sum(spec.width, spec.height, 0, spec.spp, spec.max_bounces)[..., :3]
     img = img / spec.spp
-    assert flip_ldr_linear(golden, img) <= MAX_MEAN_FLIP
-    assert rel_mse(img, golden) <= MAX_REL_MSE
+    max_flip, max_rel = BARS[name]
+    assert flip_ldr_linear(golden, img) <= max_flip
+    assert rel_mse(img, golden) <= max_rel
+
+
+def test_teapot_bar_separates_same_and_other_samples():
+    """The teapot's looser bar still tells the reference's samples apart:
+    the same render with other sample indices fails it."""
+    import oracle
+
+    spec, golden = load("teapot_full")
+    other = oracle.OracleScene(spec).render_sum(spec.width, spec.height, 1 << 20, spec.spp, spec.max_bounces)
+    other = other[..., :3] / spec.spp
+    max_flip, max_rel = BARS["teapot_full"]
+    assert flip_ldr_linear(golden, other) > 2 * max_flip
+    assert rel_mse(other, golden) > 5 * max_rel
 
 
 # ---- importer ------------------------------------------------------------------
@@ -159,6 +184,107 @@ def test_import_warns_on_unsupported_input():
     assert any("MakeNamedMedium" in w for w in spec.warnings)
 
 
+# ---- the octahedral sky (crates/cenote-pbrt/src/env.rs tests) --------------------------
+
+
+def square_to_sphere(u, v):
+    """pbrt's forward equal-area map, restated for the tests (the reference's
+    tests do the same): the inverse the resampler uses must round-trip."""
+    u, v = 2.0 * u - 1.0, 2.0 * v - 1.0
+    up, vp = abs(u), abs(v)
+    sd = 1.0 - (up + vp)
+    r = 1.0 - abs(sd)
+    phi = (1.0 if r == 0.0 else (vp - up) / r + 1.0) * math.pi / 4
+    z = math.copysign(1.0 - r * r, sd)
+    scale = r * math.sqrt(max(2.0 - r * r, 0.0))
+    return np.array([math.copysign(math.cos(phi), u) * scale, math.copysign(math.sin(phi), v) * scale, z])
+
+
+def test_octahedral_landmarks():  # env.rs:200-210
+    d = np.array([[0, 0, 1], [1, 0, 0], [-1, 0, 0], [0, 1, 0], [0, -1, 0]], np.float32)
+    assert np.allclose(_sphere_to_square(d), [[0.5, 0.5], [1.0, 0.5], [0.0, 0.5], [0.5, 1.0], [0.5, 0.0]], atol=1e-6)
+
+
+def test_octahedral_map_round_trips():  # env.rs:212-231
+    uv = [((i + 0.5) / 32, (j + 0.5) / 32) for i in range(32) for j in range(32)]
+    d = np.array([square_to_sphere(u, v) for u, v in uv], np.float32)
+    assert np.allclose(np.linalg.norm(d, axis=1), 1.0, atol=1e-5)
+    assert np.allclose(_sphere_to_square(d), uv, atol=1e-4)
+
+
+def test_resample_maps_directions_scale_and_orientation():  # env.rs:238-306
+    size = 64
+
+    def octant(d):
+        return np.where(np.asarray(d) > 0, 1.0, 0.25)
+
+    src = np.array([[octant(square_to_sphere((x + 0.5) / size, (y + 0.5) / size)) for x in range(size)]
+                    for y in range(size)], np.float32)
+
+    def direction(u, v):
+        phi, theta = 2 * math.pi * (u - 0.5), math.pi * v
+        return np.array([math.sin(theta) * math.sin(phi), math.cos(theta), -math.sin(theta) * math.cos(phi)])
+
+    def probe(img, u, v):
+        h, w = img.shape[:2]
+        return img[min(int(v * h), h - 1), min(int(u * w), w - 1)]
+
+    out = resample_octahedral(src, np.eye(3, dtype=np.float32), 2.0)
+    assert out.shape == (size, 2 * size, 3)
+    for u, v in [(0.15, 0.3), (0.4, 0.6), (0.65, 0.25), (0.9, 0.75)]:
+        assert np.allclose(probe(out, u, v), octant(direction(u, v)) * 2.0, atol=1e-3)
+    c, s = math.cos(math.pi / 2), math.sin(math.pi / 2)
+    quarter = np.array([[c, 0, s], [0, 1, 0], [-s, 0, c]], np.float32)  # a quarter turn about +Y
+    out = resample_octahedral(src, quarter, 1.0)
+    for u, v in [(0.15, 0.3), (0.65, 0.25)]:
+        assert np.allclose(probe(out, u, v), octant(np.linalg.inv(quarter) @ direction(u, v)), atol=1e-3)
+    with pytest.raises(ValueError, match="square"):
+        resample_octahedral(np.zeros((8, 16, 3), np.float32), np.eye(3, dtype=np.float32), 1.0)
+
+
+def test_zip_compressed_exr_reads(tmp_path):
+    """The reader's ZIP (16 scanlines per block) path, on a file built here
+    from the layout document: half channels, predictor + interleave, deflate."""
+    import struct
+    import zlib
+
+    from cenote_b200.exr import read_exr
+
+    h, w = 20, 7
+    ramp = np.add.outer(np.arange(h), np.arange(w)) / 32.0
+    chans = {n: (ramp * k).astype(np.float16) for k, n in enumerate(("B", "G", "R"), 1)}
+
+    def attr(name, typ, data):
+        return name.encode() + b"\0" + typ.encode() + b"\0" + struct.pack("<i", len(data)) + data
+
+    chlist = b"".join(n.encode() + b"\0" + struct.pack("<iB3xii", 1, 0, 1, 1) for n in sorted(chans)) + b"\0"
+    header = struct.pack("<ii", 20000630, 2) + attr("channels", "chlist", chlist) + \
+        attr("compression", "compression", bytes([3])) + attr("dataWindow", "box2i", struct.pack("<iiii", 0, 0, w - 1, h - 1)) + \
+        attr("displayWindow", "box2i", struct.pack("<iiii", 0, 0, w - 1, h - 1)) + \
+        attr("lineOrder", "lineOrder", bytes([0])) + attr("pixelAspectRatio", "float", struct.pack("<f", 1.0)) + \
+        attr("screenWindowCenter", "v2f", struct.pack("<ff", 0, 0)) + attr("screenWindowWidth", "float", struct.pack("<f", 1)) + b"\0"
+    blocks = []
+    for y0 in range(0, h, 16):
+        raw = b"".join(chans[n][y].tobytes() for y in range(y0, min(h, y0 + 16)) for n in sorted(chans))
+        t = np.frombuffer(raw, np.uint8)
+        inter = np.concatenate([t[0::2], t[1::2]]).astype(np.int64)
+        pred = inter.copy()
+        pred[1:] = (inter[1:] - inter[:-1] + 128) & 0xFF
+        data = zlib.compress(pred.astype(np.uint8).tobytes())
+        assert len(data) < len(raw)  # a block that would not shrink is stored raw
+        blocks.append(struct.pack("<ii", y0, len(data)) + data)
+    table_at = len(header)
+    offsets, pos = [], table_at + 8 * len(blocks)
+    for b in blocks:
+        offsets.append(pos)
+        pos += len(b)
+    path = tmp_path / "zip.exr"
+    path.write_bytes(header + struct.pack(f"<{len(blocks)}Q", *offsets) + b"".join(blocks))
+    back = read_exr(path)
+    for n in chans:
+        assert np.array_equal(back[n], chans[n].astype(np.float32))
+
+
 def test_import_rejects_a_file_without_world():
     with pytest.raises(ValueError):
         import_pbrt_text('Camera "perspective"\n')
@@ -193,6 +319,7 @@ def test_gpu_reproduces_reference_corpus_render(ctx, name):
     renderer.accumulate(scene, film, spec.spp)
     img = film.averages()
     assert np.isfinite(img).all()
+    max_flip, max_rel = BARS[name]
     flip = flip_ldr_linear(golden, img[..., :3])
-    assert flip <= MAX_MEAN_FLIP, flip
-    assert rel_mse(img[..., :3], golden) <= MAX_REL_MSE
+    assert flip <= max_flip, flip
+    assert rel_mse(img[..., :3], golden) <= max_rel
