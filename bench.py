@@ -308,6 +308,11 @@ def run_serving(args):
                                "160 GB budget, 8 slots, 64 resident jobs, a frame every 4 spp"},
         "time_to_first_frame_ms": {"p50": pct(ttff, 50), "p99": pct(ttff, 99), "max": float(ttff.max())},
         "time_to_target_ms": {"p50": pct(ttt, 50), "p99": pct(ttt, 99), "max": float(ttt.max())},
+        # Closed loop: the jobs after the first `concurrency`, which all arrive
+        # at once when the loop starts.
+        "steady_state_time_to_first_frame_ms": (
+            {"p50": pct(ttff[args.concurrency:], 50), "p99": pct(ttff[args.concurrency:], 99),
+             "jobs": int(len(ttff) - args.concurrency)} if args.concurrency and len(ttff) > args.concurrency else None),
         "aggregate_msamples_per_s": samples / (span_ms / 1e3) / 1e6,
         "samples": samples, "span_ms": span_ms,
         "failed": int(sum(1 for s in st if s.state != JOB_DONE)),

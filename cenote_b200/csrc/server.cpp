@@ -14,8 +14,12 @@
 //    with the fewest jobs; a slot runs one chunk (`frame_spp` samples, one
 //    progressive frame) of one job at a time, so jobs on different slots
 //    overlap on the device.
-//  * Each slot picks its next chunk from jobs that have no frame yet first
-//    (time to first frame), then round-robin. A job's full-size chunk is
+//  * First frames come first, device-wide: admitted jobs wait for their
+//    first chunk in one arrival-order queue that any idle slot serves, and
+//    while first frames are queued or in flight no slot starts another
+//    job's progressive chunk, so the chunks in flight drain and the first
+//    frames get the device. Otherwise a slot round-robins the chunks of the
+//    jobs bound to it. A job's full-size chunk is
 //    captured once into a CUDA graph and replayed; the graph reads the job's
 //    sample offset from device memory, advanced by a node at its end, so
 //    replays need no parameter updates. A shorter final chunk is enqueued
@@ -92,6 +96,8 @@ struct cenote_server {
     std::mutex mu;
     std::condition_variable cv;
     std::deque<uint64_t> queue;
+    std::deque<uint64_t> first_queue;  // admitted jobs waiting for their first chunk
+    uint32_t first_in_flight = 0;      // first chunks on the device
     std::map<uint64_t, std::unique_ptr<Job>> jobs;
     uint64_t next_id = 1;
     uint32_t active = 0;
@@ -116,6 +122,7 @@ struct cenote_server {
             auto& v = slots[size_t(j.slot)]->jobs;
             v.erase(std::remove(v.begin(), v.end(), j.id), v.end());
         }
+        first_queue.erase(std::remove(first_queue.begin(), first_queue.end(), j.id), first_queue.end());
         j.free_device();
         used -= j.bytes;
         j.bytes = 0;
@@ -147,25 +154,24 @@ struct cenote_server {
             size_t best = 0;
             for (size_t k = 1; k < slots.size(); ++k)
                 if (slots[k]->jobs.size() < slots[best]->jobs.size()) best = k;
-            j.slot = int(best);
-            // The sums start at zero (chunks only add) and so does the graph's
-            // sample offset; stream order puts this before the first chunk.
-            cudaMemsetAsync(j.sum.ptr, 0, px * 16, slots[best]->stream);
-            cudaMemsetAsync(j.offset.ptr, 0, 16, slots[best]->stream);
+            j.slot = int(best);  // for its progressive chunks; its first chunk runs on any idle slot
             slots[best]->jobs.push_back(j.id);
+            first_queue.push_back(j.id);
             j.state = CENOTE_JOB_RUNNING;
             j.t_admit = now_ms(t0);
             active++;
         }
     }
 
-    // The slot's next job: one without a frame yet first, then round-robin.
+    // The slot's next progressive chunk: its bound jobs round-robin, past
+    // those still waiting for a first frame.
     Job* pick(Slot& s) {
-        for (uint64_t id : s.jobs)
-            if (jobs[id]->samples == 0) return jobs[id].get();
-        if (s.jobs.empty()) return nullptr;
-        s.next %= s.jobs.size();
-        return jobs[s.jobs[s.next++]].get();
+        for (size_t k = 0; k < s.jobs.size(); ++k) {
+            s.next %= s.jobs.size();
+            Job* j = jobs[s.jobs[s.next++]].get();
+            if (j->samples > 0) return j;
+        }
+        return nullptr;
     }
 
     WavePlan plan_for(const Job& j, uint32_t n) const {
@@ -183,14 +189,24 @@ struct cenote_server {
         return p;
     }
 
-    // Enqueue the job's next chunk on its slot (no host waits).
+    // Enqueue the job's next chunk on slot `s` (no host waits). A first
+    // chunk clears the job's sums and sample offset first and is launched
+    // directly: the slot it runs on need not be the one whose path pool a
+    // captured graph would bind.
     cudaError_t launch_chunk(Slot& s, Job& j) {
+        const bool first = j.samples == 0;
+        if (first) {
+            const size_t px = size_t(j.width) * j.height;
+            cudaError_t e0 = cudaMemsetAsync(j.sum.ptr, 0, px * 16, s.stream);
+            if (e0 == cudaSuccess) e0 = cudaMemsetAsync(j.offset.ptr, 0, 16, s.stream);
+            if (e0 != cudaSuccess) return e0;
+        }
         const uint32_t n = std::min(opt.frame_spp, j.target - j.samples);
         FilmTargets film{j.sum.as<float4>(), nullptr, nullptr, nullptr};  // previews carry no guides
         WavePlan plan = plan_for(j, n);
         cudaError_t e = cudaSuccess;
         const bool full = n == opt.frame_spp;
-        if (full && opt.no_graphs == 0 && !j.graph && !j.graph_tried) {
+        if (full && !first && opt.no_graphs == 0 && !j.graph && !j.graph_tried) {
             j.graph_tried = true;
             cudaGraph_t g = nullptr;
             WaveCounts wc;
@@ -211,7 +227,7 @@ struct cenote_server {
                 e = cudaSuccess;
             }
         }
-        if (full && j.graph) {
+        if (full && !first && j.graph) {
             e = cudaGraphLaunch(j.graph, s.stream);
         } else {
             WaveCounts wc;
@@ -226,6 +242,7 @@ struct cenote_server {
         if ((e = cudaEventRecord(j.done, s.stream))) return e;
         j.pending = n;
         s.busy = j.id;
+        if (first) first_in_flight++;
         return cudaGetLastError();
     }
 
@@ -243,6 +260,7 @@ struct cenote_server {
                     if (q == cudaErrorNotReady) continue;
                     s.busy = 0;
                     progressed = true;
+                    if (j.samples == 0 && first_in_flight) first_in_flight--;
                     if (q != cudaSuccess) {
                         cudaGetLastError();
                         fail_job(j, CENOTE_E_DEVICE);
@@ -278,7 +296,13 @@ struct cenote_server {
                     }
                 }
                 if (!s.busy) {
-                    Job* j = pick(s);
+                    Job* j = nullptr;
+                    if (!first_queue.empty()) {
+                        j = jobs[first_queue.front()].get();
+                        first_queue.pop_front();
+                    } else if (first_in_flight == 0) {
+                        j = pick(s);
+                    }
                     if (j) {
                         cudaError_t e = launch_chunk(s, *j);
                         progressed = true;
