@@ -313,6 +313,10 @@ def run_serving(args):
         "steady_state_time_to_first_frame_ms": (
             {"p50": pct(ttff[args.concurrency:], 50), "p99": pct(ttff[args.concurrency:], 99),
              "jobs": int(len(ttff) - args.concurrency)} if args.concurrency and len(ttff) > args.concurrency else None),
+        "slowest_first_frames": [
+            {"job": int(k), "scene": jobs[k][1], "size": f"{jobs[k][2]}x{jobs[k][3]}", "spp": jobs[k][4],
+             "submit_ms": round(st[k].submit_ms, 1), "ttff_ms": round(float(ttff[k]), 1)}
+            for k in np.argsort(-ttff)[:6]],
         "aggregate_msamples_per_s": samples / (span_ms / 1e3) / 1e6,
         "samples": samples, "span_ms": span_ms,
         "failed": int(sum(1 for s in st if s.state != JOB_DONE)),

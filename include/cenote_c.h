@@ -407,7 +407,8 @@ typedef struct cenote_job_status {
 typedef struct cenote_server_counters {
     uint64_t submitted, completed, failed, queued, active;
     uint64_t samples;      /* pixel samples finished */
-    uint64_t bytes_in_use; /* resident bytes counted against the budget (pools + jobs) */
+    uint64_t bytes_in_use; /* bytes counted against the budget: pools, resident jobs, and finished
+                            * jobs' film buffers cached for reuse */
     uint64_t budget;
     double wall_ms;        /* since creation */
 } cenote_server_counters;
