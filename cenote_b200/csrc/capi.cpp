@@ -416,7 +416,7 @@ int32_t cenote_scene_create_textured(cenote_context* ctx, const cenote_object* o
     size_t total_tris = 0;
     for (uint32_t i = 0; i < object_count; ++i) total_tris += objects[i].triangle_count;
     tris.reserve(total_tris);
-    bool nonopaque = false;
+    bool nonopaque = false, layered = false;
     for (uint32_t i = 0; i < object_count; ++i) {
         const cenote_object& o = objects[i];
         CN_CHECK(o.positions && o.normals && o.uvs && o.indices && o.vertex_count > 0, CENOTE_E_INVALID_ARGUMENT,
@@ -453,6 +453,8 @@ int32_t cenote_scene_create_textured(cenote_context* ctx, const cenote_object* o
         bool emissive = em.x != 0.0f || em.y != 0.0f || em.z != 0.0f;
         bool opaque = o.material.opacity >= 1.0f && o.material.opacity_texture == TEXTURE_NONE;
         nonopaque = nonopaque || !opaque;
+        layered = layered || o.material.coat_weight != 0.0f || o.material.fuzz_weight != 0.0f ||
+                  o.material.transmission_weight != 0.0f || o.material.thin_walled != 0u;
         uint32_t flags = (o.camera_visible ? RAY_MASK_ALL : (RAY_MASK_ALL & ~RAY_MASK_CAMERA)) | (opaque ? TRI_OPAQUE : 0u);
         for (uint32_t t = 0; t < o.triangle_count; ++t) {
             BuildTri bt;
@@ -642,6 +644,7 @@ int32_t cenote_scene_create_textured(cenote_context* ctx, const cenote_object* o
     ds.node_count = node_count;
     ds.tri_count = tri_count;
     ds.has_nonopaque = nonopaque ? 1u : 0u;
+    ds.has_layers = layered ? 1u : 0u;
     const float extent = std::max({bmax[0] - bmin[0], bmax[1] - bmin[1], bmax[2] - bmin[2], 1e-6f});
     for (int a = 0; a < 3; ++a) ds.bbox_min[a] = tris.empty() ? 0.0f : bmin[a];
     ds.bbox_inv = tris.empty() ? 1.0f : 1.0f / extent;

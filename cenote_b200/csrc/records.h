@@ -95,7 +95,8 @@ struct DeviceScene {
     uint32_t light_count;
     uint32_t node_count, tri_count;
     uint32_t has_nonopaque;
-    uint32_t pad;
+    uint32_t has_layers;  // a material with coat, fuzz, transmission or thin walls
+
     const uint32_t* light_leaf;  // per light record: its triangle's leaf index, ~0 for delta lights
     const unsigned long long* textures;  // cudaTextureObject_t per bindless slot
     uint32_t texture_count;
