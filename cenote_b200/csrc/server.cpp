@@ -15,10 +15,11 @@
 //    progressive frame) of one job at a time, so jobs on different slots
 //    overlap on the device.
 //  * First frames come first, device-wide: admitted jobs wait for their
-//    first chunk in one arrival-order queue that any idle slot serves, and
-//    while first frames are queued or in flight no slot starts another
-//    job's progressive chunk, so the chunks in flight drain and the first
-//    frames get the device. Otherwise a slot round-robins the chunks of the
+//    first chunk in one arrival-order queue served by two slots that render
+//    nothing else (so a first frame never waits for a busy slot) and by any
+//    idle slot, and while first frames are queued or in flight no slot
+//    starts another job's progressive chunk, so the chunks in flight drain
+//    and the first frames get the device. Otherwise a slot round-robins the chunks of the
 //    jobs bound to it. A job's full-size chunk is
 //    captured once into a CUDA graph and replayed; the graph reads the job's
 //    sample offset from device memory, advanced by a node at its end, so
@@ -90,7 +91,13 @@ struct Slot {
     std::vector<uint64_t> jobs;  // resident jobs bound to this slot
     size_t next = 0;             // round-robin cursor
     uint64_t busy = 0;           // job whose chunk is in flight (0: idle)
+    bool first_only = false;     // renders first frames only (no jobs bound to it)
 };
+
+// Slots that render first frames only (index 0 .. CN_FIRST_SLOTS-1).
+#ifndef CN_FIRST_SLOTS
+#define CN_FIRST_SLOTS 2
+#endif
 
 }  // namespace
 
@@ -219,8 +226,8 @@ struct cenote_server {
             }
             used += bytes;
             j.bytes = bytes;
-            size_t best = 0;
-            for (size_t k = 1; k < slots.size(); ++k)
+            size_t best = CN_FIRST_SLOTS;
+            for (size_t k = best + 1; k < slots.size(); ++k)
                 if (slots[k]->jobs.size() < slots[best]->jobs.size()) best = k;
             j.slot = int(best);  // for its progressive chunks; its first chunk runs on any idle slot
             slots[best]->jobs.push_back(j.id);
@@ -366,7 +373,7 @@ struct cenote_server {
                     if (!first_queue.empty()) {
                         j = jobs[first_queue.front()].get();
                         first_queue.pop_front();
-                    } else if (first_in_flight == 0) {
+                    } else if (first_in_flight == 0 && !s.first_only) {
                         j = pick(s);
                     }
                     if (j) {
@@ -415,9 +422,11 @@ int32_t cenote_server_create(cenote_context* ctx, uint64_t hbm_budget, const cen
     CN_CUDA(cudaSetDevice(ctx->device));
     // Each slot's pool: path state + queues + shadow records, no guide lanes.
     const uint64_t pool_bytes = uint64_t(s->opt.pool_paths) * (16 * 5 + 8 + 4 + 8 + sizeof(ShadowRay));
-    CN_CHECK(pool_bytes * s->opt.slots <= hbm_budget, CENOTE_E_BUDGET, "the slots' path pools exceed the budget");
-    for (uint32_t k = 0; k < s->opt.slots; ++k) {
+    const uint32_t all_slots = CN_FIRST_SLOTS + s->opt.slots;
+    CN_CHECK(pool_bytes * all_slots <= hbm_budget, CENOTE_E_BUDGET, "the slots' path pools exceed the budget");
+    for (uint32_t k = 0; k < all_slots; ++k) {
         auto slot = std::make_unique<Slot>();
+        slot->first_only = k < CN_FIRST_SLOTS;
         CN_CUDA(cudaStreamCreateWithFlags(&slot->stream, cudaStreamNonBlocking));
         cenote_renderer& r = slot->renderer;
         r.ctx = ctx;
@@ -430,7 +439,7 @@ int32_t cenote_server_create(cenote_context* ctx, uint64_t hbm_budget, const cen
         CN_CUDA(r.set_guides(false));
         s->slots.push_back(std::move(slot));
     }
-    s->used = pool_bytes * s->opt.slots;
+    s->used = pool_bytes * all_slots;
     retain(ctx);
     cenote_server* raw = s.release();
     raw->thread = std::thread([raw] { raw->loop(); });
@@ -469,7 +478,8 @@ int32_t cenote_job_submit(cenote_server* s, cenote_scene* scene, uint32_t width,
     CN_CHECK(max_bounces >= 1 && max_bounces <= MAX_BOUNCES, CENOTE_E_INVALID_ARGUMENT, "bounces outside 1..=255");
     std::lock_guard<std::mutex> lock(s->mu);
     const uint64_t bytes = s->job_bytes(width, height);
-    uint64_t pools = uint64_t(s->opt.pool_paths) * (16 * 5 + 8 + 4 + 8 + sizeof(ShadowRay)) * s->opt.slots;
+    uint64_t pools = uint64_t(s->opt.pool_paths) * (16 * 5 + 8 + 4 + 8 + sizeof(ShadowRay)) *
+                     (CN_FIRST_SLOTS + s->opt.slots);
     CN_CHECK(pools + bytes <= s->budget, CENOTE_E_BUDGET, "the job alone exceeds the budget");
     auto j = std::make_unique<Job>();
     j->id = s->next_id++;

@@ -377,7 +377,8 @@ int32_t cenote_probe_texture(cenote_scene* scene, uint32_t index, uint32_t mode,
 typedef struct cenote_server cenote_server;
 
 typedef struct cenote_server_options {
-    uint32_t slots;          /* concurrent streams, each with a path pool (0: 8) */
+    uint32_t slots;          /* concurrent streams, each with a path pool (0: 8); the server adds two
+                              * more that render only first frames, their pools counted alike */
     uint32_t frame_spp;      /* samples per progressive frame (0: 4) */
     uint32_t max_active;     /* jobs resident at once (0: 64) */
     uint32_t pool_paths;     /* path capacity per slot (0: 2^21) */

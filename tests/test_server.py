@@ -92,8 +92,9 @@ def test_admission_respects_the_budget(ctx, scene_set):
     pool_paths = 1 << 16
     pool_bytes = pool_paths * (16 * 5 + 8 + 4 + 8 + 64)
     job_bytes = 128 * 128 * 32 + 256
-    # Room for the one slot's pool and two 128x128 jobs at a time.
-    budget = pool_bytes + 2 * job_bytes + 100
+    # Room for the slots' pools (one regular, two first-frame) and two 128x128
+    # jobs at a time.
+    budget = 3 * pool_bytes + 2 * job_bytes + 100
     server = Server(ctx, budget, slots=1, pool_paths=pool_paths)
     ids = [server.submit(scene_set["cornell"], 128, 128, 2, 4) for _ in range(5)]
     peak = 0
