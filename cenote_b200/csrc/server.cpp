@@ -31,7 +31,9 @@
 //    cudaFree and cudaFreeHost wait for the whole device, which stalled the
 //    loop behind every chunk in flight (measured: first frames of jobs
 //    submitted meanwhile waited 0.8 s).
-//  * After each chunk the film is resolved into the job's pinned buffer and
+//  * After the first frame, a frame's samples may run as several pieces of
+//    about one path pool each, so progressive work in flight stays small.
+//  * After each frame the film is resolved into the job's pinned buffer and
 //    an event marks it; the server thread polls events and hands each frame
 //    to the job's callback. Sample order within a film is ascending, so a
 //    job's result is bitwise the same alone and in any mix.
@@ -63,6 +65,7 @@ struct Job {
     int32_t error = CENOTE_OK;
     uint32_t samples = 0;   // completed
     uint32_t pending = 0;   // in the chunk in flight
+    bool frame_pending = false;  // the chunk in flight ends a progressive frame
     int slot = -1;
     uint64_t bytes = 0;     // resident footprint counted against the budget
     DeviceBuffer sum, avg, offset;
@@ -249,6 +252,13 @@ struct cenote_server {
         return nullptr;
     }
 
+    // Samples per progressive piece: as many as one path pool holds, at most
+    // a frame's worth.
+    uint32_t piece_spp(const Job& j) const {
+        const uint64_t px = uint64_t(j.width) * j.height;
+        return uint32_t(std::max<uint64_t>(1, std::min<uint64_t>(opt.frame_spp, uint64_t(opt.pool_paths) / px)));
+    }
+
     WavePlan plan_for(const Job& j, uint32_t n) const {
         const uint64_t px = uint64_t(j.width) * j.height;
         const uint64_t cap = opt.pool_paths;
@@ -276,11 +286,18 @@ struct cenote_server {
             if (e0 == cudaSuccess) e0 = cudaMemsetAsync(j.offset.ptr, 0, 16, s.stream);
             if (e0 != cudaSuccess) return e0;
         }
-        const uint32_t n = std::min(opt.frame_spp, j.target - j.samples);
+        // A first chunk is the whole first frame; later frames go in pieces
+        // of about one path pool (frame_spp samples at most), so a new job's
+        // first frame never waits long for progressive work in flight.
+        const uint32_t remaining = j.target - j.samples;
+        const uint32_t piece = piece_spp(j);
+        const uint32_t n = first ? std::min(opt.frame_spp, remaining)
+                                 : std::min({piece, remaining, opt.frame_spp - j.samples % opt.frame_spp});
+        const bool frame = (j.samples + n) % opt.frame_spp == 0 || j.samples + n == j.target;
         FilmTargets film{j.sum.as<float4>(), nullptr, nullptr, nullptr};  // previews carry no guides
         WavePlan plan = plan_for(j, n);
         cudaError_t e = cudaSuccess;
-        const bool full = n == opt.frame_spp;
+        const bool full = n == piece;
         if (full && !first && opt.no_graphs == 0 && !j.graph && !j.graph_tried) {
             j.graph_tried = true;
             cudaGraph_t g = nullptr;
@@ -311,11 +328,14 @@ struct cenote_server {
             if (e == cudaSuccess) launch_advance(j.offset.as<uint32_t>(), n, s.stream);
         }
         if (e != cudaSuccess) return e;
-        const uint32_t px = j.width * j.height;
-        launch_resolve(j.sum.as<float4>(), j.avg.as<float4>(), px, float(j.samples + n), s.stream);
-        if ((e = cudaMemcpyAsync(j.host, j.avg.ptr, size_t(px) * 16, cudaMemcpyDeviceToHost, s.stream))) return e;
+        if (frame) {
+            const uint32_t px = j.width * j.height;
+            launch_resolve(j.sum.as<float4>(), j.avg.as<float4>(), px, float(j.samples + n), s.stream);
+            if ((e = cudaMemcpyAsync(j.host, j.avg.ptr, size_t(px) * 16, cudaMemcpyDeviceToHost, s.stream))) return e;
+        }
         if ((e = cudaEventRecord(j.done, s.stream))) return e;
         j.pending = n;
+        j.frame_pending = frame;
         s.busy = j.id;
         if (first) first_in_flight++;
         return cudaGetLastError();
@@ -344,28 +364,30 @@ struct cenote_server {
                     j.samples += j.pending;
                     samples += uint64_t(j.pending) * j.width * j.height;
                     j.pending = 0;
-                    if (j.t_first < 0) j.t_first = now_ms(t0);
-                    if (j.fn) {
-                        cenote_frame_fn fn = j.fn;
-                        void* user = j.user;
-                        uint64_t id = j.id;
-                        uint32_t smp = j.samples, tgt = j.target, w = j.width, h = j.height;
-                        const float* frame = j.host;
-                        lock.unlock();
-                        fn(user, id, smp, tgt, frame, w, h);
-                        lock.lock();
-                    }
-                    if (j.samples >= j.target) {
-                        j.state = CENOTE_JOB_DONE;
-                        j.t_done = now_ms(t0);
-                        // Keep the final averages on the host for cenote_job_result;
-                        // release the device side.
-                        const size_t px = size_t(j.width) * j.height;
-                        float* keep = new float[px * 4];
-                        std::memcpy(keep, j.host, px * 16);
-                        results[j.id].reset(keep);
-                        retire(j);
-                        completed++;
+                    if (j.frame_pending) {  // else a piece of a frame: nothing to deliver yet
+                        if (j.t_first < 0) j.t_first = now_ms(t0);
+                        if (j.fn) {
+                            cenote_frame_fn fn = j.fn;
+                            void* user = j.user;
+                            uint64_t id = j.id;
+                            uint32_t smp = j.samples, tgt = j.target, w = j.width, h = j.height;
+                            const float* frame = j.host;
+                            lock.unlock();
+                            fn(user, id, smp, tgt, frame, w, h);
+                            lock.lock();
+                        }
+                        if (j.samples >= j.target) {
+                            j.state = CENOTE_JOB_DONE;
+                            j.t_done = now_ms(t0);
+                            // Keep the final averages on the host for cenote_job_result;
+                            // release the device side.
+                            const size_t px = size_t(j.width) * j.height;
+                            float* keep = new float[px * 4];
+                            std::memcpy(keep, j.host, px * 16);
+                            results[j.id].reset(keep);
+                            retire(j);
+                            completed++;
+                        }
                     }
                 }
                 if (!s.busy) {
