@@ -498,6 +498,13 @@ int32_t cenote_scene_create_textured(cenote_context* ctx, const cenote_object* o
                             ctx->stream));
     DeviceBuffer* bleaf = sc->add(std::max<size_t>(1, sc->lights.size()) * 4, &err);
     CN_CUDA(err);
+    std::vector<uint8_t> layers(std::max<size_t>(1, mats.size()), 0);
+    for (size_t i = 0; i < mats.size(); ++i)
+        layers[i] = (mats[i].coat_weight != 0.0f || mats[i].fuzz_weight != 0.0f || mats[i].transmission_weight != 0.0f ||
+                     mats[i].thin_walled != 0u) ? 1 : 0;
+    DeviceBuffer* blayers = sc->add(layers.size(), &err);
+    CN_CUDA(err);
+    CN_CUDA(cudaMemcpyAsync(blayers->ptr, layers.data(), layers.size(), cudaMemcpyHostToDevice, ctx->stream));
     CN_CUDA(cudaMemsetAsync(bleaf->ptr, 0xff, std::max<size_t>(1, sc->lights.size()) * 4, ctx->stream));
     if (ctx->bvh_builder == CENOTE_BVH_GPU_PLOC && !tris.empty()) {
         // Triangles in input order, identity in the w lanes; the device
@@ -649,6 +656,7 @@ int32_t cenote_scene_create_textured(cenote_context* ctx, const cenote_object* o
     for (int a = 0; a < 3; ++a) ds.bbox_min[a] = tris.empty() ? 0.0f : bmin[a];
     ds.bbox_inv = tris.empty() ? 1.0f : 1.0f / extent;
     ds.light_leaf = bleaf->as<uint32_t>();
+    ds.instance_layers = blayers->as<uint8_t>();
     sc->prep_ms[2] = float(std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t_start).count());
     retain(ctx);
     *out = sc.release();

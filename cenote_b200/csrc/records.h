@@ -98,6 +98,7 @@ struct DeviceScene {
     uint32_t has_layers;  // a material with coat, fuzz, transmission or thin walls
 
     const uint32_t* light_leaf;  // per light record: its triangle's leaf index, ~0 for delta lights
+    const uint8_t* instance_layers;  // per instance: 1 if its material has coat, fuzz, transmission or thin walls
     const unsigned long long* textures;  // cudaTextureObject_t per bindless slot
     uint32_t texture_count;
     uint32_t pad2;

@@ -120,7 +120,7 @@ cudaError_t enqueue_waves(cenote_renderer* r, const cenote_scene* sc, uint32_t w
                 if (guided) guide::launch_infer_paths(r->guide->view(), sc->ds, r->pool, b, n0, r->guide->sms, stream);
                 if (sort) {
                     launch_material_sort(view, b, n0, ctx->shape, stream);
-                    wc->launches += 2;
+                    wc->launches += sc->ds.has_layers ? 3 : 2;  // a split shading launch adds one
                 }
                 launch_shade(sc->ds, view, b, wp, n0, ctx->shape, stream);
                 mark();

@@ -68,6 +68,13 @@ __device__ __forceinline__ uint32_t warp_push(uint32_t* counter, bool pred) {
 
 __device__ __forceinline__ void flag_overflow(uint32_t* counters) { atomicOr(counters + CTR_OVERFLOW, 1u); }
 
+// The material-sort key of a closest hit (SORT_LAYERS splits the key range).
+__device__ __forceinline__ uint32_t material_key(const DeviceScene& s, uint32_t inst) {
+    if (inst == LIGHT_NONE) return 0u;
+    return __ldg(s.instance_layers + inst) ? SORT_LAYERS + inst % (SORT_BINS - SORT_LAYERS)
+                                           : 1u + inst % (SORT_LAYERS - 1u);
+}
+
 // Instrumented launches: one 64-bit add per warp for the traversal tallies.
 __device__ __forceinline__ void flush_counts(uint32_t* counters, uint32_t visits, uint32_t tests) {
     for (int o = 16; o > 0; o >>= 1) {
@@ -182,7 +189,7 @@ __global__ void __launch_bounds__(BLOCK, CN_TRAV_MIN_BLOCKS) k_intersect(DeviceS
     auto flush_keys = [&]() {
         if (!pool.sort_keys) return;
         if (__ballot_sync(0xffffffffu, finished) == 0u) return;
-        const uint32_t key = finished ? (best_inst == LIGHT_NONE ? 0u : 1u + best_inst % (SORT_BINS - 1u)) : 0xffffffffu;
+        const uint32_t key = finished ? material_key(scene, best_inst) : 0xffffffffu;
         const uint32_t peers = __match_any_sync(0xffffffffu, key);
         if (finished) {
             pool.sort_keys[qi] = key;
@@ -268,6 +275,7 @@ __global__ void __launch_bounds__(BLOCK, CN_TRAV_MIN_BLOCKS) k_intersect(DeviceS
 // those of k_intersect.
 struct IsectSource {
     const PathPool& pool;
+    const DeviceScene* scene;
     const uint32_t* queue;
     uint32_t* fetch;
     uint32_t count, bounce;
@@ -284,7 +292,7 @@ struct IsectSource {
     __device__ __forceinline__ void step(bool finished, uint32_t i, uint32_t inst) const {
         if (!pool.sort_keys) return;
         if (__ballot_sync(0xffffffffu, finished) == 0u) return;
-        const uint32_t key = finished ? (inst == LIGHT_NONE ? 0u : 1u + inst % (SORT_BINS - 1u)) : 0xffffffffu;
+        const uint32_t key = finished ? material_key(*scene, inst) : 0xffffffffu;
         const uint32_t peers = __match_any_sync(0xffffffffu, key);
         if (finished) {
             pool.sort_keys[i] = key;
@@ -303,7 +311,7 @@ __global__ void __launch_bounds__(BLOCK, CN_TRAV_MIN_BLOCKS)
     __shared__ TriQueueSmem tqs[BLOCK / 32];
     stage_top_levels(scene, top_levels, min(pool.top_nodes, TOP_NODES_MAX));
     uint32_t visits = 0, tests = 0;
-    IsectSource src{pool, pool.queue[bounce & 1u], pool.counters + CTR_FETCH_ISECT + bounce,
+    IsectSource src{pool, &scene, pool.queue[bounce & 1u], pool.counters + CTR_FETCH_ISECT + bounce,
                     min(bounce == 0 ? n0 : pool.counters[CTR_RAYS + bounce], pool.capacity), bounce};
     bool overflow = false;
     queued_closest<COUNT>(scene, tqs[threadIdx.x >> 5], src, bounce == 0 ? RAY_MASK_CAMERA : RAY_MASK_ALL, overflow,
@@ -411,12 +419,22 @@ __device__ __forceinline__ void close_record(const PathPool& pool, uint32_t path
 // of fused multiply-adds once the zeros fold: films agree within 2 ulps.
 template <bool AOV, bool GUIDE, bool LAYERS>
 __global__ void __launch_bounds__(BLOCK, CN_SHADE_MIN_BLOCKS) k_shade(DeviceScene scene, PathPool pool, uint32_t bounce,
-                                                 uint32_t max_bounces, uint32_t light_sampling, uint32_t n0) {
-    const uint32_t count = min(bounce == 0 ? n0 : pool.counters[CTR_RAYS + bounce], pool.capacity);
+                                                 uint32_t max_bounces, uint32_t light_sampling, uint32_t n0,
+                                                 uint32_t part) {
+    // part 0: the whole bounce; on a sorted bounce, 1: the misses and
+    // layer-free hits (keys below SORT_LAYERS), 2: the layered hits.
+    uint32_t count = min(bounce == 0 ? n0 : pool.counters[CTR_RAYS + bounce], pool.capacity);
+    uint32_t first = 0;
+    if (part != 0) {
+        const uint32_t split = min(pool.sort_bins[SORT_LAYERS - 1u], count);  // the end of the layer-free keys
+        if (part == 1) count = split;
+        else first = split;
+    }
     const uint32_t* queue = pool.queue[bounce & 1u];
     uint32_t* next_queue = pool.queue[(bounce + 1u) & 1u];
+    uint32_t* fetch = pool.counters + (part == 2 ? CTR_FETCH_SHADE_LAYERS : CTR_FETCH_SHADE) + bounce;
     for (;;) {
-        uint32_t base = warp_fetch(pool.counters + CTR_FETCH_SHADE + bounce);
+        uint32_t base = first + warp_fetch(fetch);
         if (base >= count) break;
         uint32_t i = base + lane_id();
         bool push_ray = false, push_shadow = false;
@@ -1051,19 +1069,32 @@ void launch_intersect(const DeviceScene& scene, const PathPool& pool, uint32_t b
 void launch_shade(const DeviceScene& scene, const PathPool& pool, uint32_t bounce, const WaveParams& wp, uint32_t n0,
                   const LaunchShape& ls, cudaStream_t stream) {
     const bool aov = pool.aov_albedo != nullptr, guided = pool.guide_out != nullptr;
-    auto args = [&](auto kernel) {
-        kernel<<<ls.grid_shade, BLOCK, 0, stream>>>(scene, pool, bounce, wp.max_bounces, wp.light_sampling, n0);
+    auto shade = [&](bool layers, uint32_t part) {
+        auto args = [&](auto kernel) {
+            kernel<<<ls.grid_shade, BLOCK, 0, stream>>>(scene, pool, bounce, wp.max_bounces, wp.light_sampling, n0,
+                                                        part);
+        };
+        if (layers) {
+            if (aov && guided) args(k_shade<true, true, true>);
+            else if (aov) args(k_shade<true, false, true>);
+            else if (guided) args(k_shade<false, true, true>);
+            else args(k_shade<false, false, true>);
+        } else {
+            if (aov && guided) args(k_shade<true, true, false>);
+            else if (aov) args(k_shade<true, false, false>);
+            else if (guided) args(k_shade<false, true, false>);
+            else args(k_shade<false, false, false>);
+        }
     };
-    if (scene.has_layers) {
-        if (aov && guided) args(k_shade<true, true, true>);
-        else if (aov) args(k_shade<true, false, true>);
-        else if (guided) args(k_shade<false, true, true>);
-        else args(k_shade<false, false, true>);
+    if (!scene.has_layers) {
+        shade(false, 0);
+    } else if (pool.order) {
+        // A sorted bounce of a scene with both kinds: the layer-free range
+        // (and the misses) without the layered lobes, then the rest.
+        shade(false, 1);
+        shade(true, 2);
     } else {
-        if (aov && guided) args(k_shade<true, true, false>);
-        else if (aov) args(k_shade<true, false, false>);
-        else if (guided) args(k_shade<false, true, false>);
-        else args(k_shade<false, false, false>);
+        shade(true, 0);
     }
 }
 

@@ -17,7 +17,8 @@ constexpr uint32_t CTR_FETCH_SHADOW = 1024;
 constexpr uint32_t CTR_OVERFLOW = 1280;
 constexpr uint32_t CTR_VISITS = 1284;   // 64-bit: wide nodes visited (instrumented launches only)
 constexpr uint32_t CTR_TESTS = 1286;    // 64-bit: triangles tested (instrumented launches only)
-constexpr uint32_t CTR_COUNT = 1296;
+constexpr uint32_t CTR_FETCH_SHADE_LAYERS = 1296;  // [b]: the layered part of a split shading launch
+constexpr uint32_t CTR_COUNT = 1552;
 
 // Structure-of-arrays path state: one 16-byte lane per logical field, so
 // every stage reads and writes with coalesced 128-bit accesses.
@@ -89,9 +90,13 @@ struct WaveParams {
     const uint32_t* sample_offset;
 };
 
-// Keys of the material sort: 0 for a miss, else 1 + the hit's instance (its
-// material slot) folded into SORT_BINS - 1 buckets.
+// Keys of the material sort: 0 for a miss; a hit's instance (its material
+// slot) folded into 1 .. SORT_LAYERS - 1 when its material has no coat,
+// fuzz, transmission or thin walls, else into SORT_LAYERS .. SORT_BINS - 1,
+// so a sorted bounce shades its layer-free paths and its layered ones as two
+// ranges.
 constexpr uint32_t SORT_BINS = 2048;
+constexpr uint32_t SORT_LAYERS = 1024;
 
 struct LaunchShape {
     int grid_isect, grid_isect_queued, grid_isect_queued_top, grid_shade, grid_shadow, grid_shadow_queued,
