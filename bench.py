@@ -8,8 +8,8 @@ count (chart: 1280x720 at 64 spp, 12 bounces — the material chart under the
 2048x1024 HDRI sky). `value` is device-timed (CUDA events on the library's
 stream around each step) with the scene resident in HBM; `e2e` is the same
 frame through the public API with a host camera update in and the resolved
-image out to pinned host memory every step. Multi-GPU (torchrun): every rank
-renders its own interleaved sample range of the frame and the films are summed
+image out to pinned host memory every step. Multi-GPU (torchrun): rank r
+renders samples r*spp .. (r+1)*spp-1 of every pixel and the films are summed
 with one NCCL all-reduce per step (weak scaling). The reference arm times the
 CPU oracle (the reference's Rust/Vulkan path cannot be built or run here) on
 the host cores.
@@ -118,6 +118,13 @@ class ClockSampler:
             return {"sm_mhz": None, "sm_max_mhz": None, "reasons": [], "samples": 0}
         return {"sm_mhz": float(np.median(sm)), "sm_max_mhz": max(mx), "reasons": sorted(reasons),
                 "samples": len(sm)}
+
+
+def rank_sample_range(rank: int, spp: int) -> tuple[int, int]:
+    """The sample indices one rank renders for a multi-GPU frame: rank r takes
+    [r * spp, (r + 1) * spp), so N ranks summing their films make one frame
+    of N * spp distinct samples per pixel (weak scaling: spp per GPU)."""
+    return rank * spp, spp
 
 
 def cpu_baseline(spec, w, seconds=12.0):
@@ -467,11 +474,13 @@ def main():
                 self.__cuda_array_interface__ = {"shape": (n,), "typestr": "<f4", "data": (ptr, False), "version": 2}
         sum_view = torch.as_tensor(_Dev(film.device_sums(), W * H * 4), device="cuda")
 
+    first_sample, _ = rank_sample_range(rank, spp)
+
     def step(k):
         film.reset()
-        r.accumulate(scene, film, spp)  # synchronous: returns when the frame is done
+        r.accumulate_range(scene, film, first_sample, spp)  # synchronous: returns when the frame is done
         if sum_view is not None:
-            dist.all_reduce(sum_view)
+            dist.all_reduce(sum_view)  # the frame's N * spp samples per pixel
             torch.cuda.synchronize()
 
     for k in range(args.warmup):
@@ -516,8 +525,12 @@ def main():
         t_a = time.perf_counter()
         scene.set_camera(spec.camera)
         film.reset()
-        r.accumulate(scene, film, spp)
-        film.averages_into(pinned.data_ptr())
+        r.accumulate_range(scene, film, first_sample, spp)
+        if sum_view is not None:
+            dist.all_reduce(sum_view)  # the frame's sums, read back whole (N * spp samples per pixel)
+            pinned.view(-1).copy_(sum_view)
+        else:
+            film.averages_into(pinned.data_ptr())
         t_b = time.perf_counter()
         if k >= args.warmup:
             e2e_ms.append((t_b - t_a) * 1e3)
@@ -551,7 +564,7 @@ def main():
         "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f32", "data": "synthetic (procedural scene, seeded)",
         "config": {"workload": w["label"], "width": W, "height": H, "spp": spp, "max_bounces": maxb,
-                   "parallelism": f"sample-interleaved x{world}" if world > 1 else "1 GPU",
+                   "parallelism": f"sample ranges x{world}, films summed by all-reduce" if world > 1 else "1 GPU",
                    "l2": "256 MB buffer written between timed steps (L2 flush); the path pool per wave also "
                          "exceeds L2",
                    "samples_per_wave": counts["samples_per_wave"], "waves_per_step": counts["waves"],
