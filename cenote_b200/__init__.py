@@ -119,7 +119,7 @@ EXPORTED_SYMBOLS = [
     "cenote_renderer_stats", "cenote_renderer_set_profiling", "cenote_render_once", "cenote_film_create", "cenote_film_destroy", "cenote_film_reset",
     "cenote_film_samples", "cenote_accumulate", "cenote_accumulate_n", "cenote_film_averages", "cenote_film_sums",
     "cenote_film_device_sums", "cenote_probe_sampler", "cenote_probe_bsdf", "cenote_probe_bsdf_sample",
-    "cenote_probe_intersect", "cenote_probe_intersect_queued", "cenote_probe_shadow", "cenote_probe_env_sample", "cenote_probe_env_pdf",
+    "cenote_probe_intersect", "cenote_probe_intersect_queued", "cenote_probe_shadow", "cenote_probe_shadow_queued", "cenote_probe_env_sample", "cenote_probe_env_pdf",
     "cenote_env_tables_static", "cenote_scene_create_textured", "cenote_texture_bytes", "cenote_texture_encode",
     "cenote_probe_texture", "cenote_server_create", "cenote_server_destroy", "cenote_job_submit", "cenote_job_poll",
     "cenote_job_wait", "cenote_job_result", "cenote_job_release", "cenote_server_stats", "cenote_guide_create",
@@ -205,6 +205,7 @@ def library() -> C.CDLL:
         "cenote_probe_intersect": (I32, [P, P, P, U32, P, P]),
         "cenote_probe_intersect_queued": (I32, [P, P, P, U32, P, P]),
         "cenote_probe_shadow": (I32, [P, P, P, P, P, U32, P]),
+        "cenote_probe_shadow_queued": (I32, [P, P, P, P, P, U32, P]),
         "cenote_probe_env_sample": (I32, [P, P, U32, P, P, P]),
         "cenote_probe_env_pdf": (I32, [P, P, U32, P]),
         "cenote_env_tables_static": (I32, [P, P, U32, U32, P, P, P, P]),
@@ -444,14 +445,16 @@ class Scene:
         _check(fn(self._h, _ptr(o), _ptr(d), n, _ptr(hits), _ptr(t)))
         return hits, t
 
-    def probe_shadow(self, origins, directions, tmax, targets):
+    def probe_shadow(self, origins, directions, tmax, targets, queued: bool = False):
+        """Shadow queries; `queued` walks them through the warp triangle queue."""
         o = np.ascontiguousarray(origins, np.float32)
         d = np.ascontiguousarray(directions, np.float32)
         tm = np.ascontiguousarray(tmax, np.float32)
         tg = np.ascontiguousarray(targets, np.uint32)
         n = len(o)
         out = np.zeros(n, np.float32)
-        _check(library().cenote_probe_shadow(self._h, _ptr(o), _ptr(d), _ptr(tm), _ptr(tg), n, _ptr(out)))
+        fn = library().cenote_probe_shadow_queued if queued else library().cenote_probe_shadow
+        _check(fn(self._h, _ptr(o), _ptr(d), _ptr(tm), _ptr(tg), n, _ptr(out)))
         return out
 
     def probe_env_sample(self, u: np.ndarray):

@@ -38,6 +38,8 @@ void probe_intersect_queued(const DeviceScene& scene, const float3* org, const f
                             float* t, uint32_t* flag, cudaStream_t s);
 void probe_shadow(const DeviceScene& scene, const float3* org, const float3* dir, const float* tmax,
                   const uint2* targets, uint32_t n, float* out, uint32_t* flag, cudaStream_t s);
+void probe_shadow_queued(const DeviceScene& scene, const float3* org, const float3* dir, const float* tmax,
+                         const uint2* targets, uint32_t n, float* out, uint32_t* flag, cudaStream_t s);
 void probe_env_sample(const DeviceScene& scene, const float2* u, uint32_t n, float3* dir, float* pdf, uint2* rc,
                       cudaStream_t s);
 void probe_env_pdf(const DeviceScene& scene, const float3* d, uint32_t n, float* pdf, cudaStream_t s);
@@ -1312,9 +1314,11 @@ int32_t cenote_probe_intersect_queued(cenote_scene* sc, const float* origins, co
     return probe_closest(sc, origins, directions, n, hits, t, true);
 }
 
-int32_t cenote_probe_shadow(cenote_scene* sc, const float* origins, const float* directions, const float* tmax,
-                            const uint32_t* targets, uint32_t n, float* out) {
+static int32_t probe_shadows(cenote_scene* sc, const float* origins, const float* directions, const float* tmax,
+                             const uint32_t* targets, uint32_t n, float* out, bool queued) {
     CN_CHECK(sc && origins && directions && tmax && targets && out, CENOTE_E_INVALID_ARGUMENT, "null argument");
+    CN_CHECK(!queued || !sc->ds.has_nonopaque, CENOTE_E_INVALID_ARGUMENT,
+             "the queued shadow walk serves scenes whose triangles are all opaque");
     if (n == 0) return CENOTE_OK;
     cenote_context* ctx = sc->ctx;
     std::lock_guard<std::mutex> lock(ctx->mu);
@@ -1323,12 +1327,22 @@ int32_t cenote_probe_shadow(cenote_scene* sc, const float* origins, const float*
     int32_t rc = with_device_io(
         ctx, {{origins, size_t(n) * 12}, {directions, size_t(n) * 12}, {tmax, size_t(n) * 4}, {targets, size_t(n) * 8}},
         {{out, size_t(n) * 4}, {&flag, 4}}, [&](std::vector<void*>& i, std::vector<void*>& o) {
-            probe_shadow(sc->ds, static_cast<float3*>(i[0]), static_cast<float3*>(i[1]), static_cast<float*>(i[2]),
-                         static_cast<uint2*>(i[3]), n, static_cast<float*>(o[0]), static_cast<uint32_t*>(o[1]),
-                         ctx->stream);
+            auto probe = queued ? probe_shadow_queued : probe_shadow;
+            probe(sc->ds, static_cast<float3*>(i[0]), static_cast<float3*>(i[1]), static_cast<float*>(i[2]),
+                  static_cast<uint2*>(i[3]), n, static_cast<float*>(o[0]), static_cast<uint32_t*>(o[1]), ctx->stream);
         });
     if (rc == CENOTE_OK && flag) return fail(CENOTE_E_OVERFLOW, "traversal bound exceeded");
     return rc;
+}
+
+int32_t cenote_probe_shadow(cenote_scene* sc, const float* origins, const float* directions, const float* tmax,
+                            const uint32_t* targets, uint32_t n, float* out) {
+    return probe_shadows(sc, origins, directions, tmax, targets, n, out, false);
+}
+
+int32_t cenote_probe_shadow_queued(cenote_scene* sc, const float* origins, const float* directions,
+                                   const float* tmax, const uint32_t* targets, uint32_t n, float* out) {
+    return probe_shadows(sc, origins, directions, tmax, targets, n, out, true);
 }
 
 int32_t cenote_probe_env_sample(cenote_scene* sc, const float* u, uint32_t n, float* directions, float* pdf,

@@ -111,6 +111,73 @@ __global__ void __launch_bounds__(128) k_probe_intersect_queued(DeviceScene scen
     if (overflow) atomicOr(flag, 1u);
 }
 
+// The queued shadow walk (trqueue.cuh, queued_any) over n queries of an
+// all-opaque scene, each warp walking its own contiguous share with refills;
+// out[i] = 1 when visible, -1 when occluded (k_probe_shadow's encoding).
+struct ProbeShadowSource {
+    const DeviceScene& scene;
+    const float3* org;
+    const float3* dir;
+    const float* tmaxs;
+    const uint2* targets;
+    float* out;
+    uint32_t* flag;
+    uint32_t cursor, end;  // the warp's next query and the end of its share (warp-uniform)
+    __device__ __forceinline__ uint32_t next(bool live, bool& drained) {
+        const uint32_t idle = __ballot_sync(0xffffffffu, !live);
+        const uint32_t i = cursor + __popc(idle & ((1u << (threadIdx.x & 31u)) - 1u));
+        cursor += __popc(idle);
+        if (cursor >= end) drained = true;
+        return (!live && i < end) ? i : ~0u;
+    }
+    __device__ __forceinline__ uint32_t leaf_of(uint32_t i) const {
+        const uint32_t light = targets[i].x, lprim = targets[i].y;
+        if (light == LIGHT_NONE) return 0xffffffffu;
+        const uint32_t first = scene.geometry[light].light;
+        return first != LIGHT_NONE ? scene.light_leaf[first + lprim] : 0xffffffffu;
+    }
+    __device__ __forceinline__ bool begin(uint32_t i, Ray& ray, AnyQuery& a) const {
+        ray = make_ray(org[i], dir[i]);
+        const uint32_t light = targets[i].x, leaf = leaf_of(i);
+        a.occluded = false;
+        a.light = light;
+        a.lprim = targets[i].y;
+        a.tm = tmaxs[i];
+        a.leaf = 0xffffffffu;
+        if (light != LIGHT_NONE && leaf == 0xffffffffu) return false;
+        if (leaf < scene.tri_count) {
+            const float4* tp = scene.tris + 3u * leaf;
+            float t, b1, b2;
+            if (tri_hit(ray, __ldg(tp), __ldg(tp + 1), __ldg(tp + 2), tmaxs[i], t, b1, b2)) {
+                a.tm = t;
+                a.leaf = leaf;
+            }
+        }
+        return true;
+    }
+    __device__ __forceinline__ void closest(uint32_t i, uint2* stack) const {
+        const float a = shadow_query(scene, make_ray(org[i], dir[i]), tmaxs[i], targets[i].x, targets[i].y,
+                                     leaf_of(i), stack);
+        if (a == -2.0f) atomicOr(flag, 1u);
+        out[i] = a < 0.0f ? -1.0f : a;
+    }
+    __device__ __forceinline__ void emit(uint32_t i, bool visible) const { out[i] = visible ? 1.0f : -1.0f; }
+    __device__ __forceinline__ uint32_t want_idle(bool drained) const { return drained ? 32u : 8u; }
+};
+
+__global__ void __launch_bounds__(128) k_probe_shadow_queued(DeviceScene scene, const float3* org, const float3* dir,
+                                                             const float* tmaxs, const uint2* targets, uint32_t n,
+                                                             float* out, uint32_t* flag) {
+    __shared__ TriQueueSmem tqs[4];
+    const uint32_t warp = blockIdx.x * 4u + (threadIdx.x >> 5);
+    const uint32_t begin = warp * PROBE_RAYS_PER_WARP;
+    if (begin >= n) return;  // whole warps only
+    ProbeShadowSource src{scene, org, dir, tmaxs, targets, out, flag, begin, min(n, begin + PROBE_RAYS_PER_WARP)};
+    bool overflow = false;
+    queued_any<false>(scene, tqs[threadIdx.x >> 5], src, overflow, nullptr, nullptr);
+    if (overflow) atomicOr(flag, 1u);
+}
+
 __global__ void k_probe_shadow(DeviceScene scene, const float3* org, const float3* dir, const float* tmaxs,
                                const uint2* targets, uint32_t n, float* out, uint32_t* flag) {
     uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -194,6 +261,11 @@ void probe_intersect_queued(const DeviceScene& scene, const float3* org, const f
 void probe_shadow(const DeviceScene& scene, const float3* org, const float3* dir, const float* tmax,
                   const uint2* targets, uint32_t n, float* out, uint32_t* flag, cudaStream_t s) {
     k_probe_shadow<<<blocks(n), 128, 0, s>>>(scene, org, dir, tmax, targets, n, out, flag);
+}
+void probe_shadow_queued(const DeviceScene& scene, const float3* org, const float3* dir, const float* tmax,
+                         const uint2* targets, uint32_t n, float* out, uint32_t* flag, cudaStream_t s) {
+    const uint32_t grid = (n + 4u * PROBE_RAYS_PER_WARP - 1u) / (4u * PROBE_RAYS_PER_WARP);
+    k_probe_shadow_queued<<<grid, 128, 0, s>>>(scene, org, dir, tmax, targets, n, out, flag);
 }
 void probe_env_sample(const DeviceScene& scene, const float2* u, uint32_t n, float3* dir, float* pdf, uint2* rc,
                       cudaStream_t s) {

@@ -353,6 +353,11 @@ int32_t cenote_probe_intersect_queued(cenote_scene* scene, const float* origins,
  * -1 when occluded. */
 int32_t cenote_probe_shadow(cenote_scene* scene, const float* origins, const float* directions,
                             const float* tmax, const uint32_t* targets, uint32_t n, float* out);
+/* The same query through the warp triangle queue the wavefront uses for
+ * all-opaque scenes (CENOTE_E_INVALID_ARGUMENT for a scene with fractional
+ * opacity); results equal cenote_probe_shadow's bit for bit. */
+int32_t cenote_probe_shadow_queued(cenote_scene* scene, const float* origins, const float* directions,
+                                   const float* tmax, const uint32_t* targets, uint32_t n, float* out);
 /* Environment importance sampling (environment.slang:94-107) for n uniform
  * pairs: direction (3 floats), pdf, and the sampled (row, column). */
 int32_t cenote_probe_env_sample(cenote_scene* scene, const float* u, uint32_t n, float* directions,

@@ -159,6 +159,9 @@ def test_shadow_queries_match(cornell):
     out = dev.probe_shadow(org, d, tmax, targets)
     ref_out = ref.shadow(org, d, tmax, targets)
     assert np.array_equal(out >= 0, ref_out >= 0)
+    # The warp triangle queue answers every query as the per-lane walk does.
+    queued = dev.probe_shadow(org, d, tmax, targets, queued=True)
+    assert np.array_equal(queued, out)
 
 
 # ---- BSDF: FP32 device vs FP64 oracle -------------------------------------------------
