@@ -33,6 +33,11 @@ namespace cn {
 
 constexpr uint32_t TQ_CAP = 64;  // FIFO entries per warp (a power of two, at least 2 x 32)
 constexpr uint32_t TQ_FULL = 0xffffffffu;
+// A closest-hit round also runs, partly filled, once this many lanes have
+// ended their walks and only wait for queued triangles, so they take new rays
+// sooner (chart intersect -4 %; 4 and 16 measured slower; the shadow walk
+// measured no gain from it).
+constexpr uint32_t TQ_WAITING = 8;
 
 // One warp's queue in shared memory (896 bytes), small enough that a full SM
 // of traversal blocks leaves the L1 cache (which holds the walks' stacks and
@@ -224,7 +229,8 @@ __device__ __forceinline__ void tq_round(const DeviceScene& s, TriQueueSmem& sm,
 //   uint32_t want_idle(bool drained)  idle lanes before the warp refills
 // Each step a walking lane expands one node and queues the triangles of the
 // leaves it hits; rounds run while the FIFO holds a warp's worth of
-// triangles, or until it is empty once no lane has nodes left. A lane whose
+// triangles, while TQ_WAITING lanes wait on it, or until it is empty once no
+// lane has nodes left. A lane whose
 // walk has ended completes when its last queued entry has been tested.
 // Sets `overflow` when a walk hit its iteration or stack bound.
 template <bool COUNT, class Src>
@@ -278,7 +284,9 @@ __device__ __forceinline__ void queued_closest(const DeviceScene& s, TriQueueSme
             }
             tq_append(sm, q, grp, last_seq);
             const bool any_walking = __any_sync(TQ_FULL, live && walking);
-            while (q.tris >= 32u || (q.tris > 0u && !any_walking)) tq_round<COUNT>(s, sm, q, ray, c, ray_mask, tests);
+            const bool many_waiting = uint32_t(__popc(__ballot_sync(TQ_FULL, live && !walking))) >= TQ_WAITING;
+            while (q.tris >= 32u || (q.tris > 0u && (!any_walking || many_waiting)))
+                tq_round<COUNT>(s, sm, q, ray, c, ray_mask, tests);
             bool finished = false;
             if (live && !walking && q.head >= last_seq) {
                 src.emit(item, make_uint4(c.inst, c.prim, __float_as_uint(c.b1), __float_as_uint(c.b2)), c.tmax);
