@@ -164,6 +164,22 @@ def test_shadow_queries_match(cornell):
     assert np.array_equal(queued, out)
 
 
+def test_queued_probes_refuse_fractional_opacity(ctx):
+    """The warp triangle queue tests candidates out of visit order, which
+    fractional opacity's Bernoulli draws depend on: its shadow probe refuses
+    such a scene (the wavefront walks them per lane)."""
+    from cenote_b200 import CenoteError, Scene
+
+    spec = scenes.textured(32, 24, 1, 2)  # a leaf quad cut out by an opacity map
+    dev = Scene(ctx, spec)
+    org = np.zeros((4, 3), np.float32)
+    d = np.tile(np.array([[0, 0, 1]], np.float32), (4, 1))
+    targets = np.full((4, 2), 0xFFFFFFFF, np.uint32)
+    with pytest.raises(CenoteError):
+        dev.probe_shadow(org, d, np.ones(4, np.float32), targets, queued=True)
+    assert dev.probe_shadow(org, d, np.ones(4, np.float32), targets).shape == (4,)
+
+
 # ---- BSDF: FP32 device vs FP64 oracle -------------------------------------------------
 
 WHITE = (1.0, 1.0, 1.0)
