@@ -269,7 +269,7 @@ def run_serving(args):
         w, h = res[rng.integers(4)]
         spp = int(np.clip(np.rint(np.exp(rng.uniform(0.0, np.log(256.0)))), 1, 256))
         jobs.append((float(arrivals[k]), n, w, h, spp))
-    server = Server(ctx, 160 << 30, slots=8, frame_spp=4, max_active=64)
+    server = Server(ctx, 160 << 30, slots=args.slots, frame_spp=4, max_active=64)
     # One small job per scene first: graph instantiation and first-touch costs
     # stay out of the measured stream; then 32 one-sample jobs per resolution,
     # whose film and frame buffers the server keeps for reuse, so the stream
@@ -317,7 +317,8 @@ def run_serving(args):
                                 if args.concurrency else f"{args.jobs} jobs, Poisson 200/s")
                                + ", scenes {closed box, material chart, large}, "
                                "resolutions {256^2, 640x360, 1280x720, 1920x1080}, spp log-uniform 1..256, "
-                               "160 GB budget, 8 slots, 64 resident jobs, a frame every 4 spp"},
+                               f"160 GB budget, {args.slots} slots (+2 for first frames), 64 resident jobs, "
+                               "a frame every 4 spp"},
         "time_to_first_frame_ms": {"p50": pct(ttff, 50), "p99": pct(ttff, 99), "max": float(ttff.max())},
         "time_to_target_ms": {"p50": pct(ttt, 50), "p99": pct(ttt, 99), "max": float(ttt.max())},
         # Closed loop: the jobs after the first `concurrency`, which all arrive
@@ -387,6 +388,7 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="chart", choices=list(WORKLOADS) + ["serving", "guiding"])
     ap.add_argument("--jobs", type=int, default=256, help="serving: jobs in the Poisson stream")
+    ap.add_argument("--slots", type=int, default=8, help="serving: the server's slots (streams with path pools)")
     ap.add_argument("--concurrency", type=int, default=0,
                     help="serving: keep this many jobs in flight (closed loop) instead of the Poisson arrivals")
     ap.add_argument("--width", type=int, default=480, help="guiding: image width")
