@@ -131,7 +131,7 @@ struct cenote_server {
         j.error = code;
         j.state = CENOTE_JOB_FAILED;
         j.t_done = now_ms(t0);
-        retire(j);
+        retire(j, false);
         failed++;
     }
 
@@ -183,17 +183,21 @@ struct cenote_server {
         }
     }
 
-    void retire(Job& j) {
+    // `reuse`: the job's chunks have all completed, so its buffers can serve
+    // the next jobs; a failed job's may still be in use by work enqueued
+    // before the failure, so they are freed (which waits for the device).
+    void retire(Job& j, bool reuse = true) {
         if (j.slot >= 0) {
             auto& v = slots[size_t(j.slot)]->jobs;
             v.erase(std::remove(v.begin(), v.end(), j.id), v.end());
         }
         first_queue.erase(std::remove(first_queue.begin(), first_queue.end(), j.id), first_queue.end());
-        // Its chunks are done (or failed): the buffers are free for the next jobs.
-        give_dev(j.sum);
-        give_dev(j.avg);
-        give_dev(j.offset);
-        give_host(j.host, size_t(j.width) * j.height * 16);
+        if (reuse) {
+            give_dev(j.sum);
+            give_dev(j.avg);
+            give_dev(j.offset);
+            give_host(j.host, size_t(j.width) * j.height * 16);
+        }
         j.free_device();
         used -= j.bytes;
         j.bytes = 0;
