@@ -178,6 +178,69 @@ WideBvh build_wide_bvh(const std::vector<BuildTri>& tris, unsigned threads) {
     (void)threads;
     b.build(0, 0, uint32_t(tris.size()), 0);
 
+    // Cost-optimal collapse (Ylitie, Karras & Laine 2017, "Efficient
+    // incoherent ray traversal on GPUs through compressed wide BVHs", §3.1):
+    // bottom-up, cost[n][i] is the cheapest SAH cost of covering n's subtree
+    // with at most i child slots of the parent (i = 1..7); a slot is either a
+    // leaf of up to three triangles or an 8-wide node whose own children are
+    // distributed over its 8 slots. c_node = 1 per node visit, c_prim = 0.3
+    // per triangle test, each weighted by the node's surface area.
+    constexpr float C_NODE = 1.0f, C_PRIM = 0.3f;
+    constexpr float INF = std::numeric_limits<float>::infinity();
+    const uint32_t n2 = b.next.load();
+    std::vector<float> cost(size_t(n2) * 8, INF);  // [n][i], i = 1..7 used
+    std::vector<uint8_t> how(size_t(n2) * 8, 0);    // i=1: 0 leaf / 1 node; i>1: 0 = as i-1, k = left gets k
+    std::vector<uint8_t> split8(n2, 0);             // left's share when n is an 8-wide node
+    for (uint32_t ni = n2; ni-- > 0;) {
+        const Node2& n = b.nodes[ni];
+        float* c = &cost[size_t(ni) * 8];
+        uint8_t* h = &how[size_t(ni) * 8];
+        const float area = n.box.area();
+        const float leaf = n.tris <= 3 ? area * C_PRIM * float(n.tris) : INF;
+        if (n.count) {
+            for (int i = 1; i < 8; ++i) c[i] = leaf;
+            continue;
+        }
+        const float* cl = &cost[size_t(n.left) * 8];
+        const float* cr = &cost[size_t(n.right) * 8];
+        float dist[9];
+        uint8_t dsplit[9] = {};
+        for (int j = 2; j <= 8; ++j) {
+            dist[j] = INF;
+            for (int k = 1; k < j; ++k) {
+                float v = cl[k] + cr[j - k];
+                if (v < dist[j]) {
+                    dist[j] = v;
+                    dsplit[j] = uint8_t(k);
+                }
+            }
+        }
+        split8[ni] = dsplit[8];
+        const float node = dist[8] + area * C_NODE;
+        c[1] = std::min(leaf, node);
+        h[1] = leaf <= node ? 0 : 1;
+        for (int i = 2; i < 8; ++i) {
+            if (dist[i] < c[i - 1]) {
+                c[i] = dist[i];
+                h[i] = dsplit[i];
+            } else {
+                c[i] = c[i - 1];
+                h[i] = 0;
+            }
+        }
+    }
+    auto is_leaf = [&](uint32_t ni) { return b.nodes[ni].count || how[size_t(ni) * 8 + 1] == 0; };
+    auto collect = [&](auto&& self, uint32_t ni, int i, std::vector<uint32_t>& kids) -> void {
+        while (i > 1 && how[size_t(ni) * 8 + i] == 0) --i;
+        if (i == 1) {
+            kids.push_back(ni);
+            return;
+        }
+        int k = how[size_t(ni) * 8 + i];
+        self(self, b.nodes[ni].left, k, kids);
+        self(self, b.nodes[ni].right, i - k, kids);
+    };
+
     struct Pending {
         uint32_t n2, wide, depth;
     };
@@ -193,25 +256,9 @@ WideBvh build_wide_bvh(const std::vector<BuildTri>& tris, unsigned threads) {
         const Node2& root = b.nodes[job.n2];
         if (root.count || root.tris <= 3) kids.push_back(job.n2);
         else {
-            kids.push_back(root.left);
-            kids.push_back(root.right);
-        }
-        while (kids.size() < 8) {
-            int pick = -1;
-            float best = -1.0f;
-            for (size_t i = 0; i < kids.size(); ++i) {
-                const Node2& k = b.nodes[kids[i]];
-                if (k.count || k.tris <= 3) continue;  // already a leaf candidate
-                float a = k.box.area();
-                if (a > best) {
-                    best = a;
-                    pick = int(i);
-                }
-            }
-            if (pick < 0) break;
-            uint32_t c = kids[pick];
-            kids[pick] = b.nodes[c].left;
-            kids.push_back(b.nodes[c].right);
+            int k = split8[job.n2];
+            collect(collect, root.left, k, kids);
+            collect(collect, root.right, 8 - k, kids);
         }
         // Octant slot assignment: child i's centre offset from the node centre
         // scored against slot s's direction (bit 2 ↔ +x, 1 ↔ +y, 0 ↔ +z);
@@ -287,8 +334,7 @@ WideBvh build_wide_bvh(const std::vector<BuildTri>& tris, unsigned threads) {
 
         uint32_t inner = 0;
         for (size_t i = 0; i < kids.size(); ++i) {
-            const Node2& k = b.nodes[kids[i]];
-            if (!(k.count || k.tris <= 3)) inner++;
+            if (!is_leaf(kids[i])) inner++;
         }
         wn.base_child = uint32_t(out.nodes.size());
         wn.base_tri = uint32_t(out.tris.size() / 12);
@@ -309,7 +355,7 @@ WideBvh build_wide_bvh(const std::vector<BuildTri>& tris, unsigned threads) {
                 if (a == 1) { wn.qlo_y[s] = ql; wn.qhi_y[s] = qh; }
                 if (a == 2) { wn.qlo_z[s] = ql; wn.qhi_z[s] = qh; }
             }
-            if (k.count || k.tris <= 3) {
+            if (is_leaf(kids[i])) {
                 std::vector<uint32_t> leaf;
                 b.gather(kids[i], leaf);
                 uint32_t cnt = uint32_t(leaf.size());  // 1..3

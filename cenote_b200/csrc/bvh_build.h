@@ -19,9 +19,10 @@ struct WideBvh {
     uint32_t depth = 0;
 };
 
-// Binned-SAH binary build (32 bins, single-triangle leaves), then a greedy
-// largest-area-first collapse into 8-wide nodes with up to three triangles
-// per leaf child, octant-ordered child slots and 8-bit quantised boxes.
+// Binned-SAH binary build (32 bins, single-triangle leaves), then a
+// cost-optimal collapse (a dynamic programme over the binary tree) into
+// 8-wide nodes with up to three triangles per leaf child, octant-ordered
+// child slots and 8-bit quantised boxes.
 // `threads` > 1 builds independent subtrees in parallel.
 WideBvh build_wide_bvh(const std::vector<BuildTri>& tris, unsigned threads);
 
