@@ -67,6 +67,44 @@ struct Builder {
         }
     }
 
+    // Exact SAH for ranges of at most SWEEP_MAX triangles: sort the range by
+    // centroid along each axis (stable, so ties keep their order and the
+    // build stays deterministic), cost every split position from prefix and
+    // suffix bounds, and leave the range sorted along the winning axis.
+    // Returns the index of the first triangle of the right child.
+    static constexpr uint32_t SWEEP_MAX = 65536;
+
+    uint32_t sweep_split(uint32_t first, uint32_t count) {
+        auto begin = idx.begin() + first, end = begin + count;
+        std::vector<float> right_area(count);
+        float best_cost = std::numeric_limits<float>::max();
+        int best_axis = 0;
+        uint32_t best_left = count / 2;
+        for (int axis = 0; axis < 3; ++axis) {
+            std::stable_sort(begin, end, [&](uint32_t x, uint32_t y) { return cen[3 * x + axis] < cen[3 * y + axis]; });
+            Box acc;
+            for (uint32_t i = count; i-- > 1;) {
+                acc.grow(tri_box[idx[first + i]]);
+                right_area[i] = acc.area();
+            }
+            Box left;
+            for (uint32_t i = 1; i < count; ++i) {
+                left.grow(tri_box[idx[first + i - 1]]);
+                float cost = left.area() * float(i) + right_area[i] * float(count - i);
+                if (cost < best_cost) {
+                    best_cost = cost;
+                    best_axis = axis;
+                    best_left = i;
+                }
+            }
+        }
+        if (best_axis != 2)
+            std::stable_sort(begin, end, [&](uint32_t x, uint32_t y) {
+                return cen[3 * x + best_axis] < cen[3 * y + best_axis];
+            });
+        return first + best_left;
+    }
+
     void build(uint32_t ni, uint32_t first, uint32_t count, int depth) {
         Node2& n = nodes[ni];
         Box box, cbox;
@@ -81,57 +119,61 @@ struct Builder {
             n.count = 1;
             return;
         }
-        constexpr int NB = 32;
-        float best_cost = std::numeric_limits<float>::max();
-        int best_axis = -1, best_split = 0;
-        for (int axis = 0; axis < 3; ++axis) {
-            float ext = cbox.hi[axis] - cbox.lo[axis];
-            if (!(ext > 0.0f)) continue;
-            float scale = float(NB) / ext;
-            Box bb[NB];
-            uint32_t bn[NB] = {};
-            for (uint32_t i = first; i < first + count; ++i) {
-                int b = std::min(NB - 1, std::max(0, int((cen[3 * idx[i] + axis] - cbox.lo[axis]) * scale)));
-                bb[b].grow(tri_box[idx[i]]);
-                bn[b]++;
-            }
-            float rarea[NB];
-            uint32_t rcount[NB];
-            Box acc;
-            uint32_t c = 0;
-            for (int b = NB - 1; b > 0; --b) {
-                acc.grow(bb[b]);
-                c += bn[b];
-                rarea[b] = acc.area();
-                rcount[b] = c;
-            }
-            Box lacc;
-            uint32_t lc = 0;
-            for (int s = 1; s < NB; ++s) {
-                lacc.grow(bb[s - 1]);
-                lc += bn[s - 1];
-                if (!lc || !rcount[s]) continue;
-                float cost = lacc.area() * float(lc) + rarea[s] * float(rcount[s]);
-                if (cost < best_cost) {
-                    best_cost = cost;
-                    best_axis = axis;
-                    best_split = s;
+        uint32_t mid;
+        if (count <= SWEEP_MAX) {
+            mid = sweep_split(first, count);
+        } else {
+            constexpr int NB = 32;
+            float best_cost = std::numeric_limits<float>::max();
+            int best_axis = -1, best_split = 0;
+            for (int axis = 0; axis < 3; ++axis) {
+                float ext = cbox.hi[axis] - cbox.lo[axis];
+                if (!(ext > 0.0f)) continue;
+                float scale = float(NB) / ext;
+                Box bb[NB];
+                uint32_t bn[NB] = {};
+                for (uint32_t i = first; i < first + count; ++i) {
+                    int b = std::min(NB - 1, std::max(0, int((cen[3 * idx[i] + axis] - cbox.lo[axis]) * scale)));
+                    bb[b].grow(tri_box[idx[i]]);
+                    bn[b]++;
+                }
+                float rarea[NB];
+                uint32_t rcount[NB];
+                Box acc;
+                uint32_t c = 0;
+                for (int b = NB - 1; b > 0; --b) {
+                    acc.grow(bb[b]);
+                    c += bn[b];
+                    rarea[b] = acc.area();
+                    rcount[b] = c;
+                }
+                Box lacc;
+                uint32_t lc = 0;
+                for (int s = 1; s < NB; ++s) {
+                    lacc.grow(bb[s - 1]);
+                    lc += bn[s - 1];
+                    if (!lc || !rcount[s]) continue;
+                    float cost = lacc.area() * float(lc) + rarea[s] * float(rcount[s]);
+                    if (cost < best_cost) {
+                        best_cost = cost;
+                        best_axis = axis;
+                        best_split = s;
+                    }
                 }
             }
-        }
-        uint32_t mid;
-        if (best_axis >= 0) {
-            float ext = cbox.hi[best_axis] - cbox.lo[best_axis];
-            float scale = float(NB) / ext;
-            float lo = cbox.lo[best_axis];
-            auto it = std::partition(idx.begin() + first, idx.begin() + first + count, [&](uint32_t t) {
-                int b = std::min(NB - 1, std::max(0, int((cen[3 * t + best_axis] - lo) * scale)));
-                return b < best_split;
-            });
-            mid = uint32_t(it - idx.begin());
-            if (mid == first || mid == first + count) mid = first + count / 2;
-        } else {
-            mid = first + count / 2;  // coincident centroids: split by index
+            if (best_axis >= 0) {
+                float ext = cbox.hi[best_axis] - cbox.lo[best_axis];
+                float scale = float(NB) / ext;
+                float lo = cbox.lo[best_axis];
+                auto it = std::partition(idx.begin() + first, idx.begin() + first + count, [&](uint32_t t) {
+                    int b = std::min(NB - 1, std::max(0, int((cen[3 * t + best_axis] - lo) * scale)));
+                    return b < best_split;
+                });
+                mid = uint32_t(it - idx.begin());
+                if (mid == first || mid == first + count) mid = first + count / 2;
+            } else {
+                mid = first + count / 2;  // coincident centroids: split by index
+            }
         }
         uint32_t l = next.fetch_add(2);
         n.left = l;

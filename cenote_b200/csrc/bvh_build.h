@@ -19,7 +19,8 @@ struct WideBvh {
     uint32_t depth = 0;
 };
 
-// Binned-SAH binary build (32 bins, single-triangle leaves), then a
+// SAH binary build (32 bins per axis above 65,536 triangles, an exact sweep
+// over sorted centroids below; single-triangle leaves), then a
 // cost-optimal collapse (a dynamic programme over the binary tree) into
 // 8-wide nodes with up to three triangles per leaf child, octant-ordered
 // child slots and 8-bit quantised boxes.
