@@ -69,19 +69,24 @@ struct Builder {
 
     // Exact SAH for ranges of at most SWEEP_MAX triangles: sort the range by
     // centroid along each axis (stable, so ties keep their order and the
-    // build stays deterministic), cost every split position from prefix and
-    // suffix bounds, and leave the range sorted along the winning axis.
+    // build stays deterministic), cost every split between two different
+    // centroids from prefix and suffix bounds, and leave the range sorted
+    // along the winning axis. Like the binned split, equal centroids stay on
+    // one side; a range whose centroids all coincide splits by index.
     // Returns the index of the first triangle of the right child.
     static constexpr uint32_t SWEEP_MAX = 65536;
 
-    uint32_t sweep_split(uint32_t first, uint32_t count) {
+    uint32_t sweep_split(uint32_t first, uint32_t count, const Box& cbox) {
         auto begin = idx.begin() + first, end = begin + count;
         std::vector<float> right_area(count);
         float best_cost = std::numeric_limits<float>::max();
-        int best_axis = 0;
-        uint32_t best_left = count / 2;
+        int best_axis = -1, sorted_axis = -1;
+        uint32_t best_left = 0;
         for (int axis = 0; axis < 3; ++axis) {
-            std::stable_sort(begin, end, [&](uint32_t x, uint32_t y) { return cen[3 * x + axis] < cen[3 * y + axis]; });
+            if (!(cbox.hi[axis] > cbox.lo[axis])) continue;
+            auto key = [&](uint32_t x) { return cen[3 * x + axis]; };
+            std::stable_sort(begin, end, [&](uint32_t x, uint32_t y) { return key(x) < key(y); });
+            sorted_axis = axis;
             Box acc;
             for (uint32_t i = count; i-- > 1;) {
                 acc.grow(tri_box[idx[first + i]]);
@@ -90,6 +95,7 @@ struct Builder {
             Box left;
             for (uint32_t i = 1; i < count; ++i) {
                 left.grow(tri_box[idx[first + i - 1]]);
+                if (!(key(idx[first + i - 1]) < key(idx[first + i]))) continue;
                 float cost = left.area() * float(i) + right_area[i] * float(count - i);
                 if (cost < best_cost) {
                     best_cost = cost;
@@ -98,7 +104,8 @@ struct Builder {
                 }
             }
         }
-        if (best_axis != 2)
+        if (best_axis < 0) return first + count / 2;  // coincident centroids
+        if (best_axis != sorted_axis)
             std::stable_sort(begin, end, [&](uint32_t x, uint32_t y) {
                 return cen[3 * x + best_axis] < cen[3 * y + best_axis];
             });
@@ -121,7 +128,7 @@ struct Builder {
         }
         uint32_t mid;
         if (count <= SWEEP_MAX) {
-            mid = sweep_split(first, count);
+            mid = sweep_split(first, count, cbox);
         } else {
             constexpr int NB = 32;
             float best_cost = std::numeric_limits<float>::max();

@@ -104,9 +104,11 @@ def test_wide_bvh_matches_oracle_hits(harness, tmp_path, name, lanes):
 
 
 def test_wide_bvh_random_soup(harness, tmp_path):
-    """A dense random triangle soup: many overlapping boxes, deep trees."""
+    """A dense random triangle soup: many overlapping boxes, deep trees. Above
+    65,536 triangles, so the root splits by binned SAH and the subtrees by the
+    exact sweep."""
     rng = np.random.default_rng(7)
-    n = 30000
+    n = 80000
     c = rng.random((n, 1, 3)) * 10.0 + rng.normal(scale=0.05, size=(n, 3, 3))
     tris = c.astype(np.float32).reshape(n, 9)
     ids = np.zeros((n, 3), np.uint32)
@@ -127,12 +129,14 @@ def test_wide_bvh_random_soup(harness, tmp_path):
 
 
 def test_degenerate_inputs(harness, tmp_path):
-    """One triangle; coincident centroids; a flat (zero-extent) axis."""
+    """One triangle; coincident centroids (few, and more than the binned
+    split's 65,536-triangle threshold); a flat (zero-extent) axis."""
     one = np.array([[0, 0, 0, 1, 0, 0, 0, 1, 0]], np.float32)
     same = np.tile(one, (40, 1))
+    many = np.tile(one, (70000, 1))
     flat = np.random.default_rng(3).random((500, 9)).astype(np.float32)
     flat[:, 2::3] = 0.25
-    for tris in (one, same, flat):
+    for tris in (one, same, many, flat):
         ids = np.zeros((len(tris), 3), np.uint32)
         ids[:, 1] = np.arange(len(tris))
         ids[:, 2] = 0x1FF
@@ -140,3 +144,5 @@ def test_degenerate_inputs(harness, tmp_path):
         d = np.array([[0, 0, -1], [0, 0, 1], [0, 0, 1]], np.float32)
         hits, t, _ = run_harness(harness, tmp_path, tris, ids, org, d)
         assert hits[2, 0] == 0xFFFFFFFF
+        if tris is not flat:  # every copy hit at the same t: the lowest primitive wins
+            assert hits[0, 0] == 0 and hits[0, 1] == 0 and t[0] == np.float32(1.0)
