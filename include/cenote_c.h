@@ -201,9 +201,10 @@ void cenote_context_destroy(cenote_context* ctx);
 /* The context's cudaStream_t, for callers that time or order work on it. */
 void* cenote_context_stream(cenote_context* ctx);
 int32_t cenote_synchronize(cenote_context* ctx);
-/* How scenes created from now on build their BVH: on the host (binned SAH,
- * the default) or on the GPU (PLOC over Morton order, collapsed on the
- * device). Either tree gives the same closest hits. */
+/* How scenes created from now on build their BVH: on the host (SAH binary
+ * tree, cost-optimal collapse to 8-wide nodes; the default) or on the GPU
+ * (PLOC over Morton order, collapsed on the device). Either tree gives the
+ * same closest hits. */
 #define CENOTE_BVH_HOST_SAH 0u
 #define CENOTE_BVH_GPU_PLOC 1u
 int32_t cenote_context_set_bvh_builder(cenote_context* ctx, uint32_t builder);
