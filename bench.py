@@ -585,7 +585,7 @@ def main():
         "rays_per_s": (rays[0] + rays[1]) * world / (ms / 1e3),
         "extension_rays_per_step": rays[0] / args.steps, "shadow_rays_per_step": rays[1] / args.steps,
         "stage_ms_per_step": {k: v / args.steps for k, v in stage.items()},
-        "scene_prep_ms": {"bvh": float(prep[0]), "bvh_builder": "GPU PLOC" if args.bvh == "gpu" else "host binned SAH",
+        "scene_prep_ms": {"bvh": float(prep[0]), "bvh_builder": "GPU PLOC" if args.bvh == "gpu" else "host SAH, cost-optimal collapse",
                           "env_tables": float(prep[1]), "total": float(prep[2]), "wall": prep_wall_ms},
         "roofline": {
             "kernel": "traversal (k_intersect + k_shadow)", "bound": "hbm",
