@@ -6,7 +6,8 @@
 // tris.bin: uint32 n, then n × (9 float corners, uint32 instance, primitive, flags)
 // rays.bin: uint32 m, then m × (3 float origin, 3 float direction)
 // hits.bin: m × (uint32 instance, primitive, b1 bits, b2 bits, float t)
-// Exit status 0 = structure valid and every ray traced within bounds.
+// Exit status 0 = structure valid and every ray traced within bounds; stdout
+// reports the tree's size and the wide nodes and triangles tested per ray.
 #include "cuda_host_shim.h"
 #include "traverse.cuh"
 #include "bvh_build.h"
@@ -85,12 +86,13 @@ int main(int argc, char** argv) {
     s.tri_count = nt;
     FILE* o = std::fopen(argv[3], "wb");
     int bad = 0;
+    uint32_t visits = 0, tests = 0;  // wide nodes expanded, triangles tested
     for (uint32_t i = 0; i < m; ++i) {
         Ray ray = make_ray(make_float3(rays[6 * i], rays[6 * i + 1], rays[6 * i + 2]),
                            make_float3(rays[6 * i + 3], rays[6 * i + 4], rays[6 * i + 5]));
         float tmax = 1e30f;
         uint32_t bi = LIGHT_NONE, bp = 0, b1s = 0, b2s = 0;
-        bool ok = traverse(s, ray, tmax, [&](uint32_t, float4 a, float4 b, float4 c, float& tm) {
+        bool ok = traverse<true>(s, ray, tmax, [&](uint32_t, float4 a, float4 b, float4 c, float& tm) {
             float t, b1, b2;
             if (!tri_hit(ray, a, b, c, tm, t, b1, b2)) return false;
             uint32_t inst = __float_as_uint(a.w), prim = __float_as_uint(b.w);
@@ -101,13 +103,14 @@ int main(int argc, char** argv) {
             b1s = __float_as_uint(b1);
             b2s = __float_as_uint(b2);
             return false;
-        });
+        }, &visits, &tests);
         if (!ok) bad++;
         float tt = bi == LIGHT_NONE ? -1.0f : tmax;
         uint32_t rec[5] = {bi, bp, b1s, b2s, __float_as_uint(tt)};
         std::fwrite(rec, 4, 5, o);
     }
     std::fclose(o);
-    std::fprintf(stdout, "nodes %u tris %u depth %u bad %d\n", nn, nt, bvh.depth, bad);
+    std::fprintf(stdout, "nodes %u tris %u depth %u bad %d visits/ray %.4f tests/ray %.4f\n", nn, nt, bvh.depth, bad,
+                 m ? double(visits) / m : 0.0, m ? double(tests) / m : 0.0);
     return bad ? 3 : 0;
 }

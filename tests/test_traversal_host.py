@@ -146,3 +146,41 @@ def test_degenerate_inputs(harness, tmp_path):
         assert hits[2, 0] == 0xFFFFFFFF
         if tris is not flat:  # every copy hit at the same t: the lowest primitive wins
             assert hits[0, 0] == 0 and hits[0, 1] == 0 and t[0] == np.float32(1.0)
+
+
+def camera_rays(spec, width, height):
+    """Pinhole rays through pixel centres from the scene camera (float64 basis
+    rounded to f32: a traversal workload, not the renderer's raygen)."""
+    cam = spec.camera
+    p = np.asarray(cam.position, np.float64)
+    f = np.asarray(cam.look_at, np.float64) - p
+    f /= np.linalg.norm(f)
+    r = np.cross(f, np.asarray(cam.up, np.float64))
+    r /= np.linalg.norm(r)
+    u = np.cross(r, f)
+    th = np.tan(np.radians(cam.vfov_degrees) / 2)
+    ys, xs = np.mgrid[0:height, 0:width]
+    sx = ((xs + 0.5) / width * 2 - 1) * th * width / height
+    sy = (1 - (ys + 0.5) / height * 2) * th
+    d = f + sx.reshape(-1, 1) * r + sy.reshape(-1, 1) * u
+    d = (d / np.linalg.norm(d, axis=1, keepdims=True)).astype(np.float32)
+    return np.broadcast_to(p, d.shape).astype(np.float32), d
+
+
+def test_tree_quality_chart(harness, tmp_path):
+    """Camera rays through the material chart: hits equal the oracle's, and the
+    tree stays as cheap to walk as the SAH-swept, cost-optimally collapsed
+    build makes it: 4.99 wide nodes and 3.85 triangles per ray here (the
+    greedily collapsed 32-bin tree needed 6.01 and 4.54); the bounds leave
+    about 5 %."""
+    spec = scenes.chart(env_size=(8, 4))
+    tris, ids = world_triangles(spec)
+    org, d = camera_rays(spec, 160, 90)
+    hits, t, log = run_harness(harness, tmp_path, tris, ids, org, d)
+    ref_hits, ref_t = oracle.OracleScene(spec).intersect(org, d)
+    assert np.array_equal(hits, ref_hits), log
+    assert np.array_equal(t.view(np.uint32), ref_t.view(np.uint32))
+    words = log.split()
+    visits = float(words[words.index("visits/ray") + 1])
+    tests = float(words[words.index("tests/ray") + 1])
+    assert visits < 5.25 and tests < 4.05, log
