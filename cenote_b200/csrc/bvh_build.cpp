@@ -32,9 +32,11 @@ struct Box {
             hi[a] = std::max(hi[a], p[a]);
         }
     }
-    float area() const {
-        float d[3];
-        for (int a = 0; a < 3; ++a) d[a] = std::max(hi[a] - lo[a], 0.0f);
+    // Half the surface area, in double: boxes of very large triangles
+    // (extents near FLT_MAX) keep finite, ordered costs.
+    double area() const {
+        double d[3];
+        for (int a = 0; a < 3; ++a) d[a] = std::max(double(hi[a]) - double(lo[a]), 0.0);
         return d[0] * d[1] + d[1] * d[2] + d[2] * d[0];
     }
 };
@@ -78,8 +80,8 @@ struct Builder {
 
     uint32_t sweep_split(uint32_t first, uint32_t count, const Box& cbox) {
         auto begin = idx.begin() + first, end = begin + count;
-        std::vector<float> right_area(count);
-        float best_cost = std::numeric_limits<float>::max();
+        std::vector<double> right_area(count);
+        double best_cost = std::numeric_limits<double>::max();
         int best_axis = -1, sorted_axis = -1;
         uint32_t best_left = 0;
         for (int axis = 0; axis < 3; ++axis) {
@@ -96,7 +98,7 @@ struct Builder {
             for (uint32_t i = 1; i < count; ++i) {
                 left.grow(tri_box[idx[first + i - 1]]);
                 if (!(key(idx[first + i - 1]) < key(idx[first + i]))) continue;
-                float cost = left.area() * float(i) + right_area[i] * float(count - i);
+                double cost = left.area() * double(i) + right_area[i] * double(count - i);
                 if (cost < best_cost) {
                     best_cost = cost;
                     best_axis = axis;
@@ -110,6 +112,26 @@ struct Builder {
                 return cen[3 * x + best_axis] < cen[3 * y + best_axis];
             });
         return first + best_left;
+    }
+
+    // Past SAH_DEPTH_MAX binary levels the split is the object median along
+    // the centroid box's longest axis (ties by triangle index), which halves
+    // the range every level: an SAH that peels one triangle off per level
+    // (nested triangles of geometrically growing size) cannot make the
+    // binary tree, the recursion or the wide tree deeper than
+    // SAH_DEPTH_MAX + log2(n) levels.
+    static constexpr int SAH_DEPTH_MAX = 48;
+
+    uint32_t median_split(uint32_t first, uint32_t count, const Box& cbox) {
+        int axis = 0;
+        for (int a = 1; a < 3; ++a)
+            if (cbox.hi[a] - cbox.lo[a] > cbox.hi[axis] - cbox.lo[axis]) axis = a;
+        auto begin = idx.begin() + first;
+        std::nth_element(begin, begin + count / 2, begin + count, [&](uint32_t x, uint32_t y) {
+            float a = cen[3 * x + axis], b = cen[3 * y + axis];
+            return a < b || (a == b && x < y);
+        });
+        return first + count / 2;
     }
 
     void build(uint32_t ni, uint32_t first, uint32_t count, int depth) {
@@ -127,11 +149,13 @@ struct Builder {
             return;
         }
         uint32_t mid;
-        if (count <= SWEEP_MAX) {
+        if (depth >= SAH_DEPTH_MAX) {
+            mid = median_split(first, count, cbox);
+        } else if (count <= SWEEP_MAX) {
             mid = sweep_split(first, count, cbox);
         } else {
             constexpr int NB = 32;
-            float best_cost = std::numeric_limits<float>::max();
+            double best_cost = std::numeric_limits<double>::max();
             int best_axis = -1, best_split = 0;
             for (int axis = 0; axis < 3; ++axis) {
                 float ext = cbox.hi[axis] - cbox.lo[axis];
@@ -144,7 +168,7 @@ struct Builder {
                     bb[b].grow(tri_box[idx[i]]);
                     bn[b]++;
                 }
-                float rarea[NB];
+                double rarea[NB];
                 uint32_t rcount[NB];
                 Box acc;
                 uint32_t c = 0;
@@ -160,7 +184,7 @@ struct Builder {
                     lacc.grow(bb[s - 1]);
                     lc += bn[s - 1];
                     if (!lc || !rcount[s]) continue;
-                    float cost = lacc.area() * float(lc) + rarea[s] * float(rcount[s]);
+                    double cost = lacc.area() * double(lc) + rarea[s] * double(rcount[s]);
                     if (cost < best_cost) {
                         best_cost = cost;
                         best_axis = axis;
@@ -237,6 +261,9 @@ WideBvh build_wide_bvh(const std::vector<BuildTri>& tris, unsigned threads) {
     constexpr float C_NODE = 1.0f, C_PRIM = 0.3f;
     constexpr float INF = std::numeric_limits<float>::infinity();
     const uint32_t n2 = b.next.load();
+    // Areas relative to the root's, so the float costs stay finite for any
+    // finite geometry.
+    const double inv_root = 1.0 / std::max(b.nodes[0].box.area(), 1e-300);
     std::vector<float> cost(size_t(n2) * 8, INF);  // [n][i], i = 1..7 used
     std::vector<uint8_t> how(size_t(n2) * 8, 0);    // i=1: 0 leaf / 1 node; i>1: 0 = as i-1, k = left gets k
     std::vector<uint8_t> split8(n2, 0);             // left's share when n is an 8-wide node
@@ -244,7 +271,7 @@ WideBvh build_wide_bvh(const std::vector<BuildTri>& tris, unsigned threads) {
         const Node2& n = b.nodes[ni];
         float* c = &cost[size_t(ni) * 8];
         uint8_t* h = &how[size_t(ni) * 8];
-        const float area = n.box.area();
+        const float area = float(n.box.area() * inv_root);
         const float leaf = n.tris <= 3 ? area * C_PRIM * float(n.tris) : INF;
         if (n.count) {
             for (int i = 1; i < 8; ++i) c[i] = leaf;
@@ -421,6 +448,19 @@ WideBvh build_wide_bvh(const std::vector<BuildTri>& tris, unsigned threads) {
         out.nodes[job.wide] = wn;
         for (const Pending& p : spawn) queue.push_back(p);
     }
+    // Stack entries a walk's node groups can need: a node with two or more
+    // inner children may leave a group on the stack while one child is
+    // walked. Children follow their parents (breadth first), so one pass
+    // from the back sees every child before its parent.
+    std::vector<uint32_t> need(out.nodes.size(), 0);
+    for (size_t i = out.nodes.size(); i-- > 0;) {
+        const WideNode& w = out.nodes[i];
+        const uint32_t inner = uint32_t(__builtin_popcount(w.imask));
+        uint32_t m = 0;
+        for (uint32_t k = 0; k < inner; ++k) m = std::max(m, need[w.base_child + k]);
+        need[i] = m + (inner >= 2 ? 1u : 0u);
+    }
+    out.stack_need = need.empty() ? 0u : need[0];
     return out;
 }
 

@@ -77,6 +77,11 @@ static_assert(sizeof(WideNode) == 80, "wide node is 80 bytes");
 // mask, bit 8 opaque) — so a hit needs no second fetch.
 constexpr uint32_t TRI_OPAQUE = 0x100u;
 
+// Entries of a walk's traversal stack (node groups and postponed triangle
+// groups). Scene creation rejects a wide BVH whose node groups alone could
+// fill it.
+constexpr int TRAVERSAL_STACK_DEPTH = 32;
+
 // What every kernel reads about the scene; passed by value (kernel params
 // live in the constant bank, uniform across the grid).
 struct DeviceScene {
@@ -101,7 +106,10 @@ struct DeviceScene {
     const uint8_t* instance_layers;  // per instance: 1 if its material has coat, fuzz, transmission or thin walls
     const unsigned long long* textures;  // cudaTextureObject_t per bindless slot
     uint32_t texture_count;
-    uint32_t pad2;
+    // TRAVERSAL_STACK_DEPTH minus the wide tree's depth: a walk postpones a
+    // triangle group onto the stack only below this height, so the node
+    // groups (one per level) that may follow always fit.
+    uint32_t stack_room;
     float bbox_min[3];    // world bounds of every triangle, for the guide's position encoding
     float bbox_inv;       // 1 / the bounds' largest extent
     // Set inside a traversal kernel (0 elsewhere): nodes 0..top_count-1 (the

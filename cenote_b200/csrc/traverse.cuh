@@ -22,7 +22,7 @@
 namespace cn {
 
 
-constexpr int TRAVERSAL_STACK = 32;
+constexpr int TRAVERSAL_STACK = TRAVERSAL_STACK_DEPTH;
 
 struct Ray {
     float3 org, dir, idir;
@@ -260,8 +260,7 @@ __device__ __forceinline__ int walk_step(const DeviceScene& s, const Ray& r, flo
         w.resumed = true;
     }
     while (w.t.y & 0x00ffffffu) {
-        if (!w.resumed && uint32_t(__popc(__activemask())) < POSTPONE) {
-            if (w.sp >= TRAVERSAL_STACK) return WALK_OVERFLOW;
+        if (!w.resumed && w.sp < s.stack_room && uint32_t(__popc(__activemask())) < POSTPONE) {
             stack[w.sp++] = w.t;
             break;
         }

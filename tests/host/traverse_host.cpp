@@ -84,6 +84,8 @@ int main(int argc, char** argv) {
     s.tris = reinterpret_cast<const float4*>(bvh.tris.data());
     s.node_count = nn;
     s.tri_count = nt;
+    if (bvh.stack_need >= uint32_t(TRAVERSAL_STACK_DEPTH)) return fail("stack need", bvh.stack_need, bvh.depth);
+    s.stack_room = uint32_t(TRAVERSAL_STACK_DEPTH) - bvh.stack_need;
     FILE* o = std::fopen(argv[3], "wb");
     int bad = 0;
     uint32_t visits = 0, tests = 0;  // wide nodes expanded, triangles tested
@@ -110,7 +112,8 @@ int main(int argc, char** argv) {
         std::fwrite(rec, 4, 5, o);
     }
     std::fclose(o);
-    std::fprintf(stdout, "nodes %u tris %u depth %u bad %d visits/ray %.4f tests/ray %.4f\n", nn, nt, bvh.depth, bad,
+    std::fprintf(stdout, "nodes %u tris %u depth %u stack %u bad %d visits/ray %.4f tests/ray %.4f\n", nn, nt,
+                 bvh.depth, bvh.stack_need, bad,
                  m ? double(visits) / m : 0.0, m ? double(tests) / m : 0.0);
     return bad ? 3 : 0;
 }

@@ -184,3 +184,43 @@ def test_tree_quality_chart(harness, tmp_path):
     visits = float(words[words.index("visits/ray") + 1])
     tests = float(words[words.index("tests/ray") + 1])
     assert visits < 5.25 and tests < 4.05, log
+
+
+def test_nested_triangles_keep_the_tree_shallow(harness, tmp_path):
+    """Nested triangles of geometrically growing size: at every level the
+    SAH's cheapest split peels the largest triangle off, which without a
+    bound makes a binary chain as deep as the input. Past 48 SAH levels the
+    builder splits at the object median, so the wide tree stays well inside
+    the traversal stack and the walk still finds the oracle's hits."""
+    n = 300
+    k = np.arange(n, dtype=np.float64)
+    s = 1.3 ** k
+    base = np.array([[-1.0, -1.0, 0.0], [1.0, -1.0, 0.0], [0.0, 1.0, 0.0]])
+    tris = (base[None] * s[:, None, None]).astype(np.float64)
+    tris[:, :, 0] += 0.1 * s[:, None]  # distinct centroids, ordered by size
+    tris[:, :, 2] = -1e-3 * k[:, None]  # layered in depth: a ray down -z meets the smallest first
+    tris = tris.astype(np.float32).reshape(n, 9)
+    ids = np.zeros((n, 3), np.uint32)
+    ids[:, 1] = np.arange(n)
+    ids[:, 2] = 0x1FF
+    rng = np.random.default_rng(5)
+    org = np.zeros((4000, 3), np.float32)
+    org[:, :2] = (rng.normal(size=(4000, 2)) * np.exp(rng.uniform(0, 40, (4000, 1)))).astype(np.float32)
+    org[:, 2] = 1.0
+    # Steep rays (z their dominant axis): every triangle's corners then sit
+    # at one depth along the ray's axis and the FP32 hit distance has no
+    # cancellation, whatever the triangle's size.
+    d = np.tile(np.array([0, 0, -1], np.float32), (4000, 1))
+    d[::2, :2] = rng.uniform(-0.5, 0.5, (2000, 2)).astype(np.float32)
+    d /= np.linalg.norm(d, axis=1, keepdims=True)
+    hits, t, log = run_harness(harness, tmp_path, tris, ids, org, d)
+    stack = int(log.split("stack ")[1].split()[0])
+    assert stack < 16, log
+    mesh = scenes.Mesh(tris.reshape(-1, 3), np.tile([0, 0, 1], (3 * n, 1)).astype(np.float32),
+                       np.zeros((3 * n, 2), np.float32), np.arange(3 * n, dtype=np.uint32).reshape(n, 3))
+    spec = scenes.SceneSpec("nested", [scenes.Object(mesh, scenes.rows(np.eye(4)), scenes.matte((0.5, 0.5, 0.5)))],
+                            scenes.Camera((0, 0, 20), (0, 0, 0)), scenes.Environment.constant((0, 0, 0)), 8, 8, 1, 1)
+    ref_hits, ref_t = oracle.OracleScene(spec).intersect(org, d)
+    assert np.array_equal(hits, ref_hits)
+    assert np.array_equal(t.view(np.uint32), ref_t.view(np.uint32))
+    assert (hits[:, 0] != 0xFFFFFFFF).mean() > 0.3
