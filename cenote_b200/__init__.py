@@ -97,7 +97,8 @@ class Stats(C.Structure):
                 ("node_visits", C.c_uint64), ("triangle_tests", C.c_uint64), ("gpu_ms", C.c_float),
                 ("raygen_ms", C.c_float), ("intersect_ms", C.c_float), ("shade_ms", C.c_float),
                 ("shadow_ms", C.c_float), ("film_ms", C.c_float), ("kernel_launches", C.c_uint32),
-                ("waves", C.c_uint32), ("samples_per_wave", C.c_uint32), ("overflow", C.c_uint32)]
+                ("waves", C.c_uint32), ("samples_per_wave", C.c_uint32), ("overflow", C.c_uint32),
+                ("surface_hits", C.c_uint64)]
 
 
 PROFILE_TIMING, PROFILE_COUNTS = 1, 2

@@ -45,7 +45,9 @@ void probe_env_sample(const DeviceScene& scene, const float2* u, uint32_t n, flo
 void probe_env_pdf(const DeviceScene& scene, const float3* d, uint32_t n, float* pdf, cudaStream_t s);
 void probe_texture(const DeviceScene& scene, uint32_t index, uint32_t mode, const float2* uv, uint32_t n, float4* out,
                    cudaStream_t s);
-cudaError_t static_env_scratch(int device, double** out, size_t* max_texels, uint32_t* max_rows);
+cudaError_t static_env_scratch(int device, double** out, size_t* max_texels, uint32_t* max_rows, cudaEvent_t* done);
+bool static_env_pending(int device);
+void static_env_set_pending(int device, bool pending);
 }  // namespace cn
 
 using namespace cn;
@@ -508,6 +510,7 @@ int32_t cenote_scene_create_textured(cenote_context* ctx, const cenote_object* o
     CN_CUDA(err);
     CN_CUDA(cudaMemcpyAsync(blayers->ptr, layers.data(), layers.size(), cudaMemcpyHostToDevice, ctx->stream));
     CN_CUDA(cudaMemsetAsync(bleaf->ptr, 0xff, std::max<size_t>(1, sc->lights.size()) * 4, ctx->stream));
+    uint32_t bvh_depth = 0;  // stack entries the tree's node groups may take
     if (ctx->bvh_builder == CENOTE_BVH_GPU_PLOC && !tris.empty()) {
         // Triangles in input order, identity in the w lanes; the device
         // builds the binary tree, collapses it and lays out the leaves.
@@ -528,8 +531,14 @@ int32_t cenote_scene_create_textured(cenote_context* ctx, const cenote_object* o
         bnodes = sc->adopt(g.nodes, size_t(g.node_count) * sizeof(WideNode));
         btris = sc->adopt(g.tris, size_t(tri_count) * 48);
         node_count = g.node_count;
+        bvh_depth = g.depth;  // bounds the node groups a walk pushes
+        CN_CHECK(g.depth < uint32_t(TRAVERSAL_STACK_DEPTH), CENOTE_E_SCENE,
+                 "the scene's BVH needs a deeper traversal stack than the walks hold");
     } else {
         WideBvh bvh = build_wide_bvh(tris, std::max(1u, std::thread::hardware_concurrency()));
+        CN_CHECK(bvh.stack_need < uint32_t(TRAVERSAL_STACK_DEPTH), CENOTE_E_SCENE,
+                 "the scene's BVH needs a deeper traversal stack than the walks hold");
+        bvh_depth = bvh.stack_need;
         bnodes = sc->add(bvh.nodes.size() * sizeof(WideNode), &err);
         CN_CUDA(err);
         btris = sc->add(bvh.tris.size() * 4, &err);
@@ -652,6 +661,7 @@ int32_t cenote_scene_create_textured(cenote_context* ctx, const cenote_object* o
     ds.light_count = uint32_t(sc->lights.size());
     ds.node_count = node_count;
     ds.tri_count = tri_count;
+    ds.stack_room = uint32_t(TRAVERSAL_STACK_DEPTH) - bvh_depth;
     ds.has_nonopaque = nonopaque ? 1u : 0u;
     ds.has_layers = layered ? 1u : 0u;
     const float extent = std::max({bmax[0] - bmin[0], bmax[1] - bmin[1], bmax[2] - bmin[2], 1e-6f});
@@ -910,10 +920,16 @@ namespace {
 // timings into the renderer's stats.
 // While alive, the scene's wide BVH nodes are a persisting access-policy
 // window on the context's stream: the waves' streaming path state does not
-// evict them from L2. The window is cleared and the persisting lines are
-// released on exit.
+// evict them from L2. The window is cleared on exit; the persisting lines
+// (a device-wide state) are released once no window of this process is
+// active on the device, so a renderer finishing does not evict the window
+// of another renderer or serving slot still running.
+std::mutex g_l2_mutex;
+int g_l2_active[64] = {};
+
 struct L2Window {
     cudaStream_t stream = nullptr;
+    int device = -1;
     L2Window(cenote_context* ctx, const cenote_scene* sc, bool on) {
         const size_t bytes = std::min(size_t(sc->ds.node_count) * sizeof(WideNode), ctx->l2_window_max);
         if (!on || bytes == 0 || ctx->l2_persist_max == 0) return;
@@ -931,17 +947,28 @@ struct L2Window {
         a.accessPolicyWindow.hitRatio = std::min(1.0f, float(ctx->l2_set_aside) / float(bytes));
         a.accessPolicyWindow.hitProp = cudaAccessPropertyPersisting;
         a.accessPolicyWindow.missProp = cudaAccessPropertyStreaming;
-        if (cudaStreamSetAttribute(ctx->stream, cudaStreamAttributeAccessPolicyWindow, &a) == cudaSuccess)
+        if (cudaStreamSetAttribute(ctx->stream, cudaStreamAttributeAccessPolicyWindow, &a) == cudaSuccess) {
             stream = ctx->stream;
-        else
+            if (ctx->device >= 0 && ctx->device < 64) {
+                device = ctx->device;
+                std::lock_guard<std::mutex> lock(g_l2_mutex);
+                g_l2_active[device]++;
+            }
+        } else {
             cudaGetLastError();
+        }
     }
     ~L2Window() {
         if (!stream) return;
         cudaStreamAttrValue a{};
         a.accessPolicyWindow.num_bytes = 0;
         cudaStreamSetAttribute(stream, cudaStreamAttributeAccessPolicyWindow, &a);
-        cudaCtxResetPersistingL2Cache();
+        bool last = true;
+        if (device >= 0) {
+            std::lock_guard<std::mutex> lock(g_l2_mutex);
+            last = --g_l2_active[device] == 0;
+        }
+        if (last) cudaCtxResetPersistingL2Cache();
     }
 };
 
@@ -971,7 +998,7 @@ int32_t run_waves(cenote_renderer* r, cenote_scene* sc, uint32_t width, uint32_t
     CN_CUDA(cudaEventRecord(ctx->t1, ctx->stream));
     int32_t rc = wait_stream(ctx->stream, ctx->sync_ev, 600000.0);
     if (rc != CENOTE_OK) return rc;
-    unsigned long long t[5];
+    unsigned long long t[6];
     CN_CUDA(cudaMemcpy(t, r->tally.ptr, sizeof t, cudaMemcpyDeviceToHost));
     float ms = 0.0f;
     cudaEventElapsedTime(&ms, ctx->t0, ctx->t1);
@@ -981,6 +1008,7 @@ int32_t run_waves(cenote_renderer* r, cenote_scene* sc, uint32_t width, uint32_t
     st.overflow = uint32_t(t[2]);
     st.node_visits = t[3] - r->tally_prev[3];
     st.triangle_tests = t[4] - r->tally_prev[4];
+    st.surface_hits = t[5] - r->tally_prev[5];
     st.samples = pixels * count;
     st.gpu_ms = ms;
     st.kernel_launches = wc.launches;
@@ -1003,7 +1031,7 @@ int32_t run_waves(cenote_renderer* r, cenote_scene* sc, uint32_t width, uint32_t
         }
     }
     r->stats = st;
-    for (int k = 0; k < 5; ++k) r->tally_prev[k] = t[k];
+    for (int k = 0; k < 6; ++k) r->tally_prev[k] = t[k];
     if (t[2]) return fail(CENOTE_E_OVERFLOW, "a traversal stack or queue bound was exceeded");
     return CENOTE_OK;
 }
@@ -1412,7 +1440,17 @@ int32_t cenote_env_tables_static(cenote_context* ctx, const float* texels, uint3
     double* scratch = nullptr;
     size_t max_texels = 0;
     uint32_t max_rows = 0;
-    CN_CUDA(static_env_scratch(ctx->device, &scratch, &max_texels, &max_rows));
+    cudaEvent_t done = nullptr;
+    CN_CUDA(static_env_scratch(ctx->device, &scratch, &max_texels, &max_rows, &done));
+    if (static_env_pending(ctx->device)) {
+        // An earlier call on this device returned before its work finished:
+        // that work may still write the scratch.
+        int32_t rc = wait_event(done, 600000.0);
+        if (rc == CENOTE_E_TIMEOUT)
+            return fail(CENOTE_E_TIMEOUT, "an earlier allocation-free environment build on this device is still running");
+        if (rc != CENOTE_OK) return rc;
+        static_env_set_pending(ctx->device, false);
+    }
     const size_t n = size_t(width) * height;
     CN_CHECK(n <= max_texels && height <= max_rows, CENOTE_E_INVALID_ARGUMENT,
              "environment " + std::to_string(width) + "x" + std::to_string(height) +
@@ -1434,7 +1472,8 @@ int32_t cenote_env_tables_static(cenote_context* ctx, const float* texels, uint3
     CN_CUDA(cudaGetLastError());
     double host_totals[2] = {0.0, 0.0};
     CN_CUDA(cudaMemcpyAsync(host_totals, totals, sizeof host_totals, cudaMemcpyDeviceToHost, ctx->stream));
-    int32_t rc = wait_stream(ctx->stream, ctx->sync_ev, 600000.0);
+    int32_t rc = wait_stream(ctx->stream, done, 600000.0);
+    if (rc == CENOTE_E_TIMEOUT) static_env_set_pending(ctx->device, true);
     if (rc != CENOTE_OK) return rc;
     if (power) *power = host_totals[1];
     return CENOTE_OK;

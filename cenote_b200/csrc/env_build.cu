@@ -160,6 +160,8 @@ namespace {
 constexpr int kMaxDevices = 64;
 std::mutex g_env_scratch_mu;
 double* g_env_scratch_ptr[kMaxDevices] = {};
+cudaEvent_t g_env_scratch_done[kMaxDevices] = {};  // recorded after each call's last write
+bool g_env_scratch_pending[kMaxDevices] = {};      // a call gave up waiting on that event
 }  // namespace
 
 // The device address of g_env_scratch on the current device. The host-side
@@ -168,7 +170,12 @@ double* g_env_scratch_ptr[kMaxDevices] = {};
 // and cached. The first lookup may load this library's kernels onto the
 // device, which is why a caller's first call should come before any stream
 // capture.
-cudaError_t static_env_scratch(int device, double** out, size_t* max_texels, uint32_t* max_rows) {
+// The same set-up creates the device's completion event (an event, not
+// memory): each call records it after its last write, and a call that gave
+// up waiting marks the scratch pending, so the next call on the device
+// first waits for that work instead of overwriting the scratch under it.
+cudaError_t static_env_scratch(int device, double** out, size_t* max_texels, uint32_t* max_rows,
+                               cudaEvent_t* done) {
     *max_texels = STATIC_ENV_MAX_TEXELS;
     *max_rows = STATIC_ENV_MAX_ROWS;
     if (device < 0 || device >= kMaxDevices) return cudaErrorInvalidDevice;
@@ -177,10 +184,23 @@ cudaError_t static_env_scratch(int device, double** out, size_t* max_texels, uin
         void* ptr = nullptr;
         cudaError_t e = cudaGetSymbolAddress(&ptr, g_env_scratch);
         if (e != cudaSuccess) return e;
+        e = cudaEventCreateWithFlags(&g_env_scratch_done[device], cudaEventDisableTiming);
+        if (e != cudaSuccess) return e;
         g_env_scratch_ptr[device] = static_cast<double*>(ptr);
     }
     *out = g_env_scratch_ptr[device];
+    *done = g_env_scratch_done[device];
     return cudaSuccess;
+}
+
+bool static_env_pending(int device) {
+    std::lock_guard<std::mutex> lock(g_env_scratch_mu);
+    return device >= 0 && device < kMaxDevices && g_env_scratch_pending[device];
+}
+
+void static_env_set_pending(int device, bool pending) {
+    std::lock_guard<std::mutex> lock(g_env_scratch_mu);
+    if (device >= 0 && device < kMaxDevices) g_env_scratch_pending[device] = pending;
 }
 
 }  // namespace cn

@@ -24,10 +24,17 @@ int32_t fail(int32_t code, const std::string& msg) {
     return code;
 }
 
-// Bounded wait: poll an event until it completes or `timeout_ms` passes.
+// Bounded wait: record an event on `s` and poll it until it completes or
+// `timeout_ms` passes.
 int32_t wait_stream(cudaStream_t s, cudaEvent_t ev, double timeout_ms) {
     cudaError_t e = cudaEventRecord(ev, s);
     if (e != cudaSuccess) return fail(CENOTE_E_DEVICE, std::string("cudaEventRecord: ") + cudaGetErrorString(e));
+    return wait_event(ev, timeout_ms);
+}
+
+// Bounded wait on an event already recorded.
+int32_t wait_event(cudaEvent_t ev, double timeout_ms) {
+    cudaError_t e;
     auto t0 = std::chrono::steady_clock::now();
     for (;;) {
         e = cudaEventQuery(ev);
@@ -116,6 +123,10 @@ cudaError_t enqueue_waves(cenote_renderer* r, const cenote_scene* sc, uint32_t w
                 const PathPool view = sort ? r->sorted_view() : r->pool;
                 if (sort) launch_sort_begin(view, stream);
                 launch_intersect(sc->ds, view, b, n0, ctx->shape, counting, stream);
+                if (counting) {
+                    launch_count_hits(view, b, n0, stream);
+                    wc->launches++;
+                }
                 mark();
                 if (guided) guide::launch_infer_paths(r->guide->view(), sc->ds, r->pool, b, n0, r->guide->sms, stream);
                 if (sort) {

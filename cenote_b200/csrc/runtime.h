@@ -40,6 +40,7 @@ const char* last_error();
 // Bounded wait: record `ev` on `s` and poll it until it completes or
 // `timeout_ms` passes (CENOTE_E_TIMEOUT).
 int32_t wait_stream(cudaStream_t s, cudaEvent_t ev, double timeout_ms);
+int32_t wait_event(cudaEvent_t ev, double timeout_ms);
 
 struct DeviceBuffer {
     void* ptr = nullptr;
@@ -167,7 +168,7 @@ struct cenote_renderer {
     static constexpr uint32_t GUIDE_RECORDS = 1u << 20;
     static constexpr uint32_t GUIDE_BATCH = 65536;
     cenote_stats stats{};
-    unsigned long long tally_prev[5] = {0, 0, 0, 0, 0};
+    unsigned long long tally_prev[6] = {0, 0, 0, 0, 0, 0};
 
     ~cenote_renderer() {
         for (cudaEvent_t e : events) cudaEventDestroy(e);

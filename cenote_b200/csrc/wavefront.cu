@@ -1004,6 +1004,22 @@ __global__ void k_tally(const uint32_t* counters, unsigned long long* tally, uin
     tally[2] |= counters[CTR_OVERFLOW];
     tally[3] += *reinterpret_cast<const unsigned long long*>(counters + CTR_VISITS);
     tally[4] += *reinterpret_cast<const unsigned long long*>(counters + CTR_TESTS);
+    tally[5] += *reinterpret_cast<const unsigned long long*>(counters + CTR_HITS);
+}
+
+// One warp-aggregated 64-bit add per warp of the rays of bounce `bounce`
+// whose closest hit is a surface.
+__global__ void k_count_hits(PathPool pool, uint32_t bounce, uint32_t n0) {
+    const uint32_t count = min(bounce == 0 ? n0 : pool.counters[CTR_RAYS + bounce], pool.capacity);
+    const uint32_t* queue = pool.queue[bounce & 1u];
+    unsigned long long hits = 0;
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < count; i += gridDim.x * blockDim.x) {
+        const uint32_t path = bounce == 0 ? i : queue[i];
+        hits += pool.hit[path].x != LIGHT_NONE ? 1u : 0u;
+    }
+    for (int o = 16; o > 0; o >>= 1) hits += __shfl_xor_sync(0xffffffffu, hits, o);
+    if (lane_id() == 0 && hits)
+        atomicAdd(reinterpret_cast<unsigned long long*>(pool.counters + CTR_HITS), hits);
 }
 
 }  // namespace
@@ -1019,6 +1035,10 @@ void launch_advance(uint32_t* counter, uint32_t n, cudaStream_t stream) { k_adva
 void launch_tally(const PathPool& pool, unsigned long long* tally, uint32_t n0, uint32_t max_bounces,
                   cudaStream_t stream) {
     k_tally<<<1, 32, 0, stream>>>(pool.counters, tally, n0, max_bounces);
+}
+
+void launch_count_hits(const PathPool& pool, uint32_t bounce, uint32_t n0, cudaStream_t stream) {
+    k_count_hits<<<1184, BLOCK, 0, stream>>>(pool, bounce, n0);
 }
 
 LaunchShape launch_shape(int device) {

@@ -17,6 +17,7 @@ constexpr uint32_t CTR_FETCH_SHADOW = 1024;
 constexpr uint32_t CTR_OVERFLOW = 1280;
 constexpr uint32_t CTR_VISITS = 1284;   // 64-bit: wide nodes visited (instrumented launches only)
 constexpr uint32_t CTR_TESTS = 1286;    // 64-bit: triangles tested (instrumented launches only)
+constexpr uint32_t CTR_HITS = 1288;     // 64-bit: closest hits on a surface (instrumented waves only)
 constexpr uint32_t CTR_FETCH_SHADE_LAYERS = 1296;  // [b]: the layered part of a split shading launch
 constexpr uint32_t CTR_COUNT = 1552;
 
@@ -149,9 +150,12 @@ void launch_material_sort(const PathPool& pool, uint32_t bounce, uint32_t n0, co
                           cudaStream_t stream);
 void launch_tonemap(const float4* avg, uint32_t* out, uint32_t pixels, float exposure_scale, cudaStream_t stream);
 // tally[0] += extension rays, [1] += shadow rays, [2] |= overflow,
-// [3] += node visits, [4] += triangle tests.
+// [3] += node visits, [4] += triangle tests, [5] += surface hits.
 void launch_tally(const PathPool& pool, unsigned long long* tally, uint32_t n0, uint32_t max_bounces,
                   cudaStream_t stream);
+// Instrumented waves: count bounce `bounce`'s rays that hit a surface into
+// CTR_HITS (misses are shaded by the same kernel but read no records).
+void launch_count_hits(const PathPool& pool, uint32_t bounce, uint32_t n0, cudaStream_t stream);
 void launch_copy_rad(const PathPool& pool, float4* out, uint32_t pixel_base, uint32_t pixel_count, cudaStream_t stream);
 // *counter += n on the device (a graph's progress counter).
 void launch_advance(uint32_t* counter, uint32_t n, cudaStream_t stream);

@@ -184,6 +184,7 @@ typedef struct cenote_stats {
     uint32_t waves;
     uint32_t samples_per_wave;
     uint32_t overflow;        /* nonzero: a device-side bound was hit */
+    uint64_t surface_hits;    /* extension rays whose closest hit is a surface (CENOTE_PROFILE_COUNTS only) */
 } cenote_stats;
 
 /* Profiling switches for subsequent calls (bit flags). TIMING records CUDA
@@ -486,7 +487,10 @@ int32_t cenote_renderer_set_guide(cenote_renderer* renderer, cenote_guide* guide
  * rejected with CENOTE_E_INVALID_ARGUMENT. The call allocates nothing on the
  * device and returns when the tables are written. Every call on a device
  * shares that scratch, so calls whose GPU work overlaps (from different
- * contexts, or threads bypassing one context) race. The first call on a
+ * contexts, or threads bypassing one context) race. A call that returns
+ * CENOTE_E_TIMEOUT leaves its work running; the next call on that device
+ * first waits for it (and returns CENOTE_E_TIMEOUT itself if it is still
+ * running after the same bound) before touching the scratch. The first call on a
  * device looks up the scratch's device address and may load the kernels, so
  * make it before any stream capture. */
 int32_t cenote_env_tables_static(cenote_context* ctx, const float* texels, uint32_t width, uint32_t height,
