@@ -1,18 +1,24 @@
 #!/usr/bin/env python
 """Benchmark: Msamples/s of the wavefront path tracer on one workload.
 
-    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference] [--workload chart]
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference] [--workload large]
 
 A step is one full frame: every pixel of the workload traced to its sample
-count (chart: 1280x720 at 64 spp, 12 bounces — the material chart under the
-2048x1024 HDRI sky). `value` is device-timed (CUDA events on the library's
-stream around each step) with the scene resident in HBM; `e2e` is the same
-frame through the public API with a host camera update in and the resolved
-image out to pinned host memory every step. Multi-GPU (torchrun): rank r
-renders samples r*spp .. (r+1)*spp-1 of every pixel and the films are summed
-with one NCCL all-reduce per step (weak scaling). The reference arm times the
-CPU oracle (the reference's Rust/Vulkan path cannot be built or run here) on
-the host cores.
+count. The default workload is the large scene (1920x1080 at 64 spp, 16
+bounces: a 2.09 M-triangle textured terrain, 500 glass/coat/fuzz instances,
+4,096 lognormal emitters), the largest single-GPU configuration; `chart`
+(1280x720, 64 spp, 12 bounces: the material chart under a 2048x1024 HDRI sky)
+and `cornell` (256x256, 16 spp) are the smaller ones, and
+`corpus:{cornell-box,veach-mis,teapot-full}` render the reference's pbrt
+corpus at its published resolutions (1024^2, 1280x720, 1280x720) for a
+ms/spp figure beside its own. `value` is device-timed (CUDA events on the
+library's stream around each step) with the scene resident in HBM; `e2e` is
+the same frame through the public API with a host camera update in and the
+resolved image out to pinned host memory every step. Multi-GPU (torchrun):
+rank r renders samples r*spp .. (r+1)*spp-1 of every pixel and the films are
+summed with one NCCL all-reduce per step (weak scaling). The reference arm
+times the CPU oracle (the reference's Rust/Vulkan path cannot be built or run
+here) on the host cores.
 """
 from __future__ import annotations
 
@@ -42,10 +48,32 @@ WORKLOADS = {
                         "each) + 4,096 lognormal(0,2) emitter triangles + 128 BC1/BC5 1024^2 textures, "
                         "1920x1080, 64 spp, 16 bounces"),
 }
+# The reference's pbrt corpus (imported scenes stored in tests/golden) at the
+# resolutions of its published steady-state ms/spp on an RTX 4070 Ti SUPER
+# (README.md:76-78): cross-hardware context, not a like-for-like baseline.
+CORPUS = {
+    "cornell-box": ("cornell_box", 1024, 1024, 5.5),
+    "veach-mis": ("veach_mis", 1280, 720, 2.6),
+    "teapot-full": ("teapot_full", 1280, 720, 8.0),
+}
+for _name, (_fx, _w, _h, _ms) in CORPUS.items():
+    WORKLOADS[f"corpus:{_name}"] = dict(scene=f"corpus:{_fx}", width=_w, height=_h, spp=64, max_bounces=0,
+                                        label=f"pbrt corpus {_name} (imported), {_w}x{_h}, 64 spp, the scene's "
+                                              "max depth", reference_ms_per_spp=_ms)
 
 
 def make_spec(w):
+    """The workload's scene. Corpus scenes come from the committed fixtures;
+    their max depth (pbrt's maxdepth) replaces the workload's 0."""
     from cenote_b200 import scenes
+    if w["scene"].startswith("corpus:"):
+        spec, extra = scenes.load_spec(ROOT / "tests" / "golden" / f"corpus_{w['scene'][7:]}.npz")
+        if "sky_octahedral" in extra:
+            from cenote_b200.pbrt import sky_environment
+            spec.environment = sky_environment(extra["sky_octahedral"].astype(np.float32),
+                                               extra["sky_world_from_light"], float(extra["sky_scale"]))
+        w["max_bounces"] = spec.max_bounces
+        return spec
     return {"chart": scenes.chart, "cornell": scenes.cornell, "large": scenes.large}[w["scene"]]()
 
 
@@ -55,6 +83,26 @@ def measured_peaks():
         d = json.loads(p.read_text())
         return d.get("hbm_gbs", 6650.0), "measured"
     return 6650.0, "fallback"
+
+
+def l2_read_peak(torch, mb=32, repeat=64, trials=5):
+    """Measured L2 bandwidth: one reduction kernel reads a `mb`-MB buffer
+    `repeat` times over (a stride-0 view of it), so after the first pass
+    every read hits the 126 MB L2; bytes read over CUDA-event time, best of
+    `trials`. One launch reads 2 GB, so launch overhead does not count."""
+    n = (mb << 20) // 4
+    a = torch.rand(n, device="cuda")
+    view = a.unsqueeze(0).expand(repeat, n)
+    torch.sum(view)
+    best = 0.0
+    for _ in range(trials):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        torch.sum(view)
+        e1.record()
+        e1.synchronize()
+        best = max(best, 4.0 * n * repeat / (e0.elapsed_time(e1) / 1e3) / 1e9)
+    return best
 
 
 def committed_traffic(workload):
@@ -386,7 +434,7 @@ def main():
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="chart", choices=list(WORKLOADS) + ["serving", "guiding"])
+    ap.add_argument("--workload", default="large", choices=list(WORKLOADS) + ["serving", "guiding"])
     ap.add_argument("--jobs", type=int, default=256, help="serving: jobs in the Poisson stream")
     ap.add_argument("--slots", type=int, default=8, help="serving: the server's slots (streams with path pools)")
     ap.add_argument("--concurrency", type=int, default=0,
@@ -553,13 +601,25 @@ def main():
     trav_launches = 2 * maxb * counts["waves"]
     achieved = alg_bytes_frame / (trav_ms_frame / 1e3) / 1e9 if trav_ms_frame > 0 else None
     peak, peak_kind = measured_peaks()
+    l2_peak = l2_read_peak(torch)
     traffic = committed_traffic(args.workload)
     # DRAM bytes per traversal launch from the committed capture of a smaller
-    # wave, scaled by paths per wave: the BVH is L2-resident, so DRAM traffic
-    # is the per-ray path-state traffic and grows with the rays per launch.
+    # wave, scaled by paths per wave (a first-order model: the per-ray
+    # path-state traffic grows with the rays per launch).
     wave_paths = W * H * min(counts["samples_per_wave"], spp)
     traffic_per_launch = (traffic["bytes_per_launch_captured"] * wave_paths / traffic["captured_paths_per_wave"]
                           if traffic and "captured_paths_per_wave" in traffic else None)
+    # Shading: bytes per path vertex = 72 path in + 52 path out + 128
+    # geometry record + 144 material + 12 indices + 96 vertex attributes +
+    # 64 shadow record + 16 radiance read-modify-write = 584 for a surface
+    # hit; a miss reads its path (72) and adds its radiance (16) = 88.
+    hits = counts["surface_hits"]
+    shade_bytes_frame = 584 * hits + 88 * (ext - hits)
+    shade_ms_frame = stage["shade_ms"] / args.steps
+    shade_achieved = shade_bytes_frame / (shade_ms_frame / 1e3) / 1e9 if shade_ms_frame > 0 else None
+    # The BVH and triangles of the chart and the closed box fit in L2 (the
+    # L2 roofline bounds their walk); the large scene's do not (HBM).
+    l2_resident = args.workload != "large"
 
     line = {
         "metric": "Msamples/s", "value": value, "unit": "Msamples/s", "n_gpus": world, "steps": args.steps,
@@ -596,8 +656,26 @@ def main():
             "launch_ms": trav_ms_frame / max(1, trav_launches),
             "nodes_per_ray": counts["node_visits"] / max(1, ext + shd),
             "tris_per_ray": counts["triangle_tests"] / max(1, ext + shd),
+            "applies": "HBM roofline: the BVH exceeds L2" if not l2_resident else
+                       "the BVH is L2-resident: roofline_l2 is the bound that applies",
+        },
+        "roofline_l2": {
+            "kernel": "traversal (k_intersect + k_shadow)", "bound": "l2", "achieved": achieved, "peak": l2_peak,
+            "unit": "GB/s", "frac": (achieved / l2_peak) if achieved else None,
+            "peak_source": "measured in this run: one reduction over a 32 MB buffer read 64 times (L2-resident)",
+        },
+        "roofline_shade": {
+            "kernel": "k_shade", "bound": "hbm", "achieved": shade_achieved, "peak": peak, "unit": "GB/s",
+            "frac": (shade_achieved / peak) if shade_achieved else None, "peak_source": peak_kind,
+            "algorithmic_bytes_per_frame": shade_bytes_frame, "surface_hits_per_frame": hits,
+            "misses_per_frame": ext - hits, "ms_per_frame": shade_ms_frame,
+            "bytes_per_vertex": "584 per surface hit, 88 per miss",
         },
     }
+    if "reference_ms_per_spp" in w:
+        line["corpus"] = {"ms_per_spp": ms / args.steps / spp, "reference_ms_per_spp": w["reference_ms_per_spp"],
+                          "reference_hardware": "RTX 4070 Ti SUPER, Vulkan ray query (README.md:76-78)",
+                          "note": "cross-hardware context, not a baseline: the reference publishes only these"}
     if rank == 0:
         line["clocks"] = clocks.summary()
         if world == 1 and not args.no_cpu_baseline:

@@ -11,7 +11,11 @@ octahedral source texels (half floats, as the sky file holds them), its
 orientation and scale instead of the resampled equirect, and the tests
 rebuild the environment with cenote_b200.pbrt.sky_environment.
 
-    python tests/golden/make_corpus.py [REFERENCE_ROOT]
+    python tests/golden/make_corpus.py REFERENCE_ROOT
+
+REFERENCE_ROOT is the reference project's checkout (its tests/scenes and
+crates/cenote-pbrt/tests/golden are read); CENOTE_REFERENCE_ROOT may give it
+instead.
 """
 from __future__ import annotations
 
@@ -30,7 +34,11 @@ from cenote_b200.scenes import Environment, save_spec  # noqa: E402
 CORPUS = [("cornell-box", 256, 256), ("veach-mis", 320, 180), ("teapot-full", 320, 180)]
 
 
-def main(root: str = "/root/reference") -> None:
+def main(root: str | None = None) -> None:
+    import os
+    root = root or os.environ.get("CENOTE_REFERENCE_ROOT")
+    if not root:
+        raise SystemExit("usage: make_corpus.py REFERENCE_ROOT (or set CENOTE_REFERENCE_ROOT)")
     ref = pathlib.Path(root)
     for name, w, h in CORPUS:
         spec = import_pbrt(str(ref / "tests/scenes" / name / "scene-v4.pbrt"), w, h)
