@@ -227,26 +227,47 @@ def rel_err(a, ref, floor):
     return np.abs(a - ref) / np.maximum(np.abs(ref), floor)
 
 
-@pytest.mark.parametrize("name", list(materials()))
-@pytest.mark.parametrize("exiting", [False, True])
-def test_bsdf_eval_pdf_fp32_vs_fp64(ctx, name, exiting):
-    """FP32 device eval/pdf against the FP64 oracle, error relative to
-    max(|oracle|, 1e-2) (values under 1e-2 per sr are compared absolutely at
-    1e-7). Outside a medium: at most 0.1% of pairs above 1e-5, none above
-    1e-4. Inside glass (exiting), grazing transmission near the critical
-    angle makes h·wi cancel in FP32: at most 1% of pairs above 1e-5, none
-    above 2e-3."""
+def bsdf_errors(ctx, name, exiting):
+    """Per pair: the larger of the value's and the pdf's error, relative to
+    max(|oracle|, 1e-2). Values under 1e-2 per steradian are compared
+    absolutely (an error of 1e-7 there counts as 1e-5), since a relative
+    error of a value that rounds toward zero says nothing."""
     mat = materials()[name]
     wo, wi = directions(20000, seed=sum(map(ord, name)))
     f, pdf = ctx.probe_bsdf(mat, wo, wi, exiting)
     rf, rpdf = oracle.bsdf_eval(mat, wo, wi, exiting)
+    assert np.all(np.isfinite(f)) and np.all(np.isfinite(pdf))
     ef = rel_err(f.astype(np.float64), rf, 1e-2).max(axis=1)
     ep = rel_err(pdf.astype(np.float64), rpdf, 1e-2)
-    e = np.maximum(ef, ep)
-    frac_budget, worst = (1e-2, 2e-3) if exiting else (1e-3, 1e-4)
-    assert (e > 1e-5).mean() <= frac_budget, (name, exiting, (e > 1e-5).mean(), np.sort(e)[-5:])
-    assert e.max() <= worst, (name, exiting, e.max())
-    assert np.all(np.isfinite(f)) and np.all(np.isfinite(pdf))
+    return np.maximum(ef, ep), wo, wi
+
+
+def worst_pairs(e, wo, wi, k=4):
+    return [(float(e[i]), round(float(wo[i, 2]), 4), round(float(wi[i, 2]), 4)) for i in np.argsort(-e)[:k]]
+
+
+@pytest.mark.parametrize("name", list(materials()))
+def test_bsdf_eval_pdf_fp32_vs_fp64(ctx, name):
+    """Outside a medium, every one of 20,000 (wo, wi) pairs of every
+    material: FP32 device eval and pdf within 1e-5 of the FP64 oracle
+    (measured worst 4.6e-6, tinted glass; below 2e-6 elsewhere)."""
+    e, wo, wi = bsdf_errors(ctx, name, False)
+    assert e.max() <= 1e-5, (name, worst_pairs(e, wo, wi))
+
+
+@pytest.mark.parametrize("name", list(materials()))
+def test_bsdf_eval_pdf_inside_a_medium(ctx, name):
+    """Leaving a medium (the closure is a bare interface with the inverse
+    IOR) the transmitted value near the critical angle is 1 − F with F → 1
+    and h·wi → 0, and FP32 cancels there. The pairs above 1e-5 must be
+    transmissions only, at most 1 % of them and none above 2e-3 (measured
+    on a B200: at most 155 of 20,000 pairs, metal r = 1; worst 1.2e-3, the
+    full stack)."""
+    e, wo, wi = bsdf_errors(ctx, name, True)
+    over = e > 1e-5
+    assert np.all(wi[over, 2] < 0.0), (name, "a reflection pair lost precision", worst_pairs(e, wo, wi))
+    assert over.mean() <= 1e-2, (name, over.mean(), worst_pairs(e, wo, wi))
+    assert e.max() <= 2e-3, (name, worst_pairs(e, wo, wi))
 
 
 @pytest.mark.parametrize("name", list(materials()))

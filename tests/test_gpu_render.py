@@ -79,12 +79,45 @@ FURNACE_MATRIX = {  # render/tests.rs:422-488
 }
 
 
+# The OpenPBR model's own energy balance where it misses 1e-3: its
+# Kulla-Conty compensation tables (tables.rs) are interpolated from 32² and
+# 16³ grids, which leaves a bias at low roughness and high IOR, and the
+# thin-walled lobe's split gains energy. Measured on a B200 at 256², 1,024 spp
+# (67 M samples; the standard error is below 1e-4): relative deviation of the
+# furnace mean from the sky's 0.5. test_furnace_is_the_oracles_model shows
+# these are the model's, not FP32's: the device and the FP64-closure oracle
+# give the same mean on the same samples.
+OPENPBR_MODEL_BIAS = {
+    "glossy-diffuse r=0.05": -1.2e-3,
+    "glossy ior=2.5": -1.2e-3,
+    "coat over diffuse": -1.2e-3,
+    "the full stack": -1.0e-3,
+    "thin glass r=0.4": +2.8e-3,
+}
+
+
 @pytest.mark.parametrize("label", list(FURNACE_MATRIX))
 def test_openpbr_furnace_matrix(ctx, label):
-    """White furnace through every lobe: the reference's 1.5% bound at 32², 64 spp."""
-    s = accumulate_mean(ctx, scenes.furnace(FURNACE_MATRIX[label]()), 32, 64)
-    mean = s[..., 0].sum() / (32 * 32 * 64)
-    assert abs(mean - 0.5) / 0.5 < 0.015, (label, mean)
+    """White furnace through every lobe (render/tests.rs:422-488) at 256²,
+    1,024 spp: the mean closes to 1e-3 of the sky, or, for the lobes whose
+    model does not, to 5e-4 of the model's measured balance."""
+    s = accumulate_mean(ctx, scenes.furnace(FURNACE_MATRIX[label](), size=256), 256, 1024)
+    dev = s[..., :3].astype(np.float64).sum(axis=(0, 1)) / (256 * 256 * 1024) / 0.5 - 1.0
+    bias = OPENPBR_MODEL_BIAS.get(label, 0.0)
+    assert np.all(np.abs(dev - bias) < (5e-4 if bias else 1e-3)), (label, dev)
+
+
+@pytest.mark.parametrize("label", list(OPENPBR_MODEL_BIAS) + ["metal r=0.5", "glass plane r=0.4"])
+def test_furnace_is_the_oracles_model(ctx, label):
+    """The furnace on the device and in the oracle over the same samples
+    (64², 256 spp): the means agree to 1e-5, so the device's furnace balance
+    is the restated model's, to FP32 rounding."""
+    spec = scenes.furnace(FURNACE_MATRIX[label](), size=64)
+    s = accumulate_mean(ctx, spec, 64, 256)
+    ref = oracle.OracleScene(spec).render_sum(64, 64, 0, 256, 8)
+    gpu = s[..., :3].astype(np.float64).sum()
+    cpu = ref[..., :3].astype(np.float64).sum()
+    assert abs(gpu / cpu - 1.0) < 1e-5, (label, gpu / cpu - 1.0)
 
 
 def glass_sphere_spec():
@@ -94,9 +127,17 @@ def glass_sphere_spec():
 
 
 def test_the_glass_furnace_closes(ctx):  # render/tests.rs:498-532
-    s = accumulate_mean(ctx, glass_sphere_spec(), 32, 128, max_bounces=16)
-    mean = s[..., 0].sum() / (32 * 32 * 128)
-    assert abs(mean - 0.5) / 0.5 < 0.015, mean
+    """A glass sphere under a grey sky (16 bounces) at 256², 1,024 spp. Paths
+    that still bounce inside after 16 vertices are cut, so the reference's
+    bound is 1.5 %; measured: −1.1 %, the same as the oracle on the same
+    samples."""
+    spec = glass_sphere_spec()
+    s = accumulate_mean(ctx, spec, 256, 1024, max_bounces=16)
+    mean = s[..., :3].astype(np.float64).sum(axis=(0, 1)) / (256 * 256 * 1024)
+    assert np.all(np.abs(mean / 0.5 - 1.0 + 0.011) < 1e-3), mean
+    small = accumulate_mean(ctx, spec, 32, 128, max_bounces=16)[..., :3].astype(np.float64).sum()
+    ref = oracle.OracleScene(spec).render_sum(32, 32, 0, 128, 16)[..., :3].astype(np.float64).sum()
+    assert abs(small / ref - 1.0) < 1e-3
 
 
 def delta_scene(light):
