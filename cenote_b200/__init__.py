@@ -672,13 +672,16 @@ class JobStatus(C.Structure):
 class ServerCounters(C.Structure):
     _fields_ = [("submitted", C.c_uint64), ("completed", C.c_uint64), ("failed", C.c_uint64),
                 ("queued", C.c_uint64), ("active", C.c_uint64), ("samples", C.c_uint64),
-                ("bytes_in_use", C.c_uint64), ("budget", C.c_uint64), ("wall_ms", C.c_double)]
+                ("bytes_in_use", C.c_uint64), ("budget", C.c_uint64), ("wall_ms", C.c_double),
+                ("waves", C.c_uint64), ("first_waves", C.c_uint64), ("wave_paths", C.c_uint64),
+                ("busy_ms", C.c_double)]
 
 
 class Server:
     """The serving loop (cenote_server_*): progressive jobs admitted by an HBM
-    budget, advanced in frame_spp chunks over `slots` streams. `on_frame(job,
-    samples, target, rgba)` runs on the server thread after every chunk."""
+    budget and traced together, job-tagged, in waves over `slots` lanes (1 or
+    2; a path pool and a stream pair each). `on_frame(job, samples, target,
+    rgba)` runs on the server thread after every frame_spp samples."""
 
     def __init__(self, ctx: Context, hbm_budget: int, slots: int = 0, frame_spp: int = 0, max_active: int = 0,
                  pool_paths: int = 0, light_sampling: int = LIGHT_SAMPLING_MIS, graphs: bool = True, on_frame=None):

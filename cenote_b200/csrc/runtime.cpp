@@ -68,6 +68,62 @@ WavePlan plan_waves(const cenote_renderer* r, uint64_t pixels, uint32_t count, b
     return p;
 }
 
+// The bounces of one wave of n0 camera paths already in the pool: per
+// bounce intersect, (the guide's inference,) the material sort, shade and
+// shadow. Timing marks bracket intersect, shade and shadow when `timing`.
+void enqueue_bounces(cenote_renderer* r, const cenote_scene* sc, const WaveParams& wp, uint32_t n0, bool guided,
+                     cudaStream_t stream, bool timing, bool counting, WaveCounts* wc) {
+    cenote_context* ctx = r->ctx;
+    auto mark = [&]() {
+        if (timing) cudaEventRecord(r->event(wc->events++), stream);
+    };
+    for (uint32_t b = 0; b < wp.max_bounces; ++b) {
+        const bool sort = r->material_sort == CENOTE_SORT_ALL || (r->material_sort == CENOTE_SORT_SECONDARY && b > 0);
+        const PathPool view = sort ? r->sorted_view() : r->pool;
+        if (sort) launch_sort_begin(view, stream);
+        launch_intersect(sc->ds, view, b, n0, ctx->shape, counting, stream);
+        if (counting) {
+            launch_count_hits(view, b, n0, stream);
+            wc->launches++;
+        }
+        mark();
+        if (guided) guide::launch_infer_paths(r->guide->view(), sc->ds, r->pool, b, n0, r->guide->sms, stream);
+        if (sort) {
+            launch_material_sort(view, b, n0, ctx->shape, stream);
+            wc->launches += sc->ds.has_layers ? 3 : 2;  // a split shading launch adds one
+        }
+        launch_shade(sc->ds, view, b, wp, n0, ctx->shape, stream);
+        mark();
+        launch_shadow(sc->ds, r->pool, b, ctx->shape, counting, stream);
+        mark();
+    }
+}
+
+// One multi-job wave on `stream` (the serving loop): the segments' camera
+// paths (`segs`, device memory, `nseg` of them, `paths` paths and `items`
+// accumulate items in all; with `hdr` those three counts are read from it on
+// the device instead, so a captured graph replays any wave), the bounces,
+// and each segment's samples added into its job's film. No guides, no
+// learned guide, no host waits. The pool must hold the wave's paths.
+cudaError_t enqueue_segments(cenote_renderer* r, const cenote_scene* sc, const WaveSegment* segs, uint32_t nseg,
+                             uint32_t paths, uint32_t items, const uint32_t* hdr, uint32_t max_bounces,
+                             cudaStream_t stream, WaveCounts* wc) {
+    r->pool.refill_idle = r->refill_idle;
+    r->pool.top_nodes = r->top_nodes;
+    r->pool.per_lane_triangles = r->per_lane_triangles;
+    WaveParams wp{};
+    wp.max_bounces = max_bounces;
+    wp.light_sampling = r->light_sampling;
+    const uint32_t n0 = hdr ? 0u : paths;  // 0: the kernels read the count raygen leaves
+    launch_wave_begin_segments(r->pool, segs, nseg, paths, hdr, r->ctx->shape, stream);
+    enqueue_bounces(r, sc, wp, n0, false, stream, false, false, wc);
+    launch_tally(r->pool, r->tally.as<unsigned long long>(), n0, max_bounces, stream);
+    launch_accumulate_segments(r->pool, segs, nseg, items, hdr, stream);
+    wc->launches += 3 + 3 * max_bounces;
+    wc->waves++;
+    return cudaGetLastError();
+}
+
 // Enqueue `count` samples from `sample0` for every pixel on `stream`, with no
 // host synchronisation (so a stream capture can record it): each wave's
 // samples go into the film in ascending order or, for a one-shot render,
@@ -117,27 +173,7 @@ cudaError_t enqueue_waves(cenote_renderer* r, const cenote_scene* sc, uint32_t w
             if (guided) cudaMemsetAsync(r->g_count.ptr, 0, 4, stream);
             launch_wave_begin(r->pool, wp, ctx->shape, stream);
             mark();
-            for (uint32_t b = 0; b < max_bounces; ++b) {
-                const bool sort = r->material_sort == CENOTE_SORT_ALL ||
-                                  (r->material_sort == CENOTE_SORT_SECONDARY && b > 0);
-                const PathPool view = sort ? r->sorted_view() : r->pool;
-                if (sort) launch_sort_begin(view, stream);
-                launch_intersect(sc->ds, view, b, n0, ctx->shape, counting, stream);
-                if (counting) {
-                    launch_count_hits(view, b, n0, stream);
-                    wc->launches++;
-                }
-                mark();
-                if (guided) guide::launch_infer_paths(r->guide->view(), sc->ds, r->pool, b, n0, r->guide->sms, stream);
-                if (sort) {
-                    launch_material_sort(view, b, n0, ctx->shape, stream);
-                    wc->launches += sc->ds.has_layers ? 3 : 2;  // a split shading launch adds one
-                }
-                launch_shade(sc->ds, view, b, wp, n0, ctx->shape, stream);
-                mark();
-                launch_shadow(sc->ds, r->pool, b, ctx->shape, counting, stream);
-                mark();
-            }
+            enqueue_bounces(r, sc, wp, n0, guided, stream, timing, counting, wc);
             launch_tally(r->pool, r->tally.as<unsigned long long>(), n0, max_bounces, stream);
             if (film)
                 launch_accumulate(r->pool, *film, wp.pixel_base, wp.pixel_count, s, film_reset && done == 0,

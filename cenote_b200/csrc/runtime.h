@@ -341,4 +341,14 @@ cudaError_t enqueue_waves(cenote_renderer* r, const cenote_scene* sc, uint32_t w
                           const FilmTargets* film, bool film_reset, float4* oneshot, const uint32_t* sample_offset,
                           cudaStream_t stream, bool timing, bool counting, WaveCounts* wc);
 
+// The bounces of one wave whose n0 camera paths are in the pool.
+void enqueue_bounces(cenote_renderer* r, const cenote_scene* sc, const WaveParams& wp, uint32_t n0, bool guided,
+                     cudaStream_t stream, bool timing, bool counting, WaveCounts* wc);
+
+// One multi-job wave (the serving loop): segments in device memory, their
+// camera paths, the bounces, and each segment's samples into its job's film.
+cudaError_t enqueue_segments(cenote_renderer* r, const cenote_scene* sc, const WaveSegment* segs, uint32_t nseg,
+                             uint32_t paths, uint32_t items, const uint32_t* hdr, uint32_t max_bounces,
+                             cudaStream_t stream, WaveCounts* wc);
+
 }  // namespace cn

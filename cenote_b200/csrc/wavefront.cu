@@ -87,6 +87,13 @@ __device__ __forceinline__ void flush_counts(uint32_t* counters, uint32_t visits
     }
 }
 
+// Paths entering bounce `bounce`: the wave's camera paths (n0, or when n0
+// is 0 the count raygen left in CTR_RAYS, as a replayed graph's waves do),
+// then the previous bounce's pushes.
+__device__ __forceinline__ uint32_t bounce_paths(const PathPool& pool, uint32_t bounce, uint32_t n0) {
+    return min(bounce == 0 && n0 != 0 ? n0 : pool.counters[CTR_RAYS + bounce], pool.capacity);
+}
+
 // ---- raygen (raygen.slang:47-112) ----------------------------------------------
 
 __device__ __forceinline__ float2 concentric_disk(float2 u) {
@@ -105,39 +112,82 @@ __device__ __forceinline__ float2 concentric_disk(float2 u) {
     return make_float2(r * c, r * s);
 }
 
+// One camera path: path slot p traces `sample` of `pixel` of a width x height
+// image with the camera's basis.
+__device__ __forceinline__ void raygen_path(const PathPool& pool, uint32_t p, uint32_t pixel, uint32_t sample,
+                                            uint32_t width, uint32_t height, float3 cam_pos, float3 cam_right,
+                                            float3 cam_up, float3 cam_fwd, float aperture) {
+    float2 j = sample_2d(pixel, sample, CAMERA_JITTER);
+    float xx = float(pixel % width) + j.x, yy = float(pixel / width) + j.y;
+    float ux = xx / float(width), uy = yy / float(height);
+    float nx = 2.0f * ux - 1.0f, ny = 1.0f - 2.0f * uy;
+    float3 target = cam_fwd + nx * cam_right + ny * cam_up;
+    float3 org = cam_pos;
+    float3 dir = normalize(target);
+    if (aperture > 0.0f) {
+        float2 d = concentric_disk(sample_2d(pixel, sample, CAMERA_LENS));
+        d.x *= aperture;
+        d.y *= aperture;
+        float3 off = d.x * normalize(cam_right) + d.y * normalize(cam_up);
+        org = org + off;
+        dir = normalize(target - off);
+    }
+    pool.org[p] = f4(org, 0.0f);
+    pool.dir[p] = f4(dir, dot(dir, normalize(cam_fwd)));
+    pool.thr[p] = make_float4(1.0f, 1.0f, 1.0f, 0.0f);
+    pool.ps[p] = make_uint2(pixel, sample);
+    pool.state[p] = MEDIUM_NONE;
+    pool.rad[p] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+    if (pool.guide_rec) pool.guide_rec[p] = ~0u;
+    if (pool.aov_albedo) {
+        pool.aov_albedo[p] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+        pool.aov_normal[p] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+        pool.aov_depth[p] = 0.0f;
+    }
+}
+
 __global__ void __launch_bounds__(BLOCK) k_raygen(PathPool pool, WaveParams wp) {
     uint32_t n = wp.pixel_count * wp.samples;
     for (uint32_t p = blockIdx.x * blockDim.x + threadIdx.x; p < n; p += gridDim.x * blockDim.x) {
         uint32_t s = p / wp.pixel_count;
         uint32_t pixel = wp.pixel_base + (p - s * wp.pixel_count);
         uint32_t sample = wp.sample_base + s + (wp.sample_offset ? __ldg(wp.sample_offset) : 0u);
-        float2 j = sample_2d(pixel, sample, CAMERA_JITTER);
-        float xx = float(pixel % wp.width) + j.x, yy = float(pixel / wp.width) + j.y;
-        float ux = xx / float(wp.width), uy = yy / float(wp.height);
-        float nx = 2.0f * ux - 1.0f, ny = 1.0f - 2.0f * uy;
-        float3 target = wp.cam_fwd + nx * wp.cam_right + ny * wp.cam_up;
-        float3 org = wp.cam_pos;
-        float3 dir = normalize(target);
-        if (wp.aperture > 0.0f) {
-            float2 d = concentric_disk(sample_2d(pixel, sample, CAMERA_LENS));
-            d.x *= wp.aperture;
-            d.y *= wp.aperture;
-            float3 off = d.x * normalize(wp.cam_right) + d.y * normalize(wp.cam_up);
-            org = org + off;
-            dir = normalize(target - off);
-        }
-        pool.org[p] = f4(org, 0.0f);
-        pool.dir[p] = f4(dir, dot(dir, normalize(wp.cam_fwd)));
-        pool.thr[p] = make_float4(1.0f, 1.0f, 1.0f, 0.0f);
-        pool.ps[p] = make_uint2(pixel, sample);
-        pool.state[p] = MEDIUM_NONE;
-        pool.rad[p] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
-        if (pool.guide_rec) pool.guide_rec[p] = ~0u;
-        if (pool.aov_albedo) {
-            pool.aov_albedo[p] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
-            pool.aov_normal[p] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
-            pool.aov_depth[p] = 0.0f;
-        }
+        raygen_path(pool, p, pixel, sample, wp.width, wp.height, wp.cam_pos, wp.cam_right, wp.cam_up, wp.cam_fwd,
+                    wp.aperture);
+    }
+}
+
+// The segment of a multi-job wave that holds item `x` (a path, or with
+// `by_pixel` an accumulate item): the last whose first item is at most x.
+__device__ __forceinline__ uint32_t find_segment(const WaveSegment* segs, uint32_t nseg, uint32_t x, bool by_pixel) {
+    uint32_t lo = 0, hi = nseg;  // answer in [lo, hi)
+    while (hi - lo > 1) {
+        const uint32_t mid = (lo + hi) >> 1;
+        const uint32_t first = by_pixel ? __ldg(&segs[mid].pixel_start) : __ldg(&segs[mid].start);
+        if (first <= x) lo = mid;
+        else hi = mid;
+    }
+    return lo;
+}
+
+// Camera paths of a multi-job wave: each path takes its job's image size,
+// camera and sample index from its segment, so it is the path a standalone
+// render of that job traces for the same (pixel, sample). With `hdr` (a
+// replayed graph) the segment and path counts come from it, and the path
+// count goes to CTR_RAYS for the kernels that follow.
+__global__ void __launch_bounds__(BLOCK) k_raygen_segments(PathPool pool, const WaveSegment* __restrict__ segs,
+                                                           uint32_t nseg, uint32_t n, const uint32_t* hdr) {
+    if (hdr) {
+        nseg = __ldg(hdr);
+        n = __ldg(hdr + 1);
+    }
+    if (blockIdx.x == 0 && threadIdx.x == 0) pool.counters[CTR_RAYS] = n;
+    for (uint32_t p = blockIdx.x * blockDim.x + threadIdx.x; p < n; p += gridDim.x * blockDim.x) {
+        const WaveSegment& g = segs[find_segment(segs, nseg, p, false)];
+        const uint32_t q = p - g.start;
+        const uint32_t s = q / g.pixel_count;
+        raygen_path(pool, p, g.pixel_base + (q - s * g.pixel_count), g.sample_base + s, g.width, g.height,
+                    g.cam_pos, g.cam_right, g.cam_up, g.cam_fwd, g.aperture);
     }
 }
 
@@ -172,7 +222,7 @@ __global__ void __launch_bounds__(BLOCK, CN_TRAV_MIN_BLOCKS) k_intersect(DeviceS
     extern __shared__ uint4 top_levels[];
     stage_top_levels(scene, top_levels, min(pool.top_nodes, TOP_NODES_MAX));  // as the launch sized it
     uint32_t visits = 0, tests = 0;
-    const uint32_t count = min(bounce == 0 ? n0 : pool.counters[CTR_RAYS + bounce], pool.capacity);
+    const uint32_t count = bounce_paths(pool, bounce, n0);
     const uint32_t* queue = pool.queue[bounce & 1u];
     const uint32_t mask = bounce == 0 ? RAY_MASK_CAMERA : RAY_MASK_ALL;
     uint32_t* fetch = pool.counters + CTR_FETCH_ISECT + bounce;
@@ -312,7 +362,7 @@ __global__ void __launch_bounds__(BLOCK, CN_TRAV_MIN_BLOCKS)
     stage_top_levels(scene, top_levels, min(pool.top_nodes, TOP_NODES_MAX));
     uint32_t visits = 0, tests = 0;
     IsectSource src{pool, &scene, pool.queue[bounce & 1u], pool.counters + CTR_FETCH_ISECT + bounce,
-                    min(bounce == 0 ? n0 : pool.counters[CTR_RAYS + bounce], pool.capacity), bounce};
+                    bounce_paths(pool, bounce, n0), bounce};
     bool overflow = false;
     queued_closest<COUNT>(scene, tqs[threadIdx.x >> 5], src, bounce == 0 ? RAY_MASK_CAMERA : RAY_MASK_ALL, overflow,
                           &visits, &tests);
@@ -423,7 +473,7 @@ __global__ void __launch_bounds__(BLOCK, CN_SHADE_MIN_BLOCKS) k_shade(DeviceScen
                                                  uint32_t part) {
     // part 0: the whole bounce; on a sorted bounce, 1: the misses and
     // layer-free hits (keys below SORT_LAYERS), 2: the layered hits.
-    uint32_t count = min(bounce == 0 ? n0 : pool.counters[CTR_RAYS + bounce], pool.capacity);
+    uint32_t count = bounce_paths(pool, bounce, n0);
     uint32_t first = 0;
     if (part != 0) {
         const uint32_t split = min(pool.sort_bins[SORT_LAYERS - 1u], count);  // the end of the layer-free keys
@@ -878,6 +928,29 @@ __global__ void k_accumulate(PathPool pool, FilmTargets film, uint32_t pixel_bas
     }
 }
 
+// A multi-job wave's radiance into each job's beauty sums: one thread per
+// (segment, pixel), adding the segment's samples in ascending order, as a
+// standalone render of the job adds them.
+__global__ void k_accumulate_segments(PathPool pool, const WaveSegment* __restrict__ segs, uint32_t nseg,
+                                      uint32_t items, const uint32_t* hdr) {
+    const float4 zero = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+    if (hdr) {
+        nseg = __ldg(hdr);
+        items = __ldg(hdr + 2);
+    }
+    for (uint32_t x = blockIdx.x * blockDim.x + threadIdx.x; x < items; x += gridDim.x * blockDim.x) {
+        const WaveSegment& g = segs[find_segment(segs, nseg, x, true)];
+        const uint32_t p = x - g.pixel_start, px = g.pixel_base + p;
+        float4 acc = g.reset ? zero : g.film[px];
+        for (uint32_t s = 0; s < g.samples; ++s) {
+            float4 v = pool.rad[g.start + s * g.pixel_count + p];
+            if (!finite4(v)) v = zero;
+            acc = (g.reset && s == 0) ? v : add4(acc, v);
+        }
+        g.film[px] = acc;
+    }
+}
+
 __global__ void k_resolve(const float4* __restrict__ sum, float4* __restrict__ avg, uint32_t n, float samples) {
     for (uint32_t p = blockIdx.x * blockDim.x + threadIdx.x; p < n; p += gridDim.x * blockDim.x) {
         float4 v = sum[p];
@@ -938,7 +1011,7 @@ __global__ void k_copy_rad(const float4* __restrict__ rad, float4* __restrict__ 
 // hands each key's paths consecutive slots.
 
 __device__ __forceinline__ uint32_t sort_count(const PathPool& pool, uint32_t bounce, uint32_t n0) {
-    return min(bounce == 0 ? n0 : pool.counters[CTR_RAYS + bounce], pool.capacity);
+    return bounce_paths(pool, bounce, n0);
 }
 
 // One block of 1024 threads: exclusive prefix sums of the SORT_BINS counts.
@@ -996,7 +1069,7 @@ __global__ void __launch_bounds__(BLOCK) k_sort_scatter(PathPool pool, uint32_t 
 // tally[0] += extension rays, tally[1] += shadow rays, tally[2] |= overflow.
 __global__ void k_tally(const uint32_t* counters, unsigned long long* tally, uint32_t n0, uint32_t max_bounces) {
     if (threadIdx.x != 0 || blockIdx.x != 0) return;
-    unsigned long long rays = n0, shadows = 0;
+    unsigned long long rays = n0 ? n0 : counters[CTR_RAYS], shadows = 0;
     for (uint32_t b = 1; b < max_bounces; ++b) rays += counters[CTR_RAYS + b];
     for (uint32_t b = 0; b < max_bounces; ++b) shadows += counters[CTR_SHADOWS + b];
     tally[0] += rays;
@@ -1010,7 +1083,7 @@ __global__ void k_tally(const uint32_t* counters, unsigned long long* tally, uin
 // One warp-aggregated 64-bit add per warp of the rays of bounce `bounce`
 // whose closest hit is a surface.
 __global__ void k_count_hits(PathPool pool, uint32_t bounce, uint32_t n0) {
-    const uint32_t count = min(bounce == 0 ? n0 : pool.counters[CTR_RAYS + bounce], pool.capacity);
+    const uint32_t count = bounce_paths(pool, bounce, n0);
     const uint32_t* queue = pool.queue[bounce & 1u];
     unsigned long long hits = 0;
     for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < count; i += gridDim.x * blockDim.x) {
@@ -1070,6 +1143,18 @@ LaunchShape launch_shape(int device) {
 void launch_wave_begin(const PathPool& pool, const WaveParams& wp, const LaunchShape& ls, cudaStream_t stream) {
     cudaMemsetAsync(pool.counters, 0, CTR_COUNT * sizeof(uint32_t), stream);
     k_raygen<<<ls.grid_stream, BLOCK, 0, stream>>>(pool, wp);
+}
+
+void launch_wave_begin_segments(const PathPool& pool, const WaveSegment* segs, uint32_t nseg, uint32_t paths,
+                                const uint32_t* hdr, const LaunchShape& ls, cudaStream_t stream) {
+    cudaMemsetAsync(pool.counters, 0, CTR_COUNT * sizeof(uint32_t), stream);
+    k_raygen_segments<<<ls.grid_stream, BLOCK, 0, stream>>>(pool, segs, nseg, paths, hdr);
+}
+
+void launch_accumulate_segments(const PathPool& pool, const WaveSegment* segs, uint32_t nseg, uint32_t items,
+                                const uint32_t* hdr, cudaStream_t stream) {
+    const uint32_t grid = hdr ? 4096u : (items == 0 ? 1u : min(4096u, (items + 255u) / 256u));
+    k_accumulate_segments<<<grid, 256, 0, stream>>>(pool, segs, nseg, items, hdr);
 }
 
 void launch_intersect(const DeviceScene& scene, const PathPool& pool, uint32_t bounce, uint32_t n0,

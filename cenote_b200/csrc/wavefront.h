@@ -91,6 +91,23 @@ struct WaveParams {
     const uint32_t* sample_offset;
 };
 
+// One job's share of a multi-job wave (the serving loop): samples
+// sample_base .. sample_base + samples - 1 of pixels pixel_base ..
+// pixel_base + pixel_count - 1 of a width x height image, traced as the
+// wave's paths start .. start + samples * pixel_count - 1 (sample-major) and
+// added into `film` as accumulate items pixel_start .. pixel_start +
+// pixel_count - 1. Segments are ordered by start (and pixel_start).
+struct WaveSegment {
+    uint32_t start, pixel_start;
+    uint32_t width, height;
+    uint32_t pixel_base, pixel_count;
+    uint32_t samples, sample_base;
+    float3 cam_pos, cam_right, cam_up, cam_fwd;  // basis pre-scaled to the focal plane when the lens is open
+    float aperture;
+    uint32_t reset;  // the segment's first sample starts the film (the job's first samples)
+    float4* film;    // the job's beauty sums
+};
+
 // Keys of the material sort: 0 for a miss; a hit's instance (its material
 // slot) folded into 1 .. SORT_LAYERS - 1 when its material has no coat,
 // fuzz, transmission or thin walls, else into SORT_LAYERS .. SORT_BINS - 1,
@@ -156,6 +173,15 @@ void launch_tally(const PathPool& pool, unsigned long long* tally, uint32_t n0, 
 // Instrumented waves: count bounce `bounce`'s rays that hit a surface into
 // CTR_HITS (misses are shaded by the same kernel but read no records).
 void launch_count_hits(const PathPool& pool, uint32_t bounce, uint32_t n0, cudaStream_t stream);
+// A multi-job wave: counters cleared and the camera paths of every segment
+// (`segs` in device memory), then, after the bounces, each segment's
+// samples added into its job's film. With `hdr` (device memory: segments,
+// paths, accumulate items) the counts are read on the device and the
+// bounce launches take n0 = 0, so one captured graph serves every wave.
+void launch_wave_begin_segments(const PathPool& pool, const WaveSegment* segs, uint32_t nseg, uint32_t paths,
+                                const uint32_t* hdr, const LaunchShape& ls, cudaStream_t stream);
+void launch_accumulate_segments(const PathPool& pool, const WaveSegment* segs, uint32_t nseg, uint32_t items,
+                                const uint32_t* hdr, cudaStream_t stream);
 void launch_copy_rad(const PathPool& pool, float4* out, uint32_t pixel_base, uint32_t pixel_count, cudaStream_t stream);
 // *counter += n on the device (a graph's progress counter).
 void launch_advance(uint32_t* counter, uint32_t n, cudaStream_t stream);

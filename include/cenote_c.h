@@ -384,13 +384,12 @@ int32_t cenote_probe_texture(cenote_scene* scene, uint32_t index, uint32_t mode,
 typedef struct cenote_server cenote_server;
 
 typedef struct cenote_server_options {
-    uint32_t slots;          /* concurrent streams, each with a path pool (0: 8); the server adds two
-                              * more that render only first frames, their pools counted alike */
+    uint32_t slots;          /* lanes (path pool + streams, one wave in flight each), 1 or 2 (0: 2) */
     uint32_t frame_spp;      /* samples per progressive frame (0: 4) */
     uint32_t max_active;     /* jobs resident at once (0: 64) */
-    uint32_t pool_paths;     /* path capacity per slot (0: 2^21) */
+    uint32_t pool_paths;     /* each lane's path pool capacity (0: 2^24); a job's image must fit it */
     uint32_t light_sampling; /* CENOTE_LIGHT_SAMPLING_* */
-    uint32_t no_graphs;      /* 1: launch every chunk directly instead of replaying a captured graph */
+    uint32_t no_graphs;      /* 1: launch every wave directly instead of replaying its group's captured graph */
 } cenote_server_options;
 
 #define CENOTE_JOB_QUEUED 0u
@@ -398,8 +397,9 @@ typedef struct cenote_server_options {
 #define CENOTE_JOB_DONE 2u
 #define CENOTE_JOB_FAILED 3u
 
-/* Called on the server thread after each chunk: `rgba` (width·height·4
- * linear averages over `samples`) is valid only during the call. */
+/* Called on the server thread after each progressive frame: `rgba`
+ * (width·height·4 linear averages over `samples`) is valid only during the
+ * call. */
 typedef void (*cenote_frame_fn)(void* user, uint64_t job, uint32_t samples, uint32_t target_spp, const float* rgba,
                                 uint32_t width, uint32_t height);
 
@@ -419,15 +419,23 @@ typedef struct cenote_server_counters {
                             * jobs' film buffers cached for reuse */
     uint64_t budget;
     double wall_ms;        /* since creation */
+    uint64_t waves;        /* waves finished */
+    uint64_t first_waves;  /* of those, waves that opened with first frames */
+    uint64_t wave_paths;   /* camera paths traced by those waves */
+    double busy_ms;        /* their device time (CUDA events around each wave) */
 } cenote_server_counters;
 
-/* `hbm_budget` bounds the pools and every resident job's film; the slots'
- * pools are allocated here (CENOTE_E_BUDGET if they alone exceed it). */
+/* The serving loop: jobs of any scenes, sizes and sample counts traced
+ * together as one wavefront of job-tagged paths (each wave: the jobs of one
+ * scene and bounce count, first frames first). `hbm_budget` bounds the path
+ * pool, every resident scene's device bytes and every admitted job's film;
+ * the pool is allocated here (CENOTE_E_BUDGET if it alone exceeds it). */
 int32_t cenote_server_create(cenote_context* ctx, uint64_t hbm_budget, const cenote_server_options* options,
                              cenote_server** out);
 /* Stops the loop after the chunks in flight; queued jobs are dropped. */
 void cenote_server_destroy(cenote_server* server);
-/* Queue a job (CENOTE_E_BUDGET if it could never fit); `fn` may be NULL. */
+/* Queue a job (CENOTE_E_BUDGET if it could never fit with its scene,
+ * CENOTE_E_INVALID_ARGUMENT if its image exceeds the pool); `fn` may be NULL. */
 int32_t cenote_job_submit(cenote_server* server, cenote_scene* scene, uint32_t width, uint32_t height,
                           uint32_t target_spp, uint32_t max_bounces, cenote_frame_fn fn, void* user, uint64_t* job);
 int32_t cenote_job_poll(cenote_server* server, uint64_t job, cenote_job_status* status);

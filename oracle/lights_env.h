@@ -304,15 +304,23 @@ inline V3f direction_from_uv(float u, float v) {  // environment.slang:80-85
     return {st * std::sin(phi), std::cos(theta), -st * std::cos(phi)};
 }
 
-// Exact bilinear filtering with the sampler's address modes (wrap in u,
-// clamp in v; environment.rs:16-17), texel centres at (i + 0.5) / n. The
-// kernels use the hardware filter, whose 8-bit sub-texel weights differ from
-// this by at most ~1/512 of a texel difference.
+// Bilinear filtering with the sampler's address modes (wrap in u, clamp in
+// v; environment.rs:16-17), texel centres at (i + 0.5) / n, as the texture
+// unit the reference and the kernels sample through computes it (measured
+// on a B200, see textures.h): the texel-space coordinate in FP32, rounded
+// to 1/256 of a texel (halves up), less half a texel; its integer part picks
+// the texels and its fraction is the weight.
 inline V3f env_bilinear(const EnvTables& e, float u, float v) {
-    float x = u * float(e.width) - 0.5f, y = v * float(e.height) - 0.5f;
-    float fx = std::floor(x), fy = std::floor(y);
-    float ax = x - fx, ay = y - fy;
-    long ix = long(fx), iy = long(fy);
+    auto axis = [](float c, uint32_t n, long* i, float* a) {
+        const float xs = c * float(n);
+        const long q = long(std::floor(double(xs) * 256.0 + 0.5)) - 128;
+        *i = q >= 0 ? q / 256 : -((-q + 255) / 256);
+        *a = float(q - *i * 256) / 256.0f;
+    };
+    long ix, iy;
+    float ax, ay;
+    axis(u, e.width, &ix, &ax);
+    axis(v, e.height, &iy, &ay);
     auto wrap = [&](long i) { long w = long(e.width); return size_t(((i % w) + w) % w); };
     auto clampi = [&](long j) { return size_t(std::min(std::max(j, 0L), long(e.height) - 1)); };
     size_t x0 = wrap(ix), x1 = wrap(ix + 1), y0 = clampi(iy), y1 = clampi(iy + 1);

@@ -9,6 +9,7 @@
 // of the same (pixel, sample) take the same path unless rounding diverges.
 #include <atomic>
 #include <cmath>
+#include <cstdlib>
 #include <cstdint>
 #include <cstring>
 #include <thread>
@@ -380,6 +381,11 @@ void trace_path(const Scene& s, uint32_t width, uint32_t height, uint32_t pixel,
         origin = origin + off;
         dir = normalize(target - off);
     }
+    // ORACLE_ULP_NUDGE (sensitivity experiments only): 1 moves every camera
+    // ray's direction by one ulp in x, 2 every ray's, the size of the
+    // rounding differences between two correct FP32 implementations.
+    static const int nudge = std::getenv("ORACLE_ULP_NUDGE") ? std::atoi(std::getenv("ORACLE_ULP_NUDGE")) : 0;
+    if (nudge == 1) dir.x = std::nextafter(dir.x, 2.0f);
     float dir_w = dot(dir, normalize(fwd));
     V3f guide(1.0f);  // the open feature throughput; a camera ray's is 1
     V3f thr(1.0f);
@@ -390,6 +396,7 @@ void trace_path(const Scene& s, uint32_t width, uint32_t height, uint32_t pixel,
     for (uint32_t bounce = 0; bounce < max_bounces; ++bounce) {
         Hit hit;
         counts.extension++;
+        if (nudge == 2) dir.x = std::nextafter(dir.x, 2.0f);
         bool found = intersect(s, origin, dir, bounce == 0 ? RAY_MASK_CAMERA : RAY_MASK_ALL, pixel, sample,
                                bounce, &hit);
         if (!found) {  // shade_miss.slang:29-75

@@ -27,10 +27,12 @@ CORPUS = ["cornell_box", "veach_mis", "teapot_full"]
 # relMSE far below a second, independent 64-spp render's (4e-3 and 0.4): the
 # same samples reproduce the same noise. teapot-full's double glass (65
 # bounces of refraction) amplifies the ulp-level differences between the
-# reference's hardware ray-triangle hits and the watertight test, and its
-# floor texture is BC7-compressed and its sky hardware-filtered there, so
-# its bars sit between the same-sample render (FLIP 0.023, relMSE 2.3e-3)
-# and an independent one (0.115, 0.068).
+# reference's hardware ray-triangle hits and the watertight test: moving
+# every ray of the oracle's own render by one ulp changes it by mean FLIP
+# 0.009 (test_teapot_parts_on_one_ulp), against 5e-6 for cornell-box. Its
+# floor texture is BC7-compressed there, too, so its bars sit between the
+# same-sample render (FLIP 0.023, relMSE 2.3e-3) and an independent one
+# (0.115, 0.068).
 BARS = {"cornell_box": (0.01, 1e-4), "veach_mis": (0.01, 1e-4), "teapot_full": (0.035, 6e-3)}
 
 
@@ -323,3 +325,37 @@ def test_gpu_reproduces_reference_corpus_render(ctx, name):
     flip = flip_ldr_linear(golden, img[..., :3])
     assert flip <= max_flip, flip
     assert rel_mse(img[..., :3], golden) <= max_rel
+
+
+def _nudged_render(name, mode):
+    """The oracle's 64-spp render of a corpus scene in a child process with
+    ORACLE_ULP_NUDGE=mode (0 off, 2: every ray's direction one ulp over)."""
+    import os
+    import subprocess
+    import sys
+    import tempfile
+    with tempfile.TemporaryDirectory() as d:
+        out = pathlib.Path(d) / "img.npy"
+        code = ("import sys, numpy as np; sys.path[:0] = [{root!r}, {tests!r}]; import oracle; "
+                "from test_corpus import load; spec, _ = load({name!r}); "
+                "img = oracle.OracleScene(spec).render_sum(spec.width, spec.height, 0, spec.spp, spec.max_bounces); "
+                "np.save({out!r}, img[..., :3] / spec.spp)").format(
+            root=str(GOLDEN.parents[1]), tests=str(GOLDEN.parent), name=name, out=str(out))
+        subprocess.run([sys.executable, "-c", code], check=True, env=dict(os.environ, ORACLE_ULP_NUDGE=str(mode)))
+        return np.load(out)
+
+
+@pytest.mark.parametrize("name", ["cornell_box", "teapot_full"])
+def test_teapot_parts_on_one_ulp(name):
+    """The same samples with every ray's direction moved by one ulp (the
+    size of the rounding differences between two correct FP32 ray casts):
+    cornell-box does not move (mean FLIP 5e-6), teapot-full's nested glass
+    moves by FLIP 0.009, relMSE 6e-4 - the part of its distance to the
+    reference's render that hardware-vs-watertight hit differences alone
+    can explain, several times over, since those differ at every hit."""
+    a, b = _nudged_render(name, 0), _nudged_render(name, 2)
+    flip = flip_ldr_linear(a, b)
+    if name == "cornell_box":
+        assert flip < 1e-4
+    else:
+        assert 0.004 < flip < 0.02 and rel_mse(b, a) > 2e-4

@@ -43,7 +43,7 @@ JOBS = [("cornell", 64, 64, 8, 6), ("chart", 96, 54, 6, 6), ("textured", 80, 45,
 @pytest.mark.gpu
 @pytest.mark.parametrize("graphs", [True, False])
 def test_jobs_match_standalone_renders_bitwise(ctx, scene_set, graphs):
-    server = Server(ctx, 8 * GIB, slots=3, pool_paths=1 << 18, graphs=graphs)
+    server = Server(ctx, 8 * GIB, slots=2, pool_paths=1 << 18, graphs=graphs)
     ids = [server.submit(scene_set[n], w, h, spp, b) for n, w, h, spp, b in JOBS]
     for j in ids:
         server.wait(j, 120000.0)
@@ -89,13 +89,17 @@ def test_progressive_frames_every_frame_spp(ctx, scene_set):
 
 @pytest.mark.gpu
 def test_admission_respects_the_budget(ctx, scene_set):
+    """The budget holds the path pool, each resident scene's device bytes
+    (BVH, triangles, records, textures, environment tables) once, and every
+    admitted job's film: room for two 128x128 jobs of one scene at a time."""
     pool_paths = 1 << 16
-    pool_bytes = pool_paths * (16 * 5 + 8 + 4 + 8 + 64)
-    job_bytes = 128 * 128 * 32 + 256
-    # Room for the slots' pools (one regular, two first-frame) and two 128x128
-    # jobs at a time.
-    budget = 3 * pool_bytes + 2 * job_bytes + 100
-    server = Server(ctx, budget, slots=1, pool_paths=pool_paths)
+    probe = Server(ctx, 8 * GIB, pool_paths=pool_paths)
+    pool_bytes = probe.stats()["bytes_in_use"]
+    probe.close()
+    scene_bytes = scene_set["cornell"].device_bytes()
+    job_bytes = 128 * 128 * 32
+    budget = pool_bytes + scene_bytes + 2 * job_bytes + 100
+    server = Server(ctx, budget, pool_paths=pool_paths)
     ids = [server.submit(scene_set["cornell"], 128, 128, 2, 4) for _ in range(5)]
     peak = 0
     done = set()
@@ -106,17 +110,38 @@ def test_admission_respects_the_budget(ctx, scene_set):
         for j in ids:
             if server.poll(j).state == JOB_DONE:
                 done.add(j)
-    assert peak <= 2
+    assert peak == 2
     with pytest.raises(CenoteError) as e:
-        server.submit(scene_set["cornell"], 512, 512, 1, 4)  # could never fit
+        server.submit(scene_set["cornell"], 200, 200, 1, 4)  # could never fit
     assert e.value.code == -8
     server.close()
 
 
 @pytest.mark.gpu
+def test_jobs_of_many_scenes_share_waves_and_match(ctx, scene_set):
+    """Twenty-four jobs of three scenes and two bounce counts submitted at
+    once, one wave in flight and two: each job's result is bitwise its
+    standalone render, whatever it shared its waves with."""
+    rng = np.random.default_rng(4)
+    jobs = []
+    for k in range(24):
+        n = ["cornell", "chart", "textured"][k % 3]
+        w, h = [(32, 32), (40, 24), (17, 33)][rng.integers(3)]
+        jobs.append((n, w, h, int(rng.integers(1, 13)), [4, 6][k % 2]))
+    for depth in (1, 2):
+        server = Server(ctx, 8 * GIB, slots=depth, frame_spp=4, pool_paths=1 << 14)
+        ids = [server.submit(scene_set[n], w, h, spp, b) for n, w, h, spp, b in jobs]
+        for j in ids:
+            server.wait(j, 120000.0)
+        for j, (n, w, h, spp, b) in zip(ids, jobs):
+            assert np.array_equal(server.result(j), standalone(ctx, scene_set[n], w, h, spp, b)), (n, w, h, spp, b)
+        server.close()
+
+
+@pytest.mark.gpu
 def test_server_rejects_bad_requests(ctx, scene_set):
     with pytest.raises(CenoteError) as e:
-        Server(ctx, 1 << 20, slots=2, pool_paths=1 << 20)  # pools alone exceed the budget
+        Server(ctx, 1 << 20, pool_paths=1 << 20)  # the pool alone exceeds the budget
     assert e.value.code == -8
     server = Server(ctx, 4 * GIB, slots=1, pool_paths=1 << 16)
     for args in [(0, 8, 1, 4), (8, 8, 0, 4), (8, 8, 1, 0), (8, 8, 1, 256)]:

@@ -229,9 +229,11 @@ def test_gpu_texture_taps_match_oracle(ctx, kind):
     """Taps of the texture unit against the oracle's decoder and filter. At
     texel centres the decoded texels of the linear formats are bit-equal
     (BC palettes included, whose precision the oracle takes from this
-    unit); filtered taps agree to the unit's blend precision (2e-5). sRGB
-    storage decodes and filters at a lower precision in the unit than the
-    oracle's exact transfer function: within 0.006."""
+    unit). Filtered taps at arbitrary coordinates agree to one step of the
+    unit's 1/256 weight quantisation times the neighbours' difference
+    (measured: at most 8e-4 on these value-noise maps). sRGB storage
+    decodes and filters at a lower precision in the unit than the oracle's
+    exact transfer function: within 0.006."""
     tex = make_texture(kind)
     rng = np.random.default_rng(2)
     size = 32
@@ -257,7 +259,7 @@ def test_gpu_texture_taps_match_oracle(ctx, kind):
             continue
         err = np.abs(got[:, :c] - ref[:, :c])
         scale = 4.0 if kind == "rgba32f" else (2.0 if mode == 3 else 1.0)
-        bound = 0.006 if srgb_storage and mode in (0, 1) else 2e-5
+        bound = 0.006 if srgb_storage else 1.5e-3
         assert err.max() <= bound * scale, (mode, err.max())
 
 
