@@ -365,6 +365,7 @@ def run_serving(args):
     counters = server.stats()
     st = [server.poll(j) for j in ids]
     ttff = np.array([s.first_frame_ms - s.submit_ms for s in st])
+    burst_end = max(s.first_frame_ms for s in st[:args.concurrency]) if args.concurrency else 0.0
     ttt = np.array([s.done_ms - s.submit_ms for s in st])
     span_ms = max(s.done_ms for s in st) - min(s.submit_ms for s in st)
     samples = sum(w * h * spp for _, _, w, h, spp in jobs)
@@ -382,10 +383,16 @@ def run_serving(args):
         "time_to_first_frame_ms": {"p50": pct(ttff, 50), "p99": pct(ttff, 99), "max": float(ttff.max())},
         "time_to_target_ms": {"p50": pct(ttt, 50), "p99": pct(ttt, 99), "max": float(ttt.max())},
         # Closed loop: the jobs after the first `concurrency`, which all arrive
-        # at once when the loop starts.
+        # at once when the loop starts; and those submitted once the opening
+        # burst's last first frame is out (past its transient).
         "steady_state_time_to_first_frame_ms": (
             {"p50": pct(ttff[args.concurrency:], 50), "p99": pct(ttff[args.concurrency:], 99),
              "jobs": int(len(ttff) - args.concurrency)} if args.concurrency and len(ttff) > args.concurrency else None),
+        "after_opening_burst_time_to_first_frame_ms": (
+            (lambda sel: {"p50": pct(ttff[sel], 50), "p99": pct(ttff[sel], 99), "max": float(ttff[sel].max()),
+                          "jobs": int(sel.sum()), "burst_cleared_ms": burst_end})(
+                np.array([s.submit_ms > burst_end for s in st]))
+            if args.concurrency and any(s.submit_ms > burst_end for s in st) else None),
         "slowest_first_frames": [
             {"job": int(k), "scene": jobs[k][1], "size": f"{jobs[k][2]}x{jobs[k][3]}", "spp": jobs[k][4],
              "submit_ms": round(st[k].submit_ms, 1), "ttff_ms": round(float(ttff[k]), 1)}
@@ -427,9 +434,10 @@ def run_knob_sweep(args, w):
             ms.append(r.stats()["gpu_ms"])
         return round(min(ms) / spp, 4)
 
-    names = ("material_sort", "samples_per_wave", "refill_idle", "top_nodes", "l2_window", "per_lane_triangles")
+    names = ("material_sort", "samples_per_wave", "refill_idle", "top_nodes", "l2_window", "per_lane_triangles",
+             "block_size", "stack_depth")
     base = tuple(best[k] for k in names)
-    values = ((0, 1, 2), (0, 4, 8, 16), (4, 8, 16, 32), (0, 80, 320), (0, 1), (0, 1))
+    values = ((0, 1, 2), (0, 4, 8, 16), (4, 8, 16, 32), (0, 80, 320), (0, 1), (0, 1), (128, 256), (16, 32))
     sweep = {"tuned": timed(base)}
     for i, vals in enumerate(values):
         for v in vals:
@@ -464,7 +472,7 @@ def main():
                     help="BVH builder: host binned SAH or GPU PLOC (scene prep, outside the timed region)")
     ap.add_argument("--tuning", default="",
                     help="pin the launch knobs instead of autotuning: sort,samples_per_wave,refill,top_nodes,l2"
-                         "[,per_lane_triangles] "
+                         "[,per_lane_triangles[,block_size,stack_depth]] "
                          "(profiling runs that must not record the tuner's probes)")
     ap.add_argument("--material-sort", type=int, default=None, choices=[0, 1, 2],
                     help="fix the material sort (0 off, 1 every bounce, 2 from the first bounce on) "
@@ -651,6 +659,8 @@ def main():
                               "top_nodes_in_shared_memory": tuning["top_nodes"],
                               "l2_persisting_bvh": bool(tuning["l2_window"]),
                               "triangle_tests": "per lane" if tuning["per_lane_triangles"] else "warp queue",
+                              "traversal_block_size": tuning["block_size"],
+                              "traversal_stack_depth": tuning["stack_depth"],
                               "chosen_by": "autotuner" if args.material_sort is None and not args.tuning else "flag",
                               "autotune_s": round(tune_s, 3)},
                    "guides": "albedo, normal and depth traced and accumulated every sample, as Renderer::accumulate does"},

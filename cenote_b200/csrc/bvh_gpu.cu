@@ -3,10 +3,10 @@
 // Hierarchy Construction", IEEE TVCG 2018) over Morton-ordered triangles,
 // collapsed level by level into the node format of records.h.
 //
-// The collapse makes the same choices as the host build (bvh_build.cpp):
-// greedy largest-area opening up to eight children, subtrees of at most three
-// triangles become leaf children, octant-scored child slots, 8-bit boxes
-// quantised in double precision. Node indices are assigned by prefix sums
+// The collapse makes the same choices as the host build (bvh_build.cpp): the
+// cost-optimal dynamic programme over the binary tree (at most eight
+// children, leaf children of at most three triangles), octant-scored child
+// slots, 8-bit boxes quantised in double precision. Node indices are assigned by prefix sums
 // per level, so the layout is deterministic and breadth first (the top levels
 // are the first nodes, which the traversal kernels may stage in shared
 // memory). Closest hits do not depend on the tree: equal distances resolve by
@@ -16,7 +16,9 @@
 #include <cub/device/device_radix_sort.cuh>
 #include <cub/device/device_scan.cuh>
 
+#include <algorithm>
 #include <cfloat>
+#include <vector>
 
 namespace cn {
 namespace {
@@ -206,36 +208,119 @@ __global__ void k_merge(Tree t, const uint32_t* __restrict__ clusters, const uin
 }
 
 // ---- collapse ------------------------------------------------------------------------
+//
+// Cost-optimal collapse (Ylitie, Karras & Laine 2017, §3.1), the host
+// build's dynamic programme: bottom-up, cost[b][i] is the cheapest SAH cost of
+// covering b's subtree with at most i child slots of the parent (i = 1..7);
+// a slot is a leaf of up to three triangles or an 8-wide node whose own
+// children spread over its 8 slots. c_node = 1 per node visit, c_prim = 0.3
+// per triangle test, each weighted by the node's surface area relative to the
+// root's. how[b][1]: 0 leaf / 1 node; how[b][i > 1]: 0 = as i - 1, k = the
+// left child gets k slots; split8[b]: the left child's share when b is an
+// 8-wide node. PLOC numbers a merged node above both its children, so the
+// nodes one merge round made form an index range whose children are all
+// lower: one launch per round, in order, is a bottom-up pass.
+struct Collapse {
+    float* cost;     // 8 per binary node (1..7 used)
+    uint8_t* how;    // 8 per binary node
+    uint8_t* split8;
+};
 
-__device__ __forceinline__ bool leafish(const Tree& t, uint32_t b) {
-    return __float_as_uint(t.lo[b].w) == NONE || t.tris[b] <= 3u;
-}
+constexpr float C_NODE = 1.0f, C_PRIM = 0.3f;
 
-// The up-to-eight binary nodes a wide node over `b` takes as children.
-__device__ int gather_kids(const Tree& t, uint32_t b, uint32_t kids[8]) {
-    int n = 0;
-    if (leafish(t, b)) {
-        kids[n++] = b;
-    } else {
-        kids[n++] = __float_as_uint(t.lo[b].w);
-        kids[n++] = __float_as_uint(t.hi[b].w);
-    }
-    while (n < 8) {
-        int pick = -1;
-        float best = -1.0f;
-        for (int i = 0; i < n; ++i) {
-            if (leafish(t, kids[i])) continue;
-            float4 l = t.lo[kids[i]], h = t.hi[kids[i]];
-            float a = half_area(make_float3(l.x, l.y, l.z), make_float3(h.x, h.y, h.z));
-            if (a > best) {
-                best = a;
-                pick = i;
+__global__ void k_collapse_cost(Tree t, Collapse c, uint32_t first, uint32_t end, double inv_root) {
+    for (uint32_t b = first + blockIdx.x * blockDim.x + threadIdx.x; b < end; b += gridDim.x * blockDim.x) {
+        const float4 lo = t.lo[b], hi = t.hi[b];
+        double d[3] = {fmax(double(hi.x) - double(lo.x), 0.0), fmax(double(hi.y) - double(lo.y), 0.0),
+                       fmax(double(hi.z) - double(lo.z), 0.0)};
+        const float area = float((d[0] * d[1] + d[1] * d[2] + d[2] * d[0]) * inv_root);
+        const uint32_t tris = t.tris[b];
+        const float leaf = tris <= 3u ? area * C_PRIM * float(tris) : __int_as_float(0x7f800000);
+        float* cb = c.cost + 8 * size_t(b);
+        uint8_t* hb = c.how + 8 * size_t(b);
+        const uint32_t l = __float_as_uint(lo.w);
+        if (l == NONE) {
+            for (int i = 0; i < 8; ++i) {
+                cb[i] = leaf;
+                hb[i] = 0;
+            }
+            c.split8[b] = 0;
+            continue;
+        }
+        const uint32_t r = __float_as_uint(hi.w);
+        float cl[8], cr[8];
+        for (int i = 1; i < 8; ++i) {
+            cl[i] = c.cost[8 * size_t(l) + i];
+            cr[i] = c.cost[8 * size_t(r) + i];
+        }
+        float dist[9];
+        uint8_t dsplit[9];
+        for (int j = 2; j <= 8; ++j) {
+            dist[j] = __int_as_float(0x7f800000);
+            dsplit[j] = 0;
+            for (int k = 1; k < j; ++k) {
+                const float v = cl[k] + cr[j - k];
+                if (v < dist[j]) {
+                    dist[j] = v;
+                    dsplit[j] = uint8_t(k);
+                }
             }
         }
-        if (pick < 0) break;
-        const uint32_t c = kids[pick];
-        kids[pick] = __float_as_uint(t.lo[c].w);
-        kids[n++] = __float_as_uint(t.hi[c].w);
+        c.split8[b] = dsplit[8] ? dsplit[8] : 4;
+        const float node = dist[8] + area * C_NODE;
+        cb[0] = 0.0f;
+        hb[0] = 0;
+        cb[1] = fminf(leaf, node);
+        hb[1] = leaf <= node ? 0 : 1;
+        for (int i = 2; i < 8; ++i) {
+            if (dist[i] < cb[i - 1]) {
+                cb[i] = dist[i];
+                hb[i] = dsplit[i];
+            } else {
+                cb[i] = cb[i - 1];
+                hb[i] = 0;
+            }
+        }
+    }
+}
+
+// A binary node the collapse turns into a leaf child: a true leaf, or a
+// subtree of at most three triangles whose leaf cost won.
+__device__ __forceinline__ bool leafish(const Tree& t, const Collapse& c, uint32_t b) {
+    return __float_as_uint(t.lo[b].w) == NONE || c.how[8 * size_t(b) + 1] == 0;
+}
+
+// The up-to-eight binary nodes a wide node over `b` takes as children, as the
+// programme chose them.
+__device__ int gather_kids(const Tree& t, const Collapse& c, uint32_t b, uint32_t kids[8]) {
+    if (leafish(t, c, b)) {
+        kids[0] = b;
+        return 1;
+    }
+    uint32_t st_node[16], st_slots[16];
+    int sp = 0, n = 0;
+    const uint32_t k = c.split8[b];
+    st_node[sp] = __float_as_uint(t.hi[b].w);
+    st_slots[sp++] = 8u - k;
+    st_node[sp] = __float_as_uint(t.lo[b].w);
+    st_slots[sp++] = k;
+    while (sp > 0 && n < 8) {
+        const uint32_t x = st_node[--sp];
+        uint32_t i = st_slots[sp];
+        while (i > 1 && c.how[8 * size_t(x) + i] == 0) --i;
+        if (i <= 1 || __float_as_uint(t.lo[x].w) == NONE) {
+            kids[n++] = x;
+            continue;
+        }
+        const uint32_t kk = c.how[8 * size_t(x) + i];
+        if (sp + 2 > 16) {  // cannot happen (at most 8 slots split): keep the node whole
+            kids[n++] = x;
+            continue;
+        }
+        st_node[sp] = __float_as_uint(t.hi[x].w);
+        st_slots[sp++] = i - kk;
+        st_node[sp] = __float_as_uint(t.lo[x].w);
+        st_slots[sp++] = kk;
     }
     return n;
 }
@@ -246,16 +331,16 @@ struct Item {
 
 // Pass 1: children of every wide node of the level, and its counts (high
 // word: inner children, low word: triangles) for the scan.
-__global__ void k_collapse_plan(Tree t, const Item* __restrict__ items, uint32_t count, uint32_t* plan,
+__global__ void k_collapse_plan(Tree t, Collapse c, const Item* __restrict__ items, uint32_t count, uint32_t* plan,
                                 unsigned long long* counts) {
     for (uint32_t w = blockIdx.x * blockDim.x + threadIdx.x; w < count; w += gridDim.x * blockDim.x) {
         uint32_t kids[8];
-        const int n = gather_kids(t, items[w].binary, kids);
+        const int n = gather_kids(t, c, items[w].binary, kids);
         uint32_t inner = 0, tris = 0;
         for (int i = 0; i < 8; ++i) {
             plan[8 * size_t(w) + i] = i < n ? kids[i] : NONE;
             if (i < n) {
-                if (leafish(t, kids[i])) tris += t.tris[kids[i]];
+                if (leafish(t, c, kids[i])) tris += t.tris[kids[i]];
                 else inner++;
             }
         }
@@ -265,7 +350,8 @@ __global__ void k_collapse_plan(Tree t, const Item* __restrict__ items, uint32_t
 
 // Pass 2: encode each wide node, emit its leaf triangles and the next
 // level's items.
-__global__ void k_collapse_emit(Tree t, const Item* __restrict__ items, uint32_t count, const uint32_t* __restrict__ plan,
+__global__ void k_collapse_emit(Tree t, Collapse cp, const Item* __restrict__ items, uint32_t count,
+                                const uint32_t* __restrict__ plan,
                                 const unsigned long long* __restrict__ offs, uint32_t child_base, uint32_t tri_base,
                                 const float4* __restrict__ in, WideNode* nodes, float4* tris_out, Item* next) {
     for (uint32_t w = blockIdx.x * blockDim.x + threadIdx.x; w < count; w += gridDim.x * blockDim.x) {
@@ -366,7 +452,7 @@ __global__ void k_collapse_emit(Tree t, const Item* __restrict__ items, uint32_t
             wn.qlo_y[s] = ql[1]; wn.qhi_y[s] = qh[1];
             wn.qlo_z[s] = ql[2]; wn.qhi_z[s] = qh[2];
             const uint32_t b = kids[i];
-            if (leafish(t, b)) {
+            if (leafish(t, cp, b)) {
                 // Its 1..3 triangles, left before right.
                 uint32_t stack[8], sp = 0, cnt = 0;
                 stack[sp++] = b;
@@ -494,6 +580,7 @@ cudaError_t build_wide_bvh_gpu(const float4* in, uint32_t n, GpuBvh* out, cudaSt
     // PLOC: merge mutual nearest neighbours until one cluster is left. Every
     // round merges at least the globally closest pair, so at most n - 1 rounds.
     uint32_t m = n, node_next = n;
+    std::vector<uint32_t> round_end;  // node_next after each merge round
     uint32_t* cur = cl0.as<uint32_t>();
     uint32_t* nxt = cl1.as<uint32_t>();
     for (uint32_t round = 0; m > 1; ++round) {
@@ -511,6 +598,7 @@ cudaError_t build_wide_bvh_gpu(const float4* in, uint32_t n, GpuBvh* out, cudaSt
         const uint32_t made = uint32_t(tot & 0xffffffffull), kept = uint32_t(tot >> 32);
         if (made == 0 || kept >= m || node_next + made > total) return cudaErrorUnknown;
         node_next += made;
+        round_end.push_back(node_next);
         m = kept;
         uint32_t* tmp = cur;
         cur = nxt;
@@ -522,6 +610,31 @@ cudaError_t build_wide_bvh_gpu(const float4* in, uint32_t n, GpuBvh* out, cudaSt
     flags.alloc(0);
     offs.alloc(0);
     scan_tmp.alloc(0);
+
+    // The collapse's costs, bottom-up: the leaves, then each merge round's
+    // nodes in the order the rounds made them.
+    Scratch ccost, chow, csplit;
+    BVH_TRY(ccost.alloc(total * 32));
+    BVH_TRY(chow.alloc(total * 8));
+    BVH_TRY(csplit.alloc(total));
+    Collapse cp{ccost.as<float>(), chow.as<uint8_t>(), csplit.as<uint8_t>()};
+    float4 root_box[2];
+    BVH_TRY(sync_read(&root_box[0], t.lo + root, 16, s));
+    BVH_TRY(sync_read(&root_box[1], t.hi + root, 16, s));
+    {
+        const double dx = std::max(double(root_box[1].x) - double(root_box[0].x), 0.0);
+        const double dy = std::max(double(root_box[1].y) - double(root_box[0].y), 0.0);
+        const double dz = std::max(double(root_box[1].z) - double(root_box[0].z), 0.0);
+        const double inv_root = 1.0 / std::max(dx * dy + dy * dz + dz * dx, 1e-300);
+        uint32_t first = 0, end = n;
+        k_collapse_cost<<<grid_for(end - first), BLOCK, 0, s>>>(t, cp, first, end, inv_root);
+        for (uint32_t e : round_end) {
+            first = end;
+            end = e;
+            if (end > first) k_collapse_cost<<<grid_for(end - first), BLOCK, 0, s>>>(t, cp, first, end, inv_root);
+        }
+        BVH_TRY(cudaGetLastError());
+    }
 
     // Collapse, one level of wide nodes at a time. Every wide node holds at
     // least two binary nodes' worth of the tree, so there are fewer than n.
@@ -545,7 +658,7 @@ cudaError_t build_wide_bvh_gpu(const float4* in, uint32_t n, GpuBvh* out, cudaSt
     while (count > 0) {
         if (depth > n) return cudaErrorUnknown;
         ++depth;
-        k_collapse_plan<<<grid_for(count), BLOCK, 0, s>>>(t, level, count, plan.as<uint32_t>(),
+        k_collapse_plan<<<grid_for(count), BLOCK, 0, s>>>(t, cp, level, count, plan.as<uint32_t>(),
                                                           counts.as<unsigned long long>());
         BVH_TRY(cub::DeviceScan::ExclusiveSum(ctmp.p, cscan_bytes, counts.as<unsigned long long>(),
                                               coffs.as<unsigned long long>(), int(count), s));
@@ -555,7 +668,7 @@ cudaError_t build_wide_bvh_gpu(const float4* in, uint32_t n, GpuBvh* out, cudaSt
         const unsigned long long tot = last[0] + last[1];
         const uint32_t inner = uint32_t(tot >> 32), ntri = uint32_t(tot & 0xffffffffull);
         if (node_total + inner > n || tri_total + ntri > n) return cudaErrorUnknown;
-        k_collapse_emit<<<grid_for(count), BLOCK, 0, s>>>(t, level, count, plan.as<uint32_t>(),
+        k_collapse_emit<<<grid_for(count), BLOCK, 0, s>>>(t, cp, level, count, plan.as<uint32_t>(),
                                                           coffs.as<unsigned long long>(), node_total, tri_total, in,
                                                           nodes.as<WideNode>(), tris.as<float4>(), next_level);
         BVH_TRY(cudaGetLastError());

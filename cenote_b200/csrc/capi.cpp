@@ -820,6 +820,11 @@ int32_t cenote_renderer_set_material_sort(cenote_renderer* r, uint32_t mode) {
     return CENOTE_OK;
 }
 
+// The traversal variant of a block size and stack depth (0 = defaults).
+static uint32_t trav_variant_of(uint32_t block, uint32_t stack) {
+    return (block == 256 ? 2u : 0u) + (stack == 16 ? 1u : 0u);
+}
+
 int32_t cenote_renderer_set_tuning(cenote_renderer* r, const cenote_tuning* t) {
     CN_CHECK(r && t, CENOTE_E_INVALID_ARGUMENT, "null argument");
     CN_CHECK(t->material_sort <= CENOTE_SORT_SECONDARY, CENOTE_E_INVALID_ARGUMENT, "unknown material-sort mode");
@@ -827,12 +832,17 @@ int32_t cenote_renderer_set_tuning(cenote_renderer* r, const cenote_tuning* t) {
     CN_CHECK(t->top_nodes <= TOP_NODES_MAX, CENOTE_E_INVALID_ARGUMENT, "more top-level nodes than shared memory holds");
     CN_CHECK(t->l2_window <= 1, CENOTE_E_INVALID_ARGUMENT, "l2_window is 0 or 1");
     CN_CHECK(t->per_lane_triangles <= 1, CENOTE_E_INVALID_ARGUMENT, "per_lane_triangles is 0 or 1");
+    CN_CHECK(t->block_size == 0 || t->block_size == 128 || t->block_size == 256, CENOTE_E_INVALID_ARGUMENT,
+             "block_size is 128 or 256");
+    CN_CHECK(t->stack_depth == 0 || t->stack_depth == 16 || t->stack_depth == 32, CENOTE_E_INVALID_ARGUMENT,
+             "stack_depth is 16 or 32");
     r->material_sort = t->material_sort;
     r->samples_per_wave = t->samples_per_wave;
     r->refill_idle = t->refill_idle;
     r->top_nodes = t->top_nodes;
     r->l2_window = t->l2_window;
     r->per_lane_triangles = t->per_lane_triangles;
+    r->trav_variant = trav_variant_of(t->block_size, t->stack_depth);
     return CENOTE_OK;
 }
 
@@ -845,6 +855,8 @@ int32_t cenote_renderer_get_tuning(cenote_renderer* r, cenote_tuning* out) {
     out->l2_window = r->l2_window;
     out->per_lane_triangles = r->per_lane_triangles;
     out->ms_per_sample = r->tuned_ms_per_sample;
+    out->block_size = uint32_t(TRAV_VARIANT_BLOCK[r->trav_variant]);
+    out->stack_depth = uint32_t(TRAV_VARIANT_STACK[r->trav_variant]);
     return CENOTE_OK;
 }
 
@@ -1060,8 +1072,15 @@ int32_t cenote_renderer_autotune(cenote_renderer* r, cenote_scene* scene, uint32
     while (probe > 2 && pixels * probe > (uint64_t(1) << 27)) probe /= 2;
     const uint32_t saved_profiling = r->profiling;
     r->profiling = 0;
-    cenote_tuning best{r->material_sort, r->samples_per_wave, r->refill_idle, r->top_nodes,
-                       r->l2_window,        r->per_lane_triangles, 0.0f};
+    cenote_tuning best{r->material_sort,
+                       r->samples_per_wave,
+                       r->refill_idle,
+                       r->top_nodes,
+                       r->l2_window,
+                       r->per_lane_triangles,
+                       0.0f,
+                       uint32_t(TRAV_VARIANT_BLOCK[r->trav_variant]),
+                       uint32_t(TRAV_VARIANT_STACK[r->trav_variant])};
     auto apply = [&](const cenote_tuning& t) {
         r->material_sort = t.material_sort;
         r->samples_per_wave = t.samples_per_wave;
@@ -1069,6 +1088,7 @@ int32_t cenote_renderer_autotune(cenote_renderer* r, cenote_scene* scene, uint32
         r->top_nodes = t.top_nodes;
         r->l2_window = t.l2_window;
         r->per_lane_triangles = t.per_lane_triangles;
+        r->trav_variant = trav_variant_of(t.block_size, t.stack_depth);
     };
     // Device time of `probe` samples, the better of two runs (the first run of
     // a new wave size also allocates).
@@ -1086,9 +1106,12 @@ int32_t cenote_renderer_autotune(cenote_renderer* r, cenote_scene* scene, uint32
     float best_ms = 0.0f;
     rc = measure(best, &best_ms);
     // An all-opaque scene chooses between the warp triangle queue and per-lane
-    // tests; fractional opacity always tests per lane.
-    const int knobs = scene->ds.has_nonopaque ? 5 : 6;
-    for (int knob = 0; knob < knobs && rc == CENOTE_OK; ++knob) {
+    // tests (fractional opacity always tests per lane); the 16-entry stack is
+    // a candidate only when the tree's node groups fit it.
+    const bool short_stack = TRAVERSAL_STACK_DEPTH - int(scene->ds.stack_room) < 16;
+    for (int knob = 0; knob < 8 && rc == CENOTE_OK; ++knob) {
+        if (knob == 5 && scene->ds.has_nonopaque) continue;
+        if (knob == 7 && !short_stack) continue;
         for (int c = 0; c < (knob == 1 ? 5 : (knob >= 4 ? 2 : 3)) && rc == CENOTE_OK; ++c) {
             cenote_tuning t = best;
             if (knob == 0) t.material_sort = uint32_t(c);
@@ -1097,9 +1120,12 @@ int32_t cenote_renderer_autotune(cenote_renderer* r, cenote_scene* scene, uint32
             if (knob == 3) t.top_nodes = c == 0 ? 0u : (c == 1 ? 80u : TOP_NODES_MAX);
             if (knob == 4) t.l2_window = uint32_t(c);
             if (knob == 5) t.per_lane_triangles = uint32_t(c);
+            if (knob == 6) t.block_size = c == 0 ? 128u : 256u;
+            if (knob == 7) t.stack_depth = c == 0 ? 32u : 16u;
             if (t.material_sort == best.material_sort && t.samples_per_wave == best.samples_per_wave &&
                 t.refill_idle == best.refill_idle && t.top_nodes == best.top_nodes && t.l2_window == best.l2_window &&
-                t.per_lane_triangles == best.per_lane_triangles)
+                t.per_lane_triangles == best.per_lane_triangles && t.block_size == best.block_size &&
+                t.stack_depth == best.stack_depth)
                 continue;
             float ms = 0.0f;
             rc = measure(t, &ms);

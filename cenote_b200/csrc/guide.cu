@@ -494,56 +494,171 @@ __device__ __forceinline__ float3 unit_pos(const DeviceScene& s, float3 p) {
                        (p.z - s.bbox_min[2]) * s.bbox_inv);
 }
 
-__global__ void __launch_bounds__(TILE, 1) k_infer_paths(Net net, DeviceScene scene, PathPool pool, uint32_t bounce,
-                                                         uint32_t n0, int* err) {
+// ---- inference in the wavefront: warp groups sharing one copy of the network ----------
+//
+// A CTA of WG warp groups (128 threads each): every group runs its own 128-row
+// tiles through the network with its own operand buffers, TMEM columns and
+// mbarrier, while the weights are staged once per CTA. With 16 warps per SM
+// the scattered loads of one group's next tile (hit records, vertices,
+// transforms) overlap the other groups' tensor-core layers. Features go
+// straight to the BF16 operand in 8-column chunks and outputs straight from
+// TMEM to global memory, so a thread holds neither its 96 inputs nor its 40
+// outputs in registers. The arithmetic (encoding, BF16 rounding, MMA order,
+// bias and ReLU) is that of forward_tile: the outputs are bitwise the same.
+constexpr uint32_t WG = 4;
+
+struct InferSmem {  // offsets in bytes
+    static constexpr uint32_t W1 = FwdSmem::W1, W2 = FwdSmem::W2, W3 = FwdSmem::W3, W4 = FwdSmem::W4;
+    static constexpr uint32_t BIAS = W4 + OUT_PAD * HIDDEN * 2;               // 64 * 3 + 48 floats
+    static constexpr uint32_t GROUPS = (BIAS + (3 * HIDDEN + OUT_PAD) * 4 + 1023u) & ~1023u;
+    static constexpr uint32_t A0 = 0, H = TILE * IN * 2, GROUP = H + TILE * HIDDEN * 2;  // within a group
+    static constexpr uint32_t BAR = GROUPS + WG * GROUP;
+    static constexpr uint32_t SLOT = BAR + 8 * WG;
+    static constexpr uint32_t FLAG = SLOT + 4;
+    static constexpr uint32_t BYTES = FLAG + 4 * WG;
+};
+static_assert(InferSmem::GROUPS % 1024 == 0 && InferSmem::BAR % 8 == 0, "alignment");
+static_assert(InferSmem::BYTES <= 227 * 1024, "shared memory");
+
+__device__ void load_net_at(uint8_t* smem, const Net& net, uint32_t bias_off) {
+    load_matrix(smem + FwdSmem::W1, net.w[0], HIDDEN, HIDDEN, IN);
+    load_matrix(smem + FwdSmem::W2, net.w[1], HIDDEN, HIDDEN, HIDDEN);
+    load_matrix(smem + FwdSmem::W3, net.w[2], HIDDEN, HIDDEN, HIDDEN);
+    load_matrix(smem + FwdSmem::W4, net.w[3], OUT_PAD, OUT_PAD, HIDDEN);
+    float* bias = reinterpret_cast<float*>(smem + bias_off);
+    for (uint32_t i = threadIdx.x; i < 3 * HIDDEN + OUT_PAD; i += blockDim.x)
+        bias[i] = i < 3 * HIDDEN ? net.b[i / HIDDEN][i % HIDDEN] : net.b[3][i - 3 * HIDDEN];
+}
+
+// Features 8c .. 8c + 7 of encode(p, n, wo), computed as encode computes them.
+__device__ __forceinline__ void encode_chunk(uint32_t c, float3 p, float3 n, float3 wo, float* f) {
+    if (c < 9) {
+        const float co[3] = {p.x, p.y, p.z};
+#pragma unroll
+        for (uint32_t k = 0; k < 4; ++k) {
+            const uint32_t q = 4 * c + k, b = q / 3, a = q % 3;
+            const float s = 3.14159265f * float(1u << b);
+            __sincosf(s * co[a], &f[2 * k], &f[2 * k + 1]);
+        }
+    } else if (c == 9) {
+        f[0] = n.x; f[1] = n.y; f[2] = n.z;
+        f[3] = wo.x; f[4] = wo.y; f[5] = wo.z;
+        f[6] = p.x; f[7] = p.y;
+    } else {
+#pragma unroll
+        for (uint32_t k = 0; k < 8; ++k) f[k] = 0.0f;
+        if (c == 10) f[0] = p.z;
+    }
+}
+
+__device__ __forceinline__ void group_sync(uint32_t g) {
+    asm volatile("bar.sync %0, %1;" ::"r"(1u + g), "r"(TILE) : "memory");
+}
+
+__global__ void __launch_bounds__(TILE * WG, 1) k_infer_paths(Net net, DeviceScene scene, PathPool pool,
+                                                              uint32_t bounce, uint32_t n0, int* err) {
     extern __shared__ __align__(1024) uint8_t smem[];
-    uint32_t* slot = reinterpret_cast<uint32_t*>(smem + FwdSmem::SLOT);
-    int* sflag = reinterpret_cast<int*>(smem + FwdSmem::FLAG);
+    uint32_t* slot = reinterpret_cast<uint32_t*>(smem + InferSmem::SLOT);
+    const uint32_t g = threadIdx.x / TILE, row = threadIdx.x % TILE;
+    uint64_t* bar = reinterpret_cast<uint64_t*>(smem + InferSmem::BAR) + g;
+    int* gflag = reinterpret_cast<int*>(smem + InferSmem::FLAG) + g;
+    uint8_t* gbase = smem + InferSmem::GROUPS + g * InferSmem::GROUP;
+    const float* bias = reinterpret_cast<const float*>(smem + InferSmem::BIAS);
     const uint32_t count = min(bounce == 0 ? n0 : pool.counters[CTR_RAYS + bounce], pool.capacity);
     const uint32_t* queue = pool.queue[bounce & 1u];
-    if (threadIdx.x == 0) {
-        umma::mbar_init(reinterpret_cast<uint64_t*>(smem + FwdSmem::BAR), 1);
-        *sflag = 0;
+    if (threadIdx.x < WG) {
+        umma::mbar_init(reinterpret_cast<uint64_t*>(smem + InferSmem::BAR) + threadIdx.x, 1);
+        reinterpret_cast<int*>(smem + InferSmem::FLAG)[threadIdx.x] = 0;
     }
-    if (threadIdx.x < 32) umma::tmem_alloc(slot, 64);
-    load_net(smem, net);
+    if (threadIdx.x < 32) umma::tmem_alloc(slot, 64 * WG);
+    load_net_at(smem, net, InferSmem::BIAS);
     umma::fence_before_sync();
     __syncthreads();
     umma::fence_after_sync();
-    const uint32_t tmem = *slot;
+    const uint32_t tmem = *slot + 64u * g;  // this group's 64 columns
+    const uint32_t base = umma::smem_u32(smem);
+    const uint32_t a_off[4] = {InferSmem::GROUPS + g * InferSmem::GROUP + InferSmem::A0,
+                               InferSmem::GROUPS + g * InferSmem::GROUP + InferSmem::H,
+                               InferSmem::GROUPS + g * InferSmem::GROUP + InferSmem::H,
+                               InferSmem::GROUPS + g * InferSmem::GROUP + InferSmem::H};
+    const uint32_t w_off[4] = {FwdSmem::W1, FwdSmem::W2, FwdSmem::W3, FwdSmem::W4};
+    const uint32_t lane_base = ((threadIdx.x / 32u) % 4u) * 32u;
     uint32_t phase = 0;
-    float feat[IN], o[OUT];
-    for (uint32_t tile = blockIdx.x; tile * TILE < count; tile += gridDim.x) {
-        const uint32_t i = tile * TILE + threadIdx.x;
+    for (uint32_t tile = blockIdx.x * WG + g; tile * TILE < count; tile += gridDim.x * WG) {
+        const uint32_t i = tile * TILE + row;
         uint32_t path = 0;
         bool hit = false;
+        float3 p = make_float3(0.0f, 0.0f, 0.0f), nrm = p, wo = p;
         if (i < count) {
             path = bounce == 0 ? i : queue[i];
-            uint4 h = pool.hit[path];
+            const uint4 h = pool.hit[path];
             hit = h.x != LIGHT_NONE;
             if (hit) {
-                float4 d4 = pool.dir[path];
-                float3 dir = make_float3(d4.x, d4.y, d4.z);
-                float3 p, n;
-                hit_frame(scene, h, dir, p, n);
-                encode(unit_pos(scene, p), n, make_float3(-dir.x, -dir.y, -dir.z), feat);
+                const float4 d4 = pool.dir[path];
+                const float3 dir = make_float3(d4.x, d4.y, d4.z);
+                float3 wp;
+                hit_frame(scene, h, dir, wp, nrm);
+                p = unit_pos(scene, wp);
+                wo = make_float3(-dir.x, -dir.y, -dir.z);
             }
         }
-        if (!hit)
-            for (uint32_t c = 0; c < IN; ++c) feat[c] = 0.0f;
-        if (!forward_tile(smem, tmem, phase, feat, o, nullptr)) {
-            if (threadIdx.x == 0) atomicExch(err, 1);
-            break;
+        for (uint32_t c = 0; c < IN / 8; ++c) {
+            float f[8];
+            if (hit) encode_chunk(c, p, nrm, wo, f);
+            else
+                for (uint32_t k = 0; k < 8; ++k) f[k] = 0.0f;
+            *reinterpret_cast<uint4*>(gbase + InferSmem::A0 + kmajor_offset(row, 8 * c, IN)) = pack8(f);
         }
-        if (hit) {
-            float* dst = pool.guide_out + size_t(path) * OUT;
-            for (uint32_t c = 0; c < OUT; c += 4) *reinterpret_cast<float4*>(dst + c) = make_float4(o[c], o[c + 1], o[c + 2], o[c + 3]);
+        bool ok = true;
+        for (int l = 0; l < 4 && ok; ++l) {
+            const uint32_t k = l == 0 ? IN : HIDDEN, n = l == 3 ? OUT_PAD : HIDDEN;
+            umma::fence_async_smem();
+            umma::fence_before_sync();
+            group_sync(g);
+            if (row == 0) {
+                umma::fence_after_sync();
+                issue_layer(tmem, base + a_off[l], base + w_off[l], k, n, bar, false);
+            }
+            if (!umma::mbar_wait(bar, phase, WAIT_LIMIT)) atomicOr(gflag, 1);
+            group_sync(g);
+            umma::fence_after_sync();
+            ok = *gflag == 0;
+            phase ^= 1u;
+            if (!ok) break;
+            const float* bl = bias + l * HIDDEN;
+            if (l < 3) {
+                for (uint32_t c0 = 0; c0 < HIDDEN; c0 += 16) {
+                    float v[16];
+                    umma::tmem_ld16(umma::tmem_at(tmem, lane_base, c0), v);
+                    umma::tmem_wait_ld();
+                    for (uint32_t c = 0; c < 16; ++c) v[c] = fmaxf(v[c] + bl[c0 + c], 0.0f);
+                    *reinterpret_cast<uint4*>(gbase + InferSmem::H + kmajor_offset(row, c0, HIDDEN)) = pack8(v);
+                    *reinterpret_cast<uint4*>(gbase + InferSmem::H + kmajor_offset(row, c0 + 8, HIDDEN)) = pack8(v + 8);
+                }
+            } else {
+                for (uint32_t c0 = 0; c0 < OUT_PAD; c0 += 16) {
+                    float v[16];
+                    umma::tmem_ld16(umma::tmem_at(tmem, lane_base, c0), v);
+                    umma::tmem_wait_ld();
+                    if (hit) {
+                        float* dst = pool.guide_out + size_t(path) * OUT + c0;
+                        for (uint32_t c = 0; c < 16 && c0 + c < OUT; c += 4)
+                            *reinterpret_cast<float4*>(dst + c) =
+                                make_float4(v[c] + bl[c0 + c], v[c + 1] + bl[c0 + c + 1], v[c + 2] + bl[c0 + c + 2],
+                                            v[c + 3] + bl[c0 + c + 3]);
+                    }
+                }
+            }
+        }
+        if (!ok) {
+            if (row == 0) atomicExch(err, 1);
+            break;
         }
     }
     umma::fence_before_sync();
     __syncthreads();
     if (threadIdx.x < 32) {
-        umma::tmem_dealloc(tmem, 64);
+        umma::tmem_dealloc(*slot, 64 * WG);
         umma::tmem_relinquish();
     }
 }
@@ -669,7 +784,7 @@ static Net view(const Buffers& b) {
 cudaError_t configure(int device, int* sms) {
     cudaError_t e = cudaFuncSetAttribute(k_forward, cudaFuncAttributeMaxDynamicSharedMemorySize, FwdSmem::BYTES);
     if (e == cudaSuccess)
-        e = cudaFuncSetAttribute(k_infer_paths, cudaFuncAttributeMaxDynamicSharedMemorySize, FwdSmem::BYTES);
+        e = cudaFuncSetAttribute(k_infer_paths, cudaFuncAttributeMaxDynamicSharedMemorySize, InferSmem::BYTES);
     if (e == cudaSuccess)
         e = cudaFuncSetAttribute(k_forward_records, cudaFuncAttributeMaxDynamicSharedMemorySize, FwdSmem::BYTES);
     if (e == cudaSuccess)
@@ -715,8 +830,8 @@ void launch_adam(const Buffers& b, float lr, uint32_t step, cudaStream_t s) {
 
 void launch_infer_paths(const Buffers& b, const DeviceScene& scene, const PathPool& pool, uint32_t bounce,
                         uint32_t n0, int sms, cudaStream_t s) {
-    // Twice the SM count: a second CTA per SM hides the first's tensor-core waits.
-    k_infer_paths<<<2 * sms, TILE, FwdSmem::BYTES, s>>>(view(b), scene, pool, bounce, n0, b.err);
+    // One CTA of WG warp groups per SM: the groups hide each other's gathers and waits.
+    k_infer_paths<<<sms, TILE * WG, InferSmem::BYTES, s>>>(view(b), scene, pool, bounce, n0, b.err);
 }
 
 void launch_resolve_records(Record* recs, const uint32_t* count, uint32_t capacity, const float4* rad, cudaStream_t s) {

@@ -155,9 +155,10 @@ struct ProbeShadowSource {
         }
         return true;
     }
+    template <int S>
     __device__ __forceinline__ void closest(uint32_t i, uint2* stack) const {
-        const float a = shadow_query(scene, make_ray(org[i], dir[i]), tmaxs[i], targets[i].x, targets[i].y,
-                                     leaf_of(i), stack);
+        const float a = shadow_query<false, S>(scene, make_ray(org[i], dir[i]), tmaxs[i], targets[i].x, targets[i].y,
+                                               leaf_of(i), stack);
         if (a == -2.0f) atomicOr(flag, 1u);
         out[i] = a < 0.0f ? -1.0f : a;
     }

@@ -111,6 +111,7 @@ cudaError_t enqueue_segments(cenote_renderer* r, const cenote_scene* sc, const W
     r->pool.refill_idle = r->refill_idle;
     r->pool.top_nodes = r->top_nodes;
     r->pool.per_lane_triangles = r->per_lane_triangles;
+    r->pool.trav_variant = r->trav_variant;
     WaveParams wp{};
     wp.max_bounces = max_bounces;
     wp.light_sampling = r->light_sampling;
@@ -140,6 +141,7 @@ cudaError_t enqueue_waves(cenote_renderer* r, const cenote_scene* sc, uint32_t w
     r->pool.refill_idle = r->refill_idle;
     r->pool.top_nodes = r->top_nodes;
     r->pool.per_lane_triangles = r->per_lane_triangles;
+    r->pool.trav_variant = r->trav_variant;
     WaveParams wp{};
     wp.width = width;
     wp.height = height;

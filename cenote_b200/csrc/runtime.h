@@ -154,6 +154,7 @@ struct cenote_renderer {
     uint32_t top_nodes = 0;    // BVH nodes staged in shared memory by the traversal kernels
     uint32_t l2_window = 0;    // mark the BVH nodes persisting in L2 during this renderer's waves
     uint32_t per_lane_triangles = 0;  // 1: no warp triangle queue in the traversal kernels
+    uint32_t trav_variant = 0;        // traversal block size and stack depth (TRAV_VARIANT_*)
     float tuned_ms_per_sample = 0.0f;
     DeviceBuffer sort_order, sort_keys, sort_bins;
     DeviceBuffer aov_albedo, aov_normal, aov_depth, aov_guide;

@@ -28,7 +28,8 @@
 //    (its paths over the group's measured rate), and it opens with that
 //    group's waiting first frames, smallest first, up to the wave's time
 //    budget, then fills with the group's progressive work unless other first
-//    frames still wait. Other waves round-robin the groups with
+//    frames still wait. No progressive wave starts while first frames wait
+//    or a first-frame wave runs. Other waves round-robin the groups with
 //    progressive work, their jobs round-robin inside, each taking at most
 //    the rest of its current frame. A progressive wave holds at most about
 //    `CN_WAVE_MS` of device time (the group's paths per millisecond measured
@@ -324,17 +325,19 @@ struct cenote_server {
     }
 
     // First frames first, the cheapest first (so a burst of arrivals costs
-    // the small jobs little): the group of the cheapest job waiting for its
-    // first frame; else the next group (round robin) with progressive work;
-    // null when nothing can run.
+    // the small jobs little), a job's wait counting against its cost (so
+    // none starves): the group of the best job waiting for its first frame;
+    // else, once no first frame waits or runs, the next group (round robin)
+    // with progressive work; null when nothing should start.
     Group* pick_group(GroupKey* key, bool* first) {
         const Job* cheapest = nullptr;
         double best = 0.0;
+        const double now = now_ms(t0);
         for (auto& kv : groups)
             for (uint64_t id : kv.second.jobs) {
                 const Job& j = *jobs[id];
                 if (!wants_first(j)) continue;
-                const double c = first_cost(j);
+                const double c = first_cost(j) - (now - j.t_submit);
                 if (!cheapest || c < best) {
                     cheapest = &j;
                     best = c;
@@ -347,6 +350,10 @@ struct cenote_server {
         }
         *first = false;
         if (groups.empty()) return nullptr;
+        // No progressive wave while a first-frame wave runs: the first frames
+        // have the device to themselves (about a tenth of the work at load).
+        for (const Wave& w : waves)
+            if (w.active && w.first) return nullptr;
         for (size_t n = 0; n < groups.size(); ++n) {
             auto it = groups.begin();
             std::advance(it, (group_cursor + n) % groups.size());

@@ -48,11 +48,11 @@ __device__ __forceinline__ void shadow_begin(const DeviceScene& scene, const Ray
     walk_begin(q.w, ray);
 }
 
-template <bool COUNT = false>
+template <bool COUNT = false, int S = TRAVERSAL_STACK>
 __device__ __forceinline__ int shadow_step(const DeviceScene& scene, const Ray& ray, ShadowQuery& q, uint2* stack,
                                            uint32_t* visits = nullptr, uint32_t* tests = nullptr) {
     if (scene.node_count == 0) return WALK_DONE;
-    return walk_step<COUNT>(scene, ray, q.tm, q.w, stack, [&](uint32_t ti, float4 a, float4 b, float4 c, float& tcur) {
+    return walk_step<COUNT, S>(scene, ray, q.tm, q.w, stack, [&](uint32_t ti, float4 a, float4 b, float4 c, float& tcur) {
         if (q.have_t && ti == q.leaf) return false;  // the target itself
         float t, b1, b2;
         if (!tri_hit(ray, a, b, c, tcur, t, b1, b2)) return false;
@@ -93,16 +93,15 @@ __device__ __forceinline__ float shadow_result(const ShadowQuery& q) {
 }
 
 // The whole query for one ray: the attenuation (>= 0) when visible, -1 when
-// occluded, -2 when a traversal bound was exceeded. `stack` holds
-// TRAVERSAL_STACK entries.
-template <bool COUNT = false>
+// occluded, -2 when a traversal bound was exceeded. `stack` holds S entries.
+template <bool COUNT = false, int S = TRAVERSAL_STACK>
 __device__ __forceinline__ float shadow_query(const DeviceScene& scene, const Ray& ray, float tmax, uint32_t light,
                                               uint32_t lprim, uint32_t leaf, uint2* stack, uint32_t* visits = nullptr,
                                               uint32_t* tests = nullptr) {
     ShadowQuery q;
     shadow_begin(scene, ray, tmax, light, lprim, leaf, q);
     for (;;) {
-        int st = shadow_step<COUNT>(scene, ray, q, stack, visits, tests);
+        int st = shadow_step<COUNT, S>(scene, ray, q, stack, visits, tests);
         if (st == WALK_OVERFLOW) return -2.0f;
         if (st == WALK_DONE) return shadow_result(q);
     }

@@ -225,7 +225,7 @@ __device__ __forceinline__ uint32_t walk_bound(const DeviceScene& s) { return 4u
 // have one), push what remains of the group and intersect the child: w.g
 // becomes its inner children, w.t its hit leaves' triangles. Returns false
 // when the stack is full.
-template <bool COUNT = false>
+template <bool COUNT = false, int S = TRAVERSAL_STACK>
 __device__ __forceinline__ bool expand_node(const DeviceScene& s, const Ray& r, float tmax, Walk& w, uint2* stack,
                                             uint32_t* visits) {
     uint32_t pos = 31u - __clz(w.g.y & 0xff000000u);
@@ -233,7 +233,7 @@ __device__ __forceinline__ bool expand_node(const DeviceScene& s, const Ray& r, 
     uint32_t slot = (pos - 24u) ^ r.oct_inv;
     uint32_t ni = w.g.x + __popc(w.g.y & 0xffu & ((1u << slot) - 1u));
     if (w.g.y & 0xff000000u) {
-        if (w.sp >= TRAVERSAL_STACK) return false;
+        if (w.sp >= S) return false;
         stack[w.sp++] = w.g;
     }
     uint32_t bc, bt, im;
@@ -246,13 +246,15 @@ __device__ __forceinline__ bool expand_node(const DeviceScene& s, const Ray& r, 
 
 // One step: expand one node (or resume one postponed triangle group), then
 // test its triangles unless too few lanes of the warp would test alongside.
-// `visit` returning true stops the walk (WALK_DONE).
-template <bool COUNT = false, class Visit>
+// `visit` returning true stops the walk (WALK_DONE). `S`: the stack's
+// entries; a triangle group is postponed only while the node groups that
+// may follow (the tree's stack need) still fit behind it.
+template <bool COUNT = false, int S = TRAVERSAL_STACK, class Visit>
 __device__ __forceinline__ int walk_step(const DeviceScene& s, const Ray& r, float& tmax, Walk& w, uint2* stack,
                                          Visit&& visit, uint32_t* visits = nullptr, uint32_t* tests = nullptr) {
     if (++w.iter > walk_bound(s)) return WALK_OVERFLOW;
     if (w.g.y & 0xff000000u) {
-        if (!expand_node<COUNT>(s, r, tmax, w, stack, visits)) return WALK_OVERFLOW;
+        if (!expand_node<COUNT, S>(s, r, tmax, w, stack, visits)) return WALK_OVERFLOW;
         w.resumed = false;
     } else {
         w.t = w.g;  // a postponed triangle group came off the stack
@@ -260,7 +262,8 @@ __device__ __forceinline__ int walk_step(const DeviceScene& s, const Ray& r, flo
         w.resumed = true;
     }
     while (w.t.y & 0x00ffffffu) {
-        if (!w.resumed && w.sp < s.stack_room && uint32_t(__popc(__activemask())) < POSTPONE) {
+        if (!w.resumed && w.sp + (TRAVERSAL_STACK_DEPTH - int(s.stack_room)) < S &&
+            uint32_t(__popc(__activemask())) < POSTPONE) {
             stack[w.sp++] = w.t;
             break;
         }

@@ -233,11 +233,11 @@ __device__ __forceinline__ void tq_round(const DeviceScene& s, TriQueueSmem& sm,
 // lane has nodes left. A lane whose
 // walk has ended completes when its last queued entry has been tested.
 // Sets `overflow` when a walk hit its iteration or stack bound.
-template <bool COUNT, class Src>
+template <bool COUNT, class Src, int S = TRAVERSAL_STACK>
 __device__ __forceinline__ void queued_closest(const DeviceScene& s, TriQueueSmem& sm, Src& src, uint32_t ray_mask,
                                                bool& overflow, uint32_t* visits, uint32_t* tests) {
     TriQueue q{0u, 0u, 0u};
-    uint2 stack[TRAVERSAL_STACK];
+    uint2 stack[S];
     Walk w;
     Ray ray;
     Closest c;
@@ -271,7 +271,7 @@ __device__ __forceinline__ void queued_closest(const DeviceScene& s, TriQueueSme
         for (;;) {
             uint2 grp = make_uint2(0u, 0u);
             if (live && walking) {
-                if (++w.iter > walk_bound(s) || !expand_node<COUNT>(s, ray, c.tmax, w, stack, visits)) {
+                if (++w.iter > walk_bound(s) || !expand_node<COUNT, S>(s, ray, c.tmax, w, stack, visits)) {
                     overflow = true;
                     walking = false;
                 } else {
@@ -347,18 +347,18 @@ __device__ __forceinline__ void tq_round_any(const DeviceScene& s, TriQueueSmem&
 //   bool begin(uint32_t item, Ray& ray, AnyQuery& a)   (per lane) false: the
 //       query has no target leaf to bound it; then `closest(item)` answers it
 //       with the per-lane closest-hit walk
-//   void closest(uint32_t item, uint2* stack)           (per lane; the stack
-//       holds TRAVERSAL_STACK entries)
+//   template <int S> void closest(uint32_t item, uint2* stack)  (per lane; the
+//       stack holds S entries)
 //   void emit(uint32_t item, bool visible)              (per lane; a query
 //       whose walk hit a bound counts as occluded)
 //   uint32_t want_idle(bool drained)
 // An occluded query stops walking at once; its entries still queued are
 // skipped, and it completes when they have left the queue.
-template <bool COUNT, class Src>
+template <bool COUNT, class Src, int S = TRAVERSAL_STACK>
 __device__ __forceinline__ void queued_any(const DeviceScene& s, TriQueueSmem& sm, Src& src, bool& overflow,
                                            uint32_t* visits, uint32_t* tests) {
     TriQueue q{0u, 0u, 0u};
-    uint2 stack[TRAVERSAL_STACK];
+    uint2 stack[S];
     Walk w;
     Ray ray;
     AnyQuery a{0.0f, 0xffffffffu, LIGHT_NONE, 0u, false};
@@ -374,7 +374,7 @@ __device__ __forceinline__ void queued_any(const DeviceScene& s, TriQueueSmem& s
                 ovf = false;
                 walking = src.begin(i, ray, a) && s.node_count != 0;
                 if (!walking && !a.occluded && s.node_count != 0) {
-                    src.closest(i, stack);  // no target leaf: the per-lane closest-hit query
+                    src.template closest<S>(i, stack);  // no target leaf: the per-lane closest-hit query
                     live = false;
                 }
                 walk_begin(w, ray);
@@ -388,7 +388,7 @@ __device__ __forceinline__ void queued_any(const DeviceScene& s, TriQueueSmem& s
         for (;;) {
             uint2 grp = make_uint2(0u, 0u);
             if (live && walking && !a.occluded) {
-                if (++w.iter > walk_bound(s) || !expand_node<COUNT>(s, ray, a.tm, w, stack, visits)) {
+                if (++w.iter > walk_bound(s) || !expand_node<COUNT, S>(s, ray, a.tm, w, stack, visits)) {
                     overflow = true;
                     ovf = true;  // dropped, as the per-lane walk drops it
                     walking = false;

@@ -217,8 +217,14 @@ __device__ __forceinline__ uint32_t refill(uint32_t* counter, uint32_t count, bo
     return i < count ? i : ~0u;
 }
 
-template <bool COUNT>
-__global__ void __launch_bounds__(BLOCK, CN_TRAV_MIN_BLOCKS) k_intersect(DeviceScene scene, PathPool pool, uint32_t bounce, uint32_t n0) {
+// Traversal kernels come in launch variants: B threads per block (the same
+// registers per thread: CN_TRAV_MIN_BLOCKS * 128 / B blocks per SM) and S
+// stack entries per lane (16 halves a lane's local-memory stack, for trees
+// whose node groups need fewer). Every variant walks the same tree to the
+// same hits.
+template <bool COUNT, int B = BLOCK, int S = TRAVERSAL_STACK>
+__global__ void __launch_bounds__(B, CN_TRAV_MIN_BLOCKS * BLOCK / B)
+    k_intersect(DeviceScene scene, PathPool pool, uint32_t bounce, uint32_t n0) {
     extern __shared__ uint4 top_levels[];
     stage_top_levels(scene, top_levels, min(pool.top_nodes, TOP_NODES_MAX));  // as the launch sized it
     uint32_t visits = 0, tests = 0;
@@ -226,7 +232,7 @@ __global__ void __launch_bounds__(BLOCK, CN_TRAV_MIN_BLOCKS) k_intersect(DeviceS
     const uint32_t* queue = pool.queue[bounce & 1u];
     const uint32_t mask = bounce == 0 ? RAY_MASK_CAMERA : RAY_MASK_ALL;
     uint32_t* fetch = pool.counters + CTR_FETCH_ISECT + bounce;
-    uint2 stack[TRAVERSAL_STACK];
+    uint2 stack[S];
     Walk w;
     Ray ray;
     float tmax = 1e30f, best_b1 = 0.0f, best_b2 = 0.0f;
@@ -303,7 +309,7 @@ __global__ void __launch_bounds__(BLOCK, CN_TRAV_MIN_BLOCKS) k_intersect(DeviceS
         const uint32_t want_idle = drained ? 32u : (pool.refill_idle ? pool.refill_idle : uint32_t(CN_REFILL_IDLE));
         for (;;) {
             if (live) {
-                int st = walk_step<COUNT>(scene, ray, tmax, w, stack, visit, &visits, &tests);
+                int st = walk_step<COUNT, S>(scene, ray, tmax, w, stack, visit, &visits, &tests);
                 if (st != WALK_CONTINUE) {
                     if (st == WALK_OVERFLOW) flag_overflow(pool.counters);
                     pool.hit[path] =
@@ -354,17 +360,18 @@ struct IsectSource {
     }
 };
 
-template <bool COUNT>
-__global__ void __launch_bounds__(BLOCK, CN_TRAV_MIN_BLOCKS)
+template <bool COUNT, int B = BLOCK, int S = TRAVERSAL_STACK>
+__global__ void __launch_bounds__(B, CN_TRAV_MIN_BLOCKS * BLOCK / B)
     k_intersect_queued(DeviceScene scene, PathPool pool, uint32_t bounce, uint32_t n0) {
     extern __shared__ uint4 top_levels[];
-    __shared__ TriQueueSmem tqs[BLOCK / 32];
+    __shared__ TriQueueSmem tqs[B / 32];
     stage_top_levels(scene, top_levels, min(pool.top_nodes, TOP_NODES_MAX));
     uint32_t visits = 0, tests = 0;
     IsectSource src{pool, &scene, pool.queue[bounce & 1u], pool.counters + CTR_FETCH_ISECT + bounce,
                     bounce_paths(pool, bounce, n0), bounce};
     bool overflow = false;
-    queued_closest<COUNT>(scene, tqs[threadIdx.x >> 5], src, bounce == 0 ? RAY_MASK_CAMERA : RAY_MASK_ALL, overflow,
+    queued_closest<COUNT, IsectSource, S>(scene, tqs[threadIdx.x >> 5], src,
+                                          bounce == 0 ? RAY_MASK_CAMERA : RAY_MASK_ALL, overflow,
                           &visits, &tests);
     if (overflow) flag_overflow(pool.counters);
     if (COUNT) flush_counts(pool.counters, visits, tests);
@@ -758,14 +765,15 @@ __global__ void __launch_bounds__(BLOCK, CN_SHADE_MIN_BLOCKS) k_shade(DeviceScen
 
 // ---- trace_shadow (trace_shadow.slang:29-72) ----------------------------------------
 
-template <bool COUNT>
-__global__ void __launch_bounds__(BLOCK, CN_TRAV_MIN_BLOCKS) k_shadow(DeviceScene scene, PathPool pool, uint32_t bounce) {
+template <bool COUNT, int B = BLOCK, int S = TRAVERSAL_STACK>
+__global__ void __launch_bounds__(B, CN_TRAV_MIN_BLOCKS * BLOCK / B)
+    k_shadow(DeviceScene scene, PathPool pool, uint32_t bounce) {
     extern __shared__ uint4 top_levels[];
     stage_top_levels(scene, top_levels, min(pool.top_nodes, TOP_NODES_MAX));  // as the launch sized it
     const uint32_t count = min(pool.counters[CTR_SHADOWS + bounce], pool.capacity);
     uint32_t* fetch = pool.counters + CTR_FETCH_SHADOW + bounce;
     uint32_t visits = 0, tests = 0;
-    uint2 stack[TRAVERSAL_STACK];
+    uint2 stack[S];
     ShadowQuery q;
     Ray ray;
     float3 contrib = f3(0.0f);
@@ -791,7 +799,7 @@ __global__ void __launch_bounds__(BLOCK, CN_TRAV_MIN_BLOCKS) k_shadow(DeviceScen
         const uint32_t want_idle = drained ? 32u : (pool.refill_idle ? pool.refill_idle : uint32_t(CN_REFILL_IDLE));
         for (;;) {
             if (live) {
-                int st = shadow_step<COUNT>(scene, ray, q, stack, &visits, &tests);
+                int st = shadow_step<COUNT, S>(scene, ray, q, stack, &visits, &tests);
                 if (st == WALK_OVERFLOW) {
                     flag_overflow(pool.counters);
                     live = false;
@@ -847,11 +855,12 @@ struct ShadowSource {
         const float4 c = rec[2], r = pool.rad[path];
         pool.rad[path] = make_float4(r.x + c.x * atten, r.y + c.y * atten, r.z + c.z * atten, r.w);
     }
+    template <int S>
     __device__ __forceinline__ void closest(uint32_t i, uint2* stack) const {
         const float4* rec = reinterpret_cast<const float4*>(pool.shadows + i);
         const float4 q0 = rec[0], q1 = rec[1], q2 = rec[2], q3 = rec[3];
-        const float atten = shadow_query(scene, make_ray(xyz(q0), xyz(q1)), q0.w, __float_as_uint(q2.w),
-                                         __float_as_uint(q3.x), __float_as_uint(q3.y), stack);
+        const float atten = shadow_query<false, S>(scene, make_ray(xyz(q0), xyz(q1)), q0.w, __float_as_uint(q2.w),
+                                                   __float_as_uint(q3.x), __float_as_uint(q3.y), stack);
         if (atten == -2.0f) flag_overflow(pool.counters);
         else if (atten >= 0.0f) add(i, atten);
     }
@@ -863,17 +872,17 @@ struct ShadowSource {
     }
 };
 
-template <bool COUNT>
-__global__ void __launch_bounds__(BLOCK, CN_TRAV_MIN_BLOCKS)
+template <bool COUNT, int B = BLOCK, int S = TRAVERSAL_STACK>
+__global__ void __launch_bounds__(B, CN_TRAV_MIN_BLOCKS * BLOCK / B)
     k_shadow_queued(DeviceScene scene, PathPool pool, uint32_t bounce) {
     extern __shared__ uint4 top_levels[];
-    __shared__ TriQueueSmem tqs[BLOCK / 32];
+    __shared__ TriQueueSmem tqs[B / 32];
     stage_top_levels(scene, top_levels, min(pool.top_nodes, TOP_NODES_MAX));
     uint32_t visits = 0, tests = 0;
     ShadowSource src{scene, pool, pool.counters + CTR_FETCH_SHADOW + bounce,
                      min(pool.counters[CTR_SHADOWS + bounce], pool.capacity)};
     bool overflow = false;
-    queued_any<COUNT>(scene, tqs[threadIdx.x >> 5], src, overflow, &visits, &tests);
+    queued_any<COUNT, ShadowSource, S>(scene, tqs[threadIdx.x >> 5], src, overflow, &visits, &tests);
     if (overflow) flag_overflow(pool.counters);
     if (COUNT) flush_counts(pool.counters, visits, tests);
 }
@@ -1114,28 +1123,53 @@ void launch_count_hits(const PathPool& pool, uint32_t bounce, uint32_t n0, cudaS
     k_count_hits<<<1184, BLOCK, 0, stream>>>(pool, bounce, n0);
 }
 
+// The traversal launch variants (block size, stack entries); index =
+// PathPool::trav_variant, the grids in LaunchShape::trav.
+template <int V> struct TravVariant;
+template <> struct TravVariant<0> { static constexpr int B = 128, S = 32; };
+template <> struct TravVariant<1> { static constexpr int B = 128, S = 16; };
+template <> struct TravVariant<2> { static constexpr int B = 256, S = 32; };
+template <> struct TravVariant<3> { static constexpr int B = 256, S = 16; };
+
+// Resident blocks per SM of kernel `k` with `block` threads and `smem`
+// dynamic shared memory, times the SM count.
+template <class K>
+int grid_for(K k, int block, size_t smem, int sms) {
+    int occ = 0;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k, block, smem);
+    return sms * (occ > 0 ? occ : 1);
+}
+
+template <int V>
+void trav_grids(LaunchShape& ls, int sms) {
+    constexpr int B = TravVariant<V>::B, S = TravVariant<V>::S;
+    const size_t top = TOP_NODES_MAX * 80u;
+    ls.trav[V][TRAV_ISECT] = grid_for(k_intersect<false, B, S>, B, top, sms);
+    // The queued kernels' own shared memory leaves fewer blocks room for the
+    // staged top levels: size their grids for the launch's dynamic memory.
+    ls.trav[V][TRAV_ISECT_QUEUED] = grid_for(k_intersect_queued<false, B, S>, B, 0, sms);
+    ls.trav[V][TRAV_ISECT_QUEUED_TOP] = grid_for(k_intersect_queued<false, B, S>, B, top, sms);
+    ls.trav[V][TRAV_SHADOW] = grid_for(k_shadow<false, B, S>, B, top, sms);
+    ls.trav[V][TRAV_SHADOW_QUEUED] = grid_for(k_shadow_queued<false, B, S>, B, 0, sms);
+    ls.trav[V][TRAV_SHADOW_QUEUED_TOP] = grid_for(k_shadow_queued<false, B, S>, B, top, sms);
+}
+
 LaunchShape launch_shape(int device) {
     int sms = 148;
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
     LaunchShape ls;
     ls.block = BLOCK;
-    int occ = 0;
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_intersect<false>, BLOCK, TOP_NODES_MAX * 80u);
-    ls.grid_isect = sms * (occ > 0 ? occ : 4);
-    // The queued kernel's own shared memory leaves fewer blocks room for the
-    // staged top levels: size its grid for the launch's dynamic shared memory.
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_intersect_queued<false>, BLOCK, 0);
-    ls.grid_isect_queued = sms * (occ > 0 ? occ : 4);
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_intersect_queued<false>, BLOCK, TOP_NODES_MAX * 80u);
-    ls.grid_isect_queued_top = sms * (occ > 0 ? occ : 4);
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_shade<true, false, true>, BLOCK, 0);
-    ls.grid_shade = sms * (occ > 0 ? occ : 4);
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_shadow<false>, BLOCK, TOP_NODES_MAX * 80u);
-    ls.grid_shadow = sms * (occ > 0 ? occ : 4);
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_shadow_queued<false>, BLOCK, 0);
-    ls.grid_shadow_queued = sms * (occ > 0 ? occ : 4);
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_shadow_queued<false>, BLOCK, TOP_NODES_MAX * 80u);
-    ls.grid_shadow_queued_top = sms * (occ > 0 ? occ : 4);
+    trav_grids<0>(ls, sms);
+    trav_grids<1>(ls, sms);
+    trav_grids<2>(ls, sms);
+    trav_grids<3>(ls, sms);
+    ls.grid_isect = ls.trav[0][TRAV_ISECT];
+    ls.grid_isect_queued = ls.trav[0][TRAV_ISECT_QUEUED];
+    ls.grid_isect_queued_top = ls.trav[0][TRAV_ISECT_QUEUED_TOP];
+    ls.grid_shadow = ls.trav[0][TRAV_SHADOW];
+    ls.grid_shadow_queued = ls.trav[0][TRAV_SHADOW_QUEUED];
+    ls.grid_shadow_queued_top = ls.trav[0][TRAV_SHADOW_QUEUED_TOP];
+    ls.grid_shade = grid_for(k_shade<true, false, true>, BLOCK, 0, sms);
     ls.grid_stream = sms * 8;
     return ls;
 }
@@ -1157,17 +1191,53 @@ void launch_accumulate_segments(const PathPool& pool, const WaveSegment* segs, u
     k_accumulate_segments<<<grid, 256, 0, stream>>>(pool, segs, nseg, items, hdr);
 }
 
-void launch_intersect(const DeviceScene& scene, const PathPool& pool, uint32_t bounce, uint32_t n0,
-                      const LaunchShape& ls, bool count_visits, cudaStream_t stream) {
+template <int V>
+void launch_intersect_v(const DeviceScene& scene, const PathPool& pool, uint32_t bounce, uint32_t n0,
+                        const LaunchShape& ls, bool count_visits, cudaStream_t stream) {
+    constexpr int B = TravVariant<V>::B, S = TravVariant<V>::S;
     const size_t smem = size_t(min(pool.top_nodes, TOP_NODES_MAX)) * 80u;
     if (!scene.has_nonopaque && !pool.per_lane_triangles) {
-        const int grid = smem ? ls.grid_isect_queued_top : ls.grid_isect_queued;
-        if (count_visits) k_intersect_queued<true><<<grid, BLOCK, smem, stream>>>(scene, pool, bounce, n0);
-        else k_intersect_queued<false><<<grid, BLOCK, smem, stream>>>(scene, pool, bounce, n0);
+        const int grid = smem ? ls.trav[V][TRAV_ISECT_QUEUED_TOP] : ls.trav[V][TRAV_ISECT_QUEUED];
+        if (count_visits) k_intersect_queued<true, B, S><<<grid, B, smem, stream>>>(scene, pool, bounce, n0);
+        else k_intersect_queued<false, B, S><<<grid, B, smem, stream>>>(scene, pool, bounce, n0);
     } else if (count_visits) {
-        k_intersect<true><<<ls.grid_isect, BLOCK, smem, stream>>>(scene, pool, bounce, n0);
+        k_intersect<true, B, S><<<ls.trav[V][TRAV_ISECT], B, smem, stream>>>(scene, pool, bounce, n0);
     } else {
-        k_intersect<false><<<ls.grid_isect, BLOCK, smem, stream>>>(scene, pool, bounce, n0);
+        k_intersect<false, B, S><<<ls.trav[V][TRAV_ISECT], B, smem, stream>>>(scene, pool, bounce, n0);
+    }
+}
+
+template <int V>
+void launch_shadow_v(const DeviceScene& scene, const PathPool& pool, uint32_t bounce, const LaunchShape& ls,
+                     bool count_visits, cudaStream_t stream) {
+    constexpr int B = TravVariant<V>::B, S = TravVariant<V>::S;
+    const size_t smem = size_t(min(pool.top_nodes, TOP_NODES_MAX)) * 80u;
+    if (!scene.has_nonopaque && !pool.per_lane_triangles) {
+        const int grid = smem ? ls.trav[V][TRAV_SHADOW_QUEUED_TOP] : ls.trav[V][TRAV_SHADOW_QUEUED];
+        if (count_visits) k_shadow_queued<true, B, S><<<grid, B, smem, stream>>>(scene, pool, bounce);
+        else k_shadow_queued<false, B, S><<<grid, B, smem, stream>>>(scene, pool, bounce);
+    } else if (count_visits) {
+        k_shadow<true, B, S><<<ls.trav[V][TRAV_SHADOW], B, smem, stream>>>(scene, pool, bounce);
+    } else {
+        k_shadow<false, B, S><<<ls.trav[V][TRAV_SHADOW], B, smem, stream>>>(scene, pool, bounce);
+    }
+}
+
+// The pool's traversal variant, with a 16-entry stack replaced by 32 entries
+// for a tree whose node groups could need 16 or more.
+static uint32_t trav_variant(const DeviceScene& scene, const PathPool& pool) {
+    uint32_t v = pool.trav_variant < TRAV_VARIANTS ? pool.trav_variant : 0u;
+    if (TRAV_VARIANT_STACK[v] == 16 && TRAVERSAL_STACK_DEPTH - int(scene.stack_room) >= 16) v &= ~1u;
+    return v;
+}
+
+void launch_intersect(const DeviceScene& scene, const PathPool& pool, uint32_t bounce, uint32_t n0,
+                      const LaunchShape& ls, bool count_visits, cudaStream_t stream) {
+    switch (trav_variant(scene, pool)) {
+    case 1: launch_intersect_v<1>(scene, pool, bounce, n0, ls, count_visits, stream); break;
+    case 2: launch_intersect_v<2>(scene, pool, bounce, n0, ls, count_visits, stream); break;
+    case 3: launch_intersect_v<3>(scene, pool, bounce, n0, ls, count_visits, stream); break;
+    default: launch_intersect_v<0>(scene, pool, bounce, n0, ls, count_visits, stream); break;
     }
 }
 
@@ -1205,15 +1275,11 @@ void launch_shade(const DeviceScene& scene, const PathPool& pool, uint32_t bounc
 
 void launch_shadow(const DeviceScene& scene, const PathPool& pool, uint32_t bounce, const LaunchShape& ls,
                    bool count_visits, cudaStream_t stream) {
-    const size_t smem = size_t(min(pool.top_nodes, TOP_NODES_MAX)) * 80u;
-    if (!scene.has_nonopaque && !pool.per_lane_triangles) {
-        const int grid = smem ? ls.grid_shadow_queued_top : ls.grid_shadow_queued;
-        if (count_visits) k_shadow_queued<true><<<grid, BLOCK, smem, stream>>>(scene, pool, bounce);
-        else k_shadow_queued<false><<<grid, BLOCK, smem, stream>>>(scene, pool, bounce);
-    } else if (count_visits) {
-        k_shadow<true><<<ls.grid_shadow, BLOCK, smem, stream>>>(scene, pool, bounce);
-    } else {
-        k_shadow<false><<<ls.grid_shadow, BLOCK, smem, stream>>>(scene, pool, bounce);
+    switch (trav_variant(scene, pool)) {
+    case 1: launch_shadow_v<1>(scene, pool, bounce, ls, count_visits, stream); break;
+    case 2: launch_shadow_v<2>(scene, pool, bounce, ls, count_visits, stream); break;
+    case 3: launch_shadow_v<3>(scene, pool, bounce, ls, count_visits, stream); break;
+    default: launch_shadow_v<0>(scene, pool, bounce, ls, count_visits, stream); break;
     }
 }
 

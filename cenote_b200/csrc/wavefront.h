@@ -63,6 +63,8 @@ struct PathPool {
     // 1: traversal lanes test their own triangles even in an all-opaque scene
     // (0: the warp triangle queue, trqueue.cuh).
     uint32_t per_lane_triangles;
+    // The traversal launch variant (block size, stack entries; TRAV_VARIANT_*).
+    uint32_t trav_variant;
 };
 
 constexpr uint32_t TOP_NODES_MAX = 320;  // 25.6 KB per 128-thread block: 8 blocks still fit an SM
@@ -116,10 +118,20 @@ struct WaveSegment {
 constexpr uint32_t SORT_BINS = 2048;
 constexpr uint32_t SORT_LAYERS = 1024;
 
+// Traversal launch variants (PathPool::trav_variant): 0 = 128 threads per
+// block and 32 stack entries per lane (the default), 1 = 128 / 16,
+// 2 = 256 / 32, 3 = 256 / 16.
+constexpr uint32_t TRAV_VARIANTS = 4;
+constexpr int TRAV_VARIANT_BLOCK[TRAV_VARIANTS] = {128, 128, 256, 256};
+constexpr int TRAV_VARIANT_STACK[TRAV_VARIANTS] = {32, 16, 32, 16};
+enum : int { TRAV_ISECT, TRAV_ISECT_QUEUED, TRAV_ISECT_QUEUED_TOP, TRAV_SHADOW, TRAV_SHADOW_QUEUED,
+             TRAV_SHADOW_QUEUED_TOP, TRAV_KINDS };
+
 struct LaunchShape {
     int grid_isect, grid_isect_queued, grid_isect_queued_top, grid_shade, grid_shadow, grid_shadow_queued,
         grid_shadow_queued_top, grid_stream;
     int block;
+    int trav[TRAV_VARIANTS][TRAV_KINDS];  // persistent grids of each traversal variant
 };
 
 LaunchShape launch_shape(int device);

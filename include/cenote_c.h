@@ -273,13 +273,17 @@ typedef struct cenote_tuning {
                                   * pending triangle tests through a queue (scenes whose triangles are all
                                   * opaque; scenes with fractional opacity always test per lane) */
     float ms_per_sample;       /* autotune: device time of one sample of every pixel at the chosen setting */
+    uint32_t block_size;       /* traversal threads per block: 128 or 256 (0 = 128) */
+    uint32_t stack_depth;      /* traversal stack entries per lane: 16 or 32 (0 = 32); 16 falls back to 32
+                                * for a tree whose node groups could need more */
 } cenote_tuning;
 int32_t cenote_renderer_set_tuning(cenote_renderer* r, const cenote_tuning* tuning);
 int32_t cenote_renderer_get_tuning(cenote_renderer* r, cenote_tuning* out);
 /* Time candidate settings on `scene` at width x height (a scratch film, a few
  * hundred ms of device time at 1080p) by coordinate descent over the sort
  * mode, samples per wave, refill threshold, shared-memory top levels, the
- * L2 persistence window and per-lane or queued triangle tests;
+ * L2 persistence window, per-lane or queued triangle tests and the
+ * traversal's block size and stack depth;
  * apply the fastest to `r` and
  * report it in `out` (nullable). The renderer's stats afterwards describe the
  * last probe. */

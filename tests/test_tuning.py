@@ -130,3 +130,28 @@ def test_bad_tuning_is_refused(ctx):
         r.set_tuning(SORT_ALL, 0, 8, 0, 2)
     with pytest.raises(CenoteError):
         r.set_tuning(SORT_ALL, 0, 8, 0, 0, 2)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("name", ["chart", "textured"])
+def test_traversal_block_size_and_stack_depth_are_bitwise_invisible(ctx, name):
+    """The traversal's launch variants (128 or 256 threads per block, 16 or
+    32 stack entries per lane) walk the same tree to the same hits: films
+    are bitwise equal whichever the tuning picks, per-lane and queued
+    triangle tests alike."""
+    from cenote_b200 import Film, Renderer, Scene, scenes
+
+    spec = scenes.chart(96, 64, env_size=(256, 128)) if name == "chart" else scenes.textured(80, 45, 4, 5, size=32)
+    s = Scene(ctx, spec)
+    films = []
+    for per_lane in (0, 1):
+        for block, stack in ((128, 32), (128, 16), (256, 32), (256, 16)):
+            r = Renderer(ctx, spec.max_bounces)
+            r.set_tuning(1, 0, 0, 0, 0, per_lane, block, stack)
+            t = r.tuning()
+            assert (t["block_size"], t["stack_depth"]) == (block, stack)
+            f = Film(ctx, spec.width, spec.height)
+            r.accumulate(s, f, 4)
+            films.append(f.sums())
+    for other in films[1:]:
+        assert np.array_equal(films[0], other)
