@@ -62,6 +62,15 @@ for _name, (_fx, _w, _h, _ms) in CORPUS.items():
                                               "max depth", reference_ms_per_spp=_ms)
 
 
+BVH_BUILDERS = {"auto": 3, "host": 0, "gpu": 2, "gpu-ploc": 1}  # cenote_c.h CENOTE_BVH_*
+BVH_LABELS = {0: "host SAH (sweep below 65,536 triangles), cost-optimal collapse",
+              1: "GPU PLOC, cost-optimal collapse", 2: "GPU binned SAH, cost-optimal collapse"}
+
+
+def bvh_builder(name):
+    return BVH_BUILDERS[name]
+
+
 def make_spec(w):
     """The workload's scene. Corpus scenes come from the committed fixtures;
     their max depth (pbrt's maxdepth) replaces the workload's 0."""
@@ -413,10 +422,10 @@ def run_knob_sweep(args, w):
     """The launch knobs one at a time around the autotuner's choice: device
     ms per sample of every pixel (the better of 3 runs of 16 spp) for each
     value of each knob, the others held at the tuned setting. One JSON line."""
-    from cenote_b200 import BVH_GPU_PLOC, BVH_HOST_SAH, Context, Film, Renderer, Scene
+    from cenote_b200 import Context, Film, Renderer, Scene
 
     ctx = Context(0)
-    ctx.set_bvh_builder(BVH_GPU_PLOC if args.bvh == "gpu" else BVH_HOST_SAH)
+    ctx.set_bvh_builder(bvh_builder(args.bvh))
     scene = Scene(ctx, make_spec(w))
     W, H = w["width"], w["height"]
     r = Renderer(ctx, w["max_bounces"])
@@ -468,8 +477,9 @@ def main():
     ap.add_argument("--scene", default="large", choices=["large", "ceiling_box"], help="guiding: the scene")
     ap.add_argument("--spp", type=int, default=0, help="override the workload's spp (profiling runs)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--bvh", default="host", choices=["host", "gpu"],
-                    help="BVH builder: host binned SAH or GPU PLOC (scene prep, outside the timed region)")
+    ap.add_argument("--bvh", default="auto", choices=list(BVH_BUILDERS),
+                    help="BVH builder (scene prep, outside the timed region): auto = GPU binned SAH from 2^20 "
+                         "triangles, else host SAH; host; gpu (binned SAH); gpu-ploc")
     ap.add_argument("--tuning", default="",
                     help="pin the launch knobs instead of autotuning: sort,samples_per_wave,refill,top_nodes,l2"
                          "[,per_lane_triangles[,block_size,stack_depth]] "
@@ -498,8 +508,7 @@ def main():
 
     import torch
     import torch.distributed as dist
-    from cenote_b200 import (BVH_GPU_PLOC, BVH_HOST_SAH, PROFILE_COUNTS, PROFILE_TIMING, Context, Film, Renderer,
-                             Scene, scenes)
+    from cenote_b200 import PROFILE_COUNTS, PROFILE_TIMING, Context, Film, Renderer, Scene, scenes
 
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -512,7 +521,7 @@ def main():
     spec = make_spec(w)
     W, H, spp, maxb = w["width"], w["height"], w["spp"], w["max_bounces"]
     ctx = Context(local)
-    ctx.set_bvh_builder(BVH_GPU_PLOC if args.bvh == "gpu" else BVH_HOST_SAH)
+    ctx.set_bvh_builder(bvh_builder(args.bvh))
     t0 = time.perf_counter()
     scene = Scene(ctx, spec)
     prep_wall_ms = (time.perf_counter() - t0) * 1e3
@@ -670,7 +679,7 @@ def main():
         "rays_per_s": (rays[0] + rays[1]) * world / (ms / 1e3),
         "extension_rays_per_step": rays[0] / args.steps, "shadow_rays_per_step": rays[1] / args.steps,
         "stage_ms_per_step": {k: v / args.steps for k, v in stage.items()},
-        "scene_prep_ms": {"bvh": float(prep[0]), "bvh_builder": "GPU PLOC" if args.bvh == "gpu" else "host SAH, cost-optimal collapse",
+        "scene_prep_ms": {"bvh": float(prep[0]), "bvh_builder": BVH_LABELS[scene.bvh_builder()],
                           "env_tables": float(prep[1]), "total": float(prep[2]), "wall": prep_wall_ms},
         "roofline": {
             "kernel": "traversal (k_intersect + k_shadow)", "bound": "hbm",

@@ -129,6 +129,7 @@ EXPORTED_SYMBOLS = [
     "cenote_film_tonemap_device", "cenote_film_restore",
     "cenote_scene_add_delta_light", "cenote_renderer_set_material_sort", "cenote_renderer_set_tuning",
     "cenote_renderer_get_tuning", "cenote_renderer_autotune", "cenote_context_set_bvh_builder",
+    "cenote_scene_bvh_builder",
 ]
 
 _lib = None
@@ -179,6 +180,7 @@ def library() -> C.CDLL:
         "cenote_renderer_get_tuning": (I32, [P, P]),
         "cenote_renderer_autotune": (I32, [P, P, U32, U32, P]),
         "cenote_context_set_bvh_builder": (I32, [P, U32]),
+        "cenote_scene_bvh_builder": (U32, [P]),
         "cenote_scene_destroy": (None, [P]),
         "cenote_scene_set_camera": (I32, [P, P]),
         "cenote_scene_prep_times": (I32, [P, P]),
@@ -246,7 +248,7 @@ def _c_camera(cam: scenes.Camera) -> CameraC:
     return c
 
 
-BVH_HOST_SAH, BVH_GPU_PLOC = 0, 1
+BVH_HOST_SAH, BVH_GPU_PLOC, BVH_GPU_SAH, BVH_AUTO = 0, 1, 2, 3
 
 
 class Context:
@@ -271,7 +273,9 @@ class Context:
         _check(library().cenote_synchronize(self._h))
 
     def set_bvh_builder(self, builder: int) -> None:
-        """BVH_HOST_SAH or BVH_GPU_PLOC for scenes created from now on."""
+        """BVH_HOST_SAH, BVH_GPU_PLOC, BVH_GPU_SAH or BVH_AUTO (the default:
+        GPU_SAH from 2^20 triangles, else HOST_SAH) for scenes created from
+        now on."""
         _check(library().cenote_context_set_bvh_builder(self._h, builder))
 
     def close(self) -> None:
@@ -414,6 +418,10 @@ class Scene:
 
     def device_bytes(self) -> int:
         return int(library().cenote_scene_device_bytes(self._h))
+
+    def bvh_builder(self) -> int:
+        """The builder this scene's BVH came from (BVH_AUTO resolved)."""
+        return int(library().cenote_scene_bvh_builder(self._h))
 
     def light_records(self) -> np.ndarray:
         n = C.c_uint32()

@@ -1,7 +1,8 @@
-// GPU construction of the compressed 8-wide BVH: a binary tree by PLOC
-// (Meister & Bittner, "Parallel Locally-Ordered Clustering for Bounding Volume
-// Hierarchy Construction", IEEE TVCG 2018) over Morton-ordered triangles,
-// collapsed level by level into the node format of records.h.
+// GPU construction of the compressed 8-wide BVH: a binary tree by binned SAH
+// (top down, breadth first, the host build's split rule) or by PLOC (Meister &
+// Bittner, "Parallel Locally-Ordered Clustering for Bounding Volume Hierarchy
+// Construction", IEEE TVCG 2018) over Morton-ordered triangles, collapsed
+// level by level into the node format of records.h.
 //
 // The collapse makes the same choices as the host build (bvh_build.cpp): the
 // cost-optimal dynamic programme over the binary tree (at most eight
@@ -49,9 +50,14 @@ __device__ __forceinline__ float half_area(float3 lo, float3 hi) {
     return dx * dy + dy * dz + dz * dx;
 }
 
-// Per-triangle boxes and the centroid bounds (ordered-int atomics into cb[6]).
+// Per-triangle boxes, the centroid bounds and the scene box (ordered-int
+// atomics into cb[0..5] and cb[6..11]).
 __global__ void k_leaf_bounds(const float4* __restrict__ in, uint32_t n, float4* lo, float4* hi, uint32_t* cb) {
-    uint32_t mn[3] = {0xffffffffu, 0xffffffffu, 0xffffffffu}, mx[3] = {0u, 0u, 0u};
+    uint32_t mn[6], mx[6];
+    for (int k = 0; k < 6; ++k) {
+        mn[k] = 0xffffffffu;
+        mx[k] = 0u;
+    }
     for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
         float4 a = in[3 * size_t(i)], b = in[3 * size_t(i) + 1], c = in[3 * size_t(i) + 2];
         float3 l = make_float3(fminf(fminf(a.x, b.x), c.x), fminf(fminf(a.y, b.y), c.y), fminf(fminf(a.z, b.z), c.z));
@@ -59,12 +65,15 @@ __global__ void k_leaf_bounds(const float4* __restrict__ in, uint32_t n, float4*
         lo[i] = make_float4(l.x, l.y, l.z, __uint_as_float(NONE));
         hi[i] = make_float4(h.x, h.y, h.z, __uint_as_float(i));
         const float cen[3] = {0.5f * (l.x + h.x), 0.5f * (l.y + h.y), 0.5f * (l.z + h.z)};
+        const float bl[3] = {l.x, l.y, l.z}, bh[3] = {h.x, h.y, h.z};
         for (int k = 0; k < 3; ++k) {
             mn[k] = min(mn[k], f2ord(cen[k]));
             mx[k] = max(mx[k], f2ord(cen[k]));
+            mn[3 + k] = min(mn[3 + k], f2ord(bl[k]));
+            mx[3 + k] = max(mx[3 + k], f2ord(bh[k]));
         }
     }
-    for (int k = 0; k < 3; ++k) {
+    for (int k = 0; k < 6; ++k) {
         for (int o = 16; o > 0; o >>= 1) {
             mn[k] = min(mn[k], __shfl_xor_sync(0xffffffffu, mn[k], o));
             mx[k] = max(mx[k], __shfl_xor_sync(0xffffffffu, mx[k], o));
@@ -74,6 +83,8 @@ __global__ void k_leaf_bounds(const float4* __restrict__ in, uint32_t n, float4*
         for (int k = 0; k < 3; ++k) {
             atomicMin(cb + k, mn[k]);
             atomicMax(cb + 3 + k, mx[k]);
+            atomicMin(cb + 6 + k, mn[3 + k]);
+            atomicMax(cb + 9 + k, mx[3 + k]);
         }
     }
 }
@@ -204,6 +215,430 @@ __global__ void k_merge(Tree t, const uint32_t* __restrict__ clusters, const uin
             t.tris[out] = t.tris[a] + t.tris[b];
         }
         next[uint32_t(o >> 32)] = out;
+    }
+}
+
+// ---- binned SAH, top down and breadth first ------------------------------------------
+//
+// The host build's rule (bvh_build.cpp) on the device: every task (a range of
+// the triangle order under one binary node) bins its triangles' centroids
+// into 32 bins per axis and splits where A_left·N_left + A_right·N_right is
+// least (ties to the lower axis, then the lower bin); equal centroids, or a
+// task past 48 levels, split by position at the middle, which bounds the
+// depth. A task of at most 8,192 triangles bins and partitions in one warp
+// (bins in shared memory); larger tasks bin in chunks of 8,192 over many
+// CTAs and partition through a device-wide scan. Each level's internal nodes
+// take a contiguous index range after the n leaves (leaf j = position j of
+// the final order), so the collapse runs bottom-up level by level. Every
+// step is deterministic (integer atomics on order-preserving float codes).
+constexpr int NBIN = 32;
+constexpr uint32_t WARP_TASK_MAX = 8192;
+constexpr uint32_t CHUNK = 8192;
+constexpr uint32_t SAH_LEVEL_MAX = 48;
+constexpr int BIN_WORDS = 13;  // box lo, box hi, centroid lo, centroid hi (ordered codes), count
+constexpr int BINS_WORDS = 3 * NBIN * BIN_WORDS;
+constexpr int SAH_WARPS = 8;
+
+struct SahTask {
+    uint32_t first, count, node, pad;
+    float4 lo, hi;    // the node's box
+    float4 clo, chi;  // its centroids' bounds
+};
+
+struct SahSplit {
+    uint32_t axis;  // 0..2: binned split on that axis; 3: by position at the middle
+    uint32_t bin;   // the right side's first bin
+    uint32_t nl;    // triangles on the left
+    uint32_t pad;
+    float4 lo[2], hi[2], clo[2], chi[2];  // left, right
+};
+
+struct SahChunk {
+    uint32_t task, slot, begin, end;
+};
+
+__device__ __forceinline__ float3 centroid_of(float4 l, float4 h) {
+    return make_float3(0.5f * (l.x + h.x), 0.5f * (l.y + h.y), 0.5f * (l.z + h.z));
+}
+
+__device__ __forceinline__ float comp(float3 v, int k) { return k == 0 ? v.x : (k == 1 ? v.y : v.z); }
+__device__ __forceinline__ float comp4(float4 v, int k) { return k == 0 ? v.x : (k == 1 ? v.y : v.z); }
+
+// The host's binning: int((c - lo) · (32 / extent)), clamped.
+__device__ __forceinline__ int bin_of(float c, float lo, float scale) {
+    return min(NBIN - 1, max(0, int((c - lo) * scale)));
+}
+
+__device__ __forceinline__ void bins_init(uint32_t* bins, uint32_t lane, uint32_t lanes) {
+    for (uint32_t w = lane; w < uint32_t(BINS_WORDS); w += lanes) {
+        const uint32_t f = w % BIN_WORDS;
+        bins[w] = (f < 3 || (f >= 6 && f < 9)) ? 0xffffffffu : 0u;
+    }
+}
+
+__device__ __forceinline__ void bins_add(uint32_t* bins, const float scale[3], const float clo[3], float4 l, float4 h) {
+    const float3 c = centroid_of(l, h);
+    const uint32_t code[12] = {f2ord(l.x), f2ord(l.y), f2ord(l.z), f2ord(h.x), f2ord(h.y), f2ord(h.z),
+                               f2ord(c.x), f2ord(c.y), f2ord(c.z), f2ord(c.x), f2ord(c.y), f2ord(c.z)};
+    for (int a = 0; a < 3; ++a) {
+        uint32_t* w = bins + (a * NBIN + bin_of(comp(c, a), clo[a], scale[a])) * BIN_WORDS;
+        for (int f = 0; f < 3; ++f) atomicMin(w + f, code[f]);
+        for (int f = 3; f < 6; ++f) atomicMax(w + f, code[f]);
+        for (int f = 6; f < 9; ++f) atomicMin(w + f, code[f]);
+        for (int f = 9; f < 12; ++f) atomicMax(w + f, code[f]);
+        atomicAdd(w + 12, 1u);
+    }
+}
+
+__device__ __forceinline__ void task_scale(const SahTask& t, float scale[3], float clo[3]) {
+    for (int a = 0; a < 3; ++a) {
+        clo[a] = comp4(t.clo, a);
+        const float ext = comp4(t.chi, a) - clo[a];
+        scale[a] = ext > 0.0f ? float(NBIN) / ext : 0.0f;
+    }
+}
+
+// Large tasks: each CTA bins one chunk in shared memory and merges it into
+// the task's global bins.
+__global__ void __launch_bounds__(BLOCK) k_sah_bin_chunks(const SahChunk* __restrict__ chunks, const SahTask* __restrict__ tasks,
+                                                        const uint32_t* __restrict__ idx, const float4* __restrict__ lo0,
+                                                        const float4* __restrict__ hi0, uint32_t* gbins) {
+    __shared__ uint32_t bins[BINS_WORDS];
+    const SahChunk ch = chunks[blockIdx.x];
+    const SahTask t = tasks[ch.task];
+    float scale[3], clo[3];
+    task_scale(t, scale, clo);
+    bins_init(bins, threadIdx.x, blockDim.x);
+    __syncthreads();
+    for (uint32_t i = ch.begin + threadIdx.x; i < ch.end; i += blockDim.x) {
+        const uint32_t p = idx[i];
+        bins_add(bins, scale, clo, lo0[p], hi0[p]);
+    }
+    __syncthreads();
+    uint32_t* g = gbins + size_t(ch.slot) * BINS_WORDS;
+    for (uint32_t w = threadIdx.x; w < uint32_t(BINS_WORDS); w += blockDim.x) {
+        const uint32_t f = w % BIN_WORDS, b = w / BIN_WORDS;
+        if (bins[b * BIN_WORDS + 12] == 0u) continue;
+        if (f == 12) atomicAdd(g + w, bins[w]);
+        else if (f < 3 || (f >= 6 && f < 9)) atomicMin(g + w, bins[w]);
+        else atomicMax(g + w, bins[w]);
+    }
+}
+
+__global__ void k_sah_bins_init(uint32_t* gbins, uint32_t sets) {
+    for (uint32_t w = blockIdx.x * blockDim.x + threadIdx.x; w < sets * uint32_t(BINS_WORDS); w += gridDim.x * blockDim.x) {
+        const uint32_t f = w % BIN_WORDS;
+        gbins[w] = (f < 3 || (f >= 6 && f < 9)) ? 0xffffffffu : 0u;
+    }
+}
+
+struct Box6 {
+    float3 lo, hi;
+};
+
+__device__ __forceinline__ Box6 box_empty() {
+    const float inf = __int_as_float(0x7f800000);
+    return {make_float3(inf, inf, inf), make_float3(-inf, -inf, -inf)};
+}
+__device__ __forceinline__ Box6 box_union(Box6 a, Box6 b) {
+    return {make_float3(fminf(a.lo.x, b.lo.x), fminf(a.lo.y, b.lo.y), fminf(a.lo.z, b.lo.z)),
+            make_float3(fmaxf(a.hi.x, b.hi.x), fmaxf(a.hi.y, b.hi.y), fmaxf(a.hi.z, b.hi.z))};
+}
+__device__ __forceinline__ Box6 box_shfl(Box6 b, int src, bool up, int delta) {
+    Box6 o;
+    if (up) {
+        o.lo = make_float3(__shfl_up_sync(0xffffffffu, b.lo.x, delta), __shfl_up_sync(0xffffffffu, b.lo.y, delta),
+                           __shfl_up_sync(0xffffffffu, b.lo.z, delta));
+        o.hi = make_float3(__shfl_up_sync(0xffffffffu, b.hi.x, delta), __shfl_up_sync(0xffffffffu, b.hi.y, delta),
+                           __shfl_up_sync(0xffffffffu, b.hi.z, delta));
+    } else {
+        o.lo = make_float3(__shfl_down_sync(0xffffffffu, b.lo.x, delta), __shfl_down_sync(0xffffffffu, b.lo.y, delta),
+                           __shfl_down_sync(0xffffffffu, b.lo.z, delta));
+        o.hi = make_float3(__shfl_down_sync(0xffffffffu, b.hi.x, delta), __shfl_down_sync(0xffffffffu, b.hi.y, delta),
+                           __shfl_down_sync(0xffffffffu, b.hi.z, delta));
+    }
+    (void)src;
+    return o;
+}
+__device__ __forceinline__ Box6 box_reduce(Box6 b) {
+    for (int o = 16; o > 0; o >>= 1) {
+        Box6 x;
+        x.lo = make_float3(__shfl_xor_sync(0xffffffffu, b.lo.x, o), __shfl_xor_sync(0xffffffffu, b.lo.y, o),
+                           __shfl_xor_sync(0xffffffffu, b.lo.z, o));
+        x.hi = make_float3(__shfl_xor_sync(0xffffffffu, b.hi.x, o), __shfl_xor_sync(0xffffffffu, b.hi.y, o),
+                           __shfl_xor_sync(0xffffffffu, b.hi.z, o));
+        b = box_union(b, x);
+    }
+    return b;
+}
+__device__ __forceinline__ float box_area(Box6 b) {
+    const float dx = fmaxf(b.hi.x - b.lo.x, 0.0f), dy = fmaxf(b.hi.y - b.lo.y, 0.0f), dz = fmaxf(b.hi.z - b.lo.z, 0.0f);
+    return dx * dy + dy * dz + dz * dx;
+}
+
+// Bin (axis, b): its triangles' box and centroid bounds (empty when count is 0).
+__device__ __forceinline__ uint32_t bin_read(const uint32_t* bins, int axis, int b, Box6* box, Box6* cbox) {
+    const uint32_t* w = bins + (axis * NBIN + b) * BIN_WORDS;
+    const uint32_t n = w[12];
+    if (n == 0u) {
+        *box = box_empty();
+        *cbox = box_empty();
+        return 0u;
+    }
+    box->lo = make_float3(ord2f(w[0]), ord2f(w[1]), ord2f(w[2]));
+    box->hi = make_float3(ord2f(w[3]), ord2f(w[4]), ord2f(w[5]));
+    cbox->lo = make_float3(ord2f(w[6]), ord2f(w[7]), ord2f(w[8]));
+    cbox->hi = make_float3(ord2f(w[9]), ord2f(w[10]), ord2f(w[11]));
+    return n;
+}
+
+__device__ __forceinline__ uint32_t lane_id() { return threadIdx.x & 31u; }
+
+// One warp per task: bin (or take the chunk passes' bins), choose the split,
+// and record the children's counts, boxes and centroid bounds.
+__global__ void __launch_bounds__(SAH_WARPS * 32) k_sah_decide(const SahTask* __restrict__ tasks, uint32_t count,
+                                                                const uint32_t* __restrict__ slots,
+                                                                const uint32_t* __restrict__ gbins,
+                                                                const uint32_t* __restrict__ idx,
+                                                                const float4* __restrict__ lo0,
+                                                                const float4* __restrict__ hi0, uint32_t by_position,
+                                                                SahSplit* splits, uint32_t* internal) {
+    extern __shared__ uint32_t sah_smem[];
+    const uint32_t wib = threadIdx.x / 32u, lane = lane_id();
+    const uint32_t w = blockIdx.x * SAH_WARPS + wib;
+    if (w >= count) return;
+    uint32_t* bins = sah_smem + wib * BINS_WORDS;
+    const SahTask t = tasks[w];
+    float scale[3], clo[3];
+    task_scale(t, scale, clo);
+    const uint32_t slot = slots ? slots[w] : NONE;
+    if (slot != NONE) {
+        for (uint32_t k = lane; k < uint32_t(BINS_WORDS); k += 32u) bins[k] = gbins[size_t(slot) * BINS_WORDS + k];
+    } else {
+        bins_init(bins, lane, 32u);
+        __syncwarp();
+        for (uint32_t i = t.first + lane; i < t.first + t.count; i += 32u) {
+            const uint32_t p = idx[i];
+            bins_add(bins, scale, clo, lo0[p], hi0[p]);
+        }
+    }
+    __syncwarp();
+    const float inf = __int_as_float(0x7f800000);
+    float best = inf;
+    uint32_t best_axis = 3u, best_bin = 0u;
+    if (!by_position) {
+        for (int a = 0; a < 3; ++a) {
+            if (!(scale[a] > 0.0f)) continue;
+            Box6 b, cb;
+            uint32_t n = bin_read(bins, a, int(lane), &b, &cb);
+            Box6 pre = b, suf = b;
+            uint32_t npre = n, nsuf = n;
+            for (int d = 1; d < 32; d <<= 1) {
+                const Box6 u = box_shfl(pre, 0, true, d);
+                const uint32_t nu = __shfl_up_sync(0xffffffffu, npre, d);
+                const Box6 v = box_shfl(suf, 0, false, d);
+                const uint32_t nv = __shfl_down_sync(0xffffffffu, nsuf, d);
+                if (lane >= uint32_t(d)) {
+                    pre = box_union(pre, u);
+                    npre += nu;
+                }
+                if (lane + uint32_t(d) < 32u) {
+                    suf = box_union(suf, v);
+                    nsuf += nv;
+                }
+            }
+            const Box6 left = box_shfl(pre, 0, true, 1);  // bins [0, lane)
+            const uint32_t nl = __shfl_up_sync(0xffffffffu, npre, 1);
+            if (lane >= 1u && nl > 0u && nsuf > 0u) {
+                const float c = box_area(left) * float(nl) + box_area(suf) * float(nsuf);
+                if (c < best) {
+                    best = c;
+                    best_axis = uint32_t(a);
+                    best_bin = lane;
+                }
+            }
+        }
+        for (int o = 16; o > 0; o >>= 1) {  // least (cost, axis, bin)
+            const float oc = __shfl_xor_sync(0xffffffffu, best, o);
+            const uint32_t oa = __shfl_xor_sync(0xffffffffu, best_axis, o);
+            const uint32_t ob = __shfl_xor_sync(0xffffffffu, best_bin, o);
+            if (oc < best || (oc == best && (oa < best_axis || (oa == best_axis && ob < best_bin)))) {
+                best = oc;
+                best_axis = oa;
+                best_bin = ob;
+            }
+        }
+    }
+    Box6 side_box[2] = {box_empty(), box_empty()}, side_cbox[2] = {box_empty(), box_empty()};
+    uint32_t nl;
+    if (best_axis < 3u) {
+        Box6 b, cb;
+        const uint32_t n = bin_read(bins, int(best_axis), int(lane), &b, &cb);
+        const int s = lane < best_bin ? 0 : 1;
+        side_box[s] = b;
+        side_cbox[s] = cb;
+        uint32_t nleft = lane < best_bin ? n : 0u;
+        for (int o = 16; o > 0; o >>= 1) nleft += __shfl_xor_sync(0xffffffffu, nleft, o);
+        nl = nleft;
+    } else {
+        nl = t.count / 2u;
+        for (uint32_t i = t.first + lane; i < t.first + t.count; i += 32u) {
+            const uint32_t p = idx[i];
+            const float4 l = lo0[p], h = hi0[p];
+            const float3 c = centroid_of(l, h);
+            const int s = (i - t.first) < nl ? 0 : 1;
+            side_box[s] = box_union(side_box[s], Box6{make_float3(l.x, l.y, l.z), make_float3(h.x, h.y, h.z)});
+            side_cbox[s] = box_union(side_cbox[s], Box6{c, c});
+        }
+    }
+    for (int s = 0; s < 2; ++s) {
+        side_box[s] = box_reduce(side_box[s]);
+        side_cbox[s] = box_reduce(side_cbox[s]);
+    }
+    if (lane == 0u) {
+        SahSplit sp;
+        sp.axis = best_axis;
+        sp.bin = best_bin;
+        sp.nl = nl;
+        sp.pad = 0u;
+        for (int s = 0; s < 2; ++s) {
+            sp.lo[s] = make_float4(side_box[s].lo.x, side_box[s].lo.y, side_box[s].lo.z, 0.0f);
+            sp.hi[s] = make_float4(side_box[s].hi.x, side_box[s].hi.y, side_box[s].hi.z, 0.0f);
+            sp.clo[s] = make_float4(side_cbox[s].lo.x, side_cbox[s].lo.y, side_cbox[s].lo.z, 0.0f);
+            sp.chi[s] = make_float4(side_cbox[s].hi.x, side_cbox[s].hi.y, side_cbox[s].hi.z, 0.0f);
+        }
+        splits[w] = sp;
+        internal[w] = (nl > 1u ? 1u : 0u) + (t.count - nl > 1u ? 1u : 0u);
+    }
+}
+
+__device__ __forceinline__ bool goes_left(const SahTask& t, const SahSplit& sp, uint32_t i, float4 l, float4 h) {
+    if (sp.axis >= 3u) return (i - t.first) < sp.nl;
+    const int a = int(sp.axis);
+    const float lo = comp4(t.clo, a), ext = comp4(t.chi, a) - lo;
+    const float scale = ext > 0.0f ? float(NBIN) / ext : 0.0f;
+    return uint32_t(bin_of(comp(centroid_of(l, h), a), lo, scale)) < sp.bin;
+}
+
+// Small tasks: one warp partitions its range stably (left side first).
+__global__ void __launch_bounds__(SAH_WARPS * 32) k_sah_partition(const SahTask* __restrict__ tasks, uint32_t count,
+                                                                   const uint32_t* __restrict__ slots,
+                                                                   const SahSplit* __restrict__ splits,
+                                                                   const uint32_t* __restrict__ idx,
+                                                                   const float4* __restrict__ lo0,
+                                                                   const float4* __restrict__ hi0, uint32_t* idx_next) {
+    const uint32_t lane = lane_id();
+    const uint32_t w = blockIdx.x * SAH_WARPS + threadIdx.x / 32u;
+    if (w >= count || (slots && slots[w] != NONE)) return;
+    const SahTask t = tasks[w];
+    const SahSplit sp = splits[w];
+    uint32_t base_l = t.first, base_r = t.first + sp.nl;
+    const uint32_t below = (1u << lane) - 1u;
+    for (uint32_t i0 = t.first; i0 < t.first + t.count; i0 += 32u) {
+        const uint32_t i = i0 + lane;
+        const bool valid = i < t.first + t.count;
+        uint32_t p = 0u;
+        bool left = false;
+        if (valid) {
+            p = idx[i];
+            left = goes_left(t, sp, i, lo0[p], hi0[p]);
+        }
+        const uint32_t ml = __ballot_sync(0xffffffffu, valid && left), mr = __ballot_sync(0xffffffffu, valid && !left);
+        const uint32_t dest = left ? base_l + __popc(ml & below) : base_r + __popc(mr & below);
+        // The sides repeat the decision's binning exactly; the bound only
+        // keeps a broken split inside the task (the collapse's triangle
+        // count then rejects the tree).
+        if (valid && dest < t.first + t.count) idx_next[dest] = p;
+        base_l += __popc(ml);
+        base_r += __popc(mr);
+    }
+}
+
+// Large tasks: side flags per chunk, a device-wide exclusive scan, then a
+// scatter by each position's rank within its task.
+__global__ void __launch_bounds__(BLOCK) k_sah_flags(const SahChunk* __restrict__ chunks, const SahTask* __restrict__ tasks,
+                                                   const SahSplit* __restrict__ splits, const uint32_t* __restrict__ idx,
+                                                   const float4* __restrict__ lo0, const float4* __restrict__ hi0,
+                                                   uint32_t* flags) {
+    const SahChunk ch = chunks[blockIdx.x];
+    const SahTask t = tasks[ch.task];
+    const SahSplit sp = splits[ch.task];
+    for (uint32_t i = ch.begin + threadIdx.x; i < ch.end; i += blockDim.x) {
+        const uint32_t p = idx[i];
+        flags[i] = goes_left(t, sp, i, lo0[p], hi0[p]) ? 1u : 0u;
+    }
+}
+
+__global__ void __launch_bounds__(BLOCK) k_sah_scatter(const SahChunk* __restrict__ chunks, const SahTask* __restrict__ tasks,
+                                                     const SahSplit* __restrict__ splits, const uint32_t* __restrict__ idx,
+                                                     const uint32_t* __restrict__ flags, const uint32_t* __restrict__ rank,
+                                                     uint32_t* idx_next) {
+    const SahChunk ch = chunks[blockIdx.x];
+    const SahTask t = tasks[ch.task];
+    const uint32_t nl = splits[ch.task].nl, r0 = rank[t.first];
+    for (uint32_t i = ch.begin + threadIdx.x; i < ch.end; i += blockDim.x) {
+        const uint32_t r = rank[i] - r0;
+        const uint32_t dest = flags[i] ? t.first + r : t.first + nl + (i - t.first - r);
+        if (dest < t.first + t.count) idx_next[dest] = idx[i];
+    }
+}
+
+// Write every task's binary node, its leaf children and its internal
+// children's tasks (numbered from node_base in task order).
+__global__ void k_sah_emit(const SahTask* __restrict__ tasks, uint32_t count, const SahSplit* __restrict__ splits,
+                           const uint32_t* __restrict__ offs, uint32_t node_base, const uint32_t* __restrict__ idx_next,
+                           const float4* __restrict__ lo0, const float4* __restrict__ hi0, Tree tr, SahTask* next,
+                           uint32_t* max_count) {
+    for (uint32_t w = blockIdx.x * blockDim.x + threadIdx.x; w < count; w += gridDim.x * blockDim.x) {
+        const SahTask t = tasks[w];
+        const SahSplit sp = splits[w];
+        const uint32_t n[2] = {sp.nl, t.count - sp.nl}, first[2] = {t.first, t.first + sp.nl};
+        uint32_t o = offs[w], id[2], big = 0u;
+        for (int s = 0; s < 2; ++s) {
+            if (n[s] > 1u) {
+                id[s] = node_base + o;
+                SahTask c;
+                c.first = first[s];
+                c.count = n[s];
+                c.node = id[s];
+                c.pad = 0u;
+                c.lo = sp.lo[s];
+                c.hi = sp.hi[s];
+                c.clo = sp.clo[s];
+                c.chi = sp.chi[s];
+                next[o++] = c;
+                big = max(big, n[s]);
+            } else {
+                id[s] = first[s];
+                const uint32_t tri = idx_next[first[s]];
+                const float4 l = lo0[tri], h = hi0[tri];
+                tr.lo[id[s]] = make_float4(l.x, l.y, l.z, __uint_as_float(NONE));
+                tr.hi[id[s]] = make_float4(h.x, h.y, h.z, __uint_as_float(tri));
+                tr.tris[id[s]] = 1u;
+            }
+        }
+        tr.lo[t.node] = make_float4(t.lo.x, t.lo.y, t.lo.z, __uint_as_float(id[0]));
+        tr.hi[t.node] = make_float4(t.hi.x, t.hi.y, t.hi.z, __uint_as_float(id[1]));
+        tr.tris[t.node] = t.count;
+        if (big) atomicMax(max_count, big);
+    }
+}
+
+// The root task from the scene bounds (cb: centroid lo/hi, then box lo/hi,
+// as ordered codes), and the identity order.
+__global__ void k_sah_root(const uint32_t* __restrict__ cb, uint32_t n, SahTask* task, uint32_t* idx) {
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) idx[i] = i;
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+        SahTask t;
+        t.first = 0u;
+        t.count = n;
+        t.node = n;
+        t.pad = 0u;
+        t.clo = make_float4(ord2f(cb[0]), ord2f(cb[1]), ord2f(cb[2]), 0.0f);
+        t.chi = make_float4(ord2f(cb[3]), ord2f(cb[4]), ord2f(cb[5]), 0.0f);
+        t.lo = make_float4(ord2f(cb[6]), ord2f(cb[7]), ord2f(cb[8]), 0.0f);
+        t.hi = make_float4(ord2f(cb[9]), ord2f(cb[10]), ord2f(cb[11]), 0.0f);
+        *task = t;
     }
 }
 
@@ -529,25 +964,19 @@ cudaError_t sync_read(void* host, const void* dev, size_t bytes, cudaStream_t s)
 
 }  // namespace
 
-cudaError_t build_wide_bvh_gpu(const float4* in, uint32_t n, GpuBvh* out, cudaStream_t s) {
-    out->node_count = 0;
-    out->depth = 0;
-    out->nodes = nullptr;
-    out->tris = nullptr;
-    if (n == 0) return cudaSuccess;
+namespace {
+
+// PLOC binary tree over the Morton order (leaf j holds the j-th triangle of
+// that order); `order` receives the node ranges a bottom-up pass takes.
+cudaError_t binary_ploc(uint32_t n, const float4* lo0, const float4* hi0, const uint32_t* cb, Tree t, uint32_t* root,
+                        std::vector<std::pair<uint32_t, uint32_t>>* order, cudaStream_t s) {
     const size_t total = 2 * size_t(n) - 1;
-    Scratch lo0, hi0, cb, keys, keys2, vals, vals2, sort_tmp, tlo, thi, ttris, cl0, cl1, nn, flags, offs, scan_tmp;
-    BVH_TRY(lo0.alloc(n * 16ull));
-    BVH_TRY(hi0.alloc(n * 16ull));
-    BVH_TRY(cb.alloc(32));
-    const uint32_t cb_init[8] = {0xffffffffu, 0xffffffffu, 0xffffffffu, 0u, 0u, 0u, 0u, 0u};
-    BVH_TRY(cudaMemcpyAsync(cb.p, cb_init, 32, cudaMemcpyHostToDevice, s));
-    k_leaf_bounds<<<grid_for(n), BLOCK, 0, s>>>(in, n, lo0.as<float4>(), hi0.as<float4>(), cb.as<uint32_t>());
+    Scratch keys, keys2, vals, vals2, sort_tmp, cl0, cl1, nn, flags, offs, scan_tmp;
     BVH_TRY(keys.alloc(n * 8ull));
     BVH_TRY(keys2.alloc(n * 8ull));
     BVH_TRY(vals.alloc(n * 4ull));
     BVH_TRY(vals2.alloc(n * 4ull));
-    k_morton<<<grid_for(n), BLOCK, 0, s>>>(lo0.as<float4>(), hi0.as<float4>(), n, cb.as<uint32_t>(),
+    k_morton<<<grid_for(n), BLOCK, 0, s>>>(lo0, hi0, n, cb,
                                            keys.as<unsigned long long>(), vals.as<uint32_t>());
     size_t sort_bytes = 0;
     BVH_TRY(cub::DeviceRadixSort::SortPairs(nullptr, sort_bytes, keys.as<unsigned long long>(),
@@ -561,16 +990,12 @@ cudaError_t build_wide_bvh_gpu(const float4* in, uint32_t n, GpuBvh* out, cudaSt
     keys2.alloc(0);
     sort_tmp.alloc(0);
 
-    BVH_TRY(tlo.alloc(total * 16));
-    BVH_TRY(thi.alloc(total * 16));
-    BVH_TRY(ttris.alloc(total * 4));
-    Tree t{tlo.as<float4>(), thi.as<float4>(), ttris.as<uint32_t>()};
     BVH_TRY(cl0.alloc(n * 4ull));
     BVH_TRY(cl1.alloc(n * 4ull));
     BVH_TRY(nn.alloc(n * 4ull));
     BVH_TRY(flags.alloc(n * 8ull));
     BVH_TRY(offs.alloc(n * 8ull));
-    k_place_leaves<<<grid_for(n), BLOCK, 0, s>>>(vals2.as<uint32_t>(), n, lo0.as<float4>(), hi0.as<float4>(), t,
+    k_place_leaves<<<grid_for(n), BLOCK, 0, s>>>(vals2.as<uint32_t>(), n, lo0, hi0, t,
                                                  cl0.as<uint32_t>());
     size_t scan_bytes = 0;
     BVH_TRY(cub::DeviceScan::ExclusiveSum(nullptr, scan_bytes, flags.as<unsigned long long>(),
@@ -580,7 +1005,7 @@ cudaError_t build_wide_bvh_gpu(const float4* in, uint32_t n, GpuBvh* out, cudaSt
     // PLOC: merge mutual nearest neighbours until one cluster is left. Every
     // round merges at least the globally closest pair, so at most n - 1 rounds.
     uint32_t m = n, node_next = n;
-    std::vector<uint32_t> round_end;  // node_next after each merge round
+    order->assign(1, {0u, n});  // the leaves, then each merge round's nodes
     uint32_t* cur = cl0.as<uint32_t>();
     uint32_t* nxt = cl1.as<uint32_t>();
     for (uint32_t round = 0; m > 1; ++round) {
@@ -597,22 +1022,165 @@ cudaError_t build_wide_bvh_gpu(const float4* in, uint32_t n, GpuBvh* out, cudaSt
         const unsigned long long tot = last[0] + last[1];
         const uint32_t made = uint32_t(tot & 0xffffffffull), kept = uint32_t(tot >> 32);
         if (made == 0 || kept >= m || node_next + made > total) return cudaErrorUnknown;
+        order->push_back({node_next, node_next + made});
         node_next += made;
-        round_end.push_back(node_next);
         m = kept;
         uint32_t* tmp = cur;
         cur = nxt;
         nxt = tmp;
     }
-    uint32_t root = 0;
-    BVH_TRY(sync_read(&root, cur, 4, s));
+    BVH_TRY(sync_read(root, cur, 4, s));
     nn.alloc(0);
     flags.alloc(0);
     offs.alloc(0);
     scan_tmp.alloc(0);
 
-    // The collapse's costs, bottom-up: the leaves, then each merge round's
-    // nodes in the order the rounds made them.
+    return cudaSuccess;
+}
+
+// Binned SAH binary tree, top down one level at a time (leaf j holds the
+// triangle at position j of the final order).
+cudaError_t binary_sah(uint32_t n, const float4* lo0, const float4* hi0, const uint32_t* cb, Tree t, uint32_t* root,
+                       std::vector<std::pair<uint32_t, uint32_t>>* order, cudaStream_t s) {
+    Scratch idx0, idx1, tasks0, tasks1, splits, internal, offs, scan_tmp, maxc, flags, rank, rank_tmp, gbins, chunks,
+        slots;
+    BVH_TRY(idx0.alloc(n * 4ull));
+    BVH_TRY(idx1.alloc(n * 4ull));
+    if (n == 1) {
+        BVH_TRY(cudaMemsetAsync(idx0.p, 0, 4, s));
+        k_place_leaves<<<1, 32, 0, s>>>(idx0.as<uint32_t>(), 1u, lo0, hi0, t, idx1.as<uint32_t>());
+        *root = 0u;
+        order->assign(1, {0u, 1u});
+        return cudaGetLastError();
+    }
+    const size_t max_tasks = n / 2 + 1;  // every task holds at least two triangles
+    BVH_TRY(tasks0.alloc(max_tasks * sizeof(SahTask)));
+    BVH_TRY(tasks1.alloc(max_tasks * sizeof(SahTask)));
+    BVH_TRY(splits.alloc(max_tasks * sizeof(SahSplit)));
+    BVH_TRY(internal.alloc(max_tasks * 4));
+    BVH_TRY(offs.alloc(max_tasks * 4));
+    BVH_TRY(maxc.alloc(4));
+    BVH_TRY(flags.alloc(n * 4ull));
+    BVH_TRY(rank.alloc(n * 4ull));
+    size_t scan_bytes = 0, rank_bytes = 0;
+    BVH_TRY(cub::DeviceScan::ExclusiveSum(nullptr, scan_bytes, internal.as<uint32_t>(), offs.as<uint32_t>(),
+                                          int(max_tasks), s));
+    BVH_TRY(scan_tmp.alloc(scan_bytes));
+    BVH_TRY(cub::DeviceScan::ExclusiveSum(nullptr, rank_bytes, flags.as<uint32_t>(), rank.as<uint32_t>(), int(n), s));
+    BVH_TRY(rank_tmp.alloc(rank_bytes));
+    const uint32_t max_large = n / WARP_TASK_MAX + 1;
+    BVH_TRY(gbins.alloc(size_t(max_large) * BINS_WORDS * 4));
+    BVH_TRY(chunks.alloc((size_t(n) / CHUNK + 2 * max_large) * sizeof(SahChunk)));
+    BVH_TRY(slots.alloc(max_tasks * 4));
+    k_sah_root<<<grid_for(n), BLOCK, 0, s>>>(cb, n, tasks0.as<SahTask>(), idx0.as<uint32_t>());
+    BVH_TRY(cudaGetLastError());
+    *root = n;
+    std::vector<std::pair<uint32_t, uint32_t>> levels;
+    SahTask* cur = tasks0.as<SahTask>();
+    SahTask* nxt = tasks1.as<SahTask>();
+    uint32_t* idx = idx0.as<uint32_t>();
+    uint32_t* idx_next = idx1.as<uint32_t>();
+    uint32_t count = 1, base = n, largest = n;
+    std::vector<SahTask> host_tasks;
+    std::vector<SahChunk> host_chunks;
+    std::vector<uint32_t> host_slots;
+    const size_t smem = size_t(SAH_WARPS) * BINS_WORDS * 4;
+    for (uint32_t level = 0; count > 0; ++level) {
+        if (level > n) return cudaErrorUnknown;
+        levels.push_back({base, base + count});
+        // Tasks above the one-warp size bin in chunks over many CTAs.
+        const bool large = largest > WARP_TASK_MAX;
+        uint32_t nchunks = 0;
+        if (large) {
+            host_tasks.resize(count);
+            BVH_TRY(sync_read(host_tasks.data(), cur, count * sizeof(SahTask), s));
+            host_chunks.clear();
+            host_slots.assign(count, NONE);
+            uint32_t nslots = 0;
+            for (uint32_t k = 0; k < count; ++k) {
+                if (host_tasks[k].count <= WARP_TASK_MAX) continue;
+                host_slots[k] = nslots;
+                for (uint32_t b0 = host_tasks[k].first; b0 < host_tasks[k].first + host_tasks[k].count; b0 += CHUNK)
+                    host_chunks.push_back({k, nslots, b0, std::min(b0 + CHUNK, host_tasks[k].first + host_tasks[k].count)});
+                ++nslots;
+            }
+            nchunks = uint32_t(host_chunks.size());
+            BVH_TRY(cudaMemcpyAsync(chunks.p, host_chunks.data(), nchunks * sizeof(SahChunk), cudaMemcpyHostToDevice, s));
+            BVH_TRY(cudaMemcpyAsync(slots.p, host_slots.data(), count * 4ull, cudaMemcpyHostToDevice, s));
+            k_sah_bins_init<<<grid_for(nslots * uint32_t(BINS_WORDS)), BLOCK, 0, s>>>(gbins.as<uint32_t>(), nslots);
+            k_sah_bin_chunks<<<nchunks, BLOCK, 0, s>>>(chunks.as<SahChunk>(), cur, idx, lo0, hi0, gbins.as<uint32_t>());
+        }
+        const uint32_t* slot_ptr = large ? slots.as<uint32_t>() : nullptr;
+        const uint32_t warps_grid = (count + SAH_WARPS - 1) / SAH_WARPS;
+        k_sah_decide<<<warps_grid, SAH_WARPS * 32, smem, s>>>(cur, count, slot_ptr, gbins.as<uint32_t>(), idx, lo0, hi0,
+                                                              level >= SAH_LEVEL_MAX ? 1u : 0u, splits.as<SahSplit>(),
+                                                              internal.as<uint32_t>());
+        BVH_TRY(cub::DeviceScan::ExclusiveSum(scan_tmp.p, scan_bytes, internal.as<uint32_t>(), offs.as<uint32_t>(),
+                                              int(count), s));
+        if (large) {
+            k_sah_flags<<<nchunks, BLOCK, 0, s>>>(chunks.as<SahChunk>(), cur, splits.as<SahSplit>(), idx, lo0, hi0,
+                                                  flags.as<uint32_t>());
+            BVH_TRY(cub::DeviceScan::ExclusiveSum(rank_tmp.p, rank_bytes, flags.as<uint32_t>(), rank.as<uint32_t>(),
+                                                  int(n), s));
+            k_sah_scatter<<<nchunks, BLOCK, 0, s>>>(chunks.as<SahChunk>(), cur, splits.as<SahSplit>(), idx,
+                                                    flags.as<uint32_t>(), rank.as<uint32_t>(), idx_next);
+        }
+        k_sah_partition<<<warps_grid, SAH_WARPS * 32, 0, s>>>(cur, count, slot_ptr, splits.as<SahSplit>(), idx, lo0,
+                                                              hi0, idx_next);
+        BVH_TRY(cudaMemsetAsync(maxc.p, 0, 4, s));
+        const uint32_t next_base = base + count;
+        k_sah_emit<<<grid_for(count), BLOCK, 0, s>>>(cur, count, splits.as<SahSplit>(), offs.as<uint32_t>(), next_base,
+                                                     idx_next, lo0, hi0, t, nxt, maxc.as<uint32_t>());
+        BVH_TRY(cudaGetLastError());
+        uint32_t last[3];
+        BVH_TRY(cudaMemcpyAsync(&last[0], offs.as<uint32_t>() + (count - 1), 4, cudaMemcpyDeviceToHost, s));
+        BVH_TRY(cudaMemcpyAsync(&last[1], internal.as<uint32_t>() + (count - 1), 4, cudaMemcpyDeviceToHost, s));
+        BVH_TRY(cudaMemcpyAsync(&last[2], maxc.p, 4, cudaMemcpyDeviceToHost, s));
+        BVH_TRY(cudaStreamSynchronize(s));
+        const uint32_t made = last[0] + last[1];
+        if (next_base + made > 2 * n - 1 || made > max_tasks) return cudaErrorUnknown;
+        // Positions outside this level's tasks are final (leaves), so only
+        // the tasks' ranges need carrying from one order to the next.
+        std::swap(idx, idx_next);
+        std::swap(cur, nxt);
+        base = next_base;
+        count = made;
+        largest = last[2];
+    }
+    order->assign(1, {0u, n});
+    for (size_t k = levels.size(); k-- > 0;) order->push_back(levels[k]);
+    return cudaSuccess;
+}
+
+}  // namespace
+
+cudaError_t build_wide_bvh_gpu(const float4* in, uint32_t n, GpuBvh* out, cudaStream_t s, bool sah) {
+    out->node_count = 0;
+    out->depth = 0;
+    out->nodes = nullptr;
+    out->tris = nullptr;
+    if (n == 0) return cudaSuccess;
+    const size_t total = 2 * size_t(n) - 1;
+    Scratch lo0, hi0, cb, tlo, thi, ttris;
+    BVH_TRY(lo0.alloc(n * 16ull));
+    BVH_TRY(hi0.alloc(n * 16ull));
+    BVH_TRY(cb.alloc(48));
+    const uint32_t cb_init[12] = {0xffffffffu, 0xffffffffu, 0xffffffffu, 0u, 0u, 0u,
+                                  0xffffffffu, 0xffffffffu, 0xffffffffu, 0u, 0u, 0u};
+    BVH_TRY(cudaMemcpyAsync(cb.p, cb_init, 48, cudaMemcpyHostToDevice, s));
+    k_leaf_bounds<<<grid_for(n), BLOCK, 0, s>>>(in, n, lo0.as<float4>(), hi0.as<float4>(), cb.as<uint32_t>());
+    BVH_TRY(tlo.alloc(total * 16));
+    BVH_TRY(thi.alloc(total * 16));
+    BVH_TRY(ttris.alloc(total * 4));
+    Tree t{tlo.as<float4>(), thi.as<float4>(), ttris.as<uint32_t>()};
+    uint32_t root = 0;
+    std::vector<std::pair<uint32_t, uint32_t>> order;  // node ranges, children's before their parents'
+    if (sah)
+        BVH_TRY(binary_sah(n, lo0.as<float4>(), hi0.as<float4>(), cb.as<uint32_t>(), t, &root, &order, s));
+    else
+        BVH_TRY(binary_ploc(n, lo0.as<float4>(), hi0.as<float4>(), cb.as<uint32_t>(), t, &root, &order, s));
+
+    // The collapse's costs, bottom-up over the builder's node ranges.
     Scratch ccost, chow, csplit;
     BVH_TRY(ccost.alloc(total * 32));
     BVH_TRY(chow.alloc(total * 8));
@@ -626,13 +1194,9 @@ cudaError_t build_wide_bvh_gpu(const float4* in, uint32_t n, GpuBvh* out, cudaSt
         const double dy = std::max(double(root_box[1].y) - double(root_box[0].y), 0.0);
         const double dz = std::max(double(root_box[1].z) - double(root_box[0].z), 0.0);
         const double inv_root = 1.0 / std::max(dx * dy + dy * dz + dz * dx, 1e-300);
-        uint32_t first = 0, end = n;
-        k_collapse_cost<<<grid_for(end - first), BLOCK, 0, s>>>(t, cp, first, end, inv_root);
-        for (uint32_t e : round_end) {
-            first = end;
-            end = e;
-            if (end > first) k_collapse_cost<<<grid_for(end - first), BLOCK, 0, s>>>(t, cp, first, end, inv_root);
-        }
+        for (const auto& r : order)
+            if (r.second > r.first)
+                k_collapse_cost<<<grid_for(r.second - r.first), BLOCK, 0, s>>>(t, cp, r.first, r.second, inv_root);
         BVH_TRY(cudaGetLastError());
     }
 

@@ -1,6 +1,6 @@
-// GPU construction of the compressed 8-wide BVH (bvh_gpu.cu): PLOC binary
-// build over Morton-ordered triangles, collapsed on the device into the node
-// format the traversal kernels walk.
+// GPU construction of the compressed 8-wide BVH (bvh_gpu.cu): a binned SAH or
+// PLOC binary build, collapsed on the device into the node format the
+// traversal kernels walk.
 #pragma once
 #include <cstdint>
 #include <cuda_runtime.h>
@@ -17,8 +17,9 @@ struct GpuBvh {
 };
 
 // `in`: n triangles as three float4 each (corners, identity in the w lanes:
-// instance, primitive, flags), device memory. Synchronises `s`.
-cudaError_t build_wide_bvh_gpu(const float4* in, uint32_t n, GpuBvh* out, cudaStream_t s);
+// instance, primitive, flags), device memory. `sah`: the binned SAH binary
+// tree (32 bins per axis at every level), else PLOC. Synchronises `s`.
+cudaError_t build_wide_bvh_gpu(const float4* in, uint32_t n, GpuBvh* out, cudaStream_t s, bool sah);
 
 // Each emissive triangle's leaf index: light_leaf[geometry[inst].light + prim] = leaf.
 void launch_light_leaves(const float4* tris, uint32_t n, const GeomRecord* geometry, uint32_t* light_leaf,

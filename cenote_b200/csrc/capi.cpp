@@ -282,7 +282,7 @@ void* cenote_context_stream(cenote_context* ctx) { return ctx ? static_cast<void
 
 int32_t cenote_context_set_bvh_builder(cenote_context* ctx, uint32_t builder) {
     CN_CHECK(ctx, CENOTE_E_INVALID_ARGUMENT, "null context");
-    CN_CHECK(builder <= CENOTE_BVH_GPU_PLOC, CENOTE_E_INVALID_ARGUMENT, "unknown BVH builder");
+    CN_CHECK(builder <= CENOTE_BVH_AUTO, CENOTE_E_INVALID_ARGUMENT, "unknown BVH builder");
     ctx->bvh_builder = builder;
     return CENOTE_OK;
 }
@@ -511,7 +511,11 @@ int32_t cenote_scene_create_textured(cenote_context* ctx, const cenote_object* o
     CN_CUDA(cudaMemcpyAsync(blayers->ptr, layers.data(), layers.size(), cudaMemcpyHostToDevice, ctx->stream));
     CN_CUDA(cudaMemsetAsync(bleaf->ptr, 0xff, std::max<size_t>(1, sc->lights.size()) * 4, ctx->stream));
     uint32_t bvh_depth = 0;  // stack entries the tree's node groups may take
-    if (ctx->bvh_builder == CENOTE_BVH_GPU_PLOC && !tris.empty()) {
+    uint32_t builder = ctx->bvh_builder;
+    if (builder == CENOTE_BVH_AUTO)
+        builder = tris.size() >= CENOTE_BVH_AUTO_GPU_MIN_TRIANGLES ? CENOTE_BVH_GPU_SAH : CENOTE_BVH_HOST_SAH;
+    sc->bvh_builder = builder;
+    if (builder != CENOTE_BVH_HOST_SAH && !tris.empty()) {
         // Triangles in input order, identity in the w lanes; the device
         // builds the binary tree, collapses it and lays out the leaves.
         std::vector<float> packed(tris.size() * 12);
@@ -527,7 +531,7 @@ int32_t cenote_scene_create_textured(cenote_context* ctx, const cenote_object* o
         CN_CUDA(staged.alloc(packed.size() * 4));
         CN_CUDA(cudaMemcpyAsync(staged.ptr, packed.data(), packed.size() * 4, cudaMemcpyHostToDevice, ctx->stream));
         GpuBvh g{};
-        CN_CUDA(build_wide_bvh_gpu(staged.as<float4>(), tri_count, &g, ctx->stream));
+        CN_CUDA(build_wide_bvh_gpu(staged.as<float4>(), tri_count, &g, ctx->stream, builder == CENOTE_BVH_GPU_SAH));
         bnodes = sc->adopt(g.nodes, size_t(g.node_count) * sizeof(WideNode));
         btris = sc->adopt(g.tris, size_t(tri_count) * 48);
         node_count = g.node_count;
@@ -733,6 +737,8 @@ int32_t cenote_scene_prep_times(cenote_scene* scene, float* ms3) {
 }
 
 uint64_t cenote_scene_device_bytes(cenote_scene* scene) { return scene ? scene->device_bytes : 0; }
+
+uint32_t cenote_scene_bvh_builder(cenote_scene* scene) { return scene ? scene->bvh_builder : CENOTE_BVH_HOST_SAH; }
 
 int32_t cenote_scene_light_records(cenote_scene* scene, void* out_records, uint32_t* out_count) {
     CN_CHECK(scene && out_count, CENOTE_E_INVALID_ARGUMENT, "null argument");

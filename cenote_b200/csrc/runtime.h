@@ -92,7 +92,7 @@ struct cenote_context {
     std::mutex mu;
     // L2 persistence (this context's own set-aside; nothing outlives it).
     size_t l2_persist_max = 0, l2_window_max = 0, l2_set_aside = 0;
-    uint32_t bvh_builder = CENOTE_BVH_HOST_SAH;  // for scenes created from now on
+    uint32_t bvh_builder = CENOTE_BVH_AUTO;  // for scenes created from now on
 };
 
 struct cenote_scene {
@@ -107,6 +107,7 @@ struct cenote_scene {
     double env_power = 0.0;
     float select_prob = 0.0f;
     float prep_ms[3] = {0, 0, 0};
+    uint32_t bvh_builder = CENOTE_BVH_HOST_SAH;  // the builder this scene's BVH came from
     uint64_t device_bytes = 0;
     DeviceBuffer* env_marginal = nullptr;
     DeviceBuffer* env_conditional = nullptr;

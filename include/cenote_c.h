@@ -202,12 +202,21 @@ void cenote_context_destroy(cenote_context* ctx);
 /* The context's cudaStream_t, for callers that time or order work on it. */
 void* cenote_context_stream(cenote_context* ctx);
 int32_t cenote_synchronize(cenote_context* ctx);
-/* How scenes created from now on build their BVH: on the host (SAH binary
- * tree, cost-optimal collapse to 8-wide nodes; the default) or on the GPU
- * (PLOC over Morton order, collapsed on the device). Either tree gives the
- * same closest hits. */
+/* How scenes created from now on build their BVH. Every builder's binary
+ * tree is collapsed by the same cost-optimal programme into 8-wide nodes, and
+ * every tree gives the same closest hits.
+ *   HOST_SAH: on the host; binned SAH above 65,536 triangles per range, the
+ *             exact SAH sweep below.
+ *   GPU_PLOC: on the device; PLOC over the Morton order.
+ *   GPU_SAH:  on the device; binned SAH (32 bins per axis) at every level.
+ *   AUTO:     (the default) GPU_SAH for scenes of at least 2^20 triangles,
+ *             where the host build takes seconds and binning loses nothing,
+ *             else HOST_SAH, whose exact sweep suits small scenes. */
 #define CENOTE_BVH_HOST_SAH 0u
 #define CENOTE_BVH_GPU_PLOC 1u
+#define CENOTE_BVH_GPU_SAH 2u
+#define CENOTE_BVH_AUTO 3u
+#define CENOTE_BVH_AUTO_GPU_MIN_TRIANGLES (1u << 20)
 int32_t cenote_context_set_bvh_builder(cenote_context* ctx, uint32_t builder);
 
 /* ---- scene (Scene::new, scene/mod.rs:254) ------------------------------------ */
@@ -233,6 +242,9 @@ int32_t cenote_scene_set_camera(cenote_scene* scene, const cenote_camera* camera
 int32_t cenote_scene_prep_times(cenote_scene* scene, float* ms3);
 /* Device bytes the scene holds (BVH + triangles + records + textures + env). */
 uint64_t cenote_scene_device_bytes(cenote_scene* scene);
+/* The builder the scene's BVH came from (CENOTE_BVH_HOST_SAH, _GPU_PLOC or
+ * _GPU_SAH: AUTO resolved by the scene's triangle count). */
+uint32_t cenote_scene_bvh_builder(cenote_scene* scene);
 /* The light list as built (80-byte records of lights.rs:79-109), and its length. */
 int32_t cenote_scene_light_records(cenote_scene* scene, void* out_records, uint32_t* out_count);
 /* The environment tables built on the device (environment.rs:221-233 layout),
