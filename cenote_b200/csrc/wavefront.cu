@@ -436,13 +436,6 @@ __device__ __forceinline__ Spawn spawn_point(const GeomRecord& g, uint32_t prim,
     return sp;
 }
 
-__device__ __forceinline__ void load_geom(const GeomRecord* rec, GeomRecord& g) {
-    const uint4* src = reinterpret_cast<const uint4*>(rec);
-    uint4* dst = reinterpret_cast<uint4*>(&g);
-#pragma unroll
-    for (int k = 0; k < int(sizeof(GeomRecord) / 16); ++k) dst[k] = __ldg(src + k);
-}
-
 __device__ __forceinline__ void load_material(const Material* rec, Material& m) {
     const uint4* src = reinterpret_cast<const uint4*>(rec);
     uint4* dst = reinterpret_cast<uint4*>(&m);
@@ -531,8 +524,10 @@ __global__ void __launch_bounds__(BLOCK, CN_SHADE_MIN_BLOCKS) k_shade(DeviceScen
                 uint2 ps = pool.ps[path];
                 const uint32_t pixel = ps.x, sample = ps.y;
                 float3 origin = xyz(pool.org[path]);
-                GeomRecord g;
-                load_geom(scene.geometry + inst, g);
+                // The instance record is read field by field where used (all
+                // lanes of a sorted warp mostly share it, so the reads hit L1):
+                // a register copy of its 144 bytes made the kernel spill more.
+                const GeomRecord& g = scene.geometry[inst];
                 Material mat;
                 load_material(scene.materials + inst, mat);
                 if (!LAYERS) {

@@ -10,6 +10,7 @@
 #include <cstdint>
 #include <cstring>
 #include <vector>
+#include "textures.h"
 #include "vec.h"
 
 namespace oracle {
@@ -309,28 +310,32 @@ inline V3f direction_from_uv(float u, float v) {  // environment.slang:80-85
 // unit the reference and the kernels sample through computes it (measured
 // on a B200, see textures.h): the texel-space coordinate in FP32, rounded
 // to 1/256 of a texel (halves up), less half a texel; its integer part picks
-// the texels and its fraction is the weight.
+// the texels and its fraction the unit's integer weights, and the FP32
+// texels filter as unit_filter_float does.
 inline V3f env_bilinear(const EnvTables& e, float u, float v) {
-    auto axis = [](float c, uint32_t n, long* i, float* a) {
+    auto axis = [](float c, uint32_t n, long* i, int32_t* a) {
         const float xs = c * float(n);
         const long q = long(std::floor(double(xs) * 256.0 + 0.5)) - 128;
         *i = q >= 0 ? q / 256 : -((-q + 255) / 256);
-        *a = float(q - *i * 256) / 256.0f;
+        *a = int32_t(q - *i * 256);
     };
     long ix, iy;
-    float ax, ay;
+    int32_t ax, ay;
     axis(u, e.width, &ix, &ax);
     axis(v, e.height, &iy, &ay);
     auto wrap = [&](long i) { long w = long(e.width); return size_t(((i % w) + w) % w); };
     auto clampi = [&](long j) { return size_t(std::min(std::max(j, 0L), long(e.height) - 1)); };
-    size_t x0 = wrap(ix), x1 = wrap(ix + 1), y0 = clampi(iy), y1 = clampi(iy + 1);
-    auto tex = [&](size_t xx, size_t yy) {
-        const float* t = &e.texels[4 * (yy * e.width + xx)];
-        return V3f(t[0], t[1], t[2]);
-    };
-    V3f a = tex(x0, y0) * (1.0f - ax) + tex(x1, y0) * ax;
-    V3f b = tex(x0, y1) * (1.0f - ax) + tex(x1, y1) * ax;
-    return a * (1.0f - ay) + b * ay;
+    const size_t xs[4] = {wrap(ix), wrap(ix + 1), wrap(ix), wrap(ix + 1)};
+    const size_t ys[4] = {clampi(iy), clampi(iy), clampi(iy + 1), clampi(iy + 1)};
+    int32_t w[4];
+    unit_weights(ax, ay, w);
+    float out[3];
+    for (int c = 0; c < 3; ++c) {
+        float t[4];
+        for (int k = 0; k < 4; ++k) t[k] = e.texels[4 * (ys[k] * e.width + xs[k]) + c];
+        out[c] = unit_filter_float(t, w);
+    }
+    return V3f(out[0], out[1], out[2]);
 }
 
 inline V3f env_radiance(const EnvTables& e, V3f d) {  // environment.slang:88-90

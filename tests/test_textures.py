@@ -10,6 +10,8 @@ renders to the oracle.
 """
 from __future__ import annotations
 
+import pathlib
+
 import numpy as np
 import pytest
 
@@ -212,6 +214,26 @@ def test_spec_archive_keeps_textures(tmp_path):
         assert np.array_equal(np.asarray(a.data), np.asarray(b.data))
 
 
+def test_oracle_reproduces_the_texture_units_taps():
+    """Taps the B200 texture unit returned, committed as golden vectors
+    (tests/golden/texture_unit_taps.npz, written by
+    oracle/measure_texture_unit.py): a random 32x32 texture per format, taps
+    at every texel centre, on texel-centre rows (one axis filtered) and at
+    random coordinates. The oracle's model of the unit reproduces every tap
+    of every format bit for bit (BC4: red; BC5: red and green)."""
+    g = np.load(pathlib.Path(__file__).parent / "golden" / "texture_unit_taps.npz")
+    codes = {"rgba8_srgb": T.TEX_RGBA8_SRGB, "rgba8_unorm": T.TEX_RGBA8_UNORM, "rgba32f": T.TEX_RGBA32F,
+             "bc1_srgb": T.TEX_BC1_SRGB, "bc1_unorm": T.TEX_BC1_UNORM, "bc4": T.TEX_BC4_UNORM, "bc5": T.TEX_BC5_UNORM}
+    for name, fmt in codes.items():
+        data = g[name + "_data"]
+        if fmt == T.TEX_RGBA32F:
+            data = data.view(np.float32).reshape(32, 32, 4)
+        tex = T.Texture(fmt, 32, 32, data)
+        ch = {"bc4": 1, "bc5": 2}.get(name, 4)
+        got = oracle.texture_sample(tex, g[name + "_uv"], 0)[:, :ch]
+        assert np.array_equal(got, g[name + "_taps"][:, :ch]), name
+
+
 # ---- the texture unit against the oracle -----------------------------------------------
 
 
@@ -243,8 +265,8 @@ def probe_scene(ctx, tex):
 def test_gpu_texture_taps_match_oracle(ctx, kind):
     """Taps of the texture unit against the oracle's model of it: decoded
     texels at texel centres and filtered taps at arbitrary coordinates
-    (repeat addressing) are bit-equal for every 8-bit and BC format, sRGB
-    storage included. The slot readers (colour conversion, scalar, tangent
+    (repeat addressing) are bit-equal for every format, sRGB storage and
+    RGBA32F included. The slot readers (colour conversion, scalar, tangent
     normal) then run in FP32 on both sides: within 1e-5."""
     tex = make_texture(kind)
     rng = np.random.default_rng(2)
@@ -256,10 +278,7 @@ def test_gpu_texture_taps_match_oracle(ctx, kind):
     for where in (centres, uv):
         got = sc.probe_texture(0, where, 0)[:, :channels]
         ref = oracle.texture_sample(tex, where, 0)[:, :channels]
-        if kind == "rgba32f":
-            assert np.abs(got - ref).max() <= 1e-5 * 4.0
-        else:
-            assert np.array_equal(got, ref), np.abs(got - ref).max()
+        assert np.array_equal(got, ref), np.abs(got - ref).max()
     for mode in (1, 2, 3):
         got = sc.probe_texture(0, uv, mode)
         ref = oracle.texture_sample(tex, uv, mode)
