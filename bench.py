@@ -348,13 +348,27 @@ def run_serving(args):
     for j in warm:
         server.wait(j)
     ids = []
+    done = {}  # job -> its status when it finished; finished jobs are released at once
+    live = []
+
+    def harvest():
+        nonlocal live
+        keep = []
+        for j in live:
+            s_ = server.poll(j)
+            if s_.state in (JOB_DONE, JOB_FAILED):
+                done[j] = s_
+                server.release(j)  # a finished job's host-side result is not kept
+            else:
+                keep.append(j)
+        live = keep
+
     with ClockSampler(0) as clocks:
         t0 = time.perf_counter()
         if args.concurrency:
             # Closed loop: `concurrency` jobs in flight, each completion
             # submitting the stream's next job at once.
             pending = list(jobs)
-            live = []
             while pending or live:
                 while pending and len(live) < args.concurrency:
                     _, n, w, h, spp = pending.pop(0)
@@ -362,17 +376,28 @@ def run_serving(args):
                     ids.append(j)
                     live.append(j)
                 time.sleep(0.002)  # each poll takes the server's lock: keep the loop light
-                live = [j for j in live if server.poll(j).state not in (JOB_DONE, JOB_FAILED)]
+                harvest()
         else:
+            last = 0.0
             for at, n, w, h, spp in jobs:
-                delay = at - (time.perf_counter() - t0)
-                if delay > 0:
-                    time.sleep(delay)
-                ids.append(server.submit(resident[n], w, h, spp, specs[n][1]))
-        for j in ids:
-            server.wait(j, 1800000.0)
+                while True:
+                    now = time.perf_counter() - t0
+                    if now >= at:
+                        break
+                    if now - last > 0.25 and at - now > 0.005:  # a poll per live job: keep it rare
+                        harvest()
+                        last = time.perf_counter() - t0
+                    else:
+                        time.sleep(min(at - now, 0.002))
+                j = server.submit(resident[n], w, h, spp, specs[n][1])
+                ids.append(j)
+                live.append(j)
+        deadline = time.perf_counter() + 1800.0
+        while live and time.perf_counter() < deadline:
+            harvest()
+            time.sleep(0.05)
     counters = server.stats()
-    st = [server.poll(j) for j in ids]
+    st = [done[j] if j in done else server.poll(j) for j in ids]
     ttff = np.array([s.first_frame_ms - s.submit_ms for s in st])
     burst_end = max(s.first_frame_ms for s in st[:args.concurrency]) if args.concurrency else 0.0
     ttt = np.array([s.done_ms - s.submit_ms for s in st])

@@ -72,30 +72,51 @@ __global__ void k_env_rows(const double* __restrict__ weight, const double* __re
 }
 
 // The flat total over every weight in row-major order, the marginal CDF and
-// the power integral: sequential by definition. One warp stages 1,024
-// weights at a time into shared memory with coalesced loads; lane 0 adds them
-// in order, so the sum rounds exactly like the host's left fold.
-__global__ void __launch_bounds__(32) k_env_marginal(const double* __restrict__ weight, const double* __restrict__ row_sum,
+// the power integral: sequential by definition. Two warps: the second stages
+// the next 1,024 weights into shared memory with coalesced loads while lane 0
+// of the first adds the current 1,024 in order (eight loads ahead of the
+// dependent adds), so the sum rounds exactly like the host's left fold and
+// only the chain of FP64 adds is serial.
+__global__ void __launch_bounds__(64) k_env_marginal(const double* __restrict__ weight, const double* __restrict__ row_sum,
                                                      const double* __restrict__ lum_sum, const double* __restrict__ solid,
                                                      float* __restrict__ marginal, double* __restrict__ out, uint32_t w,
                                                      uint32_t h) {
-    __shared__ double buf[1024];
-    const uint32_t lane = threadIdx.x;
+    __shared__ double buf[2][1024];
+    const uint32_t warp = threadIdx.x / 32u, lane = threadIdx.x % 32u;
     const size_t n = size_t(w) * h;
-    double total = 0.0;
-    for (size_t base = 0; base < n; base += 1024) {
+    const size_t chunks = (n + 1023) / 1024;
+    auto stage = [&](size_t c) {
+        const size_t base = c * 1024;
         const size_t m = n - base < 1024 ? n - base : 1024;
+        double* dst = buf[c & 1];
 #pragma unroll 8
         for (uint32_t k = 0; k < 32; ++k) {
-            size_t j = size_t(k) * 32 + lane;
-            if (j < m) buf[j] = weight[base + j];
+            const size_t j = size_t(k) * 32 + lane;
+            if (j < m) dst[j] = weight[base + j];
         }
-        __syncwarp();
-        if (lane == 0)
-            for (size_t j = 0; j < m; ++j) total = __dadd_rn(total, buf[j]);
-        __syncwarp();
+    };
+    double total = 0.0;
+    if (warp == 1 && chunks > 0) stage(0);
+    __syncthreads();
+    for (size_t c = 0; c < chunks; ++c) {
+        if (warp == 1) {
+            if (c + 1 < chunks) stage(c + 1);
+        } else if (lane == 0) {
+            const size_t m = n - c * 1024 < 1024 ? n - c * 1024 : 1024;
+            const double* src = buf[c & 1];
+            size_t j = 0;
+            for (; j + 8 <= m; j += 8) {
+                double v[8];
+#pragma unroll
+                for (int k = 0; k < 8; ++k) v[k] = src[j + k];
+#pragma unroll
+                for (int k = 0; k < 8; ++k) total = __dadd_rn(total, v[k]);
+            }
+            for (; j < m; ++j) total = __dadd_rn(total, src[j]);
+        }
+        __syncthreads();
     }
-    if (lane != 0) return;
+    if (threadIdx.x != 0) return;
     marginal[0] = 0.0f;
     double run = 0.0;
     for (uint32_t r = 0; r < h; ++r) {
@@ -135,7 +156,7 @@ void launch_env_tables(const float4* texels, const double* sin_theta, const doub
     k_env_lum<<<grid, 256, 0, stream>>>(texels, lum, uint32_t(n));
     k_env_weight<<<grid, 256, 0, stream>>>(lum, sin_theta, weight, w, h);
     k_env_rows<<<(h + 63) / 64, 64, 0, stream>>>(weight, lum, row_sum, lum_sum, conditional, w, h);
-    k_env_marginal<<<1, 32, 0, stream>>>(weight, row_sum, lum_sum, solid, marginal, totals, w, h);
+    k_env_marginal<<<1, 64, 0, stream>>>(weight, row_sum, lum_sum, solid, marginal, totals, w, h);
     k_env_pdfs<<<grid, 256, 0, stream>>>(weight, totals, pdfs, w, h);
 }
 

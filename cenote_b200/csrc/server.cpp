@@ -68,6 +68,9 @@ namespace {
 
 // Device time a progressive wave aims at; a first frame waits about this
 // long for the wave in flight.
+#ifndef CN_FIRST_EXCLUSIVE
+#define CN_FIRST_EXCLUSIVE 1  // a first-frame wave keeps the other lane idle
+#endif
 #ifndef CN_WAVE_MS
 #define CN_WAVE_MS 10.0
 #endif
@@ -352,8 +355,9 @@ struct cenote_server {
         if (groups.empty()) return nullptr;
         // No progressive wave while a first-frame wave runs: the first frames
         // have the device to themselves (about a tenth of the work at load).
-        for (const Wave& w : waves)
-            if (w.active && w.first) return nullptr;
+        if (CN_FIRST_EXCLUSIVE)
+            for (const Wave& w : waves)
+                if (w.active && w.first) return nullptr;
         for (size_t n = 0; n < groups.size(); ++n) {
             auto it = groups.begin();
             std::advance(it, (group_cursor + n) % groups.size());
