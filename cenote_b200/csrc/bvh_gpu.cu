@@ -661,7 +661,10 @@ struct Collapse {
     uint8_t* split8;
 };
 
-constexpr float C_NODE = 1.0f, C_PRIM = 0.3f;
+#ifndef CN_COLLAPSE_C_PRIM
+#define CN_COLLAPSE_C_PRIM 0.3f
+#endif
+constexpr float C_NODE = 1.0f, C_PRIM = CN_COLLAPSE_C_PRIM;
 
 __global__ void k_collapse_cost(Tree t, Collapse c, uint32_t first, uint32_t end, double inv_root) {
     for (uint32_t b = first + blockIdx.x * blockDim.x + threadIdx.x; b < end; b += gridDim.x * blockDim.x) {
