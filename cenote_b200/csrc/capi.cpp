@@ -24,6 +24,8 @@
 #include "wavefront.h"
 
 namespace cn {
+void launch_env_cuts(const float* marginal, const float* conditional, uint32_t w, uint32_t h, uint32_t* cut,
+                     cudaStream_t stream);
 void launch_env_tables(const float4* texels, const double* sin_theta, const double* solid, uint32_t w, uint32_t h,
                        double* scratch, float* marginal, float* conditional, float* pdfs, double* totals,
                        cudaStream_t stream);
@@ -598,10 +600,14 @@ int32_t cenote_scene_create_textured(cenote_context* ctx, const cenote_object* o
     CN_CUDA(err);
     sc->env_pdfs = sc->add(en * 4, &err);
     CN_CUDA(err);
+    sc->env_cut = sc->add(size_t(eh + 1) * (ENV_CUTS + 1) * 4, &err);
+    CN_CUDA(err);
     double* totals = scratch.as<double>() + 2 * en + 2 * size_t(eh);
     launch_env_tables(btex->as<float4>(), brow->as<double>(), brow->as<double>() + eh, ew, eh, scratch.as<double>(),
                       sc->env_marginal->as<float>(), sc->env_conditional->as<float>(), sc->env_pdfs->as<float>(), totals,
                       ctx->stream);
+    launch_env_cuts(sc->env_marginal->as<float>(), sc->env_conditional->as<float>(), ew, eh, sc->env_cut->as<uint32_t>(),
+                    ctx->stream);
     CN_CUDA(cudaGetLastError());
     double host_totals[2] = {0, 0};
     CN_CUDA(cudaMemcpyAsync(host_totals, totals, 16, cudaMemcpyDeviceToHost, ctx->stream));
@@ -657,6 +663,7 @@ int32_t cenote_scene_create_textured(cenote_context* ctx, const cenote_object* o
     ds.bsdf_tables = ctx->tables.as<float>();
     ds.env_marginal = sc->env_marginal->as<float>();
     ds.env_conditional = sc->env_conditional->as<float>();
+    ds.env_cut = sc->env_cut->as<uint32_t>();
     ds.env_pdfs = sc->env_pdfs->as<float>();
     ds.env_tex = sc->env_tex;
     ds.env_w = ew;

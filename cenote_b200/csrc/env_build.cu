@@ -13,6 +13,8 @@
 #include <cstdint>
 #include <mutex>
 
+#include "records.h"
+
 namespace cn {
 namespace {
 
@@ -139,7 +141,36 @@ __global__ void k_env_pdfs(const double* __restrict__ weight, const double* __re
         pdfs[i] = __double2float_rn(__dmul_rn(weight[i], scale));
 }
 
+// Cutpoint tables: for CDF r (0: the marginal over h rows; 1 + k: row k's
+// conditional over w columns) and bucket b, the last index i below the CDF's
+// count with cdf[i] <= b / ENV_CUTS, by the same search sample_cdf runs.
+__global__ void k_env_cuts(const float* __restrict__ marginal, const float* __restrict__ conditional, uint32_t* cut,
+                           uint32_t w, uint32_t h) {
+    const size_t n = size_t(h + 1) * (ENV_CUTS + 1);
+    for (size_t k = blockIdx.x * size_t(blockDim.x) + threadIdx.x; k < n; k += size_t(gridDim.x) * blockDim.x) {
+        const uint32_t r = uint32_t(k / (ENV_CUTS + 1)), b = uint32_t(k % (ENV_CUTS + 1));
+        const float* cdf = r == 0 ? marginal : conditional + size_t(r - 1) * (w + 1);
+        const uint32_t count = r == 0 ? h : w;
+        const float u = float(b) / float(ENV_CUTS);
+        uint32_t lo = 0, hi = count;
+        while (lo + 1 < hi) {
+            const uint32_t mid = (lo + hi) >> 1;
+            if (cdf[mid] <= u) lo = mid;
+            else hi = mid;
+        }
+        cut[k] = lo;
+    }
+}
+
 }  // namespace
+
+void launch_env_cuts(const float* marginal, const float* conditional, uint32_t w, uint32_t h, uint32_t* cut,
+                     cudaStream_t stream) {
+    const size_t n = size_t(h + 1) * (ENV_CUTS + 1);
+    int grid = int((n + 255) / 256);
+    if (grid > 148 * 32) grid = 148 * 32;
+    k_env_cuts<<<grid, 256, 0, stream>>>(marginal, conditional, cut, w, h);
+}
 
 // scratch: 3·w·h + 3·h doubles + 2 doubles; results into marginal (h+1),
 // conditional (h·(w+1)), pdfs (w·h) and totals (total, power).

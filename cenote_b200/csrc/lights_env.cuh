@@ -80,8 +80,16 @@ __device__ __forceinline__ LightConn sample_lights(const LightRecord* lights, ui
 }
 
 // The largest index with cdf[index] <= u, and the continuous position.
-__device__ __forceinline__ uint32_t sample_cdf(const float* cdf, uint32_t count, float u, float* position) {
-    uint32_t lo = 0, hi = count;
+// The last index i < count with cdf[i] <= u, and the position inside it.
+// The cutpoint table narrows the search first: with b = floor(u·ENV_CUTS),
+// b / ENV_CUTS <= u < (b + 1) / ENV_CUTS, so the answer lies between the
+// answers for those two values, cut[b] and cut[b + 1]; the search then runs
+// the same comparison over that range and returns the same index as a search
+// of the whole CDF, in one or two steps where the distribution is smooth.
+__device__ __forceinline__ uint32_t sample_cdf(const float* cdf, const uint32_t* cut, uint32_t count, float u,
+                                               float* position) {
+    const uint32_t b = min(uint32_t(u * float(ENV_CUTS)), ENV_CUTS - 1u);
+    uint32_t lo = __ldg(cut + b), hi = __ldg(cut + b + 1) + 1u;
     while (lo + 1 < hi) {
         uint32_t mid = (lo + hi) >> 1;
         if (__ldg(cdf + mid) <= u) lo = mid;
@@ -119,8 +127,9 @@ struct EnvSample {
 };
 __device__ __forceinline__ EnvSample env_sample(const DeviceScene& s, float2 u) {
     float v, uu;
-    uint32_t row = sample_cdf(s.env_marginal, s.env_h, u.x, &v);
-    uint32_t col = sample_cdf(s.env_conditional + size_t(row) * (s.env_w + 1), s.env_w, u.y, &uu);
+    uint32_t row = sample_cdf(s.env_marginal, s.env_cut, s.env_h, u.x, &v);
+    uint32_t col = sample_cdf(s.env_conditional + size_t(row) * (s.env_w + 1), s.env_cut + size_t(row + 1) * (ENV_CUTS + 1),
+                              s.env_w, u.y, &uu);
     float st = sinf(ENV_PI * v);
     EnvSample r;
     r.direction = env_dir(uu, v);

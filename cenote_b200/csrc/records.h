@@ -15,6 +15,9 @@
 
 namespace cn {
 
+// Buckets of the environment CDFs' cutpoint tables (a power of two, so u·ENV_CUTS is exact).
+constexpr uint32_t ENV_CUTS = 256;
+
 using Material = cenote_material;
 static_assert(sizeof(Material) == 144, "material record is 144 bytes");
 
@@ -93,6 +96,9 @@ struct DeviceScene {
     const float* bsdf_tables;
     const float* env_marginal;
     const float* env_conditional;
+    // Cutpoints of the CDFs (marginal first, then each row's conditional):
+    // ENV_CUTS + 1 per CDF, entry b the index its search returns for b / ENV_CUTS.
+    const uint32_t* env_cut;
     const float* env_pdfs;
     unsigned long long env_tex;  // cudaTextureObject_t
     uint32_t env_w, env_h;

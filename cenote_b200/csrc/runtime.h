@@ -111,6 +111,7 @@ struct cenote_scene {
     uint64_t device_bytes = 0;
     DeviceBuffer* env_marginal = nullptr;
     DeviceBuffer* env_conditional = nullptr;
+    DeviceBuffer* env_cut = nullptr;
     DeviceBuffer* env_pdfs = nullptr;
     std::vector<cudaArray_t> tex_arrays;            // the bindless table's storage
     std::vector<cudaTextureObject_t> tex_objects;
