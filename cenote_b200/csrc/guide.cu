@@ -636,17 +636,18 @@ __global__ void __launch_bounds__(TILE * WG, 1) k_infer_paths(Net net, DeviceSce
                     *reinterpret_cast<uint4*>(gbase + InferSmem::H + kmajor_offset(row, c0 + 8, HIDDEN)) = pack8(v + 8);
                 }
             } else {
+                // The raw outputs, then the mixture activated once for shading.
+                float o[OUT_PAD];
                 for (uint32_t c0 = 0; c0 < OUT_PAD; c0 += 16) {
-                    float v[16];
-                    umma::tmem_ld16(umma::tmem_at(tmem, lane_base, c0), v);
+                    umma::tmem_ld16(umma::tmem_at(tmem, lane_base, c0), o + c0);
                     umma::tmem_wait_ld();
-                    if (hit) {
-                        float* dst = pool.guide_out + size_t(path) * OUT + c0;
-                        for (uint32_t c = 0; c < 16 && c0 + c < OUT; c += 4)
-                            *reinterpret_cast<float4*>(dst + c) =
-                                make_float4(v[c] + bl[c0 + c], v[c + 1] + bl[c0 + c + 1], v[c + 2] + bl[c0 + c + 2],
-                                            v[c + 3] + bl[c0 + c + 3]);
-                    }
+                    for (uint32_t c = 0; c < 16; ++c) o[c0 + c] += bl[c0 + c];
+                }
+                if (hit) {
+                    float a[OUT_ACT];
+                    activate(o, a);
+                    float4* dst = reinterpret_cast<float4*>(pool.guide_out + size_t(path) * OUT_ACT);
+                    for (uint32_t c = 0; c < OUT_ACT; c += 4) dst[c / 4] = make_float4(a[c], a[c + 1], a[c + 2], a[c + 3]);
                 }
             }
         }

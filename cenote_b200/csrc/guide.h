@@ -15,6 +15,10 @@ constexpr uint32_t HIDDEN = 64;
 constexpr uint32_t LOBES = 8;
 constexpr uint32_t OUT = 5 * LOBES;  // per lobe: raw direction (3), raw concentration, logit
 constexpr uint32_t OUT_PAD = 48;     // the last layer's MMA width
+// The mixture as shading reads it, activated once per vertex by inference:
+// six groups of LOBES floats (mu.x, mu.y, mu.z, kappa, weight, and the vMF
+// normalisation kappa / (2 pi (1 - e^{-2 kappa}))), 16-byte aligned groups.
+constexpr uint32_t OUT_ACT = 6 * LOBES;
 constexpr uint32_t TILE = 128;       // rows per CTA tile (the MMA's M)
 constexpr uint32_t ACT = IN + 3 * HIDDEN;  // saved activations per row (BF16)
 constexpr uint32_t FREQS = 12;       // frequency bands of the position encoding
@@ -122,44 +126,61 @@ __device__ inline void lobe_weights(const float* o, float* w) {
     for (int i = 0; i < LOBES; ++i) w[i] /= s;
 }
 
-__device__ inline float mixture_pdf(const float* o, float3 d) {
+
+// The activated mixture (OUT_ACT layout) from the raw outputs: the lobes'
+// means, concentrations, softmax weights and vMF normalisations, computed
+// as lobe(), lobe_weights() and vmf_pdf() compute them.
+__device__ inline void activate(const float* o, float* a) {
     float w[LOBES];
     lobe_weights(o, w);
-    float q = 0.0f;
-    for (int i = 0; i < LOBES; ++i) {
+    for (uint32_t i = 0; i < LOBES; ++i) {
         Lobe L = lobe(o + 5 * i);
-        q += w[i] * vmf_pdf(L.kappa, L.mu.x * d.x + L.mu.y * d.y + L.mu.z * d.z);
+        a[i] = L.mu.x;
+        a[LOBES + i] = L.mu.y;
+        a[2 * LOBES + i] = L.mu.z;
+        a[3 * LOBES + i] = L.kappa;
+        a[4 * LOBES + i] = w[i];
+        a[5 * LOBES + i] = L.kappa / (6.283185307f * (1.0f - expf(-2.0f * L.kappa)));
+    }
+}
+
+// The mixture's density at direction d: the sum over lobes of weight times
+// the vMF density (vmf_pdf), read from the activated layout.
+__device__ inline float mixture_pdf_act(const float* a, float3 d) {
+    float q = 0.0f;
+    for (uint32_t i = 0; i < LOBES; ++i) {
+        const float cosw = a[i] * d.x + a[LOBES + i] * d.y + a[2 * LOBES + i] * d.z;
+        const float kappa = a[3 * LOBES + i];
+        q += a[4 * LOBES + i] * (a[5 * LOBES + i] * expf(kappa * (cosw - 1.0f)));
     }
     return q;
 }
 
 // A direction from the mixture: lobe by u_lobe, then the vMF around its mean
 // (inverse-cdf cos theta = 1 + log(u + (1 - u) e^{-2 kappa}) / kappa).
-__device__ inline float3 mixture_sample(const float* o, float u_lobe, float u1, float u2) {
-    float w[LOBES];
-    lobe_weights(o, w);
+__device__ inline float3 mixture_sample_act(const float* a, float u_lobe, float u1, float u2) {
     int pick = LOBES - 1;
     float acc = 0.0f;
-    for (int i = 0; i < LOBES; ++i) {
-        acc += w[i];
+    for (int i = 0; i < int(LOBES); ++i) {
+        acc += a[4 * LOBES + i];
         if (u_lobe < acc) {
             pick = i;
             break;
         }
     }
-    Lobe L = lobe(o + 5 * pick);
-    float ct = 1.0f + logf(u1 + (1.0f - u1) * __expf(-2.0f * L.kappa)) / L.kappa;
+    const float kappa = a[3 * LOBES + pick];
+    float ct = 1.0f + logf(u1 + (1.0f - u1) * __expf(-2.0f * kappa)) / kappa;
     ct = fminf(fmaxf(ct, -1.0f), 1.0f);
     float st = sqrtf(fmaxf(0.0f, 1.0f - ct * ct));
     float sp, cp;
     __sincosf(6.283185307f * u2, &sp, &cp);
     // Frame around mu (Duff et al. 2017).
-    float3 n = L.mu;
+    float3 n = make_float3(a[pick], a[LOBES + pick], a[2 * LOBES + pick]);
     float sg = n.z >= 0.0f ? 1.0f : -1.0f;
-    float a = -1.0f / (sg + n.z);
-    float b = n.x * n.y * a;
-    float3 t = make_float3(1.0f + sg * n.x * n.x * a, sg * b, -sg * n.x);
-    float3 bt = make_float3(b, sg + n.y * n.y * a, -n.y);
+    float aa = -1.0f / (sg + n.z);
+    float b = n.x * n.y * aa;
+    float3 t = make_float3(1.0f + sg * n.x * n.x * aa, sg * b, -sg * n.x);
+    float3 bt = make_float3(b, sg + n.y * n.y * aa, -n.y);
     return make_float3(st * cp * t.x + st * sp * bt.x + ct * n.x, st * cp * t.y + st * sp * bt.y + ct * n.y,
                        st * cp * t.z + st * sp * bt.z + ct * n.z);
 }
@@ -189,7 +210,7 @@ struct PathPool;
 
 namespace guide {
 
-// The 40 mixture outputs of every hit path of `bounce` into pool.guide_out.
+// The activated mixture (OUT_ACT floats) of every hit path of `bounce` into pool.guide_out.
 void launch_infer_paths(const Buffers& b, const DeviceScene& scene, const PathPool& pool, uint32_t bounce,
                         uint32_t n0, int sms, cudaStream_t s);
 // Turn the wave's records into target weights L / pdf (L from the paths'

@@ -79,7 +79,6 @@ __device__ __forceinline__ LightConn sample_lights(const LightRecord* lights, ui
     return r;
 }
 
-// The largest index with cdf[index] <= u, and the continuous position.
 // The last index i < count with cdf[i] <= u, and the position inside it.
 // The cutpoint table narrows the search first: with b = floor(u·ENV_CUTS),
 // b / ENV_CUTS <= u < (b + 1) / ENV_CUTS, so the answer lies between the

@@ -218,7 +218,7 @@ struct cenote_renderer {
     cudaError_t set_learned_guide(bool on) {
         if (on && g_cap < pool_cap) {
             cudaError_t e;
-            if ((e = g_out.alloc(pool_cap * guide::OUT * 4)) || (e = g_rec.alloc(pool_cap * 4))) return e;
+            if ((e = g_out.alloc(pool_cap * guide::OUT_ACT * 4)) || (e = g_rec.alloc(pool_cap * 4))) return e;
             g_cap = pool_cap;
         }
         if (on && !g_records.ptr) {

@@ -582,7 +582,7 @@ __global__ void __launch_bounds__(BLOCK, CN_SHADE_MIN_BLOCKS) k_shade(DeviceScen
                 float g_alpha = 0.0f;
                 const float* g_out = nullptr;
                 if (GUIDE) {
-                    g_out = pool.guide_out + size_t(path) * guide::OUT;
+                    g_out = pool.guide_out + size_t(path) * guide::OUT_ACT;
                     if (cl.w_diffuse + cl.w_fuzz > 0.0f || cl.alpha > 0.05f) g_alpha = pool.sink->fraction;
                 }
                 // Guides (shade_surface.slang:322-340): camera rays are fully
@@ -644,7 +644,7 @@ __global__ void __launch_bounds__(BLOCK, CN_SHADE_MIN_BLOCKS) k_shade(DeviceScen
                             EvalPdf ep = eval_pdf(cl, wl, wo);
                             float p_scatter = ep.pdf;
                             if (GUIDE && g_alpha > 0.0f)
-                                p_scatter = g_alpha * guide::mixture_pdf(g_out, cdir) + (1.0f - g_alpha) * ep.pdf;
+                                p_scatter = g_alpha * guide::mixture_pdf_act(g_out, cdir) + (1.0f - g_alpha) * ep.pdf;
                             float w = mis ? power_heuristic(nee, p_scatter) : 1.0f;
                             float3 unshadowed = thr * crad * ep.f * fabsf(wl.z) * (w / nee);
                             if (any_pos(unshadowed)) {
@@ -669,7 +669,7 @@ __global__ void __launch_bounds__(BLOCK, CN_SHADE_MIN_BLOCKS) k_shade(DeviceScen
                     if (GUIDE && g_alpha > 0.0f && u_lobe < g_alpha) {
                         // A direction from the guide's mixture (the pick's leftover
                         // chooses the lobe); lobe labels follow the hemisphere.
-                        float3 d = guide::mixture_sample(g_out, u_lobe / g_alpha, u.x, u.y);
+                        float3 d = guide::mixture_sample_act(g_out, u_lobe / g_alpha, u.x, u.y);
                         sc.wi = frame.to_local(d);
                         sc.pdf = 0.0f;
                         sc.lobe = sc.wi.z < 0.0f ? LOBE_TRANSMISSION : LOBE_DIFFUSE;
@@ -683,7 +683,7 @@ __global__ void __launch_bounds__(BLOCK, CN_SHADE_MIN_BLOCKS) k_shade(DeviceScen
                         sc.pdf = ep.pdf;
                         fsc = ep.f;
                         if (GUIDE && g_alpha > 0.0f)
-                            sc.pdf = g_alpha * guide::mixture_pdf(g_out, frame.to_world(sc.wi)) + (1.0f - g_alpha) * ep.pdf;
+                            sc.pdf = g_alpha * guide::mixture_pdf_act(g_out, frame.to_world(sc.wi)) + (1.0f - g_alpha) * ep.pdf;
                     }
                     float3 wiw = frame.to_world(sc.wi);
                     float3 scattered = f3(0.0f);
