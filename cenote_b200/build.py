@@ -92,7 +92,7 @@ def build(verbose: bool = False, ptxas_info: bool = False, defines=(), out_dir: 
                                                   (inc / "tables_blob.inc").stat().st_mtime):
             continue
         _run(["g++", "-O2", "-std=c++17", "-fPIC", "-ffp-contract=off", "-Wall", "-Wextra", "-Wno-unused-parameter",
-              f"-I{_cuda_include(nvcc)}", f"-I{inc}", "-c", str(s), "-o", str(o)])
+              *dflags, f"-I{_cuda_include(nvcc)}", f"-I{inc}", "-c", str(s), "-o", str(o)])
     if not lib.exists() or lib.stat().st_mtime < max(o.stat().st_mtime for o in objs):
         _run([nvcc, *ARCH, "-shared", "-o", str(lib), *map(str, objs), "-lpthread"])
     return lib

@@ -16,7 +16,10 @@
 namespace cn {
 
 // Buckets of the environment CDFs' cutpoint tables (a power of two, so u·ENV_CUTS is exact).
-constexpr uint32_t ENV_CUTS = 256;
+#ifndef CN_ENV_CUTS
+#define CN_ENV_CUTS 256
+#endif
+constexpr uint32_t ENV_CUTS = CN_ENV_CUTS;
 
 using Material = cenote_material;
 static_assert(sizeof(Material) == 144, "material record is 144 bytes");
