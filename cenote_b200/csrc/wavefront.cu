@@ -40,9 +40,13 @@ constexpr int BLOCK = 128;
 #ifndef CN_SHADE_MIN_BLOCKS
 #define CN_SHADE_MIN_BLOCKS 6
 #endif
-// The same for the traversal kernels (8 → 64 registers).
+// The same for the traversal kernels (8 → 64 registers), and for the
+// closest-hit walks alone (which spill a little at 64 registers).
 #ifndef CN_TRAV_MIN_BLOCKS
 #define CN_TRAV_MIN_BLOCKS 8
+#endif
+#ifndef CN_ISECT_MIN_BLOCKS
+#define CN_ISECT_MIN_BLOCKS CN_TRAV_MIN_BLOCKS
 #endif
 
 __device__ __forceinline__ uint32_t lane_id() { return threadIdx.x & 31u; }
@@ -223,7 +227,7 @@ __device__ __forceinline__ uint32_t refill(uint32_t* counter, uint32_t count, bo
 // whose node groups need fewer). Every variant walks the same tree to the
 // same hits.
 template <bool COUNT, int B = BLOCK, int S = TRAVERSAL_STACK>
-__global__ void __launch_bounds__(B, CN_TRAV_MIN_BLOCKS * BLOCK / B)
+__global__ void __launch_bounds__(B, CN_ISECT_MIN_BLOCKS * BLOCK / B)
     k_intersect(DeviceScene scene, PathPool pool, uint32_t bounce, uint32_t n0) {
     extern __shared__ uint4 top_levels[];
     stage_top_levels(scene, top_levels, min(pool.top_nodes, TOP_NODES_MAX));  // as the launch sized it
@@ -361,7 +365,7 @@ struct IsectSource {
 };
 
 template <bool COUNT, int B = BLOCK, int S = TRAVERSAL_STACK>
-__global__ void __launch_bounds__(B, CN_TRAV_MIN_BLOCKS * BLOCK / B)
+__global__ void __launch_bounds__(B, CN_ISECT_MIN_BLOCKS * BLOCK / B)
     k_intersect_queued(DeviceScene scene, PathPool pool, uint32_t bounce, uint32_t n0) {
     extern __shared__ uint4 top_levels[];
     __shared__ TriQueueSmem tqs[B / 32];
