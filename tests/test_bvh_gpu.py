@@ -82,3 +82,14 @@ def test_unknown_builder_is_refused():
 
     with pytest.raises(CenoteError):
         Context(0).set_bvh_builder(4)
+
+
+def test_auto_builder_builds_large_scenes_on_the_gpu():
+    """BVH_AUTO (the default) builds a scene of at least 2^20 triangles with
+    the GPU binned-SAH builder: the large scene's 3.08 M triangles."""
+    from cenote_b200 import Context, Scene
+
+    ctx = Context(0)
+    scene = Scene(ctx, scenes.large(64, 36, 1, 2, texture_size=64, textures=8))
+    assert scene.bvh_builder() == BVH_GPU_SAH
+    assert scene.prep_times_ms()[0] > 0.0
