@@ -469,9 +469,9 @@ def run_knob_sweep(args, w):
         return round(min(ms) / spp, 4)
 
     names = ("material_sort", "samples_per_wave", "refill_idle", "top_nodes", "l2_window", "per_lane_triangles",
-             "block_size", "stack_depth")
+             "block_size", "stack_depth", "sort_by_location")
     base = tuple(best[k] for k in names)
-    values = ((0, 1, 2), (0, 4, 8, 16), (4, 8, 16, 32), (0, 80, 320), (0, 1), (0, 1), (128, 256), (16, 32))
+    values = ((0, 1, 2), (0, 4, 8, 16), (4, 8, 16, 32), (0, 80, 320), (0, 1), (0, 1), (128, 256), (16, 32), (0, 1))
     sweep = {"tuned": timed(base)}
     for i, vals in enumerate(values):
         for v in vals:
@@ -507,7 +507,7 @@ def main():
                          "triangles, else host SAH; host; gpu (binned SAH); gpu-ploc")
     ap.add_argument("--tuning", default="",
                     help="pin the launch knobs instead of autotuning: sort,samples_per_wave,refill,top_nodes,l2"
-                         "[,per_lane_triangles[,block_size,stack_depth]] "
+                         "[,per_lane_triangles[,block_size,stack_depth[,sort_by_location]]] "
                          "(profiling runs that must not record the tuner's probes)")
     ap.add_argument("--material-sort", type=int, default=None, choices=[0, 1, 2],
                     help="fix the material sort (0 off, 1 every bounce, 2 from the first bounce on) "
@@ -695,6 +695,7 @@ def main():
                               "triangle_tests": "per lane" if tuning["per_lane_triangles"] else "warp queue",
                               "traversal_block_size": tuning["block_size"],
                               "traversal_stack_depth": tuning["stack_depth"],
+                              "sort_key": "location" if tuning["sort_by_location"] else "instance",
                               "chosen_by": "autotuner" if args.material_sort is None and not args.tuning else "flag",
                               "autotune_s": round(tune_s, 3)},
                    "guides": "albedo, normal and depth traced and accumulated every sample, as Renderer::accumulate does"},

@@ -85,7 +85,8 @@ class DeltaLightC(C.Structure):
 class TuningC(C.Structure):
     _fields_ = [("material_sort", C.c_uint32), ("samples_per_wave", C.c_uint32), ("refill_idle", C.c_uint32),
                 ("top_nodes", C.c_uint32), ("l2_window", C.c_uint32), ("per_lane_triangles", C.c_uint32),
-                ("ms_per_sample", C.c_float), ("block_size", C.c_uint32), ("stack_depth", C.c_uint32)]
+                ("ms_per_sample", C.c_float), ("block_size", C.c_uint32), ("stack_depth", C.c_uint32),
+                ("sort_by_location", C.c_uint32)]
 
 
 class Options(C.Structure):
@@ -612,9 +613,9 @@ class Renderer:
 
     def set_tuning(self, material_sort: int, samples_per_wave: int = 0, refill_idle: int = 0,
                    top_nodes: int = 0, l2_window: int = 0, per_lane_triangles: int = 0, block_size: int = 0,
-                   stack_depth: int = 0) -> None:
+                   stack_depth: int = 0, sort_by_location: int = 0) -> None:
         t = TuningC(material_sort, samples_per_wave, refill_idle, top_nodes, l2_window, per_lane_triangles, 0.0,
-                    block_size, stack_depth)
+                    block_size, stack_depth, sort_by_location)
         _check(library().cenote_renderer_set_tuning(self._h, C.byref(t)))
 
     def autotune(self, scene: Scene, width: int, height: int) -> dict:

@@ -849,6 +849,7 @@ int32_t cenote_renderer_set_tuning(cenote_renderer* r, const cenote_tuning* t) {
              "block_size is 128 or 256");
     CN_CHECK(t->stack_depth == 0 || t->stack_depth == 16 || t->stack_depth == 32, CENOTE_E_INVALID_ARGUMENT,
              "stack_depth is 16 or 32");
+    CN_CHECK(t->sort_by_location <= 1, CENOTE_E_INVALID_ARGUMENT, "sort_by_location is 0 or 1");
     r->material_sort = t->material_sort;
     r->samples_per_wave = t->samples_per_wave;
     r->refill_idle = t->refill_idle;
@@ -856,6 +857,7 @@ int32_t cenote_renderer_set_tuning(cenote_renderer* r, const cenote_tuning* t) {
     r->l2_window = t->l2_window;
     r->per_lane_triangles = t->per_lane_triangles;
     r->trav_variant = trav_variant_of(t->block_size, t->stack_depth);
+    r->sort_by_location = t->sort_by_location;
     return CENOTE_OK;
 }
 
@@ -870,6 +872,7 @@ int32_t cenote_renderer_get_tuning(cenote_renderer* r, cenote_tuning* out) {
     out->ms_per_sample = r->tuned_ms_per_sample;
     out->block_size = uint32_t(TRAV_VARIANT_BLOCK[r->trav_variant]);
     out->stack_depth = uint32_t(TRAV_VARIANT_STACK[r->trav_variant]);
+    out->sort_by_location = r->sort_by_location;
     return CENOTE_OK;
 }
 
@@ -1093,7 +1096,8 @@ int32_t cenote_renderer_autotune(cenote_renderer* r, cenote_scene* scene, uint32
                        r->per_lane_triangles,
                        0.0f,
                        uint32_t(TRAV_VARIANT_BLOCK[r->trav_variant]),
-                       uint32_t(TRAV_VARIANT_STACK[r->trav_variant])};
+                       uint32_t(TRAV_VARIANT_STACK[r->trav_variant]),
+                       r->sort_by_location};
     auto apply = [&](const cenote_tuning& t) {
         r->material_sort = t.material_sort;
         r->samples_per_wave = t.samples_per_wave;
@@ -1102,6 +1106,7 @@ int32_t cenote_renderer_autotune(cenote_renderer* r, cenote_scene* scene, uint32
         r->l2_window = t.l2_window;
         r->per_lane_triangles = t.per_lane_triangles;
         r->trav_variant = trav_variant_of(t.block_size, t.stack_depth);
+        r->sort_by_location = t.sort_by_location;
     };
     // Device time of `probe` samples, the better of two runs (the first run of
     // a new wave size also allocates).
@@ -1122,9 +1127,10 @@ int32_t cenote_renderer_autotune(cenote_renderer* r, cenote_scene* scene, uint32
     // tests (fractional opacity always tests per lane); the 16-entry stack is
     // a candidate only when the tree's node groups fit it.
     const bool short_stack = TRAVERSAL_STACK_DEPTH - int(scene->ds.stack_room) < 16;
-    for (int knob = 0; knob < 8 && rc == CENOTE_OK; ++knob) {
+    for (int knob = 0; knob < 9 && rc == CENOTE_OK; ++knob) {
         if (knob == 5 && scene->ds.has_nonopaque) continue;
         if (knob == 7 && !short_stack) continue;
+        if (knob == 8 && best.material_sort == CENOTE_SORT_NONE) continue;
         for (int c = 0; c < (knob == 1 ? 5 : (knob >= 4 ? 2 : 3)) && rc == CENOTE_OK; ++c) {
             cenote_tuning t = best;
             if (knob == 0) t.material_sort = uint32_t(c);
@@ -1135,10 +1141,11 @@ int32_t cenote_renderer_autotune(cenote_renderer* r, cenote_scene* scene, uint32
             if (knob == 5) t.per_lane_triangles = uint32_t(c);
             if (knob == 6) t.block_size = c == 0 ? 128u : 256u;
             if (knob == 7) t.stack_depth = c == 0 ? 32u : 16u;
+            if (knob == 8) t.sort_by_location = uint32_t(c);
             if (t.material_sort == best.material_sort && t.samples_per_wave == best.samples_per_wave &&
                 t.refill_idle == best.refill_idle && t.top_nodes == best.top_nodes && t.l2_window == best.l2_window &&
                 t.per_lane_triangles == best.per_lane_triangles && t.block_size == best.block_size &&
-                t.stack_depth == best.stack_depth)
+                t.stack_depth == best.stack_depth && t.sort_by_location == best.sort_by_location)
                 continue;
             float ms = 0.0f;
             rc = measure(t, &ms);

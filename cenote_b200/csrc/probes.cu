@@ -92,7 +92,7 @@ struct ProbeSource {
         hits[i] = h;
         tout[i] = h.x == LIGHT_NONE ? -1.0f : t;
     }
-    __device__ __forceinline__ void step(bool, uint32_t, uint32_t) const {}
+    __device__ __forceinline__ void step(bool, uint32_t, uint32_t, float) const {}
     __device__ __forceinline__ uint32_t want_idle(bool drained) const { return drained ? 32u : 8u; }
 };
 

@@ -112,6 +112,7 @@ cudaError_t enqueue_segments(cenote_renderer* r, const cenote_scene* sc, const W
     r->pool.top_nodes = r->top_nodes;
     r->pool.per_lane_triangles = r->per_lane_triangles;
     r->pool.trav_variant = r->trav_variant;
+    r->pool.sort_location = r->sort_by_location;
     WaveParams wp{};
     wp.max_bounces = max_bounces;
     wp.light_sampling = r->light_sampling;
@@ -142,6 +143,7 @@ cudaError_t enqueue_waves(cenote_renderer* r, const cenote_scene* sc, uint32_t w
     r->pool.top_nodes = r->top_nodes;
     r->pool.per_lane_triangles = r->per_lane_triangles;
     r->pool.trav_variant = r->trav_variant;
+    r->pool.sort_location = r->sort_by_location;
     WaveParams wp{};
     wp.width = width;
     wp.height = height;

@@ -157,6 +157,7 @@ struct cenote_renderer {
     uint32_t l2_window = 0;    // mark the BVH nodes persisting in L2 during this renderer's waves
     uint32_t per_lane_triangles = 0;  // 1: no warp triangle queue in the traversal kernels
     uint32_t trav_variant = 0;        // traversal block size and stack depth (TRAV_VARIANT_*)
+    uint32_t sort_by_location = 0;    // 1: the material sort keys layer-free hits by location
     float tuned_ms_per_sample = 0.0f;
     DeviceBuffer sort_order, sort_keys, sort_bins;
     DeviceBuffer aov_albedo, aov_normal, aov_depth, aov_guide;

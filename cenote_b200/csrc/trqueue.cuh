@@ -225,7 +225,7 @@ __device__ __forceinline__ void tq_round(const DeviceScene& s, TriQueueSmem& sm,
 //   uint32_t next(bool live, bool& drained)  an item for each idle lane (~0u: none)
 //   void ray(uint32_t item, float3& org, float3& dir)      (per lane)
 //   void emit(uint32_t item, uint4 hit, float t)          (per lane)
-//   void step(bool finished, uint32_t item, uint32_t instance)  after every step
+//   void step(bool finished, uint32_t item, uint32_t instance, float t)  after every step
 //   uint32_t want_idle(bool drained)  idle lanes before the warp refills
 // Each step a walking lane expands one node and queues the triangles of the
 // leaves it hits; rounds run while the FIFO holds a warp's worth of
@@ -293,7 +293,7 @@ __device__ __forceinline__ void queued_closest(const DeviceScene& s, TriQueueSme
                 finished = true;
                 live = false;
             }
-            src.step(finished, item, c.inst);
+            src.step(finished, item, c.inst, c.tmax);
             if (uint32_t(__popc(__ballot_sync(TQ_FULL, !live))) >= want_idle) break;
         }
     }

@@ -72,11 +72,23 @@ __device__ __forceinline__ uint32_t warp_push(uint32_t* counter, bool pred) {
 
 __device__ __forceinline__ void flag_overflow(uint32_t* counters) { atomicOr(counters + CTR_OVERFLOW, 1u); }
 
-// The material-sort key of a closest hit (SORT_LAYERS splits the key range).
-__device__ __forceinline__ uint32_t material_key(const DeviceScene& s, uint32_t inst) {
+// The material-sort key of a closest hit at distance t along path `path`'s
+// ray (SORT_LAYERS splits the key range). Layer-free hits take their
+// instance, or with pool.sort_location the Morton index of the 32 x 32 cell
+// of the scene's x/z extent their point lies in: their next rays then leave
+// nearby points together, which the next walk's caches reward on some scenes
+// (the autotuner decides).
+__device__ __forceinline__ uint32_t material_key(const DeviceScene& s, const PathPool& pool, uint32_t inst,
+                                                 uint32_t path, float t) {
     if (inst == LIGHT_NONE) return 0u;
-    return __ldg(s.instance_layers + inst) ? SORT_LAYERS + inst % (SORT_BINS - SORT_LAYERS)
-                                           : 1u + inst % (SORT_LAYERS - 1u);
+    if (__ldg(s.instance_layers + inst)) return SORT_LAYERS + inst % (SORT_BINS - SORT_LAYERS);
+    if (!pool.sort_location) return 1u + inst % (SORT_LAYERS - 1u);
+    const float4 o = pool.org[path], d = pool.dir[path];
+    const float fx = (o.x + t * d.x - s.bbox_min[0]) * s.bbox_inv, fz = (o.z + t * d.z - s.bbox_min[2]) * s.bbox_inv;
+    const uint32_t cx = min(31u, uint32_t(fmaxf(fx, 0.0f) * 32.0f)), cz = min(31u, uint32_t(fmaxf(fz, 0.0f) * 32.0f));
+    uint32_t m = 0u;
+    for (uint32_t b = 0; b < 5u; ++b) m |= (((cx >> b) & 1u) << (2u * b)) | (((cz >> b) & 1u) << (2u * b + 1u));
+    return 1u + m % (SORT_LAYERS - 1u);
 }
 
 // Instrumented launches: one 64-bit add per warp for the traversal tallies.
@@ -249,7 +261,7 @@ __global__ void __launch_bounds__(B, CN_ISECT_MIN_BLOCKS * BLOCK / B)
     auto flush_keys = [&]() {
         if (!pool.sort_keys) return;
         if (__ballot_sync(0xffffffffu, finished) == 0u) return;
-        const uint32_t key = finished ? material_key(scene, best_inst) : 0xffffffffu;
+        const uint32_t key = finished ? material_key(scene, pool, best_inst, path, tmax) : 0xffffffffu;
         const uint32_t peers = __match_any_sync(0xffffffffu, key);
         if (finished) {
             pool.sort_keys[qi] = key;
@@ -349,10 +361,10 @@ struct IsectSource {
     __device__ __forceinline__ void emit(uint32_t i, uint4 hit, float) const { pool.hit[path_of(i)] = hit; }
     // Material sort: each finished ray's key goes to its queue slot and into
     // the key counts, one atomic per distinct key per warp.
-    __device__ __forceinline__ void step(bool finished, uint32_t i, uint32_t inst) const {
+    __device__ __forceinline__ void step(bool finished, uint32_t i, uint32_t inst, float t) const {
         if (!pool.sort_keys) return;
         if (__ballot_sync(0xffffffffu, finished) == 0u) return;
-        const uint32_t key = finished ? material_key(*scene, inst) : 0xffffffffu;
+        const uint32_t key = finished ? material_key(*scene, pool, inst, path_of(i), t) : 0xffffffffu;
         const uint32_t peers = __match_any_sync(0xffffffffu, key);
         if (finished) {
             pool.sort_keys[i] = key;

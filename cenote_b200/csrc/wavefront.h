@@ -65,6 +65,7 @@ struct PathPool {
     uint32_t per_lane_triangles;
     // The traversal launch variant (block size, stack entries; TRAV_VARIANT_*).
     uint32_t trav_variant;
+    uint32_t sort_location;  // 1: layer-free hits sort by their location's Morton cell, not by instance
 };
 
 constexpr uint32_t TOP_NODES_MAX = 320;  // 25.6 KB per 128-thread block: 8 blocks still fit an SM

@@ -288,14 +288,18 @@ typedef struct cenote_tuning {
     uint32_t block_size;       /* traversal threads per block: 128 or 256 (0 = 128) */
     uint32_t stack_depth;      /* traversal stack entries per lane: 16 or 32 (0 = 32); 16 falls back to 32
                                 * for a tree whose node groups could need more */
+    uint32_t sort_by_location; /* 1: the material sort orders a bounce's hits on layer-free materials by
+                                * where they lie (a 32 x 32 Morton cell of the scene's x/z extent) rather
+                                * than by instance, so the next bounce's rays leave nearby points together */
 } cenote_tuning;
 int32_t cenote_renderer_set_tuning(cenote_renderer* r, const cenote_tuning* tuning);
 int32_t cenote_renderer_get_tuning(cenote_renderer* r, cenote_tuning* out);
 /* Time candidate settings on `scene` at width x height (a scratch film, a few
  * hundred ms of device time at 1080p) by coordinate descent over the sort
  * mode, samples per wave, refill threshold, shared-memory top levels, the
- * L2 persistence window, per-lane or queued triangle tests and the
- * traversal's block size and stack depth;
+ * L2 persistence window, per-lane or queued triangle tests, the
+ * traversal's block size and stack depth and the sort's key (instance or
+ * location);
  * apply the fastest to `r` and
  * report it in `out` (nullable). The renderer's stats afterwards describe the
  * last probe. */

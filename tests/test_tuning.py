@@ -155,3 +155,28 @@ def test_traversal_block_size_and_stack_depth_are_bitwise_invisible(ctx, name):
             films.append(f.sums())
     for other in films[1:]:
         assert np.array_equal(films[0], other)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("name", ["chart", "textured"])
+def test_sort_by_location_is_bitwise_invisible(ctx, name):
+    """The material sort's key (instance, or the Morton cell of the hit's
+    location) only reorders how a bounce is shaded and the next one is
+    walked: films are bitwise equal, per-lane and queued triangle tests
+    alike, sorting every bounce or from the first bounce on."""
+    from cenote_b200 import Film, Renderer, Scene, scenes
+
+    spec = scenes.chart(96, 64, env_size=(256, 128)) if name == "chart" else scenes.textured(80, 45, 4, 5, size=32)
+    s = Scene(ctx, spec)
+    films = []
+    for sort in (1, 2):
+        for per_lane in (0, 1):
+            for location in (0, 1):
+                r = Renderer(ctx, spec.max_bounces)
+                r.set_tuning(sort, 0, 0, 0, 0, per_lane, 0, 0, location)
+                assert r.tuning()["sort_by_location"] == location
+                f = Film(ctx, spec.width, spec.height)
+                r.accumulate(s, f, 4)
+                films.append(f.sums())
+    for other in films[1:]:
+        assert np.array_equal(films[0], other)
