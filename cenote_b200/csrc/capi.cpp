@@ -1127,13 +1127,18 @@ int32_t cenote_renderer_autotune(cenote_renderer* r, cenote_scene* scene, uint32
     // tests (fractional opacity always tests per lane); the 16-entry stack is
     // a candidate only when the tree's node groups fit it.
     const bool short_stack = TRAVERSAL_STACK_DEPTH - int(scene->ds.stack_room) < 16;
-    for (int knob = 0; knob < 9 && rc == CENOTE_OK; ++knob) {
+    // The sort mode and the sort's key are searched together (the key
+    // changes which mode pays): none, every bounce or from the first bounce
+    // on, each sorted mode keyed by instance or by location.
+    for (int knob = 0; knob < 8 && rc == CENOTE_OK; ++knob) {
         if (knob == 5 && scene->ds.has_nonopaque) continue;
         if (knob == 7 && !short_stack) continue;
-        if (knob == 8 && best.material_sort == CENOTE_SORT_NONE) continue;
-        for (int c = 0; c < (knob == 1 ? 5 : (knob >= 4 ? 2 : 3)) && rc == CENOTE_OK; ++c) {
+        for (int c = 0; c < (knob == 0 ? 5 : (knob == 1 ? 5 : (knob >= 4 ? 2 : 3))) && rc == CENOTE_OK; ++c) {
             cenote_tuning t = best;
-            if (knob == 0) t.material_sort = uint32_t(c);
+            if (knob == 0) {
+                t.material_sort = c == 0 ? CENOTE_SORT_NONE : (c % 2 ? CENOTE_SORT_ALL : CENOTE_SORT_SECONDARY);
+                t.sort_by_location = c >= 3 ? 1u : 0u;
+            }
             if (knob == 1) t.samples_per_wave = spws[c];
             if (knob == 2) t.refill_idle = c == 0 ? 4u : (c == 1 ? 8u : 16u);
             if (knob == 3) t.top_nodes = c == 0 ? 0u : (c == 1 ? 80u : TOP_NODES_MAX);
@@ -1141,7 +1146,6 @@ int32_t cenote_renderer_autotune(cenote_renderer* r, cenote_scene* scene, uint32
             if (knob == 5) t.per_lane_triangles = uint32_t(c);
             if (knob == 6) t.block_size = c == 0 ? 128u : 256u;
             if (knob == 7) t.stack_depth = c == 0 ? 32u : 16u;
-            if (knob == 8) t.sort_by_location = uint32_t(c);
             if (t.material_sort == best.material_sort && t.samples_per_wave == best.samples_per_wave &&
                 t.refill_idle == best.refill_idle && t.top_nodes == best.top_nodes && t.l2_window == best.l2_window &&
                 t.per_lane_triangles == best.per_lane_triangles && t.block_size == best.block_size &&
