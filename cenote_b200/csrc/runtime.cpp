@@ -6,6 +6,14 @@
 
 #include "runtime.h"
 
+// 1: a wave that covers a whole image whose sides are multiples of 8 and 4
+// hands its camera paths out in 8 x 4 pixel tiles (WaveParams::tile_width);
+// 0: row-major pixels. Films are the same either way (a path's samples are
+// keyed by its pixel and sample, not by its slot).
+#ifndef CN_TILE_PIXELS
+#define CN_TILE_PIXELS 1
+#endif
+
 namespace cn {
 
 void camera_basis(const cenote_camera& cam, float aspect, WaveParams& wp);
@@ -170,6 +178,10 @@ cudaError_t enqueue_waves(cenote_renderer* r, const cenote_scene* sc, uint32_t w
         for (uint64_t base = 0; base < pixels; base += plan.range) {
             wp.pixel_base = uint32_t(base);
             wp.pixel_count = uint32_t(std::min<uint64_t>(plan.range, pixels - base));
+            wp.tile_width = CN_TILE_PIXELS && base == 0 && wp.pixel_count == pixels && width % 8 == 0 &&
+                                    height % 4 == 0
+                                ? width
+                                : 0u;
             wp.samples = s;
             wp.sample_base = sample0 + done;
             const uint32_t n0 = wp.pixel_count * s;
@@ -180,10 +192,10 @@ cudaError_t enqueue_waves(cenote_renderer* r, const cenote_scene* sc, uint32_t w
             enqueue_bounces(r, sc, wp, n0, guided, stream, timing, counting, wc);
             launch_tally(r->pool, r->tally.as<unsigned long long>(), n0, max_bounces, stream);
             if (film)
-                launch_accumulate(r->pool, *film, wp.pixel_base, wp.pixel_count, s, film_reset && done == 0,
-                                  stream);
+                launch_accumulate(r->pool, *film, wp.pixel_base, wp.pixel_count, wp.tile_width, s,
+                                  film_reset && done == 0, stream);
             else
-                launch_copy_rad(r->pool, oneshot, wp.pixel_base, wp.pixel_count, stream);
+                launch_copy_rad(r->pool, oneshot, wp.pixel_base, wp.pixel_count, wp.tile_width, stream);
             mark();
             if (guided) {
                 guide::Record* recs = r->g_records.as<guide::Record>();

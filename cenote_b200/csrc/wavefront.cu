@@ -166,7 +166,7 @@ __global__ void __launch_bounds__(BLOCK) k_raygen(PathPool pool, WaveParams wp) 
     uint32_t n = wp.pixel_count * wp.samples;
     for (uint32_t p = blockIdx.x * blockDim.x + threadIdx.x; p < n; p += gridDim.x * blockDim.x) {
         uint32_t s = p / wp.pixel_count;
-        uint32_t pixel = wp.pixel_base + (p - s * wp.pixel_count);
+        uint32_t pixel = wp.pixel_base + wave_pixel(p - s * wp.pixel_count, wp.tile_width);
         uint32_t sample = wp.sample_base + s + (wp.sample_offset ? __ldg(wp.sample_offset) : 0u);
         raygen_path(pool, p, pixel, sample, wp.width, wp.height, wp.cam_pos, wp.cam_right, wp.cam_up, wp.cam_fwd,
                     wp.aperture);
@@ -910,11 +910,11 @@ __device__ __forceinline__ float4 add4(float4 a, float4 b) {
 
 // accumulate.slang:38-67, all samples of a wave in ascending order.
 template <bool AOV>
-__global__ void k_accumulate(PathPool pool, FilmTargets film, uint32_t pixel_base, uint32_t count, uint32_t samples,
-                             uint32_t reset) {
+__global__ void k_accumulate(PathPool pool, FilmTargets film, uint32_t pixel_base, uint32_t count, uint32_t tile_width,
+                             uint32_t samples, uint32_t reset) {
     const float4 zero = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
     for (uint32_t p = blockIdx.x * blockDim.x + threadIdx.x; p < count; p += gridDim.x * blockDim.x) {
-        const uint32_t px = pixel_base + p;
+        const uint32_t px = pixel_base + wave_pixel(p, tile_width);
         float4 acc = reset ? zero : film.sum[px];
         float4 alb = zero, nrm = zero;
         float dep = 0.0f;
@@ -1018,9 +1018,10 @@ __global__ void k_resolve1(const float* __restrict__ sum, float* __restrict__ av
     for (uint32_t p = blockIdx.x * blockDim.x + threadIdx.x; p < n; p += gridDim.x * blockDim.x) avg[p] = sum[p] / samples;
 }
 
-__global__ void k_copy_rad(const float4* __restrict__ rad, float4* __restrict__ out, uint32_t base, uint32_t count) {
+__global__ void k_copy_rad(const float4* __restrict__ rad, float4* __restrict__ out, uint32_t base, uint32_t count,
+                           uint32_t tile_width) {
     for (uint32_t p = blockIdx.x * blockDim.x + threadIdx.x; p < count; p += gridDim.x * blockDim.x)
-        out[base + p] = rad[p];
+        out[base + wave_pixel(p, tile_width)] = rad[p];
 }
 
 // ---- material sort -----------------------------------------------------------------
@@ -1306,13 +1307,15 @@ void launch_wave(const DeviceScene& scene, const PathPool& pool, const WaveParam
 }
 
 void launch_accumulate(const PathPool& pool, const FilmTargets& film, uint32_t pixel_base, uint32_t pixel_count,
-                       uint32_t samples, bool reset, cudaStream_t stream) {
+                       uint32_t tile_width, uint32_t samples, bool reset, cudaStream_t stream) {
     int grid = int((pixel_count + 255) / 256);
     if (grid > 148 * 16) grid = 148 * 16;
     if (pool.aov_albedo && film.albedo)
-        k_accumulate<true><<<grid, 256, 0, stream>>>(pool, film, pixel_base, pixel_count, samples, reset ? 1u : 0u);
+        k_accumulate<true><<<grid, 256, 0, stream>>>(pool, film, pixel_base, pixel_count, tile_width, samples,
+                                                     reset ? 1u : 0u);
     else
-        k_accumulate<false><<<grid, 256, 0, stream>>>(pool, film, pixel_base, pixel_count, samples, reset ? 1u : 0u);
+        k_accumulate<false><<<grid, 256, 0, stream>>>(pool, film, pixel_base, pixel_count, tile_width, samples,
+                                                      reset ? 1u : 0u);
 }
 
 void launch_sort_begin(const PathPool& pool, cudaStream_t stream) {
@@ -1344,10 +1347,11 @@ void launch_resolve(const float4* sum, float4* avg, uint32_t pixels, float sampl
     k_resolve<<<grid, 256, 0, stream>>>(sum, avg, pixels, samples);
 }
 
-void launch_copy_rad(const PathPool& pool, float4* out, uint32_t pixel_base, uint32_t pixel_count, cudaStream_t stream) {
+void launch_copy_rad(const PathPool& pool, float4* out, uint32_t pixel_base, uint32_t pixel_count, uint32_t tile_width,
+                     cudaStream_t stream) {
     int grid = int((pixel_count + 255) / 256);
     if (grid > 148 * 16) grid = 148 * 16;
-    k_copy_rad<<<grid, 256, 0, stream>>>(pool.rad, out, pixel_base, pixel_count);
+    k_copy_rad<<<grid, 256, 0, stream>>>(pool.rad, out, pixel_base, pixel_count, tile_width);
 }
 
 }  // namespace cn

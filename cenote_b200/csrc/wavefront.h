@@ -92,7 +92,21 @@ struct WaveParams {
     // When set, added to every sample index: a replayed CUDA graph reads its
     // progress from device memory instead of baked launch parameters.
     const uint32_t* sample_offset;
+    // Non-zero (the image width, a multiple of 8, with the height a multiple
+    // of 4 and the wave covering the whole image): camera paths take their
+    // pixels in 8 x 4 tiles, 32 consecutive paths to a tile (wave_pixel).
+    uint32_t tile_width;
 };
+
+// The pixel of a wave's local path index j (within one sample): j itself,
+// or with tiling the row-major order of 8 x 4 tiles of a tile_width-wide
+// image, each tile's 32 pixels row-major inside it, so a warp's camera rays
+// leave a square of the image instead of a 32-pixel strip.
+__host__ __device__ inline uint32_t wave_pixel(uint32_t j, uint32_t tile_width) {
+    if (tile_width == 0u) return j;
+    const uint32_t t = j >> 5, k = j & 31u, tiles_x = tile_width >> 3;
+    return ((t / tiles_x) * 4u + (k >> 3)) * tile_width + (t % tiles_x) * 8u + (k & 7u);
+}
 
 // One job's share of a multi-job wave (the serving loop): samples
 // sample_base .. sample_base + samples - 1 of pixels pixel_base ..
@@ -165,8 +179,10 @@ struct FilmTargets {
 // channel drops that buffer's sample, depth drops only NaN); reset
 // overwrites with the first sample instead. The guides accumulate when both
 // the pool and the film carry them.
+// With tile_width set (a tiled whole-image wave) local index p is pixel
+// wave_pixel(p, tile_width).
 void launch_accumulate(const PathPool& pool, const FilmTargets& film, uint32_t pixel_base, uint32_t pixel_count,
-                       uint32_t samples, bool reset, cudaStream_t stream);
+                       uint32_t tile_width, uint32_t samples, bool reset, cudaStream_t stream);
 void launch_resolve(const float4* sum, float4* avg, uint32_t pixels, float samples, cudaStream_t stream);
 void launch_resolve1(const float* sum, float* avg, uint32_t pixels, float samples, cudaStream_t stream);
 // The display transform (tonemap.slang): linear ACEScg averages -> sRGB RGBA8.
@@ -195,7 +211,8 @@ void launch_wave_begin_segments(const PathPool& pool, const WaveSegment* segs, u
                                 const uint32_t* hdr, const LaunchShape& ls, cudaStream_t stream);
 void launch_accumulate_segments(const PathPool& pool, const WaveSegment* segs, uint32_t nseg, uint32_t items,
                                 const uint32_t* hdr, cudaStream_t stream);
-void launch_copy_rad(const PathPool& pool, float4* out, uint32_t pixel_base, uint32_t pixel_count, cudaStream_t stream);
+void launch_copy_rad(const PathPool& pool, float4* out, uint32_t pixel_base, uint32_t pixel_count, uint32_t tile_width,
+                     cudaStream_t stream);
 // *counter += n on the device (a graph's progress counter).
 void launch_advance(uint32_t* counter, uint32_t n, cudaStream_t stream);
 
