@@ -336,11 +336,21 @@ cudaError_t upload_texture(const cenote_texture& t, cudaStream_t stream, cudaArr
         fmt = cudaCreateChannelDesc<cudaChannelFormatKindUnsignedBlockCompressed5>();
         block = true;
         break;
+    case CENOTE_TEXTURE_BC7_SRGB:
+        fmt = cudaCreateChannelDesc<cudaChannelFormatKindUnsignedBlockCompressed7SRGB>();
+        block = true;
+        break;
+    case CENOTE_TEXTURE_BC7_UNORM:
+        fmt = cudaCreateChannelDesc<cudaChannelFormatKindUnsignedBlockCompressed7>();
+        block = true;
+        break;
     default:
         return cudaErrorInvalidValue;
     }
     if (block) {
-        row = size_t(w / 4) * (t.format == CENOTE_TEXTURE_BC5_UNORM ? 16 : 8);
+        const bool wide = t.format == CENOTE_TEXTURE_BC5_UNORM || t.format == CENOTE_TEXTURE_BC7_SRGB ||
+                          t.format == CENOTE_TEXTURE_BC7_UNORM;
+        row = size_t(w / 4) * (wide ? 16 : 8);
         rows = h / 4;
     }
     cudaError_t e = cudaMallocArray(arr, &fmt, w, h);
@@ -356,7 +366,10 @@ cudaError_t upload_texture(const cenote_texture& t, cudaStream_t stream, cudaArr
     td.addressMode[1] = cudaAddressModeWrap;
     td.filterMode = cudaFilterModeLinear;
     td.normalizedCoords = 1;
-    td.sRGB = (t.format == CENOTE_TEXTURE_RGBA8_SRGB || t.format == CENOTE_TEXTURE_BC1_SRGB) ? 1 : 0;
+    td.sRGB = (t.format == CENOTE_TEXTURE_RGBA8_SRGB || t.format == CENOTE_TEXTURE_BC1_SRGB ||
+               t.format == CENOTE_TEXTURE_BC7_SRGB)
+                  ? 1
+                  : 0;
     td.readMode = t.format == CENOTE_TEXTURE_RGBA32F ? cudaReadModeElementType : cudaReadModeNormalizedFloat;
     e = cudaCreateTextureObject(obj, &res, &td, nullptr);
     if (e != cudaSuccess && block) {

@@ -1,7 +1,7 @@
-// Host texture prep: sizes and a BC1/BC4/BC5 block encoder, the step
+// Host texture prep: sizes and the BC block encoders, the step
 // crates/cenote/src/texture.rs:221-405 runs before upload (there with an
-// external BC7/BC6H/BC4/BC5 encoder; here with the formats the CUDA texture
-// unit decodes and the procedural textures of the large scene use).
+// external BC7/BC6H/BC4/BC5 encoder; here BC7 as the reference's colour
+// format, in bc7_encode.cpp, and BC1/BC4/BC5 below).
 //
 // Encoder, per 4x4 block (written for this library):
 //  * BC1: endpoints from the block's principal colour axis (mean + power
@@ -38,6 +38,8 @@ uint64_t texture_bytes(uint32_t format, uint32_t w, uint32_t h) {
     case CENOTE_TEXTURE_BC4_UNORM:
         return (w % 4 || h % 4) ? 0 : (px / 16) * 8;
     case CENOTE_TEXTURE_BC5_UNORM:
+    case CENOTE_TEXTURE_BC7_SRGB:
+    case CENOTE_TEXTURE_BC7_UNORM:
         return (w % 4 || h % 4) ? 0 : (px / 16) * 16;
     default:
         return 0;
@@ -202,22 +204,26 @@ void encode_bc4_block(const uint8_t* v, uint8_t* out) {
 bool texture_encode(uint32_t format, const uint8_t* rgba, uint32_t w, uint32_t h, uint8_t* out) {
     if (texture_bytes(format, w, h) == 0) return false;
     const bool bc1 = format == CENOTE_TEXTURE_BC1_SRGB || format == CENOTE_TEXTURE_BC1_UNORM;
-    if (!bc1 && format != CENOTE_TEXTURE_BC4_UNORM && format != CENOTE_TEXTURE_BC5_UNORM) return false;
+    const bool bc7 = format == CENOTE_TEXTURE_BC7_SRGB || format == CENOTE_TEXTURE_BC7_UNORM;
+    if (!bc1 && !bc7 && format != CENOTE_TEXTURE_BC4_UNORM && format != CENOTE_TEXTURE_BC5_UNORM) return false;
     const uint32_t bw = w / 4, bh = h / 4;
-    const size_t block = format == CENOTE_TEXTURE_BC5_UNORM ? 16 : 8;
+    const size_t block = (format == CENOTE_TEXTURE_BC5_UNORM || bc7) ? 16 : 8;
     auto rows = [&](uint32_t by0, uint32_t by1) {
         for (uint32_t by = by0; by < by1; ++by)
             for (uint32_t bx = 0; bx < bw; ++bx) {
                 uint8_t* dst = out + block * (size_t(by) * bw + bx);
                 Rgb px[16];
-                uint8_t ch[2][16];
+                uint8_t ch[2][16], raw[16][4];
                 for (int t = 0; t < 16; ++t) {
                     const uint8_t* p = rgba + 4 * ((size_t(by) * 4 + t / 4) * w + bx * 4 + t % 4);
                     px[t] = {float(p[0]), float(p[1]), float(p[2])};
                     ch[0][t] = p[0];
                     ch[1][t] = p[1];
+                    std::memcpy(raw[t], p, 4);
                 }
-                if (bc1) {
+                if (bc7) {
+                    encode_bc7_block(raw, dst);
+                } else if (bc1) {
                     encode_bc1_block(px, dst);
                 } else {
                     encode_bc4_block(ch[0], dst);

@@ -408,8 +408,7 @@ class PbrtImport:
                 img = np.concatenate([np.repeat(img[..., :1], 3, 2), img[..., 1:]], 2)
             if img.shape[2] == 3:
                 img = np.concatenate([img, np.full(img.shape[:2] + (1,), 255, np.uint8)], 2)
-            self.textures.append(scenes.Texture(scenes.TEX_RGBA8_SRGB if srgb else scenes.TEX_RGBA8_UNORM,
-                                                img.shape[1], img.shape[0], np.ascontiguousarray(img)))
+            self.textures.append(scenes.prepared_texture(img, "color" if color else "data", srgb))
             self.texture_slots[key] = len(self.textures) - 1
         return self.texture_slots[key]
 

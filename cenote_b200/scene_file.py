@@ -319,8 +319,7 @@ def _texture(sf: SceneFile, ref: dict, kind: str, cache: dict, textures: list) -
         if img.shape[2] == 3:
             img = np.concatenate([img, np.full(img.shape[:2] + (1,), 255, np.uint8)], 2)
         srgb = kind == "color" and (space is None or space.name == "Srgb")
-        tex = scenes.Texture(scenes.TEX_RGBA8_SRGB if srgb else scenes.TEX_RGBA8_UNORM, img.shape[1], img.shape[0],
-                             np.ascontiguousarray(img))
+        tex = scenes.prepared_texture(img, kind, srgb)
     textures.append(tex)
     cache[key] = len(textures) - 1
     return cache[key]

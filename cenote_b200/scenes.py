@@ -320,6 +320,7 @@ class DeltaLight:
 # Texture formats of the bindless table (include/cenote_c.h CENOTE_TEXTURE_*).
 TEX_RGBA8_SRGB, TEX_RGBA8_UNORM, TEX_RGBA32F = 1, 2, 3
 TEX_BC1_SRGB, TEX_BC1_UNORM, TEX_BC4_UNORM, TEX_BC5_UNORM = 4, 5, 6, 7
+TEX_BC7_SRGB, TEX_BC7_UNORM = 8, 9
 
 
 @dataclass
@@ -344,6 +345,23 @@ def rgba8_texture(rgb, srgb: bool = True, alpha=None) -> Texture:
     px[..., :3] = (rgb * np.float32(255) + np.float32(0.5)).astype(np.uint8)
     px[..., 3] = 255 if alpha is None else (np.clip(alpha, 0, 1) * 255 + 0.5).astype(np.uint8)
     return Texture(TEX_RGBA8_SRGB if srgb else TEX_RGBA8_UNORM, w, h, px)
+
+
+def prepared_texture(rgba8, usage: str = "color", srgb: bool = True) -> Texture:
+    """An 8-bit image (H, W, 4) stored the way the reference's texture prep
+    stores it (crates/cenote/src/texture.rs:249-405): colour as BC7 (an sRGB
+    view when `srgb`), scalars as BC4 on red, tangent-space normals as BC5 on
+    x/y. An image whose sides are not multiples of 4 stays RGBA8 (the
+    reference pads it to whole blocks instead)."""
+    from . import encode_texture  # host BC encoder of the library
+
+    rgba8 = np.ascontiguousarray(rgba8, np.uint8)
+    h, w = rgba8.shape[:2]
+    tex = Texture(TEX_RGBA8_SRGB if srgb else TEX_RGBA8_UNORM, w, h, rgba8)
+    if w % 4 or h % 4:
+        return tex
+    fmt = {"color": TEX_BC7_SRGB if srgb else TEX_BC7_UNORM, "data": TEX_BC4_UNORM, "normal": TEX_BC5_UNORM}[usage]
+    return encode_texture(fmt, tex)
 
 
 def _lerp_axis(n: int, cells: int, wrap: bool):
@@ -536,9 +554,9 @@ def load_spec(path) -> tuple[SceneSpec, dict]:
     return spec, {k[2:]: z[k] for k in z.files if k.startswith("x_")}
 
 
-def textured(width=160, height=90, spp=8, max_bounces=6, size=64, seed=7) -> SceneSpec:
+def textured(width=160, height=90, spp=8, max_bounces=6, size=64, seed=7, color_format=TEX_BC1_SRGB) -> SceneSpec:
     """Every texture slot and format on one small set: a ground tiled 4x with a
-    BC1 sRGB base colour, a BC5 normal map and a BC4 roughness map; a metal
+    base colour in `color_format` (BC1 or BC7 sRGB), a BC5 normal map and a BC4 roughness map; a metal
     panel with an RGBA8 metalness map; a leaf quad cut out by a BC4 opacity
     map; a ceiling emitter whose emission an RGBA8 sRGB map modulates; an
     RGBA32F base colour on a back wall. Textures are seeded value noise."""
@@ -547,7 +565,7 @@ def textured(width=160, height=90, spp=8, max_bounces=6, size=64, seed=7) -> Sce
     noise = [value_noise(size, seed + k) for k in range(6)]
     col = np.stack([0.2 + 0.7 * noise[0], 0.2 + 0.6 * noise[1], 0.1 + 0.5 * noise[0] * noise[2]], -1)
     textures = [
-        encode_texture(TEX_BC1_SRGB, rgba8_texture(col, srgb=True)),                                 # 0 base colour
+        encode_texture(color_format, rgba8_texture(col, srgb=True)),                                 # 0 base colour
         encode_texture(TEX_BC5_UNORM, rgba8_texture(normal_map_from_height(noise[3], 6.0), False)),  # 1 normal
         encode_texture(TEX_BC4_UNORM, rgba8_texture(np.repeat(0.15 + 0.8 * noise[4][..., None], 3, -1), False)),
         rgba8_texture(np.repeat((noise[5] > 0.5)[..., None].astype(float), 3, -1), srgb=False),       # 3 metalness

@@ -129,6 +129,8 @@ typedef struct cenote_camera {
 #define CENOTE_TEXTURE_BC1_UNORM 5u   /* BC1 blocks, linear */
 #define CENOTE_TEXTURE_BC4_UNORM 6u   /* BC4 blocks: one channel (scalar masks) */
 #define CENOTE_TEXTURE_BC5_UNORM 7u   /* BC5 blocks: two channels (tangent-space normals) */
+#define CENOTE_TEXTURE_BC7_SRGB 8u    /* BC7 blocks, RGBA colour in sRGB transfer (texture.rs:249-281) */
+#define CENOTE_TEXTURE_BC7_UNORM 9u   /* BC7 blocks, RGBA linear */
 
 typedef struct cenote_texture {
     uint32_t format; /* CENOTE_TEXTURE_* */
@@ -136,14 +138,16 @@ typedef struct cenote_texture {
     uint32_t height;
     uint32_t pad;
     /* Row 0 first: w·h texels, or the 4x4 blocks row-major over w/4 x h/4
-     * (8 bytes per BC1/BC4 block, 16 per BC5 block). */
+     * (8 bytes per BC1/BC4 block, 16 per BC5/BC7 block). */
     const void* data;
 } cenote_texture;
 
 /* Bytes of `data` for a texture of this format and size; 0 if invalid. */
 uint64_t cenote_texture_bytes(uint32_t format, uint32_t width, uint32_t height);
-/* Encode RGBA8 texels (w·h·4 bytes, row 0 first) into BC1 (RGB), BC4 (R) or
- * BC5 (R, G) blocks: `out` holds cenote_texture_bytes(format, w, h) bytes.
+/* Encode RGBA8 texels (w·h·4 bytes, row 0 first) into BC1 (RGB), BC4 (R),
+ * BC5 (R, G) or BC7 (RGBA; the bytes as stored, so an sRGB texture is
+ * encoded in its stored space) blocks: `out` holds
+ * cenote_texture_bytes(format, w, h) bytes.
  * Host work, no device needed (the prep step of texture.rs:221-405). */
 int32_t cenote_texture_encode(uint32_t format, const uint8_t* rgba8, uint32_t width, uint32_t height, void* out);
 

@@ -34,7 +34,19 @@ FORMATS = {
     "bc1_unorm": (T.TEX_BC1_UNORM, 8),
     "bc4": (T.TEX_BC4_UNORM, 8),
     "bc5": (T.TEX_BC5_UNORM, 16),
+    "bc7_srgb": (T.TEX_BC7_SRGB, 16),
+    "bc7_unorm": (T.TEX_BC7_UNORM, 16),
 }
+
+
+def bc7_blocks(n, rng):
+    """n random BC7 blocks cycling through the eight modes and the invalid
+    ninth (no mode bit in the first byte)."""
+    b = rng.integers(0, 256, (n, 16), dtype=np.uint8)
+    for k in range(n):
+        mode = k % 9
+        b[k, 0] = 0 if mode == 8 else (int(b[k, 0]) & ~((1 << (mode + 1)) - 1) & 255) | (1 << mode)
+    return b.reshape(-1)
 
 
 def random_texture(fmt, bpb, size, rng):
@@ -42,6 +54,8 @@ def random_texture(fmt, bpb, size, rng):
         data = rng.integers(0, 256, size * size * 4, dtype=np.uint8)
     elif bpb < 0:
         data = (rng.random((size, size, 4)) * 4.0).astype(np.float32)
+    elif fmt in (T.TEX_BC7_SRGB, T.TEX_BC7_UNORM):
+        data = bc7_blocks((size // 4) * (size // 4), rng)
     else:
         data = rng.integers(0, 256, (size // 4) * (size // 4) * bpb, dtype=np.uint8)
     return T.Texture(fmt, size, size, data)

@@ -170,9 +170,9 @@ def test_textured_material_and_ply_mesh(tmp_path):
         Instance((name: "i", mesh: Some("tri"), material: Some("m"))),
     ])""")
     spec = load_scene_file(tmp_path / "t.ron", 16, 16)
-    assert len(spec.textures) == 2  # colour (sRGB) and data (linear) views of one image
+    assert len(spec.textures) == 2  # colour (BC7, sRGB view) and data (BC4 on red) of one image
     fmts = sorted(t.format for t in spec.textures)
-    assert fmts == [scenes.TEX_RGBA8_SRGB, scenes.TEX_RGBA8_UNORM]
+    assert fmts == [scenes.TEX_BC4_UNORM, scenes.TEX_BC7_SRGB]
     m = spec.objects[0].material
     assert m["base_color_texture"] != m["specular_roughness_texture"]
     assert np.allclose(spec.objects[0].mesh.normals, [0, 0, 1])

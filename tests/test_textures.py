@@ -223,7 +223,8 @@ def test_oracle_reproduces_the_texture_units_taps():
     of every format bit for bit (BC4: red; BC5: red and green)."""
     g = np.load(pathlib.Path(__file__).parent / "golden" / "texture_unit_taps.npz")
     codes = {"rgba8_srgb": T.TEX_RGBA8_SRGB, "rgba8_unorm": T.TEX_RGBA8_UNORM, "rgba32f": T.TEX_RGBA32F,
-             "bc1_srgb": T.TEX_BC1_SRGB, "bc1_unorm": T.TEX_BC1_UNORM, "bc4": T.TEX_BC4_UNORM, "bc5": T.TEX_BC5_UNORM}
+             "bc1_srgb": T.TEX_BC1_SRGB, "bc1_unorm": T.TEX_BC1_UNORM, "bc4": T.TEX_BC4_UNORM, "bc5": T.TEX_BC5_UNORM,
+             "bc7_srgb": T.TEX_BC7_SRGB, "bc7_unorm": T.TEX_BC7_UNORM}
     for name, fmt in codes.items():
         data = g[name + "_data"]
         if fmt == T.TEX_RGBA32F:
@@ -234,10 +235,116 @@ def test_oracle_reproduces_the_texture_units_taps():
         assert np.array_equal(got, g[name + "_taps"][:, :ch]), name
 
 
+# ---- BC7 ------------------------------------------------------------------------------
+
+
+def bc7_blocks(n, seed=5, modes=range(8)):
+    """n random BC7 blocks, cycling through `modes` (8: the invalid ninth,
+    no mode bit in the first byte)."""
+    modes = list(modes)
+    b = np.random.default_rng(seed).integers(0, 256, (n, 16), dtype=np.uint8)
+    for k in range(n):
+        m = modes[k % len(modes)]
+        b[k, 0] = 0 if m == 8 else (int(b[k, 0]) & ~((1 << (m + 1)) - 1) & 255) | (1 << m)
+    return b
+
+
+def bc7_bytes(blocks, w, h):
+    """RGBA8 texels (h, w, 4) of a BC7 texture, as the oracle decodes them."""
+    tex = T.Texture(T.TEX_BC7_UNORM, w, h, np.ascontiguousarray(blocks).reshape(-1))
+    return np.rint(oracle.texture_decode(tex) * 255).astype(np.uint8)
+
+
+def test_bc7_decoder_matches_an_independent_decoder():
+    """The oracle's BC7 decoder (the format restated from its definition)
+    against Pillow's BCn decoder on 4,096 random blocks of each of the eight
+    modes: every texel equal. (Pillow returns opaque black for a block with no
+    mode bit, where the oracle follows the texture unit; the GPU taps check
+    that case.)"""
+    Image = pytest.importorskip("PIL.Image")
+    for mode in range(8):
+        b = bc7_blocks(4096, seed=mode, modes=[mode])
+        ours = bc7_bytes(b, 256, 64)
+        theirs = np.asarray(Image.frombytes("RGBA", (256, 64), b.tobytes(), "bcn", 7))
+        assert np.array_equal(ours, theirs), mode
+
+
+def test_bc7_tables_are_the_formats():
+    """Spot checks of the generated partition and anchor tables against the
+    format's definition: partition 0 splits the block into columns {0, 1} and
+    {2, 3}, partition 13 into rows {0, 1} and {2, 3}; the first sixteen
+    two-subset partitions anchor subset 1 at texel 15; each anchor lies in
+    its own subset."""
+    text = (pathlib.Path(__file__).resolve().parents[1] / "cenote_b200" / "csrc" / "bc7_tables.h").read_text()
+    import re
+
+    def table(name):
+        body = text[text.index(name):]
+        body = body[body.index("{") + 1:body.index("};")]
+        return np.array([int(x) for x in re.findall(r"\d+", body)])
+
+    p2, p3 = table("PARTITION2").reshape(64, 16), table("PARTITION3").reshape(64, 16)
+    a2, a3 = table("ANCHOR2"), table("ANCHOR3").reshape(64, 2)
+    assert p2[0].tolist() == [0, 0, 1, 1] * 4
+    assert p2[13].tolist() == [0] * 8 + [1] * 8
+    assert (a2[:16] == 15).all()
+    assert all(p2[k, a2[k]] == 1 for k in range(64))
+    assert all(p3[k, a3[k, 0]] == 1 and p3[k, a3[k, 1]] == 2 for k in range(64))
+    assert (p2[:, 0] == 0).all() and (p3[:, 0] == 0).all()
+
+
+def test_bc7_encoder():
+    """The library's BC7 encoder: a smooth texture round-trips above 45 dB
+    PSNR, a busy one at least 4 dB above BC1, blocks of one colour exactly
+    (the reference's checker floor, two colours in 4x4-aligned squares,
+    decodes to its own bytes), random opaque blocks at least as well as BC1,
+    and sRGB and linear textures encode to the same blocks (the encoder sees
+    the stored bytes)."""
+
+    def psnr(a, b):
+        mse = np.mean((a.astype(float) - b.astype(float)) ** 2)
+        return np.inf if mse == 0 else 10 * np.log10(255.0 ** 2 / mse)
+
+    def noise(size):
+        return T.rgba8_texture(np.stack([T.value_noise(size, k, octaves=3) for k in (1, 2, 3)], -1), srgb=False)
+
+    src = noise(256)
+    enc = encode_texture(T.TEX_BC7_UNORM, src)
+    assert enc.data.size == 256 * 256
+    assert psnr(bc7_bytes(enc.data, 256, 256), src.data) > 45.0
+    busy = noise(64)
+    bc1 = np.rint(oracle.texture_decode(encode_texture(T.TEX_BC1_UNORM, busy)) * 255).astype(np.uint8)
+    bc7 = bc7_bytes(encode_texture(T.TEX_BC7_UNORM, busy).data, 64, 64)
+    assert psnr(bc7[..., :3], busy.data[..., :3]) > psnr(bc1[..., :3], busy.data[..., :3]) + 4.0
+    srgb = encode_texture(T.TEX_BC7_SRGB, T.Texture(T.TEX_RGBA8_SRGB, 256, 256, src.data))
+    assert np.array_equal(srgb.data, enc.data)
+
+    checker = np.empty((32, 32, 4), np.uint8)
+    cells = ((np.arange(32)[:, None] // 8 + np.arange(32)[None, :] // 8) % 2).astype(bool)
+    checker[...] = (154, 151, 137, 255)
+    checker[cells] = (221, 219, 215, 255)
+    enc = encode_texture(T.TEX_BC7_SRGB, T.Texture(T.TEX_RGBA8_SRGB, 32, 32, checker))
+    assert np.array_equal(bc7_bytes(enc.data, 32, 32), checker)
+    solid = np.random.default_rng(4).integers(0, 256, (256, 4), dtype=np.uint8)
+    tiles = np.repeat(np.repeat(solid.reshape(16, 16, 4), 4, 0), 4, 1)
+    enc = encode_texture(T.TEX_BC7_UNORM, T.Texture(T.TEX_RGBA8_UNORM, 64, 64, np.ascontiguousarray(tiles)))
+    err = np.abs(bc7_bytes(enc.data, 64, 64).astype(int) - tiles).max(-1)
+    assert (err == 0).mean() > 0.9 and err.max() <= 1
+
+    rnd = np.random.default_rng(9).integers(0, 256, (64, 64, 4), dtype=np.uint8)
+    rnd[..., 3] = 255
+    tex = T.Texture(T.TEX_RGBA8_UNORM, 64, 64, rnd)
+    bc7 = bc7_bytes(encode_texture(T.TEX_BC7_UNORM, tex).data, 64, 64)
+    bc1 = np.rint(oracle.texture_decode(encode_texture(T.TEX_BC1_UNORM, tex)) * 255).astype(np.uint8)
+    assert psnr(bc7[..., :3], rnd[..., :3]) >= psnr(bc1[..., :3], rnd[..., :3])
+    assert (bc7[..., 3] == 255).all()
+
+
 # ---- the texture unit against the oracle -----------------------------------------------
 
 
-FORMATS = ["rgba8_srgb", "rgba8_unorm", "rgba32f", "bc1_srgb", "bc1_unorm", "bc4", "bc5"]
+FORMATS = ["rgba8_srgb", "rgba8_unorm", "rgba32f", "bc1_srgb", "bc1_unorm", "bc4", "bc5", "bc7_srgb", "bc7_unorm",
+           "bc7_modes", "bc7_modes_srgb"]
 
 
 def make_texture(kind, size=32):
@@ -246,9 +353,13 @@ def make_texture(kind, size=32):
     if kind == "rgba32f":
         return T.Texture(T.TEX_RGBA32F, size, size,
                          np.concatenate([rgb * 4.0, rng.random((size, size, 1))], -1).astype(np.float32))
+    if kind.startswith("bc7_modes"):  # random blocks of every mode, the invalid one included
+        fmt = T.TEX_BC7_SRGB if kind.endswith("srgb") else T.TEX_BC7_UNORM
+        return T.Texture(fmt, size, size, bc7_blocks((size // 4) ** 2, modes=range(9)).reshape(-1))
     src = T.rgba8_texture(rgb, srgb=kind.endswith("srgb"))
     fmt = {"rgba8_srgb": None, "rgba8_unorm": None, "bc1_srgb": T.TEX_BC1_SRGB, "bc1_unorm": T.TEX_BC1_UNORM,
-           "bc4": T.TEX_BC4_UNORM, "bc5": T.TEX_BC5_UNORM}[kind]
+           "bc4": T.TEX_BC4_UNORM, "bc5": T.TEX_BC5_UNORM, "bc7_srgb": T.TEX_BC7_SRGB,
+           "bc7_unorm": T.TEX_BC7_UNORM}[kind]
     return src if fmt is None else encode_texture(fmt, src)
 
 
@@ -302,10 +413,11 @@ def gpu_render(ctx, spec, spp, max_bounces):
 
 
 @pytest.mark.gpu
-def test_gpu_textured_render_matches_oracle(ctx):
+@pytest.mark.parametrize("color_format", [T.TEX_BC1_SRGB, T.TEX_BC7_SRGB])
+def test_gpu_textured_render_matches_oracle(ctx, color_format):
     from cenote_b200.metrics import rel_mse
 
-    spec = T.textured(96, 54, 16, 6)
+    spec = T.textured(96, 54, 16, 6, color_format=color_format)
     got = gpu_render(ctx, spec, 16, 6)
     ref = oracle.OracleScene(spec).render_guides(96, 54, 0, 16, 6)
     ref = {k: v / 16 for k, v in ref.items()}
