@@ -123,6 +123,7 @@ EXPORTED_SYMBOLS = [
     "cenote_film_device_sums", "cenote_probe_sampler", "cenote_probe_bsdf", "cenote_probe_bsdf_sample",
     "cenote_probe_intersect", "cenote_probe_intersect_queued", "cenote_probe_shadow", "cenote_probe_shadow_queued", "cenote_probe_env_sample", "cenote_probe_env_pdf",
     "cenote_env_tables_static", "cenote_scene_create_textured", "cenote_texture_bytes", "cenote_texture_encode",
+    "cenote_texture_encode_float",
     "cenote_probe_texture", "cenote_server_create", "cenote_server_destroy", "cenote_job_submit", "cenote_job_poll",
     "cenote_job_wait", "cenote_job_result", "cenote_job_release", "cenote_server_stats", "cenote_guide_create",
     "cenote_guide_destroy", "cenote_guide_params", "cenote_guide_set_params", "cenote_guide_forward",
@@ -155,6 +156,7 @@ def library() -> C.CDLL:
         "cenote_scene_create_textured": (I32, [P, P, U32, P, P, P, U32, P, U32, P]),
         "cenote_texture_bytes": (C.c_uint64, [U32, U32, U32]),
         "cenote_texture_encode": (I32, [U32, P, U32, U32, P]),
+        "cenote_texture_encode_float": (I32, [U32, P, U32, U32, P]),
         "cenote_probe_texture": (I32, [P, U32, U32, P, U32, P]),
         "cenote_server_create": (I32, [P, C.c_uint64, P, P]),
         "cenote_server_destroy": (None, [P]),
@@ -350,6 +352,17 @@ def encode_texture(fmt: int, tex: scenes.Texture) -> scenes.Texture:
         raise CenoteError(-1, f"format {fmt} cannot hold a {tex.width}x{tex.height} texture")
     out = np.zeros(n, np.uint8)
     _check(library().cenote_texture_encode(fmt, _ptr(src), tex.width, tex.height, _ptr(out)))
+    return scenes.Texture(fmt, tex.width, tex.height, out)
+
+
+def encode_texture_float(fmt: int, tex: scenes.Texture) -> scenes.Texture:
+    """BC6H-encode an RGBA32F texture (unsigned; the host prep step)."""
+    src = np.ascontiguousarray(tex.data, np.float32)
+    n = texture_bytes(fmt, tex.width, tex.height)
+    if n == 0:
+        raise CenoteError(-1, f"format {fmt} cannot hold a {tex.width}x{tex.height} texture")
+    out = np.zeros(n, np.uint8)
+    _check(library().cenote_texture_encode_float(fmt, _ptr(src), tex.width, tex.height, _ptr(out)))
     return scenes.Texture(fmt, tex.width, tex.height, out)
 
 

@@ -21,7 +21,7 @@ LIB = PKG / "libcenote_b200.so"
 
 CU_SOURCES = ["wavefront.cu", "probes.cu", "env_build.cu", "guide.cu", "bvh_gpu.cu"]
 CPP_SOURCES = ["capi.cpp", "runtime.cpp", "server.cpp", "guide_api.cpp", "bvh_build.cpp", "texture_prep.cpp",
-               "bc7_encode.cpp"]
+               "bc7_encode.cpp", "bc6h_encode.cpp"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
 

@@ -344,12 +344,21 @@ cudaError_t upload_texture(const cenote_texture& t, cudaStream_t stream, cudaArr
         fmt = cudaCreateChannelDesc<cudaChannelFormatKindUnsignedBlockCompressed7>();
         block = true;
         break;
+    case CENOTE_TEXTURE_BC6H_UF16:
+        fmt = cudaCreateChannelDesc<cudaChannelFormatKindUnsignedBlockCompressed6H>();
+        block = true;
+        break;
+    case CENOTE_TEXTURE_BC6H_SF16:
+        fmt = cudaCreateChannelDesc<cudaChannelFormatKindSignedBlockCompressed6H>();
+        block = true;
+        break;
     default:
         return cudaErrorInvalidValue;
     }
     if (block) {
         const bool wide = t.format == CENOTE_TEXTURE_BC5_UNORM || t.format == CENOTE_TEXTURE_BC7_SRGB ||
-                          t.format == CENOTE_TEXTURE_BC7_UNORM;
+                          t.format == CENOTE_TEXTURE_BC7_UNORM || t.format == CENOTE_TEXTURE_BC6H_UF16 ||
+                          t.format == CENOTE_TEXTURE_BC6H_SF16;
         row = size_t(w / 4) * (wide ? 16 : 8);
         rows = h / 4;
     }
@@ -370,7 +379,9 @@ cudaError_t upload_texture(const cenote_texture& t, cudaStream_t stream, cudaArr
                t.format == CENOTE_TEXTURE_BC7_SRGB)
                   ? 1
                   : 0;
-    td.readMode = t.format == CENOTE_TEXTURE_RGBA32F ? cudaReadModeElementType : cudaReadModeNormalizedFloat;
+    const bool floats = t.format == CENOTE_TEXTURE_RGBA32F || t.format == CENOTE_TEXTURE_BC6H_UF16 ||
+                        t.format == CENOTE_TEXTURE_BC6H_SF16;
+    td.readMode = floats ? cudaReadModeElementType : cudaReadModeNormalizedFloat;
     e = cudaCreateTextureObject(obj, &res, &td, nullptr);
     if (e != cudaSuccess && block) {
         // Block formats decode to unorm floats by themselves; accept the
@@ -1489,6 +1500,14 @@ int32_t cenote_texture_encode(uint32_t format, const uint8_t* rgba8, uint32_t wi
     CN_CHECK(rgba8 && out, CENOTE_E_INVALID_ARGUMENT, "null argument");
     CN_CHECK(texture_encode(format, rgba8, width, height, static_cast<uint8_t*>(out)), CENOTE_E_INVALID_ARGUMENT,
              "not a BC format, or a size it cannot take (BC extents are multiples of 4)");
+    return CENOTE_OK;
+}
+
+int32_t cenote_texture_encode_float(uint32_t format, const float* rgba32f, uint32_t width, uint32_t height,
+                                    void* out) {
+    CN_CHECK(rgba32f && out, CENOTE_E_INVALID_ARGUMENT, "null argument");
+    CN_CHECK(texture_encode_float(format, rgba32f, width, height, static_cast<uint8_t*>(out)),
+             CENOTE_E_INVALID_ARGUMENT, "not BC6H unsigned, or a size it cannot take (extents are multiples of 4)");
     return CENOTE_OK;
 }
 

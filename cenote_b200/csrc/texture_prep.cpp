@@ -40,6 +40,8 @@ uint64_t texture_bytes(uint32_t format, uint32_t w, uint32_t h) {
     case CENOTE_TEXTURE_BC5_UNORM:
     case CENOTE_TEXTURE_BC7_SRGB:
     case CENOTE_TEXTURE_BC7_UNORM:
+    case CENOTE_TEXTURE_BC6H_UF16:
+    case CENOTE_TEXTURE_BC6H_SF16:
         return (w % 4 || h % 4) ? 0 : (px / 16) * 16;
     default:
         return 0;
@@ -232,6 +234,26 @@ bool texture_encode(uint32_t format, const uint8_t* rgba, uint32_t w, uint32_t h
             }
     };
     // Blocks are independent: split the block rows over the host's threads.
+    const uint32_t threads = std::max(1u, std::min(std::thread::hardware_concurrency(), std::max(1u, bh / 16)));
+    std::vector<std::thread> pool;
+    for (uint32_t k = 0; k < threads; ++k)
+        pool.emplace_back(rows, bh * k / threads, bh * (k + 1) / threads);
+    for (auto& t : pool) t.join();
+    return true;
+}
+
+bool texture_encode_float(uint32_t format, const float* rgba, uint32_t w, uint32_t h, uint8_t* out) {
+    if (format != CENOTE_TEXTURE_BC6H_UF16 || texture_bytes(format, w, h) == 0) return false;
+    const uint32_t bw = w / 4, bh = h / 4;
+    auto rows = [&](uint32_t by0, uint32_t by1) {
+        for (uint32_t by = by0; by < by1; ++by)
+            for (uint32_t bx = 0; bx < bw; ++bx) {
+                float px[16][4];
+                for (int t = 0; t < 16; ++t)
+                    std::memcpy(px[t], rgba + 4 * ((size_t(by) * 4 + t / 4) * w + bx * 4 + t % 4), 16);
+                encode_bc6h_block(px, out + 16 * (size_t(by) * bw + bx));
+            }
+    };
     const uint32_t threads = std::max(1u, std::min(std::thread::hardware_concurrency(), std::max(1u, bh / 16)));
     std::vector<std::thread> pool;
     for (uint32_t k = 0; k < threads; ++k)

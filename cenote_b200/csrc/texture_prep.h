@@ -13,5 +13,11 @@ bool texture_encode(uint32_t format, const uint8_t* rgba, uint32_t width, uint32
 // One 4x4 block of RGBA8 texels (row-major) -> one 16-byte BC7 block
 // (bc7_encode.cpp).
 void encode_bc7_block(const uint8_t px[16][4], uint8_t out[16]);
+// RGBA float texels -> BC6H unsigned blocks (RGB; alpha is dropped); false
+// for another format or an invalid size.
+bool texture_encode_float(uint32_t format, const float* rgba, uint32_t width, uint32_t height, uint8_t* out);
+// One 4x4 block of RGBA floats (row-major) -> one 16-byte BC6H unsigned
+// block (bc6h_encode.cpp).
+void encode_bc6h_block(const float px[16][4], uint8_t out[16]);
 
 }  // namespace cn

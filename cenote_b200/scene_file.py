@@ -309,7 +309,7 @@ def _texture(sf: SceneFile, ref: dict, kind: str, cache: dict, textures: list) -
         ch = read_exr(path)
         rgba = np.stack([ch["R"], ch.get("G", ch["R"]), ch.get("B", ch["R"]),
                          ch.get("A", np.ones_like(ch["R"]))], -1).astype(np.float32)
-        tex = scenes.Texture(scenes.TEX_RGBA32F, rgba.shape[1], rgba.shape[0], np.ascontiguousarray(rgba))
+        tex = scenes.prepared_float_texture(rgba, kind)
     else:
         img = read_png(path)
         if img.shape[2] == 1:

@@ -321,6 +321,7 @@ class DeltaLight:
 TEX_RGBA8_SRGB, TEX_RGBA8_UNORM, TEX_RGBA32F = 1, 2, 3
 TEX_BC1_SRGB, TEX_BC1_UNORM, TEX_BC4_UNORM, TEX_BC5_UNORM = 4, 5, 6, 7
 TEX_BC7_SRGB, TEX_BC7_UNORM = 8, 9
+TEX_BC6H_UF16, TEX_BC6H_SF16 = 10, 11
 
 
 @dataclass
@@ -362,6 +363,23 @@ def prepared_texture(rgba8, usage: str = "color", srgb: bool = True) -> Texture:
         return tex
     fmt = {"color": TEX_BC7_SRGB if srgb else TEX_BC7_UNORM, "data": TEX_BC4_UNORM, "normal": TEX_BC5_UNORM}[usage]
     return encode_texture(fmt, tex)
+
+
+def prepared_float_texture(rgba32f, usage: str = "color") -> Texture:
+    """A float image (H, W, 4) stored the way the reference's prep stores it
+    (texture.rs:283-405): colour as BC6H unsigned (negatives clamp to zero,
+    alpha dropped), scalars and normal maps quantised to 8 bits
+    (round(clamp(v, 0, 1) * 255)) and then BC4 / BC5. Sides that are not
+    multiples of 4 keep RGBA32F for colour."""
+    from . import encode_texture_float
+
+    rgba32f = np.ascontiguousarray(rgba32f, np.float32)
+    h, w = rgba32f.shape[:2]
+    if usage == "color":
+        tex = Texture(TEX_RGBA32F, w, h, rgba32f)
+        return tex if (w % 4 or h % 4) else encode_texture_float(TEX_BC6H_UF16, tex)
+    q = np.rint(np.clip(rgba32f, 0.0, 1.0) * np.float32(255)).astype(np.uint8)
+    return prepared_texture(q, usage, srgb=False)
 
 
 def _lerp_axis(n: int, cells: int, wrap: bool):

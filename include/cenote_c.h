@@ -131,6 +131,8 @@ typedef struct cenote_camera {
 #define CENOTE_TEXTURE_BC5_UNORM 7u   /* BC5 blocks: two channels (tangent-space normals) */
 #define CENOTE_TEXTURE_BC7_SRGB 8u    /* BC7 blocks, RGBA colour in sRGB transfer (texture.rs:249-281) */
 #define CENOTE_TEXTURE_BC7_UNORM 9u   /* BC7 blocks, RGBA linear */
+#define CENOTE_TEXTURE_BC6H_UF16 10u  /* BC6H blocks, unsigned FP16 RGB (HDR colour, texture.rs:283-306) */
+#define CENOTE_TEXTURE_BC6H_SF16 11u  /* BC6H blocks, signed FP16 RGB */
 
 typedef struct cenote_texture {
     uint32_t format; /* CENOTE_TEXTURE_* */
@@ -138,7 +140,7 @@ typedef struct cenote_texture {
     uint32_t height;
     uint32_t pad;
     /* Row 0 first: w·h texels, or the 4x4 blocks row-major over w/4 x h/4
-     * (8 bytes per BC1/BC4 block, 16 per BC5/BC7 block). */
+     * (8 bytes per BC1/BC4 block, 16 per BC5/BC6H/BC7 block). */
     const void* data;
 } cenote_texture;
 
@@ -150,6 +152,11 @@ uint64_t cenote_texture_bytes(uint32_t format, uint32_t width, uint32_t height);
  * cenote_texture_bytes(format, w, h) bytes.
  * Host work, no device needed (the prep step of texture.rs:221-405). */
 int32_t cenote_texture_encode(uint32_t format, const uint8_t* rgba8, uint32_t width, uint32_t height, void* out);
+/* Encode RGBA float texels (w·h·4 floats, row 0 first) into BC6H unsigned
+ * blocks (CENOTE_TEXTURE_BC6H_UF16: RGB, negatives clamp to zero, alpha is
+ * dropped), as texture.rs:283-306 prepares float colour. Host work. */
+int32_t cenote_texture_encode_float(uint32_t format, const float* rgba32f, uint32_t width, uint32_t height,
+                                    void* out);
 
 /* Equirect environment, RGBA f32 ACEScg, row 0 = +Y (environment.rs:33-79). */
 typedef struct cenote_environment {

@@ -36,7 +36,22 @@ FORMATS = {
     "bc5": (T.TEX_BC5_UNORM, 16),
     "bc7_srgb": (T.TEX_BC7_SRGB, 16),
     "bc7_unorm": (T.TEX_BC7_UNORM, 16),
+    "bc6h_uf16": (T.TEX_BC6H_UF16, 16),
+    "bc6h_sf16": (T.TEX_BC6H_SF16, 16),
 }
+
+# BC6H mode bits (two for modes 1-2, five for the rest) and one reserved value.
+BC6H_MODE_BITS = [0, 1, 2, 6, 10, 14, 18, 22, 26, 30, 3, 7, 11, 15, 19]
+
+
+def bc6h_blocks(n, rng):
+    """n random BC6H blocks cycling through the fourteen modes and a reserved one."""
+    b = rng.integers(0, 256, (n, 16), dtype=np.uint8)
+    for k in range(n):
+        mv = BC6H_MODE_BITS[k % len(BC6H_MODE_BITS)]
+        mask = 3 if mv < 2 else 31
+        b[k, 0] = (int(b[k, 0]) & ~mask & 255) | mv
+    return b.reshape(-1)
 
 
 def bc7_blocks(n, rng):
@@ -56,6 +71,8 @@ def random_texture(fmt, bpb, size, rng):
         data = (rng.random((size, size, 4)) * 4.0).astype(np.float32)
     elif fmt in (T.TEX_BC7_SRGB, T.TEX_BC7_UNORM):
         data = bc7_blocks((size // 4) * (size // 4), rng)
+    elif fmt in (T.TEX_BC6H_UF16, T.TEX_BC6H_SF16):
+        data = bc6h_blocks((size // 4) * (size // 4), rng)
     else:
         data = rng.integers(0, 256, (size // 4) * (size // 4) * bpb, dtype=np.uint8)
     return T.Texture(fmt, size, size, data)

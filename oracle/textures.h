@@ -66,6 +66,11 @@
 // tables, and RGBA8 out. bc7_block restates it; the texture unit then filters
 // the bytes as it filters RGBA8 (sRGB or linear), which the GPU test checks
 // tap by tap on random blocks of every mode.
+//
+// BC6H decodes exactly too (bc6h_block; the unit's texel-centre taps equal it
+// in all fourteen modes, signed and unsigned, a wrapped endpoint of the
+// signed transformed modes sign-extended as the format says), and its FP16
+// texels filter as unit_filter_half states.
 #pragma once
 #include <cmath>
 #include <cstdint>
@@ -87,6 +92,8 @@ enum TexFormat : uint32_t {
     TEX_BC5_UNORM = 7,
     TEX_BC7_SRGB = 8,
     TEX_BC7_UNORM = 9,
+    TEX_BC6H_UF16 = 10,
+    TEX_BC6H_SF16 = 11,
 };
 
 // The texture unit's sRGB decode: value = SRGB_M[v] · 2^(SRGB_E[v] - 8).
@@ -306,10 +313,226 @@ inline void bc7_block(const uint8_t* b, uint8_t out[16][4]) {
     }
 }
 
+// BC6H (the reference's HDR colour format, texture.rs:283-306): 14 modes of
+// one or two regions (the first 32 two-subset partitions of BC7), a base
+// endpoint and, in the transformed modes, the others as signed deltas from
+// it; endpoints unquantise to 16 bits, interpolate with BC7's 3- or 4-bit
+// weights and scale by 31/64 (unsigned) or 31/32 (signed) into FP16 bits.
+// Each mode's layout is listed below as (field, top bit, bottom bit) runs in
+// stream order, fields 0-11 = r,g,b of endpoints w, x, y, z (the
+// specification's rw..bz), 12 = the partition; a run whose top bit is below
+// its bottom bit is stored reversed (the high bits of modes 13 and 14).
+namespace bc6h_layout {
+struct Run {
+    uint8_t field, hi, lo;
+};
+enum : uint8_t { RW, GW, BW, RX, GX, BX, RY, GY, BY, RZ, GZ, BZ, D };
+struct Mode {
+    uint8_t value;   // the mode bits (2 for modes 1-2, else 5), LSB first
+    uint8_t bits;    // how many mode bits
+    uint8_t regions, transformed, prec, dr, dg, db;
+    Run runs[32];
+    uint8_t nruns;
+};
+}  // namespace bc6h_layout
+
+inline const bc6h_layout::Mode* bc6h_modes() {
+    using namespace bc6h_layout;
+    static const Mode M[14] = {
+        {0, 2, 2, 1, 10, 5, 5, 5,
+         {{GY, 4, 4}, {BY, 4, 4}, {BZ, 4, 4}, {RW, 9, 0}, {GW, 9, 0}, {BW, 9, 0}, {RX, 4, 0}, {GZ, 4, 4}, {GY, 3, 0},
+          {GX, 4, 0}, {BZ, 0, 0}, {GZ, 3, 0}, {BX, 4, 0}, {BZ, 1, 1}, {BY, 3, 0}, {RY, 4, 0}, {BZ, 2, 2}, {RZ, 4, 0},
+          {BZ, 3, 3}, {D, 4, 0}}, 20},
+        {1, 2, 2, 1, 7, 6, 6, 6,
+         {{GY, 5, 5}, {GZ, 4, 4}, {GZ, 5, 5}, {RW, 6, 0}, {BZ, 0, 0}, {BZ, 1, 1}, {BY, 4, 4}, {GW, 6, 0}, {BY, 5, 5},
+          {BZ, 2, 2}, {GY, 4, 4}, {BW, 6, 0}, {BZ, 3, 3}, {BZ, 5, 5}, {BZ, 4, 4}, {RX, 5, 0}, {GY, 3, 0}, {GX, 5, 0},
+          {GZ, 3, 0}, {BX, 5, 0}, {BY, 3, 0}, {RY, 5, 0}, {RZ, 5, 0}, {D, 4, 0}}, 24},
+        {2, 5, 2, 1, 11, 5, 4, 4,
+         {{RW, 9, 0}, {GW, 9, 0}, {BW, 9, 0}, {RX, 4, 0}, {RW, 10, 10}, {GY, 3, 0}, {GX, 3, 0}, {GW, 10, 10},
+          {BZ, 0, 0}, {GZ, 3, 0}, {BX, 3, 0}, {BW, 10, 10}, {BZ, 1, 1}, {BY, 3, 0}, {RY, 4, 0}, {BZ, 2, 2},
+          {RZ, 4, 0}, {BZ, 3, 3}, {D, 4, 0}}, 19},
+        {6, 5, 2, 1, 11, 4, 5, 4,
+         {{RW, 9, 0}, {GW, 9, 0}, {BW, 9, 0}, {RX, 3, 0}, {RW, 10, 10}, {GZ, 4, 4}, {GY, 3, 0}, {GX, 4, 0},
+          {GW, 10, 10}, {GZ, 3, 0}, {BX, 3, 0}, {BW, 10, 10}, {BZ, 1, 1}, {BY, 3, 0}, {RY, 3, 0}, {BZ, 0, 0},
+          {BZ, 2, 2}, {RZ, 3, 0}, {GY, 4, 4}, {BZ, 3, 3}, {D, 4, 0}}, 21},
+        {10, 5, 2, 1, 11, 4, 4, 5,
+         {{RW, 9, 0}, {GW, 9, 0}, {BW, 9, 0}, {RX, 3, 0}, {RW, 10, 10}, {BY, 4, 4}, {GY, 3, 0}, {GX, 3, 0},
+          {GW, 10, 10}, {BZ, 0, 0}, {GZ, 3, 0}, {BX, 4, 0}, {BW, 10, 10}, {BY, 3, 0}, {RY, 3, 0}, {BZ, 1, 1},
+          {BZ, 2, 2}, {RZ, 3, 0}, {BZ, 4, 4}, {BZ, 3, 3}, {D, 4, 0}}, 21},
+        {14, 5, 2, 1, 9, 5, 5, 5,
+         {{RW, 8, 0}, {BY, 4, 4}, {GW, 8, 0}, {GY, 4, 4}, {BW, 8, 0}, {BZ, 4, 4}, {RX, 4, 0}, {GZ, 4, 4}, {GY, 3, 0},
+          {GX, 4, 0}, {BZ, 0, 0}, {GZ, 3, 0}, {BX, 4, 0}, {BZ, 1, 1}, {BY, 3, 0}, {RY, 4, 0}, {BZ, 2, 2}, {RZ, 4, 0},
+          {BZ, 3, 3}, {D, 4, 0}}, 20},
+        {18, 5, 2, 1, 8, 6, 5, 5,
+         {{RW, 7, 0}, {GZ, 4, 4}, {BY, 4, 4}, {GW, 7, 0}, {BZ, 2, 2}, {GY, 4, 4}, {BW, 7, 0}, {BZ, 3, 3}, {BZ, 4, 4},
+          {RX, 5, 0}, {GY, 3, 0}, {GX, 4, 0}, {BZ, 0, 0}, {GZ, 3, 0}, {BX, 4, 0}, {BZ, 1, 1}, {BY, 3, 0}, {RY, 5, 0},
+          {RZ, 5, 0}, {D, 4, 0}}, 20},
+        {22, 5, 2, 1, 8, 5, 6, 5,
+         {{RW, 7, 0}, {BZ, 0, 0}, {BY, 4, 4}, {GW, 7, 0}, {GY, 5, 5}, {GY, 4, 4}, {BW, 7, 0}, {GZ, 5, 5}, {BZ, 4, 4},
+          {RX, 4, 0}, {GZ, 4, 4}, {GY, 3, 0}, {GX, 5, 0}, {GZ, 3, 0}, {BX, 4, 0}, {BZ, 1, 1}, {BY, 3, 0}, {RY, 4, 0},
+          {BZ, 2, 2}, {RZ, 4, 0}, {BZ, 3, 3}, {D, 4, 0}}, 22},
+        {26, 5, 2, 1, 8, 5, 5, 6,
+         {{RW, 7, 0}, {BZ, 1, 1}, {BY, 4, 4}, {GW, 7, 0}, {BY, 5, 5}, {GY, 4, 4}, {BW, 7, 0}, {BZ, 5, 5}, {BZ, 4, 4},
+          {RX, 4, 0}, {GZ, 4, 4}, {GY, 3, 0}, {GX, 4, 0}, {BZ, 0, 0}, {GZ, 3, 0}, {BX, 5, 0}, {BY, 3, 0}, {RY, 4, 0},
+          {BZ, 2, 2}, {RZ, 4, 0}, {BZ, 3, 3}, {D, 4, 0}}, 22},
+        {30, 5, 2, 0, 6, 6, 6, 6,
+         {{RW, 5, 0}, {GZ, 4, 4}, {BZ, 0, 0}, {BZ, 1, 1}, {BY, 4, 4}, {GW, 5, 0}, {GY, 5, 5}, {BY, 5, 5}, {BZ, 2, 2},
+          {GY, 4, 4}, {BW, 5, 0}, {GZ, 5, 5}, {BZ, 3, 3}, {BZ, 5, 5}, {BZ, 4, 4}, {RX, 5, 0}, {GY, 3, 0}, {GX, 5, 0},
+          {GZ, 3, 0}, {BX, 5, 0}, {BY, 3, 0}, {RY, 5, 0}, {RZ, 5, 0}, {D, 4, 0}}, 24},
+        {3, 5, 1, 0, 10, 10, 10, 10,
+         {{RW, 9, 0}, {GW, 9, 0}, {BW, 9, 0}, {RX, 9, 0}, {GX, 9, 0}, {BX, 9, 0}}, 6},
+        {7, 5, 1, 1, 11, 9, 9, 9,
+         {{RW, 9, 0}, {GW, 9, 0}, {BW, 9, 0}, {RX, 8, 0}, {RW, 10, 10}, {GX, 8, 0}, {GW, 10, 10}, {BX, 8, 0},
+          {BW, 10, 10}}, 9},
+        {11, 5, 1, 1, 12, 8, 8, 8,
+         {{RW, 9, 0}, {GW, 9, 0}, {BW, 9, 0}, {RX, 7, 0}, {RW, 10, 11}, {GX, 7, 0}, {GW, 10, 11}, {BX, 7, 0},
+          {BW, 10, 11}}, 9},
+        {15, 5, 1, 1, 16, 4, 4, 4,
+         {{RW, 9, 0}, {GW, 9, 0}, {BW, 9, 0}, {RX, 3, 0}, {RW, 10, 15}, {GX, 3, 0}, {GW, 10, 15}, {BX, 3, 0},
+          {BW, 10, 15}}, 9},
+    };
+    return M;
+}
+
+// One BC6H block into FP16 bit patterns per texel (RGB, row-major); `sign`
+// selects the signed format. A block of a reserved mode decodes to zeros.
+inline void bc6h_block(const uint8_t* b, bool sign, uint16_t out[16][3]) {
+    using namespace bc6h_layout;
+    static constexpr int W3[8] = {0, 9, 18, 27, 37, 46, 55, 64};
+    static constexpr int W4[16] = {0, 4, 9, 13, 17, 21, 26, 30, 34, 38, 43, 47, 51, 55, 60, 64};
+    int pos = 0;
+    auto get = [&](int n) {
+        uint32_t v = 0;
+        for (int i = 0; i < n; ++i, ++pos) v |= uint32_t((b[pos >> 3] >> (pos & 7)) & 1u) << i;
+        return v;
+    };
+    uint32_t mv = get(2);
+    if (mv >= 2) mv |= get(3) << 2;
+    const Mode* mode = nullptr;
+    for (int k = 0; k < 14; ++k)
+        if (bc6h_modes()[k].value == mv) mode = &bc6h_modes()[k];
+    if (!mode) {
+        std::memset(out, 0, sizeof(uint16_t) * 48);
+        return;
+    }
+    int32_t f[13] = {};
+    for (int r = 0; r < mode->nruns; ++r) {
+        const Run& run = mode->runs[r];
+        if (run.hi >= run.lo) {
+            for (int bit = run.lo; bit <= run.hi; ++bit) f[run.field] |= int32_t(get(1)) << bit;
+        } else {
+            for (int bit = run.lo; bit >= run.hi; --bit) f[run.field] |= int32_t(get(1)) << bit;
+        }
+    }
+    const int prec = mode->prec;
+    const int delta[3] = {mode->dr, mode->dg, mode->db};
+    auto sext = [](int32_t v, int bits) { return (v ^ (1 << (bits - 1))) - (1 << (bits - 1)); };
+    const int ne = 2 * mode->regions;
+    int32_t e[4][3];
+    for (int k = 0; k < ne; ++k)
+        for (int c = 0; c < 3; ++c) e[k][c] = f[3 * k + c];
+    if (sign)
+        for (int c = 0; c < 3; ++c) e[0][c] = sext(e[0][c], prec);
+    for (int k = 1; k < ne; ++k)
+        for (int c = 0; c < 3; ++c) {
+            if (mode->transformed) {
+                e[k][c] = (e[0][c] + sext(e[k][c], delta[c])) & ((1 << prec) - 1);
+                if (sign) e[k][c] = sext(e[k][c], prec);
+            } else if (sign) {
+                e[k][c] = sext(e[k][c], prec);
+            }
+        }
+    auto unquantise = [&](int32_t v) -> int32_t {
+        if (!sign) {
+            if (prec >= 15) return v;
+            if (v == 0) return 0;
+            if (v == (1 << prec) - 1) return 0xFFFF;
+            return ((v << 16) + 0x8000) >> prec;
+        }
+        if (prec >= 16) return v;
+        const bool neg = v < 0;
+        int32_t a = neg ? -v : v, u;
+        if (a == 0) u = 0;
+        else if (a >= (1 << (prec - 1)) - 1) u = 0x7FFF;
+        else u = ((a << 15) + 0x4000) >> (prec - 1);
+        return neg ? -u : u;
+    };
+    for (int k = 0; k < ne; ++k)
+        for (int c = 0; c < 3; ++c) e[k][c] = unquantise(e[k][c]);
+    const uint32_t part = uint32_t(f[D]);
+    const int ib = mode->regions == 2 ? 3 : 4;
+    for (int t = 0; t < 16; ++t) {
+        const bool anchor = t == 0 || (mode->regions == 2 && t == bc7::ANCHOR2[part]);
+        const uint32_t i = get(ib - (anchor ? 1 : 0));
+        const int s = mode->regions == 2 ? bc7::PARTITION2[part][t] : 0;
+        const int w = ib == 3 ? W3[i] : W4[i];
+        for (int c = 0; c < 3; ++c) {
+            const int32_t v = ((64 - w) * e[2 * s][c] + w * e[2 * s + 1][c] + 32) >> 6;
+            if (!sign) {
+                out[t][c] = uint16_t((v * 31) >> 6);
+            } else {
+                const int32_t h = v < 0 ? -(((-v) * 31) >> 5) : (v * 31) >> 5;
+                out[t][c] = uint16_t(h < 0 ? 0x8000 | -h : h);
+            }
+        }
+    }
+}
+
+inline float half_to_float(uint16_t h) {
+    const int32_t e = (h >> 10) & 31, m = h & 1023;
+    const float v = e == 0 ? std::ldexp(float(m), -24) : (e == 31 ? (m ? NAN : INFINITY) : std::ldexp(float(m | 1024), e - 25));
+    return (h & 0x8000) ? -v : v;
+}
+
+// The unit's filter of FP16 texels (BC6H, measured on a B200 like the other
+// formats: every tap of random blocks of every mode reproduced): the taps of
+// nonzero weight and value align to the largest one's exponent E, each an
+// 11-bit significand with 4 more fraction bits below it (bits shifted out
+// are dropped), the signed weighted sum is exact, and the result rounds to
+// FP16, ties away from zero.
+inline float unit_filter_half(const float t[4], const int32_t w[4]) {
+    auto parts = [](float v, int64_t* sig, int32_t* e) {
+        int ex;
+        std::frexp(std::fabs(v), &ex);
+        *e = std::max(ex - 1, -14);
+        *sig = int64_t(std::ldexp(std::fabs(v), 10 - *e));
+    };
+    int32_t big = -1000;
+    for (int k = 0; k < 4; ++k)
+        if (w[k] > 0 && t[k] != 0.0f) {
+            int64_t sig;
+            int32_t e;
+            parts(t[k], &sig, &e);
+            big = std::max(big, e);
+        }
+    if (big == -1000) return 0.0f;
+    int64_t s = 0;
+    for (int k = 0; k < 4; ++k)
+        if (w[k] > 0 && t[k] != 0.0f) {
+            int64_t sig;
+            int32_t e;
+            parts(t[k], &sig, &e);
+            const int32_t shift = big - e;
+            const int64_t m = shift >= 40 ? 0 : (sig << 4) >> shift;
+            s += (t[k] < 0.0f ? -1 : 1) * int64_t(w[k]) * m;
+        }
+    // value = s · 2^(big - 22): 10 significand bits, 4 extra, 8 of weight.
+    const bool neg = s < 0;
+    int64_t a = neg ? -s : s;
+    if (a == 0) return 0.0f;
+    int32_t n = 0;
+    while ((a >> n) > 1) ++n;
+    const int32_t lead = n + big - 22;
+    const int32_t drop = (std::max(lead, -14) - 10) - (big - 22);
+    if (drop > 0) a = ((a + (int64_t(1) << (drop - 1))) >> drop) << drop;
+    const float r = std::min(std::ldexp(float(a), big - 22), 65504.0f);
+    return neg ? -r : r;
+}
+
 // A decoded texture: per texel and channel the value the unit returns at the
 // texel's centre (`texels`, linear RGBA float, row 0 first) and the code it
 // filters (`codes`: a 16-bit level, an sRGB byte, or unused for RGBA32F).
-enum ChannelKind : uint32_t { CH_LEVEL = 0, CH_SRGB = 1, CH_FLOAT = 2 };
+enum ChannelKind : uint32_t { CH_LEVEL = 0, CH_SRGB = 1, CH_FLOAT = 2, CH_HALF = 3 };
 
 struct Texture {
     uint32_t width = 0, height = 0;
@@ -344,6 +567,23 @@ struct Texture {
         case TEX_RGBA32F:
             std::memcpy(texels.data(), data, texels.size() * 4);
             return true;
+        case TEX_BC6H_UF16:
+        case TEX_BC6H_SF16: {
+            if (w % 4 || h % 4) return false;
+            for (int c = 0; c < 4; ++c) kind[c] = CH_HALF;
+            const uint32_t bw = w / 4, bh = h / 4;
+            for (uint32_t by = 0; by < bh; ++by)
+                for (uint32_t bx = 0; bx < bw; ++bx) {
+                    uint16_t px[16][3];
+                    bc6h_block(p + 16 * (size_t(by) * bw + bx), format == TEX_BC6H_SF16, px);
+                    for (int t = 0; t < 16; ++t) {
+                        const size_t i = (size_t(by) * 4 + t / 4) * w + bx * 4 + t % 4;
+                        for (int c = 0; c < 3; ++c) texels[4 * i + c] = half_to_float(px[t][c]);
+                        texels[4 * i + 3] = 1.0f;
+                    }
+                }
+            return true;
+        }
         case TEX_BC7_SRGB:
         case TEX_BC7_UNORM: {
             if (w % 4 || h % 4) return false;
@@ -424,9 +664,9 @@ struct Texture {
         unit_weights(a, b, w);
         const uint32_t xs[4] = {x0, x1, x0, x1}, ys[4] = {y0, y0, y1, y1};
         for (int c = 0; c < 4; ++c) {
-            if (kind[c] == CH_FLOAT) {
+            if (kind[c] == CH_FLOAT || kind[c] == CH_HALF) {
                 const float t[4] = {at(x0, y0)[c], at(x1, y0)[c], at(x0, y1)[c], at(x1, y1)[c]};
-                out[c] = unit_filter_float(t, w);
+                out[c] = kind[c] == CH_HALF ? unit_filter_half(t, w) : unit_filter_float(t, w);
             } else if (kind[c] == CH_LEVEL) {
                 int64_t s = 0;
                 for (int k = 0; k < 4; ++k) s += int64_t(w[k]) * code_at(xs[k], ys[k])[c];

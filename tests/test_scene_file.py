@@ -178,6 +178,33 @@ def test_textured_material_and_ply_mesh(tmp_path):
     assert np.allclose(spec.objects[0].mesh.normals, [0, 0, 1])
 
 
+def test_float_textures_are_prepared_like_the_reference(tmp_path):
+    """An EXR texture (texture.rs:283-405): as a colour, BC6H unsigned; as
+    data, quantised to 8 bits and BC4 on red; the colour decodes to the
+    source within BC6H's precision."""
+    from cenote_b200.exr import write_exr
+    import oracle
+
+    rng = np.random.default_rng(3)
+    img = (0.5 + rng.random((8, 8, 1)) * np.array([1.0, 0.9, 0.8])).astype(np.float32)
+    write_exr(tmp_path / "hdr.exr", {"R": img[..., 0], "G": img[..., 1], "B": img[..., 2]})
+    (tmp_path / "tri.ply").write_text("ply\nformat ascii 1.0\nelement vertex 3\nproperty float x\nproperty float y\n"
+                                      "property float z\nelement face 1\nproperty list uchar int vertex_indices\n"
+                                      "end_header\n0 0 0\n1 0 0\n0 1 0\n3 0 1 2\n")
+    (tmp_path / "t.ron").write_text("""(version: 1, ops: [
+        Mesh((name: "tri", source: Some(Ply(path: "tri.ply")))),
+        Material((name: "m", base_color: Some(Texture((path: "hdr.exr"))),
+                  specular_roughness: Some(Texture((path: "hdr.exr"))))),
+        Instance((name: "i", mesh: Some("tri"), material: Some("m"))),
+    ])""")
+    spec = load_scene_file(tmp_path / "t.ron", 16, 16)
+    fmts = sorted(t.format for t in spec.textures)
+    assert fmts == [scenes.TEX_BC4_UNORM, scenes.TEX_BC6H_UF16]
+    colour = next(t for t in spec.textures if t.format == scenes.TEX_BC6H_UF16)
+    back = oracle.texture_decode(colour)[..., :3]
+    assert np.abs(back / img - 1.0).max() < 0.08  # white noise over 1.6 stops in 16 palette steps
+
+
 @pytest.mark.gpu
 def test_gpu_scene_file_renders_like_the_oracle(ctx, tmp_path):
     """A scene loaded from the change-set file, rendered by the CUDA path and
