@@ -40,6 +40,14 @@ constexpr int BLOCK = 128;
 #ifndef CN_SHADE_MIN_BLOCKS
 #define CN_SHADE_MIN_BLOCKS 6
 #endif
+// The same for the variant with the coat, fuzz, transmission and thin-wall
+// lobes, which needs more registers than the layer-free one: 4 (128
+// registers, 82 / 152 bytes of spills per thread instead of 374 / 908 at 80)
+// shades the terrain in 86.2 ms per frame against 87.2 at 6 and 89.0 at 5
+// (two runs each); the layer-free variant keeps 6.
+#ifndef CN_SHADE_LAYERED_MIN_BLOCKS
+#define CN_SHADE_LAYERED_MIN_BLOCKS 4
+#endif
 // The same for the traversal kernels (8 → 64 registers), and for the
 // closest-hit walks alone (which spill a little at 64 registers).
 #ifndef CN_TRAV_MIN_BLOCKS
@@ -484,7 +492,8 @@ __device__ __forceinline__ void close_record(const PathPool& pool, uint32_t path
 // material chart). The arithmetic is the same but for the compiler's choice
 // of fused multiply-adds once the zeros fold: films agree within 2 ulps.
 template <bool AOV, bool GUIDE, bool LAYERS>
-__global__ void __launch_bounds__(BLOCK, CN_SHADE_MIN_BLOCKS) k_shade(DeviceScene scene, PathPool pool, uint32_t bounce,
+__global__ void __launch_bounds__(BLOCK, LAYERS ? CN_SHADE_LAYERED_MIN_BLOCKS : CN_SHADE_MIN_BLOCKS)
+    k_shade(DeviceScene scene, PathPool pool, uint32_t bounce,
                                                  uint32_t max_bounces, uint32_t light_sampling, uint32_t n0,
                                                  uint32_t part) {
     // part 0: the whole bounce; on a sorted bounce, 1: the misses and
@@ -1182,6 +1191,7 @@ LaunchShape launch_shape(int device) {
     ls.grid_shadow_queued = ls.trav[0][TRAV_SHADOW_QUEUED];
     ls.grid_shadow_queued_top = ls.trav[0][TRAV_SHADOW_QUEUED_TOP];
     ls.grid_shade = grid_for(k_shade<true, false, true>, BLOCK, 0, sms);
+    ls.grid_shade_free = grid_for(k_shade<true, false, false>, BLOCK, 0, sms);
     ls.grid_stream = sms * 8;
     return ls;
 }
@@ -1258,8 +1268,8 @@ void launch_shade(const DeviceScene& scene, const PathPool& pool, uint32_t bounc
     const bool aov = pool.aov_albedo != nullptr, guided = pool.guide_out != nullptr;
     auto shade = [&](bool layers, uint32_t part) {
         auto args = [&](auto kernel) {
-            kernel<<<ls.grid_shade, BLOCK, 0, stream>>>(scene, pool, bounce, wp.max_bounces, wp.light_sampling, n0,
-                                                        part);
+            kernel<<<layers ? ls.grid_shade : ls.grid_shade_free, BLOCK, 0, stream>>>(
+                scene, pool, bounce, wp.max_bounces, wp.light_sampling, n0, part);
         };
         if (layers) {
             if (aov && guided) args(k_shade<true, true, true>);

@@ -143,7 +143,7 @@ enum : int { TRAV_ISECT, TRAV_ISECT_QUEUED, TRAV_ISECT_QUEUED_TOP, TRAV_SHADOW, 
              TRAV_SHADOW_QUEUED_TOP, TRAV_KINDS };
 
 struct LaunchShape {
-    int grid_isect, grid_isect_queued, grid_isect_queued_top, grid_shade, grid_shadow, grid_shadow_queued,
+    int grid_isect, grid_isect_queued, grid_isect_queued_top, grid_shade, grid_shade_free, grid_shadow, grid_shadow_queued,
         grid_shadow_queued_top, grid_stream;
     int block;
     int trav[TRAV_VARIANTS][TRAV_KINDS];  // persistent grids of each traversal variant
