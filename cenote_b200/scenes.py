@@ -572,12 +572,13 @@ def load_spec(path) -> tuple[SceneSpec, dict]:
     return spec, {k[2:]: z[k] for k in z.files if k.startswith("x_")}
 
 
-def textured(width=160, height=90, spp=8, max_bounces=6, size=64, seed=7, color_format=TEX_BC1_SRGB) -> SceneSpec:
+def textured(width=160, height=90, spp=8, max_bounces=6, size=64, seed=7, color_format=TEX_BC1_SRGB,
+             float_format=TEX_RGBA32F) -> SceneSpec:
     """Every texture slot and format on one small set: a ground tiled 4x with a
     base colour in `color_format` (BC1 or BC7 sRGB), a BC5 normal map and a BC4 roughness map; a metal
     panel with an RGBA8 metalness map; a leaf quad cut out by a BC4 opacity
-    map; a ceiling emitter whose emission an RGBA8 sRGB map modulates; an
-    RGBA32F base colour on a back wall. Textures are seeded value noise."""
+    map; a ceiling emitter whose emission an RGBA8 sRGB map modulates; a
+    float base colour on a back wall (`float_format`: RGBA32F or BC6H). Textures are seeded value noise."""
     from . import encode_texture  # host BC encoder of the library
 
     noise = [value_noise(size, seed + k) for k in range(6)]
@@ -593,6 +594,10 @@ def textured(width=160, height=90, spp=8, max_bounces=6, size=64, seed=7, color_
         Texture(TEX_RGBA32F, 8, 8, np.ascontiguousarray(
             np.concatenate([np.random.default_rng(seed).random((8, 8, 3)), np.ones((8, 8, 1))], -1), np.float32)),
     ]
+    if float_format == TEX_BC6H_UF16:  # the back wall's float colour as BC6H, as texture prep stores HDR colour
+        from . import encode_texture_float
+
+        textures[-1] = encode_texture_float(TEX_BC6H_UF16, textures[-1])
     ident = rows(np.eye(4))
     tiled = np.array([[0, 0], [0, 4], [4, 4], [4, 0]], np.float32)
     ground = material(base_color=(0.8, 0.8, 0.8), specular_weight=1.0, specular_roughness=0.5)

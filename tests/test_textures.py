@@ -499,11 +499,12 @@ def gpu_render(ctx, spec, spp, max_bounces):
 
 
 @pytest.mark.gpu
-@pytest.mark.parametrize("color_format", [T.TEX_BC1_SRGB, T.TEX_BC7_SRGB])
-def test_gpu_textured_render_matches_oracle(ctx, color_format):
+@pytest.mark.parametrize("color_format,float_format", [(T.TEX_BC1_SRGB, T.TEX_RGBA32F),
+                                                       (T.TEX_BC7_SRGB, T.TEX_BC6H_UF16)])
+def test_gpu_textured_render_matches_oracle(ctx, color_format, float_format):
     from cenote_b200.metrics import rel_mse
 
-    spec = T.textured(96, 54, 16, 6, color_format=color_format)
+    spec = T.textured(96, 54, 16, 6, color_format=color_format, float_format=float_format)
     got = gpu_render(ctx, spec, 16, 6)
     ref = oracle.OracleScene(spec).render_guides(96, 54, 0, 16, 6)
     ref = {k: v / 16 for k, v in ref.items()}
