@@ -352,8 +352,11 @@ def prepared_texture(rgba8, usage: str = "color", srgb: bool = True) -> Texture:
     """An 8-bit image (H, W, 4) stored the way the reference's texture prep
     stores it (crates/cenote/src/texture.rs:249-405): colour as BC7 (an sRGB
     view when `srgb`), scalars as BC4 on red, tangent-space normals as BC5 on
-    x/y. An image whose sides are not multiples of 4 stays RGBA8 (the
-    reference pads it to whole blocks instead)."""
+    x/y. Colour is encoded opaque, as the reference's encoder profile does
+    (texture.rs:273-276, opaque settings): its alpha becomes 255 (no slot
+    reads a colour texture's alpha), which also opens BC7's two-subset RGB
+    modes to it. An image whose sides are not multiples of 4 stays RGBA8
+    (the reference pads it to whole blocks instead)."""
     from . import encode_texture  # host BC encoder of the library
 
     rgba8 = np.ascontiguousarray(rgba8, np.uint8)
@@ -361,6 +364,10 @@ def prepared_texture(rgba8, usage: str = "color", srgb: bool = True) -> Texture:
     tex = Texture(TEX_RGBA8_SRGB if srgb else TEX_RGBA8_UNORM, w, h, rgba8)
     if w % 4 or h % 4:
         return tex
+    if usage == "color":
+        rgba8 = rgba8.copy()
+        rgba8[..., 3] = 255
+        tex = Texture(tex.format, w, h, rgba8)
     fmt = {"color": TEX_BC7_SRGB if srgb else TEX_BC7_UNORM, "data": TEX_BC4_UNORM, "normal": TEX_BC5_UNORM}[usage]
     return encode_texture(fmt, tex)
 

@@ -341,6 +341,26 @@ def test_bc7_encoder():
     assert (bc7[..., 3] == 255).all()
 
 
+def test_colour_prep_is_opaque_bc7():
+    """Texture prep stores an 8-bit colour image as BC7 with alpha 255, as
+    the reference's opaque encoder profile does (texture.rs:273-276); its RGB
+    comes back better than when the block's alpha noise is encoded too (mode 6
+    alone), and a scalar image becomes BC4 on red."""
+    rng = np.random.default_rng(6)
+    rgb = np.stack([T.value_noise(32, k, octaves=2) for k in (1, 2, 3)], -1)
+    img = T.rgba8_texture(rgb, srgb=True).data.copy()
+    img[..., 3] = rng.integers(0, 256, (32, 32), dtype=np.uint8)
+    tex = T.prepared_texture(img, "color", srgb=True)
+    assert tex.format == T.TEX_BC7_SRGB
+    back = bc7_bytes(tex.data, 32, 32)
+    assert (back[..., 3] == 255).all()
+    err = np.abs(back[..., :3].astype(int) - img[..., :3]).mean()
+    kept = bc7_bytes(encode_texture(T.TEX_BC7_SRGB, T.Texture(T.TEX_RGBA8_SRGB, 32, 32, img)).data, 32, 32)
+    assert err < 6.0 and err < 0.5 * np.abs(kept[..., :3].astype(int) - img[..., :3]).mean()  # 4.6 vs 14.7 levels
+    assert T.prepared_texture(img, "data", srgb=False).format == T.TEX_BC4_UNORM
+    assert T.prepared_texture(img[:30, :30], "color").format == T.TEX_RGBA8_SRGB  # not whole blocks
+
+
 # ---- BC6H -----------------------------------------------------------------------------
 
 # Mode bits of the fourteen BC6H modes (two bits for modes 1-2, five for the
