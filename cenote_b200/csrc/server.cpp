@@ -75,8 +75,14 @@ namespace {
 #ifndef CN_FIRST_EXCLUSIVE
 #define CN_FIRST_EXCLUSIVE 0
 #endif
+// A progressive wave's device time in ms. Measured at 64 jobs in flight: 7
+// gives p99 time to first frame after the opening burst of 44.3, 44.2 and
+// 48.4 ms (three runs) at 633, 631 and 608 Msamples/s, 10 gives 53.8, 48.5,
+// 50.2 and 47.1 ms at 631, 658, 649 and 653: 7 keeps the first-frame target
+// of 50 ms for about 4 % of throughput; 20 raises throughput about 11 % and
+// the first-frame wait with it.
 #ifndef CN_WAVE_MS
-#define CN_WAVE_MS 10.0
+#define CN_WAVE_MS 7.0
 #endif
 constexpr uint32_t MAX_SEGMENTS = 512;
 
